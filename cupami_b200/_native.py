@@ -1,0 +1,271 @@
+"""ctypes binding of ``libcupami_b200.so`` (the C ABI in include/cupami_b200.h).
+
+The library is built in-tree next to this file by ``cupami_b200.build``.  There
+is no fallback: if the library or a CUDA device is missing, the miners raise,
+exactly as the reference raises when CuPy or a device is missing
+(``cupami/frequentPattern/cuApriori.py:458-471``).
+"""
+
+from __future__ import annotations
+
+import atexit
+import ctypes
+import threading
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libcupami_b200.so"
+
+CPM_OK = 0
+CPM_EINVAL = -1
+CPM_ENOMEM = -2
+CPM_ECUDA = -3
+CPM_EOVERFLOW = -4
+CPM_ETIMEOUT = -5
+CPM_ENODEV = -6
+CPM_EINTERNAL = -7
+
+CPM_ECLAT = 0
+CPM_APRIORI = 1
+CPM_ORDER_ECLAT = 0
+CPM_ORDER_APRIORI = 1
+CPM_ORDER_NONE = 2
+CPM_SCHED_PLAIN = 0
+CPM_SCHED_LEARNED = 1
+
+_ERRORS = {
+    CPM_EINVAL: "invalid argument", CPM_ENOMEM: "out of memory", CPM_ECUDA: "CUDA error",
+    CPM_EOVERFLOW: "buffer overflow", CPM_ETIMEOUT: "device wait ran out", CPM_ENODEV: "no CUDA device",
+    CPM_EINTERNAL: "internal error",
+}
+
+
+class NativeError(RuntimeError):
+    """A C-ABI call returned a negative status."""
+
+    def __init__(self, code, message):
+        super().__init__(f"{_ERRORS.get(code, 'error')} ({code}): {message}")
+        self.code = code
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [
+        ("scheduler", ctypes.c_int32), ("pair_engine", ctypes.c_int32),
+        ("pair_batch", ctypes.c_uint64), ("intersection_bytes", ctypes.c_uint64),
+        ("arena_bytes", ctypes.c_uint64), ("spin_limit", ctypes.c_uint64),
+        ("collect_trace", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "n_patterns", "n_frequent_items", "n_frequent_pairs", "frames", "work_items",
+        "intersections", "bytes_alg", "pair_ops", "kernel_launches", "retries")] + [
+        (n, ctypes.c_double) for n in (
+            "ms_pack", "ms_pairs", "ms_deep", "ms_total", "deep_gbs", "pair_tops")]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_P = ctypes.c_void_p
+_U64 = ctypes.c_uint64
+_SIGNATURES = {
+    "cpm_init": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
+    "cpm_shutdown": (None, [_P]),
+    "cpm_last_error": (ctypes.c_char_p, [_P]),
+    "cpm_version": (ctypes.c_char_p, []),
+    "cpm_default_opts": (ctypes.c_int, [ctypes.POINTER(Opts)]),
+    "cpm_db_from_csr": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, ctypes.POINTER(_P)]),
+    "cpm_db_from_ids": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.POINTER(_P)]),
+    "cpm_db_info": (ctypes.c_int, [_P, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_uint32),
+                                   ctypes.POINTER(_U64)]),
+    "cpm_db_labels": (ctypes.c_int, [_P, _P]),
+    "cpm_db_free": (None, [_P]),
+    "cpm_mine": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.c_int, ctypes.POINTER(Opts),
+                                ctypes.POINTER(_P)]),
+    "cpm_result_size": (ctypes.c_int, [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
+    "cpm_result_copy": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P]),
+    "cpm_result_tree": (ctypes.c_int, [_P, _P, _P, _P]),
+    "cpm_result_stats": (ctypes.c_int, [_P, ctypes.POINTER(Stats)]),
+    "cpm_result_free": (None, [_P]),
+    "cpm_build_bitsets": (ctypes.c_int, [_P, _P, _P, _U64, _U64, ctypes.c_uint32, _P]),
+    "cpm_count_supports": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, _P]),
+    "cpm_intersect_extensions": (ctypes.c_int, [_P, _P, _P, _U64, _U64, _P, _P]),
+    "cpm_synchronize": (ctypes.c_int, [_P]),
+}
+
+_lib = None
+_lock = threading.RLock()
+_contexts: dict[int, "Context"] = {}
+
+
+def library():
+    """Load the shared library (raises ImportError when it has not been built)."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not LIB_PATH.exists():
+                    raise ImportError(
+                        f"{LIB_PATH.name} is not built; run cupami_b200.build.build() "
+                        "(nvcc for sm_100a) before mining")
+                lib = ctypes.CDLL(str(LIB_PATH))
+                for name, (res, args) in _SIGNATURES.items():
+                    fn = getattr(lib, name)
+                    fn.restype = res
+                    fn.argtypes = args
+                _lib = lib
+    return _lib
+
+
+def declared_symbols():
+    return list(_SIGNATURES)
+
+
+class Context:
+    """One cpm_ctx (device + stream).  Calls on a context must not overlap."""
+
+    def __init__(self, device=0):
+        lib = library()
+        handle = _P()
+        code = lib.cpm_init(int(device), ctypes.byref(handle))
+        if code == CPM_ENODEV:
+            raise RuntimeError("GPU mining requires a CUDA device; no CUDA device was found.")
+        if code != CPM_OK:
+            raise RuntimeError(f"could not initialise CUDA device {device} (status {code})")
+        self.handle = handle
+        self.device = device
+        self.lock = threading.Lock()
+
+    def check(self, code):
+        if code != CPM_OK:
+            msg = library().cpm_last_error(self.handle)
+            raise NativeError(code, msg.decode() if msg else "")
+
+    def close(self):
+        if self.handle:
+            library().cpm_shutdown(self.handle)
+            self.handle = None
+
+
+def context(device=0) -> Context:
+    library()
+    ctx = _contexts.get(device)
+    if ctx is None:
+        with _lock:
+            ctx = _contexts.get(device)
+            if ctx is None:
+                ctx = Context(device)
+                _contexts[device] = ctx
+    return ctx
+
+
+@atexit.register
+def _shutdown():
+    for ctx in list(_contexts.values()):
+        try:
+            ctx.close()
+        except Exception:  # interpreter teardown
+            pass
+    _contexts.clear()
+
+
+def _ptr(a):
+    return a.ctypes.data if a.size else None
+
+
+class Database:
+    """Device tidsets of one transaction database (owned by the library)."""
+
+    def __init__(self, ctx: Context, handle, labels=None):
+        self.ctx = ctx
+        self.handle = handle
+        n_tx, n_items, words = _U64(), ctypes.c_uint32(), _U64()
+        ctx.check(library().cpm_db_info(handle, ctypes.byref(n_tx), ctypes.byref(n_items),
+                                        ctypes.byref(words)))
+        self.n_transactions = n_tx.value
+        self.n_items = n_items.value
+        self.words = words.value
+        self.labels = labels
+
+    @classmethod
+    def from_columns(cls, ctx, offsets, cols, n_items):
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        cols = np.ascontiguousarray(cols, dtype=np.uint32)
+        handle = _P()
+        with ctx.lock:
+            ctx.check(library().cpm_db_from_csr(ctx.handle, _ptr(offsets), offsets.size - 1,
+                                                _ptr(cols), cols.size, int(n_items),
+                                                ctypes.byref(handle)))
+        return cls(ctx, handle)
+
+    @classmethod
+    def from_ids(cls, ctx, offsets, ids):
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        handle = _P()
+        with ctx.lock:
+            ctx.check(library().cpm_db_from_ids(ctx.handle, _ptr(offsets), offsets.size - 1,
+                                                _ptr(ids), ids.size, ctypes.byref(handle)))
+        db = cls(ctx, handle)
+        labels = np.zeros(db.n_items, dtype=np.uint32)
+        if db.n_items:
+            ctx.check(library().cpm_db_labels(handle, labels.ctypes.data))
+        db.labels = labels
+        return db
+
+    def mine(self, min_sup, algorithm, opts=None, order=None):
+        if opts is None:
+            opts = Opts()
+            library().cpm_default_opts(ctypes.byref(opts))
+        res = _P()
+        with self.ctx.lock:
+            self.ctx.check(library().cpm_mine(self.ctx.handle, self.handle, int(min_sup),
+                                              int(algorithm), ctypes.byref(opts), ctypes.byref(res)))
+        try:
+            return Result.collect(res, CPM_ORDER_ECLAT if order is None else order)
+        finally:
+            library().cpm_result_free(res)
+
+    def close(self):
+        if self.handle:
+            library().cpm_db_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Result:
+    """Mined patterns as arrays: pattern k = items[offsets[k]:offsets[k+1]]."""
+
+    def __init__(self, offsets, items, supports, stats):
+        self.offsets = offsets
+        self.items = items
+        self.supports = supports
+        self.stats = stats
+
+    @classmethod
+    def collect(cls, handle, order):
+        lib = library()
+        n, slots = _U64(), _U64()
+        if lib.cpm_result_size(handle, ctypes.byref(n), ctypes.byref(slots)) != CPM_OK:
+            raise NativeError(CPM_EINTERNAL, "result size")
+        offsets = np.zeros(n.value + 1, dtype=np.uint64)
+        items = np.zeros(max(1, slots.value), dtype=np.uint32)
+        supports = np.zeros(max(1, n.value), dtype=np.uint64)
+        code = lib.cpm_result_copy(handle, int(order), offsets.ctypes.data, items.ctypes.data,
+                                   supports.ctypes.data)
+        if code != CPM_OK:
+            raise NativeError(code, "result copy")
+        st = Stats()
+        lib.cpm_result_stats(handle, ctypes.byref(st))
+        return cls(offsets, items[:slots.value], supports[:n.value], st.as_dict())
+
+    def __len__(self):
+        return int(self.supports.size)

@@ -1,0 +1,975 @@
+// cupami_b200 runtime: the C ABI declared in include/cupami_b200.h.
+//
+// Host side of the vertical-bitset miner: device memory, database loading,
+// the Eclat and Apriori drivers, and result ordering.  All arithmetic on
+// transactions runs in the CUDA kernels included below; the host only plans
+// (buffer sizes, class order) and moves counts and results.
+#include "../../include/cupami_b200.h"
+#include "common.cuh"
+#include "k_basic.cuh"
+#include "k_pairs.cuh"
+#include "k_gram_tc.cuh"
+#include "k_deep.cuh"
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <unordered_set>
+#include <vector>
+#include <chrono>
+#include <cstdlib>
+
+using namespace cpm;
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+
+struct cpm_ctx {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[8] = {};
+    std::string err;
+    bool tc_ok = true;  // tensor-core Gram usable on this device
+};
+
+struct cpm_db {
+    cpm_ctx *ctx = nullptr;
+    uint64_t n_tx = 0, words = 0, stride = 2;
+    uint32_t n_items = 0;
+    uint64_t *d_bits = nullptr;
+    uint32_t *d_support = nullptr;
+    std::vector<uint32_t> labels;  // raw ids in column order (cpm_db_from_ids)
+    // Deep-level buffer sizes that the last mine() of this database needed.
+    uint64_t hint_frames = 0, hint_members = 0, hint_queue = 0, hint_patterns = 0, hint_arena = 0;
+};
+
+struct cpm_result {
+    std::vector<uint32_t> parent, item, support;
+    cpm_stats stats{};
+    int algo = CPM_ECLAT;
+};
+
+static int set_err(cpm_ctx *ctx, int code, const char *fmt, ...) {
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        ctx->err = buf;
+    }
+    return code;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return set_err(ctx, e_ == cudaErrorMemoryAllocation ? CPM_ENOMEM : CPM_ECUDA,      \
+                           "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__,  \
+                           __LINE__);                                                          \
+    } while (0)
+
+#define CKR(expr)                 \
+    do {                          \
+        int r_ = (expr);          \
+        if (r_ != CPM_OK) return r_; \
+    } while (0)
+
+template <class T>
+static int dalloc(cpm_ctx *ctx, T **p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMallocAsync((void **)p, count * sizeof(T), ctx->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(ctx, CPM_ENOMEM, "device allocation of %zu bytes failed: %s",
+                       count * sizeof(T), cudaGetErrorString(e));
+    }
+    return CPM_OK;
+}
+
+template <class T>
+static void dfree(cpm_ctx *ctx, T *&p) {
+    if (p) cudaFreeAsync((void *)p, ctx->stream);
+    p = nullptr;
+}
+
+// RAII list of device buffers freed at scope exit (stream ordered).
+struct DevScope {
+    cpm_ctx *ctx;
+    std::vector<void *> ptrs;
+    explicit DevScope(cpm_ctx *c) : ctx(c) {}
+    template <class T>
+    int alloc(T **p, size_t count) {
+        int r = dalloc(ctx, p, count);
+        if (r == CPM_OK) ptrs.push_back((void *)*p);
+        return r;
+    }
+    ~DevScope() {
+        for (void *p : ptrs) cudaFreeAsync(p, ctx->stream);
+    }
+};
+
+extern "C" const char *cpm_version(void) { return "cupami_b200 0.1 (sm_100a)"; }
+
+extern "C" int cpm_default_opts(cpm_opts *o) {
+    if (!o) return CPM_EINVAL;
+    memset(o, 0, sizeof *o);
+    o->scheduler = CPM_SCHED_PLAIN;
+    o->spin_limit = 1ull << 26;
+    return CPM_OK;
+}
+
+extern "C" int cpm_init(int device, cpm_ctx **out) {
+    if (!out) return CPM_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return CPM_ENODEV;
+    }
+    if (device < 0 || device >= n) return CPM_EINVAL;
+    cpm_ctx *ctx = new cpm_ctx();
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+    int major = 0, minor = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device);
+    if (e == cudaSuccess) {
+        // Keep freed blocks in the stream-ordered pool between calls.
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t thr = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return CPM_ECUDA;
+    }
+    ctx->tc_ok = (major == 10 && minor == 0);
+    *out = ctx;
+    return CPM_OK;
+}
+
+extern "C" void cpm_shutdown(cpm_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto &e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+extern "C" const char *cpm_last_error(const cpm_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+extern "C" int cpm_synchronize(cpm_ctx *ctx) {
+    if (!ctx) return CPM_EINVAL;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CPM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// databases
+// ---------------------------------------------------------------------------
+
+// Offsets of the non-empty rows only (empty baskets are dropped and the rest
+// renumbered in order, cuApriori.py:391-392).
+static int compact_offsets(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows, uint64_t nnz,
+                           std::vector<uint64_t> &out) {
+    out.clear();
+    out.reserve(n_rows + 1);
+    if (n_rows == 0) {
+        if (nnz) return set_err(ctx, CPM_EINVAL, "nnz must be 0 when there are no rows");
+        out.push_back(0);
+        return CPM_OK;
+    }
+    if (offsets[0] != 0 || offsets[n_rows] != nnz)
+        return set_err(ctx, CPM_EINVAL, "offsets must start at 0 and end at nnz");
+    out.push_back(0);
+    for (uint64_t r = 0; r < n_rows; ++r) {
+        if (offsets[r + 1] < offsets[r]) return set_err(ctx, CPM_EINVAL, "offsets must be nondecreasing");
+        if (offsets[r + 1] > offsets[r]) out.push_back(offsets[r + 1]);
+    }
+    return CPM_OK;
+}
+
+static int db_alloc_bits(cpm_ctx *ctx, cpm_db *db) {
+    db->words = (db->n_tx + 63) / 64;
+    db->stride = std::max<uint64_t>(2, (db->words + 1) & ~1ull);
+    CKR(dalloc(ctx, &db->d_bits, (size_t)std::max<uint32_t>(1, db->n_items) * db->stride));
+    CKR(dalloc(ctx, &db->d_support, db->n_items));
+    CK(cudaMemsetAsync(db->d_bits, 0, (size_t)std::max<uint32_t>(1, db->n_items) * db->stride * 8, ctx->stream));
+    return CPM_OK;
+}
+
+static int db_pack(cpm_ctx *ctx, cpm_db *db, const uint64_t *d_off, const uint32_t *d_ids,
+                   const uint32_t *d_lut) {
+    if (db->n_tx) {
+        const unsigned threads = 256;
+        const unsigned blocks = (unsigned)((db->n_tx + threads - 1) / threads);
+        k_pack<<<blocks, threads, 0, ctx->stream>>>(d_off, d_ids, d_lut, db->n_tx, db->stride,
+                                                    reinterpret_cast<uint32_t *>(db->d_bits));
+        CK(cudaGetLastError());
+    }
+    if (db->n_items) {
+        const unsigned threads = 256;
+        const unsigned blocks = (unsigned)(((uint64_t)db->n_items * 32 + threads - 1) / threads);
+        k_item_support<<<blocks, threads, 0, ctx->stream>>>(db->d_bits, db->stride, db->n_items, db->d_support);
+        CK(cudaGetLastError());
+    }
+    return CPM_OK;
+}
+
+extern "C" int cpm_db_from_csr(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows,
+                               const uint32_t *cols, uint64_t nnz, uint32_t n_items, cpm_db **out) {
+    if (!ctx || !out || (!offsets && n_rows) || (!cols && nnz)) return CPM_EINVAL;
+    *out = nullptr;
+    CK(cudaSetDevice(ctx->device));
+    std::vector<uint64_t> off;
+    CKR(compact_offsets(ctx, offsets, n_rows, nnz, off));
+    for (uint64_t k = 0; k < nnz; ++k)
+        if (cols[k] >= n_items) return set_err(ctx, CPM_EINVAL, "column %u out of range (n_items %u)", cols[k], n_items);
+    cpm_db *db = new cpm_db();
+    db->ctx = ctx;
+    db->n_tx = off.size() - 1;
+    db->n_items = n_items;
+    int r = db_alloc_bits(ctx, db);
+    DevScope tmp(ctx);
+    uint64_t *d_off = nullptr;
+    uint32_t *d_ids = nullptr;
+    if (r == CPM_OK) r = tmp.alloc(&d_off, off.size());
+    if (r == CPM_OK) r = tmp.alloc(&d_ids, nnz);
+    if (r == CPM_OK && cudaMemcpyAsync(d_off, off.data(), off.size() * 8, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+        r = set_err(ctx, CPM_ECUDA, "offset upload failed");
+    if (r == CPM_OK && nnz && cudaMemcpyAsync(d_ids, cols, nnz * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+        r = set_err(ctx, CPM_ECUDA, "column upload failed");
+    if (r == CPM_OK) r = db_pack(ctx, db, d_off, d_ids, nullptr);
+    if (r == CPM_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        r = set_err(ctx, CPM_ECUDA, "pack failed: %s", cudaGetErrorString(cudaGetLastError()));
+    if (r != CPM_OK) {
+        cpm_db_free(db);
+        return r;
+    }
+    *out = db;
+    return CPM_OK;
+}
+
+// Decimal-string order of integer labels: "1" < "10" < "100" < "11" < "2".
+static inline uint64_t decimal_key(uint32_t v) {
+    char d[10];
+    int n = 0;
+    do { d[n++] = (char)(v % 10); v /= 10; } while (v);
+    uint64_t key = 0;
+    for (int i = 0; i < 10; ++i) key = key * 11 + (i < n ? (uint64_t)d[n - 1 - i] + 1 : 0);
+    return key;
+}
+
+extern "C" int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows,
+                               const uint32_t *ids, uint64_t nnz, cpm_db **out) {
+    if (!ctx || !out || (!offsets && n_rows) || (!ids && nnz)) return CPM_EINVAL;
+    *out = nullptr;
+    CK(cudaSetDevice(ctx->device));
+    std::vector<uint64_t> off;
+    CKR(compact_offsets(ctx, offsets, n_rows, nnz, off));
+    uint32_t max_id = 0;
+    for (uint64_t k = 0; k < nnz; ++k) max_id = std::max(max_id, ids[k]);
+    DevScope tmp(ctx);
+    uint64_t *d_off = nullptr;
+    uint32_t *d_ids = nullptr, *d_lut = nullptr, *d_present = nullptr;
+    CKR(tmp.alloc(&d_off, off.size()));
+    CKR(tmp.alloc(&d_ids, nnz));
+    CK(cudaMemcpyAsync(d_off, off.data(), off.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (nnz) CK(cudaMemcpyAsync(d_ids, ids, nnz * 4, cudaMemcpyHostToDevice, ctx->stream));
+    // Distinct ids: a presence bitmap over [0, max_id] built on the device.
+    const uint64_t pw = (uint64_t)max_id / 32 + 1;
+    CKR(tmp.alloc(&d_present, pw));
+    CK(cudaMemsetAsync(d_present, 0, pw * 4, ctx->stream));
+    if (nnz) {
+        const unsigned blocks = (unsigned)std::min<uint64_t>((nnz + 255) / 256, (uint64_t)ctx->sms * 16);
+        k_mark_ids<<<blocks, 256, 0, ctx->stream>>>(d_ids, nnz, d_present);
+        CK(cudaGetLastError());
+    }
+    std::vector<uint32_t> present(pw);
+    CK(cudaMemcpyAsync(present.data(), d_present, pw * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<uint32_t> uniq;
+    for (uint64_t w = 0; w < pw; ++w)
+        for (uint32_t m = present[w]; m; m &= m - 1) uniq.push_back((uint32_t)(w * 32 + __builtin_ctz(m)));
+    std::vector<uint64_t> keys(uniq.size());
+    for (size_t i = 0; i < uniq.size(); ++i) keys[i] = decimal_key(uniq[i]);
+    std::vector<uint32_t> order(uniq.size());
+    std::iota(order.begin(), order.end(), 0u);
+    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return keys[a] < keys[b]; });
+    cpm_db *db = new cpm_db();
+    db->ctx = ctx;
+    db->n_tx = off.size() - 1;
+    db->n_items = (uint32_t)uniq.size();
+    db->labels.resize(uniq.size());
+    // Column lookup: dense table over the id range when it is small enough,
+    // otherwise ids are first replaced by their rank among the distinct ids.
+    std::vector<uint32_t> rank(uniq.size());
+    for (size_t c = 0; c < order.size(); ++c) {
+        db->labels[c] = uniq[order[c]];
+        rank[order[c]] = (uint32_t)c;
+    }
+    int r = db_alloc_bits(ctx, db);
+    if (r == CPM_OK) {
+        if ((uint64_t)max_id < (1ull << 26)) {
+            std::vector<uint32_t> lut((uint64_t)max_id + 1, 0);
+            for (size_t i = 0; i < uniq.size(); ++i) lut[uniq[i]] = rank[i];
+            r = tmp.alloc(&d_lut, lut.size());
+            if (r == CPM_OK &&
+                cudaMemcpyAsync(d_lut, lut.data(), lut.size() * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+                r = set_err(ctx, CPM_ECUDA, "lookup upload failed");
+            if (r == CPM_OK) r = db_pack(ctx, db, d_off, d_ids, d_lut);
+            if (r == CPM_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+                r = set_err(ctx, CPM_ECUDA, "pack failed");
+        } else {
+            std::vector<uint32_t> cols(nnz);
+            for (uint64_t k = 0; k < nnz; ++k)
+                cols[k] = rank[std::lower_bound(uniq.begin(), uniq.end(), ids[k]) - uniq.begin()];
+            if (nnz && cudaMemcpyAsync(d_ids, cols.data(), nnz * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+                r = set_err(ctx, CPM_ECUDA, "column upload failed");
+            if (r == CPM_OK) r = db_pack(ctx, db, d_off, d_ids, nullptr);
+            if (r == CPM_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+                r = set_err(ctx, CPM_ECUDA, "pack failed");
+        }
+    }
+    if (r != CPM_OK) {
+        cpm_db_free(db);
+        return r;
+    }
+    *out = db;
+    return CPM_OK;
+}
+
+extern "C" int cpm_db_info(const cpm_db *db, uint64_t *n_tx, uint32_t *n_items, uint64_t *words) {
+    if (!db) return CPM_EINVAL;
+    if (n_tx) *n_tx = db->n_tx;
+    if (n_items) *n_items = db->n_items;
+    if (words) *words = db->words;
+    return CPM_OK;
+}
+
+extern "C" int cpm_db_labels(const cpm_db *db, uint32_t *ids_out) {
+    if (!db || !ids_out) return CPM_EINVAL;
+    if (db->labels.size() != db->n_items) return CPM_EINVAL;
+    std::copy(db->labels.begin(), db->labels.end(), ids_out);
+    return CPM_OK;
+}
+
+extern "C" void cpm_db_free(cpm_db *db) {
+    if (!db) return;
+    cpm_ctx *ctx = db->ctx;
+    cudaSetDevice(ctx->device);
+    dfree(ctx, db->d_bits);
+    dfree(ctx, db->d_support);
+    cudaStreamSynchronize(ctx->stream);
+    delete db;
+}
+
+// ---------------------------------------------------------------------------
+// mining
+// ---------------------------------------------------------------------------
+
+static double elapsed_ms(cpm_ctx *ctx, int a, int b) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[a], ctx->ev[b]);
+    return ms;
+}
+
+// Frequent singletons: ordered list of columns whose support passes.
+static int mine_singletons(cpm_ctx *ctx, cpm_db *db, long long ms, DevScope &ds, uint32_t **d_freq,
+                           uint32_t &F, uint64_t &launches) {
+    uint32_t *d_count = nullptr;
+    CKR(ds.alloc(d_freq, db->n_items));
+    CKR(ds.alloc(&d_count, 1));
+    CK(cudaMemsetAsync(d_count, 0, 4, ctx->stream));
+    if (db->n_items) {
+        k_compact_frequent<<<1, 1024, 0, ctx->stream>>>(db->d_support, db->n_items, ms, *d_freq, d_count);
+        CK(cudaGetLastError());
+        launches++;
+    }
+    CK(cudaMemcpyAsync(&F, d_count, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CPM_OK;
+}
+
+// Pair Gram C[F][F] (upper triangle) on the tensor cores or the CUDA cores.
+static int pair_gram(cpm_ctx *ctx, cpm_db *db, const uint32_t *d_freq, uint32_t F, const cpm_opts &o,
+                     DevScope &ds, uint32_t **d_C, cpm_stats &st) {
+    CKR(ds.alloc(d_C, (size_t)F * F));
+    const bool use_tc = o.pair_engine == 1 || (o.pair_engine == 0 && ctx->tc_ok && gram_tc_worthwhile(F, db->n_tx));
+    if (use_tc) {
+        CKR(gram_tc_launch(ctx->stream, ctx->sms, db->d_bits, db->stride, d_freq, F, db->n_tx, *d_C, &st.pair_ops,
+                           &st.kernel_launches)
+                ? set_err(ctx, CPM_ECUDA, "tensor-core Gram launch failed: %s", cudaGetErrorString(cudaGetLastError()))
+                : CPM_OK);
+        return CPM_OK;
+    }
+    CK(cudaMemsetAsync(*d_C, 0, (size_t)F * F * 4, ctx->stream));
+    const uint32_t nt = (F + 63) / 64;
+    const uint32_t tiles = nt * (nt + 1) / 2;
+    // Split K so that the grid covers the GPU a few times over.
+    uint64_t ksplit = std::max<uint64_t>(1, (uint64_t)ctx->sms * 4 / tiles);
+    ksplit = std::min<uint64_t>(ksplit, std::max<uint64_t>(1, db->stride / 64));
+    const uint64_t k_chunk = ((db->stride + ksplit - 1) / ksplit + 15) / 16 * 16;
+    ksplit = (db->stride + k_chunk - 1) / k_chunk;
+    dim3 grid(tiles, (unsigned)ksplit);
+    k_gram_simt<<<grid, 256, 0, ctx->stream>>>(db->d_bits, db->stride, d_freq, F, nt, k_chunk, *d_C);
+    CK(cudaGetLastError());
+    st.kernel_launches += 1;
+    st.pair_ops += 2ull * db->n_tx * F * (uint64_t)F;
+    return CPM_OK;
+}
+
+struct DeepBuffers {
+    DFrame *frames = nullptr;
+    uint32_t *mem_pat = nullptr, *mem_item = nullptr;
+    const uint64_t **mem_bits = nullptr;
+    unsigned long long *queue = nullptr;
+    uint64_t *arena = nullptr;
+    uint32_t *pat_parent = nullptr, *pat_item = nullptr, *pat_sup = nullptr;
+    unsigned long long *root_cost = nullptr;
+    DeepState *st = nullptr;
+    uint64_t frames_cap = 0, members_cap = 0, queue_cap = 0, arena_slots = 0, pat_cap = 0;
+    void release(cpm_ctx *ctx) {
+        dfree(ctx, frames); dfree(ctx, mem_pat); dfree(ctx, mem_item); dfree(ctx, mem_bits);
+        dfree(ctx, queue); dfree(ctx, arena); dfree(ctx, pat_parent); dfree(ctx, pat_item);
+        dfree(ctx, pat_sup); dfree(ctx, root_cost); dfree(ctx, st);
+    }
+};
+
+static int grow(cpm_ctx *ctx, DeepBuffers &b, uint64_t frames_cap, uint64_t members_cap, uint64_t queue_cap,
+                uint64_t arena_slots, uint64_t pat_cap, uint64_t stride, uint64_t n_roots) {
+    b.release(ctx);
+    b.frames_cap = frames_cap; b.members_cap = members_cap; b.queue_cap = queue_cap;
+    b.arena_slots = arena_slots; b.pat_cap = pat_cap;
+    CKR(dalloc(ctx, &b.frames, frames_cap));
+    CKR(dalloc(ctx, &b.mem_pat, members_cap));
+    CKR(dalloc(ctx, &b.mem_item, members_cap));
+    CKR(dalloc(ctx, &b.mem_bits, members_cap));
+    CKR(dalloc(ctx, &b.queue, queue_cap));
+    CKR(dalloc(ctx, &b.arena, arena_slots * stride));
+    CKR(dalloc(ctx, &b.pat_parent, pat_cap));
+    CKR(dalloc(ctx, &b.pat_item, pat_cap));
+    CKR(dalloc(ctx, &b.pat_sup, pat_cap));
+    CKR(dalloc(ctx, &b.root_cost, std::max<uint64_t>(1, n_roots)));
+    CKR(dalloc(ctx, &b.st, 1));
+    return CPM_OK;
+}
+
+static int mine_eclat(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o, cpm_result *res) {
+    cpm_stats &st = res->stats;
+    DevScope ds(ctx);
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    uint32_t *d_freq = nullptr;
+    uint32_t F = 0;
+    CKR(mine_singletons(ctx, db, ms, ds, &d_freq, F, st.kernel_launches));
+    st.n_frequent_items = F;
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    // Pair level.
+    std::vector<uint32_t> cnt(F, 0);
+    std::vector<uint64_t> off(F + 1, 0);
+    uint32_t *d_C = nullptr, *d_cnt = nullptr;
+    uint64_t *d_off = nullptr;
+    if (F >= 2) {
+        CKR(pair_gram(ctx, db, d_freq, F, o, ds, &d_C, st));
+        CKR(ds.alloc(&d_cnt, F));
+        k_pair_count<<<(unsigned)(((uint64_t)F * 32 + 255) / 256), 256, 0, ctx->stream>>>(d_C, F, ms, d_cnt);
+        CK(cudaGetLastError());
+        st.kernel_launches++;
+        CK(cudaMemcpyAsync(cnt.data(), d_cnt, (size_t)F * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (uint32_t i = 0; i < F; ++i) off[i + 1] = off[i] + cnt[i];
+    }
+    const uint64_t P2 = off[F];
+    st.n_frequent_pairs = P2;
+    // Top-level classes (cuEclat.py:195-200): rows with at least two members.
+    std::vector<uint32_t> roots;
+    for (uint32_t i = 0; i < F; ++i)
+        if (cnt[i] >= 2) roots.push_back(i);
+    // Plain scheduler: largest class first (more members, more descendants).
+    std::stable_sort(roots.begin(), roots.end(), [&](uint32_t a, uint32_t b) { return cnt[a] > cnt[b]; });
+    std::vector<DFrame> frames(roots.size());
+    std::vector<unsigned long long> init;
+    for (size_t k = 0; k < roots.size(); ++k) {
+        const uint32_t i = roots[k];
+        frames[k].mask = nullptr;  // filled on the device side below
+        frames[k].mem_off = off[i];
+        frames[k].m = cnt[i];
+        frames[k].root = (uint32_t)k;
+    }
+    // Units of all top-level classes, interleaved by position so that the
+    // long first positions of the largest classes start first.
+    {
+        std::vector<std::pair<uint32_t, uint32_t>> units;
+        for (size_t k = 0; k < roots.size(); ++k)
+            for (uint32_t p = 0; p + 1 < cnt[roots[k]]; ++p) units.push_back({cnt[roots[k]] - p - 1, (uint32_t)k});
+        std::vector<uint64_t> idx(units.size());
+        std::iota(idx.begin(), idx.end(), 0ull);
+        std::stable_sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) { return units[a].first > units[b].first; });
+        init.reserve(units.size());
+        for (uint64_t u : idx) {
+            const uint32_t k = units[u].second;
+            const uint32_t p = cnt[roots[k]] - 1 - units[u].first;
+            init.push_back(((unsigned long long)k << 32) | p);
+        }
+    }
+    const uint64_t stride = db->stride;
+    DeepBuffers b;
+    // First guesses scale with the pair level; a database that was mined
+    // before starts from what it needed then.
+    uint64_t frames_cap = std::max<uint64_t>({1024, roots.size() * 8 + P2 * 2, db->hint_frames});
+    uint64_t members_cap = std::max<uint64_t>({4096, P2 * 16, db->hint_members});
+    uint64_t queue_cap = std::max<uint64_t>({4096, init.size() * 8 + P2 * 4, db->hint_queue});
+    uint64_t pat_cap = std::max<uint64_t>({4096, (F + P2) * 16, db->hint_patterns});
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const uint64_t arena_budget = (uint64_t)(free_b * 0.6) / (stride * 8);
+    uint64_t arena_slots = o.arena_bytes ? o.arena_bytes / (stride * 8)
+                                         : std::min<uint64_t>(arena_budget, std::max<uint64_t>(
+                                               {(uint64_t)ctx->sms * 8 * 4 + 1024, P2 * 8, db->hint_arena}));
+    arena_slots = std::max<uint64_t>(arena_slots, (uint64_t)ctx->sms * 8 * 2 + 64);
+    const uint64_t spin = o.spin_limit ? o.spin_limit : (1ull << 26);
+    // Shared-memory prefix when the tidset fits next to the static buffers.
+    const size_t prefix_bytes = stride * 8;
+    const bool smem_prefix = prefix_bytes <= 200 * 1024;
+    int cta_per_sm = 1;
+    if (smem_prefix) {
+        CK(cudaFuncSetAttribute(k_deep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prefix_bytes));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cta_per_sm, k_deep<true>, 256, prefix_bytes));
+    } else {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cta_per_sm, k_deep<false>, 256, 0));
+    }
+    cta_per_sm = std::max(1, cta_per_sm);
+    const unsigned grid = (unsigned)(ctx->sms * cta_per_sm);
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    DeepState hs{};
+    for (int attempt = 0;; ++attempt) {
+        CKR(grow(ctx, b, frames_cap, members_cap, queue_cap, arena_slots, pat_cap + F + P2, stride, roots.size()));
+        // Singletons and pairs land in the pattern arrays; classes get their masks.
+        if (F) {
+            k_emit_singletons<<<(F + 255) / 256, 256, 0, ctx->stream>>>(d_freq, F, db->d_support, b.pat_parent,
+                                                                        b.pat_item, b.pat_sup);
+            CK(cudaGetLastError());
+            st.kernel_launches++;
+        }
+        if (P2) {
+            if (!d_off) CKR(ds.alloc(&d_off, F + 1));
+            CK(cudaMemcpyAsync(d_off, off.data(), (F + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+            if (b.members_cap < P2) return set_err(ctx, CPM_EINTERNAL, "member table too small");
+            k_pair_emit<<<(unsigned)(((uint64_t)F * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+                d_C, F, ms, d_freq, d_off, db->d_bits, stride, b.pat_parent, b.pat_item, b.pat_sup, b.mem_pat,
+                b.mem_item, b.mem_bits);
+            CK(cudaGetLastError());
+            st.kernel_launches++;
+        }
+        if (roots.empty()) {
+            hs = DeepState{};
+            hs.n_patterns = F + P2;
+            break;
+        }
+        // Frame masks point at the class item's tidset.
+        std::vector<uint32_t> hfreq(F);
+        CK(cudaMemcpyAsync(hfreq.data(), d_freq, (size_t)F * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (size_t k = 0; k < roots.size(); ++k) frames[k].mask = db->d_bits + (uint64_t)hfreq[roots[k]] * stride;
+        CK(cudaMemcpyAsync(b.frames, frames.data(), frames.size() * sizeof(DFrame), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemsetAsync(b.queue, 0xff, b.queue_cap * 8, ctx->stream));
+        CK(cudaMemcpyAsync(b.queue, init.data(), init.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemsetAsync(b.root_cost, 0, std::max<size_t>(1, roots.size()) * 8, ctx->stream));
+        hs = DeepState{};
+        hs.q_tail = init.size();
+        hs.pending = init.size();
+        hs.n_patterns = F + P2;
+        hs.n_frames = roots.size();
+        hs.n_members = P2;
+        CK(cudaMemcpyAsync(b.st, &hs, sizeof hs, cudaMemcpyHostToDevice, ctx->stream));
+        DeepParams P;
+        P.frames = b.frames; P.frames_cap = b.frames_cap;
+        P.mem_pat = b.mem_pat; P.mem_item = b.mem_item; P.mem_bits = b.mem_bits; P.members_cap = b.members_cap;
+        P.queue = b.queue; P.queue_cap = b.queue_cap;
+        P.arena = b.arena; P.arena_slots = b.arena_slots;
+        P.pat_parent = b.pat_parent; P.pat_item = b.pat_item; P.pat_sup = b.pat_sup; P.pat_cap = b.pat_cap;
+        P.root_cost = b.root_cost; P.st = b.st; P.stride = stride; P.minsup = ms; P.spin_limit = spin;
+        if (smem_prefix) k_deep<true><<<grid, 256, prefix_bytes, ctx->stream>>>(P);
+        else k_deep<false><<<grid, 256, 0, ctx->stream>>>(P);
+        CK(cudaGetLastError());
+        st.kernel_launches++;
+        CK(cudaMemcpyAsync(&hs, b.st, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (!hs.error) break;
+        if (hs.error & DEEP_ERR_SPIN)
+            return set_err(ctx, CPM_ETIMEOUT, "deep-level kernel wait ran out of spins (limit %llu)",
+                           (unsigned long long)spin);
+        if (attempt >= 12)
+            return set_err(ctx, CPM_EOVERFLOW,
+                           "deep-level buffers still too small after retries (error 0x%x, frames %llu/%llu, "
+                           "members %llu/%llu, queue %llu/%llu, arena %llu/%llu, patterns %llu/%llu)",
+                           hs.error, hs.n_frames, (unsigned long long)b.frames_cap, hs.n_members,
+                           (unsigned long long)b.members_cap, hs.q_tail, (unsigned long long)b.queue_cap,
+                           hs.arena_next, (unsigned long long)b.arena_slots, hs.n_patterns,
+                           (unsigned long long)b.pat_cap);
+        if (getenv("CPM_DEBUG"))
+            fprintf(stderr, "cpm: deep retry %d error 0x%x frames %llu/%llu members %llu/%llu queue %llu/%llu "
+                    "arena %llu/%llu patterns %llu/%llu\n", attempt, hs.error, hs.n_frames,
+                    (unsigned long long)b.frames_cap, hs.n_members, (unsigned long long)b.members_cap, hs.q_tail,
+                    (unsigned long long)b.queue_cap, hs.arena_next, (unsigned long long)b.arena_slots,
+                    hs.n_patterns, (unsigned long long)b.pat_cap);
+        st.retries++;
+        // Counters at the failure are lower bounds of the final need: grow
+        // every buffer past them (one overflow usually means several).
+        frames_cap = std::max<uint64_t>(frames_cap * 4, hs.n_frames * 4);
+        members_cap = std::max<uint64_t>(members_cap * 4, hs.n_members * 4);
+        queue_cap = std::max<uint64_t>(queue_cap * 4, hs.q_tail * 4);
+        pat_cap = std::max<uint64_t>(pat_cap * 4, hs.n_patterns * 4);
+        if (hs.error & DEEP_ERR_ARENA) {
+            if (arena_slots >= arena_budget)
+                return set_err(ctx, CPM_EOVERFLOW, "deep-level arena exceeds device memory (%llu slots)",
+                               (unsigned long long)arena_slots);
+        }
+        arena_slots = std::min<uint64_t>(arena_budget, std::max<uint64_t>(arena_slots * 4, hs.arena_next * 4));
+    }
+    // Remember what this database needed so that the next mine() starts there.
+    db->hint_frames = std::max<uint64_t>(db->hint_frames, hs.n_frames + hs.n_frames / 4 + 64);
+    db->hint_members = std::max<uint64_t>(db->hint_members, hs.n_members + hs.n_members / 4 + 64);
+    db->hint_queue = std::max<uint64_t>(db->hint_queue, hs.q_tail + hs.q_tail / 4 + 64);
+    db->hint_patterns = std::max<uint64_t>(db->hint_patterns, hs.n_patterns + hs.n_patterns / 4 + 64);
+    db->hint_arena = std::max<uint64_t>(db->hint_arena, hs.arena_next + hs.arena_next / 4 + 64);
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    const uint64_t n = hs.n_patterns;
+    res->parent.resize(n);
+    res->item.resize(n);
+    res->support.resize(n);
+    if (n) {
+        CK(cudaMemcpyAsync(res->parent.data(), b.pat_parent, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(res->item.data(), b.pat_item, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(res->support.data(), b.pat_sup, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaEventRecord(ctx->ev[4], ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    b.release(ctx);
+    st.n_patterns = n;
+    st.frames = hs.n_frames;
+    st.work_items = hs.work_items;
+    st.intersections = hs.intersections;
+    st.bytes_alg = hs.bytes_alg;
+    st.ms_pairs = elapsed_ms(ctx, 1, 2);
+    st.ms_deep = elapsed_ms(ctx, 2, 3);
+    st.ms_total = elapsed_ms(ctx, 0, 4);
+    st.deep_gbs = st.ms_deep > 0 ? st.bytes_alg / (st.ms_deep * 1e6) : 0.0;
+    st.pair_tops = st.ms_pairs > 0 ? st.pair_ops / (st.ms_pairs * 1e9) : 0.0;
+    return CPM_OK;
+}
+
+// Apriori (cuApriori.py:501-535): level 2 from the pair Gram, then prefix-join
+// candidates with full subset pruning, each counted by complete intersection.
+static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o, cpm_result *res) {
+    cpm_stats &st = res->stats;
+    DevScope ds(ctx);
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    uint32_t *d_freq = nullptr;
+    uint32_t F = 0;
+    CKR(mine_singletons(ctx, db, ms, ds, &d_freq, F, st.kernel_launches));
+    st.n_frequent_items = F;
+    std::vector<uint32_t> freq(F);
+    std::vector<uint32_t> sup1(db->n_items);
+    if (F) CK(cudaMemcpyAsync(freq.data(), d_freq, (size_t)F * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (db->n_items) CK(cudaMemcpyAsync(sup1.data(), db->d_support, (size_t)db->n_items * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (uint32_t i = 0; i < F; ++i) {
+        res->parent.push_back(0xffffffffu);
+        res->item.push_back(freq[i]);
+        res->support.push_back(sup1[freq[i]]);
+    }
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    // Level 2: the pair Gram over the frequent items.
+    std::vector<uint32_t> level;  // flattened patterns of the current level (frequent indices)
+    std::vector<uint32_t> level_id;
+    uint32_t k = 1;
+    for (uint32_t i = 0; i < F; ++i) { level.push_back(i); level_id.push_back(i); }
+    if (F >= 2) {
+        uint32_t *d_C = nullptr;
+        CKR(pair_gram(ctx, db, d_freq, F, o, ds, &d_C, st));
+        std::vector<uint32_t> C((size_t)F * F);
+        CK(cudaMemcpyAsync(C.data(), d_C, C.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        std::vector<uint32_t> nl, nid;
+        for (uint32_t i = 0; i < F; ++i)
+            for (uint32_t j = i + 1; j < F; ++j)
+                if ((long long)C[(size_t)i * F + j] >= ms) {
+                    nl.push_back(i); nl.push_back(j);
+                    nid.push_back((uint32_t)res->parent.size());
+                    res->parent.push_back(i);
+                    res->item.push_back(freq[j]);
+                    res->support.push_back(C[(size_t)i * F + j]);
+                }
+        st.n_frequent_pairs = nid.size();
+        level.swap(nl);
+        level_id.swap(nid);
+        k = 2;
+    } else {
+        level.clear();
+        level_id.clear();
+    }
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    // Frequent index -> column for candidate rows.
+    uint32_t *d_cand = nullptr, *d_sup = nullptr;
+    size_t cand_cap = 0;
+    while (!level.empty()) {
+        const uint64_t n = level.size() / k;
+        // Hash set of the level for the subset test.
+        struct H {
+            size_t operator()(const std::string &s) const { return std::hash<std::string>()(s); }
+        };
+        std::unordered_set<std::string, H> seen;
+        seen.reserve(n * 2);
+        for (uint64_t a = 0; a < n; ++a) seen.insert(std::string((const char *)&level[a * k], k * 4));
+        std::vector<uint32_t> cand, cand_parent;
+        std::vector<uint32_t> sub(k);
+        for (uint64_t a = 0; a < n; ++a) {
+            const uint32_t *pa = &level[a * k];
+            for (uint64_t b2 = a + 1; b2 < n; ++b2) {
+                const uint32_t *pb = &level[b2 * k];
+                if (memcmp(pa, pb, (k - 1) * 4)) break;
+                // candidate = pa + pb[k-1]; all k-subsets must be frequent
+                bool ok = true;
+                for (uint32_t drop = 0; drop + 1 < k && ok; ++drop) {  // dropping the last two gives pa/pb
+                    uint32_t t = 0;
+                    for (uint32_t i = 0; i < k; ++i)
+                        if (i != drop) sub[t++] = pa[i];
+                    sub[t++] = pb[k - 1];
+                    ok = seen.count(std::string((const char *)sub.data(), k * 4)) > 0;
+                }
+                if (!ok) continue;
+                for (uint32_t i = 0; i < k; ++i) cand.push_back(pa[i]);
+                cand.push_back(pb[k - 1]);
+                cand_parent.push_back(level_id[a]);
+            }
+        }
+        const uint64_t nc = cand_parent.size();
+        if (!nc) break;
+        const uint32_t w = k + 1;
+        std::vector<uint32_t> rows(cand.size());
+        for (size_t i = 0; i < cand.size(); ++i) rows[i] = freq[cand[i]];
+        if (rows.size() > cand_cap) {
+            dfree(ctx, d_cand);
+            dfree(ctx, d_sup);
+            cand_cap = rows.size() * 2;
+            CKR(dalloc(ctx, &d_cand, cand_cap));
+            CKR(dalloc(ctx, &d_sup, cand_cap));
+        }
+        CK(cudaMemcpyAsync(d_cand, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+        k_count_kway<<<(unsigned)((nc * 32 + 255) / 256), 256, 0, ctx->stream>>>(db->d_bits, db->stride, d_cand, nc, w, d_sup);
+        CK(cudaGetLastError());
+        st.kernel_launches++;
+        std::vector<uint32_t> sup(nc);
+        CK(cudaMemcpyAsync(sup.data(), d_sup, nc * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        st.intersections += nc * (w - 1);
+        st.bytes_alg += nc * w * db->stride * 8;
+        std::vector<uint32_t> nl, nid;
+        for (uint64_t c = 0; c < nc; ++c) {
+            if ((long long)sup[c] < ms) continue;
+            nl.insert(nl.end(), cand.begin() + c * w, cand.begin() + (c + 1) * w);
+            nid.push_back((uint32_t)res->parent.size());
+            res->parent.push_back(cand_parent[c]);
+            res->item.push_back(freq[cand[c * w + w - 1]]);
+            res->support.push_back(sup[c]);
+        }
+        level.swap(nl);
+        level_id.swap(nid);
+        k = w;
+    }
+    dfree(ctx, d_cand);
+    dfree(ctx, d_sup);
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    st.n_patterns = res->parent.size();
+    st.ms_pairs = elapsed_ms(ctx, 1, 2);
+    st.ms_deep = elapsed_ms(ctx, 2, 3);
+    st.ms_total = elapsed_ms(ctx, 0, 3);
+    st.deep_gbs = st.ms_deep > 0 ? st.bytes_alg / (st.ms_deep * 1e6) : 0.0;
+    st.pair_tops = st.ms_pairs > 0 ? st.pair_ops / (st.ms_pairs * 1e9) : 0.0;
+    return CPM_OK;
+}
+
+extern "C" int cpm_mine(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, int algo, const cpm_opts *opts,
+                        cpm_result **out) {
+    if (!ctx || !db || !out || db->ctx != ctx) return CPM_EINVAL;
+    if (algo != CPM_ECLAT && algo != CPM_APRIORI) return set_err(ctx, CPM_EINVAL, "unknown algorithm %d", algo);
+    *out = nullptr;
+    CK(cudaSetDevice(ctx->device));
+    cpm_opts o;
+    if (opts) o = *opts;
+    else cpm_default_opts(&o);
+    // Supports are 32-bit counts; thresholds beyond every count pass nothing.
+    const long long ms = (long long)std::max<int64_t>(std::min<int64_t>(min_sup, (int64_t)1 << 40), -1);
+    cpm_result *res = new cpm_result();
+    res->algo = algo;
+    const auto t0 = std::chrono::steady_clock::now();
+    int r = algo == CPM_ECLAT ? mine_eclat(ctx, db, ms, o, res) : mine_apriori(ctx, db, ms, o, res);
+    if (r != CPM_OK) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaGetLastError();
+        delete res;
+        return r;
+    }
+    (void)t0;
+    *out = res;
+    return CPM_OK;
+}
+
+extern "C" int cpm_result_size(const cpm_result *res, uint64_t *n_patterns, uint64_t *n_item_slots) {
+    if (!res) return CPM_EINVAL;
+    const uint64_t n = res->parent.size();
+    if (n_patterns) *n_patterns = n;
+    if (n_item_slots) {
+        // depth of every pattern (parents always precede children)
+        std::vector<uint32_t> depth(n);
+        uint64_t tot = 0;
+        for (uint64_t k = 0; k < n; ++k) {
+            depth[k] = res->parent[k] == 0xffffffffu ? 1 : depth[res->parent[k]] + 1;
+            tot += depth[k];
+        }
+        *n_item_slots = tot;
+    }
+    return CPM_OK;
+}
+
+extern "C" int cpm_result_tree(const cpm_result *res, int64_t *parent, uint32_t *item, uint64_t *support) {
+    if (!res) return CPM_EINVAL;
+    for (size_t k = 0; k < res->parent.size(); ++k) {
+        if (parent) parent[k] = res->parent[k] == 0xffffffffu ? -1 : (int64_t)res->parent[k];
+        if (item) item[k] = res->item[k];
+        if (support) support[k] = res->support[k];
+    }
+    return CPM_OK;
+}
+
+extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offsets, uint32_t *items,
+                               uint64_t *supports) {
+    if (!res || !offsets || !supports) return CPM_EINVAL;
+    if (order != CPM_ORDER_ECLAT && order != CPM_ORDER_APRIORI && order != CPM_ORDER_NONE) return CPM_EINVAL;
+    const uint64_t n = res->parent.size();
+    // Patterns in device order, items sorted ascending within each.
+    std::vector<uint32_t> depth(n);
+    std::vector<uint64_t> start(n + 1, 0);
+    for (uint64_t k = 0; k < n; ++k) {
+        const uint32_t p = res->parent[k];
+        if (p != 0xffffffffu && p >= k) return CPM_EINTERNAL;
+        depth[k] = p == 0xffffffffu ? 1 : depth[p] + 1;
+        start[k + 1] = start[k] + depth[k];
+    }
+    std::vector<uint32_t> flat(start[n]);
+    for (uint64_t k = 0; k < n; ++k) {
+        uint32_t *dst = flat.data() + start[k];
+        const uint32_t p = res->parent[k];
+        if (p != 0xffffffffu) memcpy(dst, flat.data() + start[p], (depth[k] - 1) * 4);
+        dst[depth[k] - 1] = res->item[k];
+    }
+    for (uint64_t k = 0; k < n; ++k) {
+        uint32_t *a = flat.data() + start[k];
+        // parent part is sorted already; insert the last item in place
+        uint32_t d = depth[k];
+        for (uint32_t i = d - 1; i > 0 && a[i] < a[i - 1]; --i) std::swap(a[i], a[i - 1]);
+    }
+    std::vector<uint64_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0ull);
+    auto pat = [&](uint64_t k) { return flat.data() + start[k]; };
+    if (order == CPM_ORDER_APRIORI) {
+        std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+            if (depth[a] != depth[b]) return depth[a] < depth[b];
+            return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
+        });
+    } else if (order == CPM_ORDER_ECLAT) {
+        // cuEclat inserts singletons, then pairs, then every deeper pattern in
+        // the order of its class search: key (x1..x_{k-1}, -1, x_k).
+        std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+            const uint32_t ga = std::min<uint32_t>(depth[a], 3), gb = std::min<uint32_t>(depth[b], 3);
+            if (ga != gb) return ga < gb;
+            if (ga < 3) return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
+            const uint32_t *x = pat(a), *y = pat(b);
+            const int64_t la = depth[a] + 1, lb = depth[b] + 1;
+            for (int64_t i = 0; i < std::min(la, lb); ++i) {
+                const int64_t u = i < la - 2 ? (int64_t)x[i] : (i == la - 2 ? (int64_t)-1 : (int64_t)x[la - 2]);
+                const int64_t v = i < lb - 2 ? (int64_t)y[i] : (i == lb - 2 ? (int64_t)-1 : (int64_t)y[lb - 2]);
+                if (u != v) return u < v;
+            }
+            return la < lb;
+        });
+    }
+    uint64_t pos = 0;
+    offsets[0] = 0;
+    for (uint64_t r = 0; r < n; ++r) {
+        const uint64_t k = idx[r];
+        if (items) memcpy(items + pos, pat(k), depth[k] * 4);
+        pos += depth[k];
+        offsets[r + 1] = pos;
+        supports[r] = res->support[k];
+    }
+    return CPM_OK;
+}
+
+extern "C" int cpm_result_stats(const cpm_result *res, cpm_stats *stats) {
+    if (!res || !stats) return CPM_EINVAL;
+    *stats = res->stats;
+    return CPM_OK;
+}
+
+extern "C" void cpm_result_free(cpm_result *res) { delete res; }
+
+// ---------------------------------------------------------------------------
+// reference kernel-module API
+// ---------------------------------------------------------------------------
+
+extern "C" int cpm_build_bitsets(cpm_ctx *ctx, const uint64_t *d_rows, const uint32_t *d_columns, uint64_t count,
+                                 uint64_t transactions, uint32_t items, uint32_t *d_bitsets) {
+    if (!ctx || (count && (!d_rows || !d_columns)) || (items && !d_bitsets)) return CPM_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    const uint64_t words = (transactions + 31) / 32;
+    if (items && words) CK(cudaMemsetAsync(d_bitsets, 0, (size_t)items * words * 4, ctx->stream));
+    if (count) {
+        const unsigned blocks = (unsigned)std::min<uint64_t>((count + 255) / 256, (uint64_t)ctx->sms * 32);
+        k_ref_build<<<blocks, 256, 0, ctx->stream>>>(d_rows, d_columns, count, words, d_bitsets);
+        CK(cudaGetLastError());
+    }
+    return CPM_OK;
+}
+
+extern "C" int cpm_count_supports(cpm_ctx *ctx, const uint32_t *d_bitsets, uint64_t words32,
+                                  const uint32_t *d_candidates, uint64_t n_candidates, uint32_t width,
+                                  uint64_t *d_supports) {
+    if (!ctx || (n_candidates && (!d_candidates || !d_supports || !width))) return CPM_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    if (!n_candidates) return CPM_OK;
+    k_ref_count<<<(unsigned)((n_candidates * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+        d_bitsets, words32, d_candidates, n_candidates, width, reinterpret_cast<unsigned long long *>(d_supports));
+    CK(cudaGetLastError());
+    return CPM_OK;
+}
+
+extern "C" int cpm_intersect_extensions(cpm_ctx *ctx, const uint32_t *d_prefix, const uint32_t *d_extensions,
+                                        uint64_t words32, uint64_t n_extensions, uint32_t *d_out,
+                                        uint64_t *d_supports) {
+    if (!ctx || (n_extensions && (!d_prefix || !d_extensions || !d_out || !d_supports))) return CPM_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    if (!n_extensions) return CPM_OK;
+    k_ref_intersect<<<(unsigned)((n_extensions * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+        d_prefix, d_extensions, words32, n_extensions, d_out, reinterpret_cast<unsigned long long *>(d_supports));
+    CK(cudaGetLastError());
+    return CPM_OK;
+}

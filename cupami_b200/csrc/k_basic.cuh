@@ -1,0 +1,166 @@
+// Packing, singleton supports, ordered compaction, k-way support counting and
+// the reference kernel-module API kernels.
+//
+// Layout: item-major tidsets, bit (r % 64) of 64-bit word (r / 64) of row c is
+// set when non-empty transaction r holds column c.  Rows are `stride` words
+// apart, stride = ceil(N/64) rounded up to an even count so that every row
+// starts on a 16-byte boundary and can be read with 128-bit loads.
+#pragma once
+#include "common.cuh"
+
+namespace cpm {
+
+// One thread per transaction.  Threads of a warp hold 32 consecutive rows, so
+// they share one 32-bit word of every tidset; threads that reach the same
+// column in the same step merge their bits with __match_any_sync and one
+// atomicOr (the match mask is exactly the OR of their 1 << lane bits).
+// Reference: _bitsets.py:20-28 (one atomicOr per occurrence).
+__global__ void k_pack(const uint64_t *__restrict__ offsets, const uint32_t *__restrict__ ids,
+                       const uint32_t *__restrict__ lut, uint64_t n_tx, uint64_t stride,
+                       uint32_t *__restrict__ bits32) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned lane = threadIdx.x & 31;
+    const bool valid = r < n_tx;
+    const uint64_t b = valid ? offsets[r] : 0;
+    const uint32_t len = valid ? (uint32_t)(offsets[r + 1] - b) : 0;
+    const uint32_t maxlen = warp_max_u32(len);
+    const uint64_t word32 = r >> 5;
+    for (uint32_t k = 0; k < maxlen; ++k) {
+        uint32_t c = 0xffffffffu;
+        if (k < len) {
+            c = __ldg(ids + b + k);
+            if (lut) c = __ldg(lut + c);
+        }
+        const unsigned grp = __match_any_sync(CPM_FULL, c);
+        if (c != 0xffffffffu && lane == (unsigned)(__ffs(grp) - 1))
+            atomicOr(bits32 + (uint64_t)c * stride * 2 + word32, grp);
+    }
+}
+
+// Marks which raw ids occur (presence bitmap over the id universe).
+__global__ void k_mark_ids(const uint32_t *__restrict__ ids, uint64_t nnz, uint32_t *__restrict__ present) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = ids[i];
+        atomicOr(present + (v >> 5), 1u << (v & 31));
+    }
+}
+
+// support[c] = popcount of row c; one warp per row, 128-bit loads.
+__global__ void k_item_support(const uint64_t *__restrict__ bits, uint64_t stride, uint32_t n_items,
+                               uint32_t *__restrict__ support) {
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (warp >= n_items) return;
+    const ulonglong2 *row = reinterpret_cast<const ulonglong2 *>(bits + warp * stride);
+    uint32_t s = 0;
+    for (uint64_t v = lane; v < stride / 2; v += 32) s += popc2(ld_stream(row + v));
+    s = warp_sum_u32(s);
+    if (!lane) support[warp] = s;
+}
+
+// Ordered compaction of the columns whose support passes: out[k] = k-th
+// passing column in increasing order; *count = number passing.  One CTA.
+__global__ void k_compact_frequent(const uint32_t *__restrict__ support, uint32_t n_items,
+                                   long long minsup, uint32_t *__restrict__ out,
+                                   uint32_t *__restrict__ count) {
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t base;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t start = 0; start < n_items; start += blockDim.x) {
+        const uint32_t c = start + threadIdx.x;
+        const bool pass = c < n_items && (long long)support[c] >= minsup;
+        const unsigned bal = __ballot_sync(CPM_FULL, pass);
+        if (!lane) warp_tot[wid] = __popc(bal);
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+        for (unsigned w = 0; w < nw; ++w) {
+            if (w < wid) before += warp_tot[w];
+            total += warp_tot[w];
+        }
+        if (pass) out[base + before + __popc(bal & ((1u << lane) - 1))] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) base += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *count = base;
+}
+
+// Writes the singleton pattern records (parent none, item, support).
+__global__ void k_emit_singletons(const uint32_t *__restrict__ freq, uint32_t F,
+                                  const uint32_t *__restrict__ support, uint32_t *__restrict__ pat_parent,
+                                  uint32_t *__restrict__ pat_item, uint32_t *__restrict__ pat_sup) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= F) return;
+    pat_parent[i] = 0xffffffffu;
+    pat_item[i] = freq[i];
+    pat_sup[i] = support[freq[i]];
+}
+
+// k-way complete intersection (GPApriori counting, _bitsets.py:30-53): one
+// warp per candidate, candidate c = rows cand[c*width .. +width).
+__global__ void k_count_kway(const uint64_t *__restrict__ bits, uint64_t stride,
+                             const uint32_t *__restrict__ cand, uint64_t n, uint32_t width,
+                             uint32_t *__restrict__ support) {
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const uint32_t *cc = cand + warp * width;
+    uint32_t s = 0;
+    for (uint64_t v = lane; v < stride / 2; v += 32) {
+        ulonglong2 acc = make_ulonglong2(~0ull, ~0ull);
+        for (uint32_t j = 0; j < width; ++j)
+            acc = and2(acc, ld_stream(reinterpret_cast<const ulonglong2 *>(bits + (uint64_t)cc[j] * stride) + v));
+        s += popc2(acc);
+    }
+    s = warp_sum_u32(s);
+    if (!lane) support[warp] = s;
+}
+
+// ---- reference kernel-module API (32-bit word layout of _bitsets.py) ------
+
+__global__ void k_ref_build(const uint64_t *__restrict__ rows, const uint32_t *__restrict__ cols,
+                            uint64_t count, uint64_t words, uint32_t *__restrict__ bits) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        atomicOr(bits + (uint64_t)cols[i] * words + rows[i] / 32, 1u << (rows[i] % 32));
+}
+
+__global__ void k_ref_count(const uint32_t *__restrict__ bits, uint64_t words,
+                            const uint32_t *__restrict__ cand, uint64_t n, uint32_t width,
+                            unsigned long long *__restrict__ support) {
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const uint32_t *cc = cand + warp * width;
+    unsigned long long s = 0;
+    for (uint64_t w = lane; w < words; w += 32) {
+        uint32_t acc = 0xffffffffu;
+        for (uint32_t j = 0; j < width; ++j) acc &= __ldg(bits + (uint64_t)cc[j] * words + w);
+        s += __popc(acc);
+    }
+    s = warp_sum_u64(s);
+    if (!lane) support[warp] = s;
+}
+
+__global__ void k_ref_intersect(const uint32_t *__restrict__ prefix, const uint32_t *__restrict__ ext,
+                                uint64_t words, uint64_t n, uint32_t *__restrict__ out,
+                                unsigned long long *__restrict__ support) {
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    unsigned long long s = 0;
+    const uint32_t *e = ext + warp * words;
+    uint32_t *o = out + warp * words;
+    for (uint64_t w = lane; w < words; w += 32) {
+        const uint32_t v = __ldg(prefix + w) & __ldg(e + w);
+        o[w] = v;
+        s += __popc(v);
+    }
+    s = warp_sum_u64(s);
+    if (!lane) support[warp] = s;
+}
+
+}  // namespace cpm

@@ -1,0 +1,366 @@
+"""Drop-in ``cuApriori`` on the B200 vertical-bitset engine.
+
+Same constructor, threshold rule, output and timing API as cuPAMI's
+``cupami.frequentPattern.cuApriori`` (``cupami/frequentPattern/cuApriori.py:173-593``);
+the mining runs in ``libcupami_b200.so`` (sm_100a kernels behind a C ABI), not
+in CuPy.  There is no CPU fallback: without the library or a CUDA device,
+``mine()`` raises.
+
+Input handling follows the reference's semantics:
+
+* labels are ``str(value).strip()``; repeated labels in a basket count once;
+  empty baskets are dropped and do not count towards the transaction total
+  (``cuApriori.py:435-450``);
+* item order is the sorted order of the label strings (``cuApriori.py:397``);
+* ``minSup`` floats in (0, 1] are fractions rounded up, anything else is
+  ``int(minSup)`` (``cuApriori.py:452-456``).
+
+Integer inputs (BIN files, Parquet ``list<uint32>`` columns and
+:class:`~cupami_b200.datasets.TransactionCSR` objects) take a numeric path:
+the CSR arrays go to the device as they are and the library orders the ids as
+their decimal strings sort, which yields the same labels and columns as the
+string path without building Python baskets.
+"""
+
+from __future__ import annotations
+
+import csv
+import io
+import math
+import struct
+import sys
+import time
+from itertools import chain
+from pathlib import Path
+from urllib.parse import urlparse
+from urllib.request import urlopen
+
+import numpy as np
+
+from .. import _native
+from ..datasets import TransactionCSR
+
+_BIN_MAGIC = b"CUPAMI01"
+
+
+class _PatternDict(dict):
+    """``_finalPatterns`` built on first use from the mined arrays."""
+
+
+class cuApriori:
+    """Level-wise frequent itemset mining with device-side support counting.
+
+    Parameters mirror the reference: ``iFile`` (rows, CSV/TSV/text path, BIN,
+    Parquet, HTTP(S) text URL or a ``TransactionCSR``), ``minSup``, ``sep``,
+    ``use_gds`` and ``use_gpu_io`` ("auto", True or False).
+    """
+
+    _ALGORITHM = _native.CPM_APRIORI
+    _ORDER = _native.CPM_ORDER_APRIORI
+
+    #: Deep-level scheduler: "plain" (size ordered) or "learned" (cost model).
+    scheduler = "plain"
+
+    def __init__(self, iFile, minSup, sep=None, use_gds="auto", use_gpu_io="auto"):
+        loading_start = time.perf_counter()
+        if use_gds not in ("auto", True, False):
+            raise ValueError('use_gds must be "auto", True, or False')
+        if use_gpu_io not in ("auto", True, False):
+            raise ValueError('use_gpu_io must be "auto", True, or False')
+        self.iFile = iFile
+        self.minSup = minSup
+        self.sep = sep
+        self.use_gds = use_gds
+        self.use_gpu_io = use_gpu_io
+        self._csr = None
+        self._inputBackend = {"backend": "cpu", "reason": "Text or Parquet input"}
+        if use_gds is True and (not isinstance(iFile, (str, Path))
+                                or Path(iFile).suffix.lower() != ".bin"
+                                or urlparse(str(iFile)).scheme in ("http", "https")):
+            raise ValueError("Required GDS input currently supports local BIN files only")
+        self._Database = self._readTransactions(iFile)
+        if self._Database is not None:
+            self._transactionCount = len(self._Database)
+        self._minSup = self._getSupportCount(minSup, self._transactionCount)
+        self._patterns = None          # cached dict built from the arrays
+        self._result = None            # _native.Result of the latest mine()
+        self._labels = []
+        self._startTime = 0.0
+        self._endTime = 0.0
+        self._loadingTime = time.perf_counter() - loading_start
+
+    # ---- input -----------------------------------------------------------
+
+    def _readTransactions(self, source):
+        if isinstance(source, TransactionCSR):
+            return self._useCsr(source.offsets, source.items, "numpy-cuda",
+                                "Integer CSR arrays; no Python transactions")
+        if isinstance(source, str) and urlparse(source).scheme in ("http", "https"):
+            with urlopen(source, timeout=30) as response:
+                stream = io.TextIOWrapper(response, encoding="utf-8", newline="")
+                return self._readDelimitedFile(stream)
+        if isinstance(source, (str, Path)):
+            suffix = Path(source).suffix.lower()
+            if suffix == ".bin":
+                return self._readBinaryFile(Path(source))
+            if suffix == ".parquet":
+                return self._readParquetFile(source)
+            with Path(source).open("r", newline="", encoding="utf-8") as stream:
+                return self._readDelimitedFile(stream)
+        return self._cleanTransactions(source)
+
+    def _useCsr(self, offsets, ids, backend, reason):
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        ids = np.ascontiguousarray(ids, dtype=np.uint32)
+        self._csr = (offsets, ids)
+        self._transactionCount = int(np.count_nonzero(offsets[1:] > offsets[:-1]))
+        previous = self._inputBackend.get("reason")
+        self._inputBackend = {"backend": backend, "reason": reason}
+        if previous and backend == "numpy-cuda":
+            self._inputBackend["gds_fallback_reason"] = previous
+        self._inputBackend["direct_gds_verified"] = False
+        return None
+
+    def _gdsUnavailable(self):
+        reason = "GDS (cuFile/KvikIO) is not part of this engine"
+        self._inputBackend = {"backend": "cpu", "reason": reason}
+        if self.use_gds is True:
+            raise RuntimeError(f"GDS input requested but unavailable: {reason}")
+
+    def _readBinaryFile(self, path):
+        """The CUPAMI01 BIN layout (docs/transaction-formats.md, 'Transactional BIN')."""
+        with path.open("rb") as source:
+            header = source.read(32)
+            if len(header) != 32:
+                raise ValueError("Invalid BIN file: truncated header")
+            magic, count, total, universe = struct.unpack("<8sQQQ", header)
+            if magic != _BIN_MAGIC:
+                raise ValueError("Invalid BIN file: expected CUPAMI01 format")
+            if not 1 <= universe <= 0xFFFFFFFF:
+                raise ValueError("Invalid BIN file: item universe must fit in uint32")
+            if path.stat().st_size != 32 + 8 * (count + 1) + 4 * total:
+                raise ValueError("Invalid BIN file: size does not match header")
+            if self.use_gds is False:
+                self._inputBackend = {"backend": "cpu", "reason": "GDS disabled"}
+            else:
+                self._gdsUnavailable()
+            offsets = np.fromfile(source, dtype="<u8", count=count + 1)
+            ids = np.fromfile(source, dtype="<u4", count=total)
+        if offsets.size != count + 1 or ids.size != total:
+            raise ValueError("Invalid BIN file: truncated arrays")
+        if offsets[0] != 0 or offsets[-1] != total or np.any(offsets[1:] < offsets[:-1]):
+            raise ValueError("Invalid BIN file: invalid transaction offsets")
+        if np.any(ids > universe):
+            raise ValueError("Invalid BIN file: item ID outside configured universe")
+        if self.use_gpu_io is False:
+            rows = (ids[offsets[i]:offsets[i + 1]].tolist() for i in range(count))
+            return self._cleanTransactions(rows)
+        return self._useCsr(offsets, ids, "numpy-cuda",
+                            "Bulk numeric BIN reads and GPU transfers; no Python transactions")
+
+    def _readParquetFile(self, path):
+        try:
+            import pyarrow as pa
+            import pyarrow.parquet as pq
+        except ImportError as error:
+            raise ImportError("Parquet input requires pyarrow: pip install pyarrow") from error
+        parquet = pq.ParquetFile(path)
+        schema = parquet.schema_arrow
+        if "items" not in schema.names:
+            raise ValueError("Invalid Parquet file: missing items column")
+        itemType = schema.field("items").type
+        if not pa.types.is_list(itemType) or not pa.types.is_uint32(itemType.value_type):
+            raise ValueError("Invalid Parquet file: items must be a list of uint32 IDs")
+        column = parquet.read(columns=["items"]).column("items").combine_chunks()
+        if column.null_count or (len(column) and column.values.null_count):
+            raise ValueError("Invalid Parquet file: null transactions or item IDs")
+        if self.use_gpu_io is False:
+            return self._cleanTransactions(column.to_pylist())
+        offsets = np.asarray(column.offsets, dtype=np.int64)
+        values = np.asarray(column.values, dtype=np.uint32)
+        base = offsets[0] if offsets.size else 0
+        return self._useCsr((offsets - base).astype(np.uint64), values[base:offsets[-1]] if offsets.size else values,
+                            "arrow-cuda", "Parquet list arrays sent to the GPU; no Python transactions")
+
+    def _readDelimitedFile(self, inputStream):
+        firstLine = inputStream.readline()
+        delimiter = self.sep
+        if delimiter is None:
+            delimiter = "\t" if "\t" in firstLine else ","
+        rows = csv.reader(chain((firstLine,), inputStream), delimiter=delimiter)
+        return self._cleanTransactions(rows)
+
+    def _cleanTransactions(self, rows):
+        transactions = []
+        for row in rows:
+            transaction = self._cleanTransaction(row)
+            if transaction:
+                transactions.append(transaction)
+        return transactions
+
+    @staticmethod
+    def _cleanTransaction(transaction):
+        seen = {}
+        for value in transaction:
+            label = str(value).strip()
+            if label:
+                seen.setdefault(label, None)
+        return tuple(seen)
+
+    @staticmethod
+    def _getSupportCount(minSup, transactionCount):
+        if isinstance(minSup, float) and 0 < minSup <= 1:
+            return math.ceil(minSup * transactionCount)
+        return int(minSup)
+
+    @staticmethod
+    def _getCudaModule():
+        """The native device context; raises like the reference when CUDA is missing."""
+        return _native.context(0)
+
+    def getInputBackend(self):
+        return dict(self._inputBackend)
+
+    # ---- mining ------------------------------------------------------------
+
+    def _deviceDatabase(self, ctx):
+        """Tidsets on the device plus the label of every column (sorted strings)."""
+        if self._csr is not None:
+            offsets, ids = self._csr
+            db = _native.Database.from_ids(ctx, offsets, ids)
+            labels = [str(v) for v in db.labels.tolist()]
+            return db, labels
+        labels = sorted({item for row in self._Database for item in row})
+        index = {label: i for i, label in enumerate(labels)}
+        offsets = np.zeros(len(self._Database) + 1, dtype=np.uint64)
+        np.cumsum(np.fromiter((len(r) for r in self._Database), dtype=np.uint64,
+                              count=len(self._Database)), out=offsets[1:])
+        cols = np.fromiter((index[item] for row in self._Database for item in row),
+                           dtype=np.uint32, count=int(offsets[-1]))
+        return _native.Database.from_columns(ctx, offsets, cols, len(labels)), labels
+
+    def _options(self):
+        opts = _native.Opts()
+        _native.library().cpm_default_opts(opts)
+        opts.scheduler = (_native.CPM_SCHED_LEARNED if self.scheduler == "learned"
+                          else _native.CPM_SCHED_PLAIN)
+        return opts
+
+    def mine(self):
+        self._startTime = time.perf_counter()
+        ctx = self._getCudaModule()
+        db, labels = self._deviceDatabase(ctx)
+        try:
+            result = db.mine(self._minSup, self._ALGORITHM, self._options(), self._ORDER)
+        finally:
+            db.close()
+        self._labels = labels
+        self._result = result
+        self._patterns = None
+        self._endTime = time.perf_counter()
+
+    # ---- output --------------------------------------------------------------
+
+    def _patternTuples(self):
+        res = self._result
+        if res is None:
+            return []
+        labels = self._labels
+        o = res.offsets.tolist()
+        items = [labels[c] for c in res.items.tolist()]
+        return [tuple(items[o[k]:o[k + 1]]) for k in range(len(o) - 1)]
+
+    @property
+    def _finalPatterns(self):
+        if self._patterns is None:
+            res = self._result
+            tuples = self._patternTuples()
+            supports = res.supports.tolist() if res is not None else []
+            self._patterns = _PatternDict(zip(tuples, supports))
+        return self._patterns
+
+    @_finalPatterns.setter
+    def _finalPatterns(self, value):
+        self._patterns = value
+
+    def getPatternArrays(self):
+        """``(offsets, columns, supports, labels)`` without building a dict."""
+        res = self._result
+        if res is None:
+            return (np.zeros(1, np.uint64), np.zeros(0, np.uint32), np.zeros(0, np.uint64), [])
+        return res.offsets, res.items, res.supports, list(self._labels)
+
+    def getKernelStats(self):
+        """Device-side counters of the latest mine() (launches, bytes, times)."""
+        return dict(self._result.stats) if self._result is not None else {}
+
+    def getPatterns(self):
+        return {"\t".join(pattern): support for pattern, support in self._finalPatterns.items()}
+
+    def getPatternsAsDataFrame(self):
+        import pandas as pd
+
+        rows = [("\t".join(pattern), support) for pattern, support in self._finalPatterns.items()]
+        return pd.DataFrame(rows, columns=["Patterns", "Support"])
+
+    def save(self, outputFile):
+        with Path(outputFile).open("w", encoding="utf-8") as file:
+            for pattern, support in sorted(self._finalPatterns.items()):
+                file.write(f"{chr(9).join(pattern)} : {support}\n")
+
+    def getRuntime(self):
+        """Mining time in seconds, excluding constructor input loading."""
+        return self._endTime - self._startTime
+
+    def getLoadingTime(self):
+        """Constructor input parsing/loading time."""
+        return self._loadingTime
+
+    def getMiningTime(self):
+        """Time of the latest mine() call, including device packing."""
+        return self.getRuntime()
+
+    def getTotalRuntime(self):
+        return self.getLoadingTime() + self.getMiningTime()
+
+    def getMemoryRSS(self):
+        try:
+            import psutil
+        except ImportError:
+            return 0
+        return int(psutil.Process().memory_info().rss)
+
+    def getMemoryUSS(self):
+        try:
+            import psutil
+        except ImportError:
+            return 0
+        return int(psutil.Process().memory_full_info().uss)
+
+    def printResults(self):
+        print("Total number of Frequent Patterns:", len(self._finalPatterns))
+        print("Total Memory in USS:", self.getMemoryUSS())
+        print("Total Memory in RSS:", self.getMemoryRSS())
+        print("Loading time (seconds):", self.getLoadingTime())
+        print("Mining time (seconds):", self.getMiningTime())
+        print("Total time (seconds):", self.getTotalRuntime())
+
+
+Apriori = cuApriori
+
+
+def _cli(cls, argv):
+    if len(argv) not in (4, 5):
+        sys.exit(f"Usage: python -m {cls.__module__} <inputFile> <outputFile> <minSup> [sep]")
+    try:
+        minSup = int(argv[3])
+    except ValueError:
+        minSup = float(argv[3])
+    miner = cls(argv[1], minSup, argv[4] if len(argv) == 5 else None)
+    miner.mine()
+    miner.save(argv[2])
+    miner.printResults()
+
+
+if __name__ == "__main__":
+    _cli(cuApriori, sys.argv)

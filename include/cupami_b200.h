@@ -1,0 +1,164 @@
+/*
+ * cupami_b200 -- C ABI of the B200 vertical-bitset frequent-itemset engine.
+ *
+ * The entry points replace the GPU path behind cuPAMI's cuEclat / cuApriori.
+ * Reference locations are given relative to the cuPAMI project root.
+ *
+ *   cpm_db_from_csr / cpm_db_from_ids
+ *       replace cuApriori._getDevicePairs + _bitsets.build_bitsets
+ *       (cupami/frequentPattern/cuApriori.py:378-404,
+ *        cupami/frequentPattern/_bitsets.py:20-28, 91-100)
+ *   cpm_mine(algo = CPM_ECLAT)
+ *       replaces cuEclat.mine + cuEclat._searchClass
+ *       (cupami/frequentPattern/cuEclat.py:168-245)
+ *   cpm_mine(algo = CPM_APRIORI)
+ *       replaces cuApriori.mine + _generateCandidates + _countCandidateSupports
+ *       (cupami/frequentPattern/cuApriori.py:473-535)
+ *   cpm_build_bitsets / cpm_count_supports / cpm_intersect_extensions
+ *       replace the three kernel wrappers of cupami/frequentPattern/_bitsets.py:91-125
+ *       one for one (same 32-bit word layout, device pointers in, device
+ *       pointers out) for callers that drive their own search, such as the
+ *       cuSpatialEclat hooks (cupami/georeferencedFrequentPattern/cuSpatialEclat.py:197-211).
+ *
+ * Conventions
+ *   - Every function returns CPM_OK (0) or a negative CPM_E* code; no C++
+ *     exception crosses the boundary.  cpm_last_error(ctx) describes the last
+ *     failure on that context.
+ *   - A context owns one CUDA device and one stream.  Calls on one context
+ *     must not overlap (no internal locking); use one context per thread.
+ *   - Pointers named d_* are device pointers on the context's device; every
+ *     other pointer is host memory owned by the caller and only read or
+ *     written during the call.
+ *   - Item columns are indices into the caller's label table.  The reference
+ *     orders labels as sorted strings (cuApriori.py:397); cpm_db_from_ids does
+ *     that ordering itself for integer ids and returns the label table.
+ *   - Supports pass when support >= min_sup (cuEclat.py:177,191,236).  A
+ *     min_sup <= 0 lets every candidate through, zero supports included.
+ */
+#ifndef CUPAMI_B200_H
+#define CUPAMI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CPM_OK          0
+#define CPM_EINVAL     -1   /* bad argument */
+#define CPM_ENOMEM     -2   /* device or host allocation failed */
+#define CPM_ECUDA      -3   /* CUDA runtime error */
+#define CPM_EOVERFLOW  -4   /* a device queue or arena stayed too small after retries */
+#define CPM_ETIMEOUT   -5   /* a bounded device wait ran out (spin limit) */
+#define CPM_ENODEV     -6   /* no usable CUDA device */
+#define CPM_EINTERNAL  -7
+
+#define CPM_ECLAT    0
+#define CPM_APRIORI  1
+
+/* Pattern order produced by cpm_result_copy. */
+#define CPM_ORDER_ECLAT    0  /* insertion order of cuEclat.mine (cuEclat.py:168-245) */
+#define CPM_ORDER_APRIORI  1  /* insertion order of cuApriori.mine: by length, then tuple */
+#define CPM_ORDER_NONE     2  /* device emission order (fastest) */
+
+/* Deep-level scheduler. */
+#define CPM_SCHED_PLAIN    0  /* frames admitted largest first by member count */
+#define CPM_SCHED_LEARNED  1  /* frames ordered by the cost model's predicted subtree cost */
+
+typedef struct cpm_ctx cpm_ctx;
+typedef struct cpm_db cpm_db;
+typedef struct cpm_result cpm_result;
+
+typedef struct {
+    int32_t  scheduler;            /* CPM_SCHED_* */
+    int32_t  pair_engine;          /* 0 auto, 1 tensor-core Gram, 2 CUDA-core Gram */
+    uint64_t pair_batch;           /* mirrors cuEclat._PAIR_BATCH_SIZE; 0 = no limit */
+    uint64_t intersection_bytes;   /* mirrors cuEclat._INTERSECTION_BATCH_BYTES; 0 = no limit */
+    uint64_t arena_bytes;          /* device arena for child tidsets; 0 = automatic */
+    uint64_t spin_limit;           /* bounded device waits; 0 = default */
+    int32_t  collect_trace;        /* 1: record per-frame features and costs for the cost model */
+    int32_t  reserved[7];
+} cpm_opts;
+
+typedef struct {
+    uint64_t n_patterns;
+    uint64_t n_frequent_items;
+    uint64_t n_frequent_pairs;
+    uint64_t frames;               /* deep equivalence classes processed */
+    uint64_t work_items;           /* (frame, position) units processed */
+    uint64_t intersections;        /* sibling AND+popcount operations */
+    uint64_t bytes_alg;            /* sum over units of 8*W*(1 + siblings + survivors) */
+    uint64_t pair_ops;             /* tensor ops issued by the pair Gram (2*K*rows*cols) */
+    uint64_t kernel_launches;
+    uint64_t retries;              /* arena/queue overflow retries */
+    double   ms_pack;
+    double   ms_pairs;
+    double   ms_deep;
+    double   ms_total;
+    double   deep_gbs;             /* bytes_alg / ms_deep */
+    double   pair_tops;            /* pair_ops / ms_pairs */
+} cpm_stats;
+
+/* ---- context ------------------------------------------------------------ */
+int         cpm_init(int device, cpm_ctx **out);
+void        cpm_shutdown(cpm_ctx *ctx);
+const char *cpm_last_error(const cpm_ctx *ctx);
+const char *cpm_version(void);
+int         cpm_default_opts(cpm_opts *opts);
+
+/* ---- databases ------------------------------------------------------------ */
+/* CSR of item columns.  Empty rows are dropped and the rest renumbered in
+ * order (cuApriori.py:391-392, 401-403); repeated columns in a row are
+ * harmless.  Every column must be < n_items. */
+int cpm_db_from_csr(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows,
+                    const uint32_t *cols, uint64_t nnz, uint32_t n_items, cpm_db **out);
+
+/* CSR of raw integer item ids (the BIN layout, docs/transaction-formats.md).
+ * The library finds the distinct ids, orders them as their decimal strings
+ * sort (cuApriori.py:383-385) and maps every id to its column.  After the
+ * call, cpm_db_labels() returns the ids in column order. */
+int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows,
+                    const uint32_t *ids, uint64_t nnz, cpm_db **out);
+
+int  cpm_db_info(const cpm_db *db, uint64_t *n_transactions, uint32_t *n_items,
+                 uint64_t *words);
+int  cpm_db_labels(const cpm_db *db, uint32_t *ids_out);  /* n_items entries */
+void cpm_db_free(cpm_db *db);
+
+/* ---- mining --------------------------------------------------------------- */
+int  cpm_mine(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, int algo,
+              const cpm_opts *opts, cpm_result **out);
+int  cpm_result_size(const cpm_result *res, uint64_t *n_patterns, uint64_t *n_item_slots);
+/* Flattened patterns in the requested order: pattern k is
+ * items[offsets[k] .. offsets[k+1]) (columns, increasing), support supports[k]. */
+int  cpm_result_copy(const cpm_result *res, int order, uint64_t *offsets,
+                     uint32_t *items, uint64_t *supports);
+/* Pattern tree form: pattern k = pattern parent[k] (or nothing when -1) plus item[k]. */
+int  cpm_result_tree(const cpm_result *res, int64_t *parent, uint32_t *item,
+                     uint64_t *support);
+int  cpm_result_stats(const cpm_result *res, cpm_stats *stats);
+void cpm_result_free(cpm_result *res);
+
+/* ---- reference kernel-module API (cupami/frequentPattern/_bitsets.py) ------- */
+/* d_bitsets: uint32[items][ceil(transactions/32)], zero-filled here, then one
+ * bit per (row, column) pair (_bitsets.py:20-28, 91-100). */
+int cpm_build_bitsets(cpm_ctx *ctx, const uint64_t *d_rows, const uint32_t *d_columns,
+                      uint64_t count, uint64_t transactions, uint32_t items,
+                      uint32_t *d_bitsets);
+/* supports[c] = popcount of the AND of the width rows candidates[c][0..width)
+ * over words32 words (_bitsets.py:30-53, 103-113). */
+int cpm_count_supports(cpm_ctx *ctx, const uint32_t *d_bitsets, uint64_t words32,
+                       const uint32_t *d_candidates, uint64_t n_candidates, uint32_t width,
+                       uint64_t *d_supports);
+/* out[e] = prefix & extensions[e]; supports[e] = popcount(out[e])
+ * (_bitsets.py:55-77, 116-125). */
+int cpm_intersect_extensions(cpm_ctx *ctx, const uint32_t *d_prefix,
+                             const uint32_t *d_extensions, uint64_t words32,
+                             uint64_t n_extensions, uint32_t *d_out, uint64_t *d_supports);
+/* Waits for the context's stream. */
+int cpm_synchronize(cpm_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUPAMI_B200_H */

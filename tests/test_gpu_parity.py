@@ -1,0 +1,114 @@
+"""CUDA path vs the reference's outputs and the CPU oracle (bit-exact)."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).parent / "golden"
+
+
+def _miner(algo):
+    import cupami_b200
+
+    return cupami_b200.cuEclat if algo == "cuEclat" else cupami_b200.cuApriori
+
+
+def test_native_library_is_loaded():
+    import cupami_b200._native as n
+
+    ctx = n.context(0)
+    assert ctx.handle
+    assert n.LIB_PATH.exists()
+
+
+def test_every_golden_case_in_reference_order(golden):
+    for case in golden["cases"]:
+        for algo, runs in case["results"].items():
+            for run in runs:
+                miner = _miner(algo)(case["rows"], run["minSup"])
+                assert miner._minSup == run["resolved"]
+                miner.mine()
+                got = list(miner.getPatterns().items())
+                assert got == [tuple(p) for p in run["patterns"]], (case["name"], algo, run["minSup"])
+
+
+def test_quickstart_known_answer(golden):
+    from cupami_b200 import TransactionCSR
+
+    q = golden["quickstart"]
+    data = np.load(GOLDEN / q["data"])
+    csr = TransactionCSR(data["offsets"], data["items"], 50)
+    for algo in ("cuEclat", "cuApriori"):
+        miner = _miner(algo)(csr, 0.01)
+        miner.mine()
+        got = miner.getPatterns()
+        assert len(got) == 1275
+        assert list(got.items()) == [tuple(p) for p in q["results"][algo]["patterns"]]
+
+
+def test_small_batches_and_dense_known_answer():
+    import cupami_b200
+
+    rows = [list(range(8))] * 65
+    miner = cupami_b200.cuEclat(rows, 1)
+    miner._PAIR_BATCH_SIZE = 3
+    miner._INTERSECTION_BATCH_BYTES = 12
+    miner.mine()
+    assert len(miner.getPatterns()) == 255
+    assert "0\t1\t2\t3\t4\t5\t6\t7" in miner.getPatterns()
+
+
+def test_repeated_mining_is_identical():
+    import cupami_b200
+
+    miner = cupami_b200.cuEclat([[1, 2], [2, 3], [1, 2, 3]], 1)
+    miner.mine()
+    first = miner.getPatterns()
+    miner.mine()
+    assert miner.getPatterns() == first
+    assert miner.getRuntime() >= 0
+
+
+def _oracle_check(oracle_lib, csr, minsup, algo="eclat"):
+    import cupami_b200
+
+    labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, minsup, algo)
+    want = oracle_lib.to_dict(labels, arrays)
+    cls = cupami_b200.cuEclat if algo == "eclat" else cupami_b200.cuApriori
+    miner = cls(csr, minsup)
+    miner.mine()
+    got = miner.getPatterns()
+    assert list(got.items()) == list(want.items())
+    return miner
+
+
+@pytest.mark.parametrize("name", ["uniform-10k", "planted-100k", "dense-fixed-64k", "dense-bernoulli-64k"])
+def test_workloads_match_oracle(oracle_lib, name):
+    from cupami_b200 import datasets
+
+    csr, minsup = datasets.workload(name)
+    miner = _oracle_check(oracle_lib, csr, minsup, "eclat")
+    if name == "dense-fixed-64k":
+        assert miner.getPatterns() == {}
+    if name in ("uniform-10k", "planted-100k"):
+        _oracle_check(oracle_lib, csr, minsup, "apriori")
+
+
+def test_batched_databases_match_oracle(oracle_lib):
+    from cupami_b200 import datasets
+
+    for csr in datasets.batched_zipf(limit=6):
+        _oracle_check(oracle_lib, csr, 0.01, "eclat")
+
+
+@pytest.mark.parametrize("count", [0, 1, 31, 32, 33, 63, 64, 65, 127, 128, 129, 1000])
+def test_word_boundaries_dense(oracle_lib, count):
+    from cupami_b200 import TransactionCSR
+
+    rng = np.random.default_rng(count)
+    rows = [[int(i) for i in np.nonzero(rng.random(10) < 0.6)[0]] for _ in range(count)]
+    csr = TransactionCSR.from_rows(rows, universe=10)
+    _oracle_check(oracle_lib, csr, max(1, count // 6), "eclat")
+    _oracle_check(oracle_lib, csr, max(1, count // 6), "apriori")
