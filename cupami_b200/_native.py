@@ -89,6 +89,7 @@ _SIGNATURES = {
     "cpm_result_copy": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P]),
     "cpm_result_tree": (ctypes.c_int, [_P, _P, _P, _P]),
     "cpm_result_stats": (ctypes.c_int, [_P, ctypes.POINTER(Stats)]),
+    "cpm_result_from_tree": (ctypes.c_int, [_P, _P, _P, _U64, ctypes.POINTER(_P)]),
     "cpm_result_free": (None, [_P]),
     "cpm_build_bitsets": (ctypes.c_int, [_P, _P, _P, _U64, _U64, ctypes.c_uint32, _P]),
     "cpm_count_supports": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, _P]),
@@ -269,3 +270,19 @@ class Result:
 
     def __len__(self):
         return int(self.supports.size)
+
+    @classmethod
+    def from_tree(cls, parent, item, support, order):
+        """Order a host pattern tree (no device work)."""
+        parent = np.ascontiguousarray(parent, dtype=np.int64)
+        item = np.ascontiguousarray(item, dtype=np.uint32)
+        support = np.ascontiguousarray(support, dtype=np.uint64)
+        handle = _P()
+        code = library().cpm_result_from_tree(_ptr(parent), _ptr(item), _ptr(support), parent.size,
+                                              ctypes.byref(handle))
+        if code != CPM_OK:
+            raise NativeError(code, "invalid pattern tree")
+        try:
+            return cls.collect(handle, order)
+        finally:
+            library().cpm_result_free(handle)

@@ -874,17 +874,15 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
         depth[k] = p == 0xffffffffu ? 1 : depth[p] + 1;
         start[k + 1] = start[k] + depth[k];
     }
+    // Parents precede children, so a parent's list is already sorted when a
+    // child copies it; the child's own item is then moved into place.
     std::vector<uint32_t> flat(start[n]);
     for (uint64_t k = 0; k < n; ++k) {
-        uint32_t *dst = flat.data() + start[k];
-        const uint32_t p = res->parent[k];
-        if (p != 0xffffffffu) memcpy(dst, flat.data() + start[p], (depth[k] - 1) * 4);
-        dst[depth[k] - 1] = res->item[k];
-    }
-    for (uint64_t k = 0; k < n; ++k) {
         uint32_t *a = flat.data() + start[k];
-        // parent part is sorted already; insert the last item in place
-        uint32_t d = depth[k];
+        const uint32_t p = res->parent[k];
+        const uint32_t d = depth[k];
+        if (p != 0xffffffffu) memcpy(a, flat.data() + start[p], (d - 1) * 4);
+        a[d - 1] = res->item[k];
         for (uint32_t i = d - 1; i > 0 && a[i] < a[i - 1]; --i) std::swap(a[i], a[i - 1]);
     }
     std::vector<uint64_t> idx(n);
@@ -921,6 +919,27 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
         offsets[r + 1] = pos;
         supports[r] = res->support[k];
     }
+    return CPM_OK;
+}
+
+extern "C" int cpm_result_from_tree(const int64_t *parent, const uint32_t *item, const uint64_t *support,
+                                    uint64_t n, cpm_result **out) {
+    if (!out || (n && (!parent || !item || !support))) return CPM_EINVAL;
+    *out = nullptr;
+    cpm_result *res = new cpm_result();
+    res->parent.resize(n);
+    res->item.assign(item, item + n);
+    res->support.resize(n);
+    for (uint64_t k = 0; k < n; ++k) {
+        if (parent[k] >= (int64_t)k || parent[k] < -1 || support[k] > 0xffffffffull) {
+            delete res;
+            return CPM_EINVAL;
+        }
+        res->parent[k] = parent[k] < 0 ? 0xffffffffu : (uint32_t)parent[k];
+        res->support[k] = (uint32_t)support[k];
+    }
+    res->stats.n_patterns = n;
+    *out = res;
     return CPM_OK;
 }
 

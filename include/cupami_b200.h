@@ -137,6 +137,11 @@ int  cpm_result_copy(const cpm_result *res, int order, uint64_t *offsets,
 int  cpm_result_tree(const cpm_result *res, int64_t *parent, uint32_t *item,
                      uint64_t *support);
 int  cpm_result_stats(const cpm_result *res, cpm_stats *stats);
+/* Builds a result from a pattern tree held in host memory (parent[k] < k or
+ * -1).  No device work: lets callers and tests reorder patterns with
+ * cpm_result_copy without a GPU. */
+int  cpm_result_from_tree(const int64_t *parent, const uint32_t *item, const uint64_t *support,
+                          uint64_t n, cpm_result **out);
 void cpm_result_free(cpm_result *res);
 
 /* ---- reference kernel-module API (cupami/frequentPattern/_bitsets.py) ------- */
