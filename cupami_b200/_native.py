@@ -95,6 +95,8 @@ _SIGNATURES = {
     "cpm_count_supports": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, _P]),
     "cpm_intersect_extensions": (ctypes.c_int, [_P, _P, _P, _U64, _U64, _P, _P]),
     "cpm_synchronize": (ctypes.c_int, [_P]),
+    "cpm_mine_eclat_noalloc": (ctypes.c_int, [_P, _P, _U64, ctypes.c_uint32, _U64, ctypes.c_int64,
+                                              _P, _P, _P, _U64, ctypes.POINTER(_U64)]),
 }
 
 _lib = None

@@ -21,6 +21,7 @@
 #include <vector>
 #include <chrono>
 #include <cstdlib>
+#include <mutex>
 
 using namespace cpm;
 
@@ -990,5 +991,235 @@ extern "C" int cpm_intersect_extensions(cpm_ctx *ctx, const uint32_t *d_prefix, 
     k_ref_intersect<<<(unsigned)((n_extensions * 32 + 255) / 256), 256, 0, ctx->stream>>>(
         d_prefix, d_extensions, words32, n_extensions, d_out, reinterpret_cast<unsigned long long *>(d_supports));
     CK(cudaGetLastError());
+    return CPM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Eclat with no device allocation
+// ---------------------------------------------------------------------------
+// Some callers cannot allocate device memory when they mine: their device
+// memory belongs to another runtime's pool, or their process forbids
+// allocation after start-up.  cpm_mine_eclat_noalloc takes the tidsets and the
+// output arrays from the caller and keeps every intermediate buffer (frequent
+// list, pair Gram, class tables, work queue, child tidsets) in the one static
+// device array below, CPM_NOALLOC_SCRATCH_BYTES long, which every GPU that
+// loads this library holds until the process exits.
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[CPM_NOALLOC_SCRATCH_BYTES];
+
+// Device address of g_noalloc_scratch per device.  In host code the symbol
+// name is only a host-side stand-in, so the address must come from
+// cudaGetSymbolAddress with the device current.  Resolved on the first call
+// for each device, which is why that first call should come before any
+// stream capture.
+static std::mutex g_noalloc_mutex;
+static unsigned char *g_noalloc_addr[256] = {};
+
+static int noalloc_scratch(cpm_ctx *ctx, unsigned char **out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (ctx->device < 0 || ctx->device >= 256) return set_err(ctx, CPM_EINVAL, "device index out of range");
+    if (!g_noalloc_addr[ctx->device]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            cudaGetLastError();
+            return set_err(ctx, CPM_ECUDA, "cudaGetSymbolAddress of the static scratch failed: %s",
+                           cudaGetErrorString(e));
+        }
+        g_noalloc_addr[ctx->device] = static_cast<unsigned char *>(p);
+    }
+    *out = g_noalloc_addr[ctx->device];
+    return CPM_OK;
+}
+
+// 256-byte aligned pieces of the static scratch.
+struct NoallocCarve {
+    unsigned char *base;
+    uint64_t used;
+    uint64_t left() const {
+        const uint64_t off = (used + 255) & ~255ull;
+        return off >= CPM_NOALLOC_SCRATCH_BYTES ? 0 : CPM_NOALLOC_SCRATCH_BYTES - off;
+    }
+    template <class T>
+    T *take(uint64_t count) {
+        const uint64_t off = (used + 255) & ~255ull;
+        const uint64_t bytes = std::max<uint64_t>(1, count) * sizeof(T);
+        if (off > CPM_NOALLOC_SCRATCH_BYTES || bytes > CPM_NOALLOC_SCRATCH_BYTES - off) return nullptr;
+        used = off + bytes;
+        return reinterpret_cast<T *>(base + off);
+    }
+};
+
+extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint64_t stride, uint32_t n_items,
+                                      uint64_t n_transactions, int64_t min_sup, uint32_t *d_parent,
+                                      uint32_t *d_item, uint32_t *d_support, uint64_t capacity,
+                                      uint64_t *n_patterns) {
+    if (!ctx || !n_patterns) return CPM_EINVAL;
+    *n_patterns = 0;
+    if ((n_items && !d_bits) || (capacity && (!d_parent || !d_item || !d_support)))
+        return set_err(ctx, CPM_EINVAL, "null input or output pointer");
+    if (stride < 2 || (stride & 1) || (reinterpret_cast<uintptr_t>(d_bits) & 15))
+        return set_err(ctx, CPM_EINVAL, "tidset rows need an even stride and a 16-byte aligned base");
+    if (n_transactions > stride * 64) return set_err(ctx, CPM_EINVAL, "stride too small for the transactions");
+    CK(cudaSetDevice(ctx->device));
+    unsigned char *base = nullptr;
+    CKR(noalloc_scratch(ctx, &base));
+    NoallocCarve carve{base, 0};
+    const long long ms = (long long)std::max<int64_t>(std::min<int64_t>(min_sup, (int64_t)1 << 40), -1);
+    const unsigned long long limit_mib = CPM_NOALLOC_SCRATCH_BYTES >> 20;
+    uint32_t *d_item_sup = carve.take<uint32_t>(n_items);
+    uint32_t *d_freq = carve.take<uint32_t>(n_items);
+    uint32_t *d_count = carve.take<uint32_t>(1);
+    DeepState *d_st = carve.take<DeepState>(1);
+    if (!d_item_sup || !d_freq || !d_count || !d_st)
+        return set_err(ctx, CPM_EINVAL, "%u items exceed the %llu MiB static scratch", n_items, limit_mib);
+    // Singletons.
+    if (n_items) {
+        k_item_support<<<(unsigned)(((uint64_t)n_items * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+            d_bits, stride, n_items, d_item_sup);
+        CK(cudaGetLastError());
+    }
+    CK(cudaMemsetAsync(d_count, 0, 4, ctx->stream));
+    if (n_items) {
+        k_compact_frequent<<<1, 1024, 0, ctx->stream>>>(d_item_sup, n_items, ms, d_freq, d_count);
+        CK(cudaGetLastError());
+    }
+    uint32_t F = 0;
+    CK(cudaMemcpyAsync(&F, d_count, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (F > capacity)
+        return set_err(ctx, CPM_EOVERFLOW, "output capacity %llu is below the %u frequent items",
+                       (unsigned long long)capacity, F);
+    if (F) {
+        k_emit_singletons<<<(F + 255) / 256, 256, 0, ctx->stream>>>(d_freq, F, d_item_sup, d_parent, d_item,
+                                                                    d_support);
+        CK(cudaGetLastError());
+    }
+    if (F < 2) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        *n_patterns = F;
+        return CPM_OK;
+    }
+    // Pair level on the CUDA cores (the same Gram and threshold as cpm_mine).
+    uint32_t *d_C = carve.take<uint32_t>((uint64_t)F * F);
+    uint32_t *d_cnt = carve.take<uint32_t>(F);
+    uint64_t *d_off = carve.take<uint64_t>((uint64_t)F + 1);
+    if (!d_C || !d_cnt || !d_off)
+        return set_err(ctx, CPM_EINVAL, "%u frequent items need a %llu-byte pair matrix, beyond the %llu MiB static "
+                       "scratch", F, (unsigned long long)F * F * 4, limit_mib);
+    CK(cudaMemsetAsync(d_C, 0, (size_t)F * F * 4, ctx->stream));
+    {
+        const uint32_t nt = (F + 63) / 64;
+        const uint32_t tiles = nt * (nt + 1) / 2;
+        uint64_t ksplit = std::max<uint64_t>(1, (uint64_t)ctx->sms * 4 / tiles);
+        ksplit = std::min<uint64_t>(ksplit, std::max<uint64_t>(1, stride / 64));
+        const uint64_t k_chunk = ((stride + ksplit - 1) / ksplit + 15) / 16 * 16;
+        ksplit = (stride + k_chunk - 1) / k_chunk;
+        k_gram_simt<<<dim3(tiles, (unsigned)ksplit), 256, 0, ctx->stream>>>(d_bits, stride, d_freq, F, nt, k_chunk,
+                                                                              d_C);
+        CK(cudaGetLastError());
+    }
+    k_pair_count<<<(unsigned)(((uint64_t)F * 32 + 255) / 256), 256, 0, ctx->stream>>>(d_C, F, ms, d_cnt);
+    CK(cudaGetLastError());
+    std::vector<uint32_t> cnt(F);
+    std::vector<uint64_t> off(F + 1, 0);
+    CK(cudaMemcpyAsync(cnt.data(), d_cnt, (size_t)F * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (uint32_t i = 0; i < F; ++i) off[i + 1] = off[i] + cnt[i];
+    const uint64_t P2 = off[F];
+    if (F + P2 > capacity)
+        return set_err(ctx, CPM_EOVERFLOW, "output capacity %llu is below the %llu singletons and pairs",
+                       (unsigned long long)capacity, (unsigned long long)(F + P2));
+    std::vector<uint32_t> roots;
+    for (uint32_t i = 0; i < F; ++i)
+        if (cnt[i] >= 2) roots.push_back(i);
+    std::stable_sort(roots.begin(), roots.end(), [&](uint32_t a, uint32_t b) { return cnt[a] > cnt[b]; });
+    std::vector<unsigned long long> init;
+    for (size_t k = 0; k < roots.size(); ++k)
+        for (uint32_t p = 0; p + 1 < cnt[roots[k]]; ++p) init.push_back(((unsigned long long)k << 32) | p);
+    std::stable_sort(init.begin(), init.end(), [&](unsigned long long a, unsigned long long b) {
+        return cnt[roots[a >> 32]] - (uint32_t)a > cnt[roots[b >> 32]] - (uint32_t)b;
+    });
+    // Deep-level tables from what is left: the queue and frame tables are
+    // bounded by the output capacity, members and child tidsets share the rest.
+    const uint64_t rest = carve.left();
+    const uint64_t frames_cap = std::min<uint64_t>(capacity + roots.size(), rest / 16 / sizeof(DFrame)) + 1;
+    const uint64_t queue_cap = std::min<uint64_t>(capacity + init.size(), rest / 16 / 8) + 1;
+    DFrame *d_frames = carve.take<DFrame>(frames_cap);
+    unsigned long long *d_queue = carve.take<unsigned long long>(queue_cap);
+    unsigned long long *d_root_cost = carve.take<unsigned long long>(roots.size());
+    const uint64_t members_cap = std::max<uint64_t>(P2, carve.left() / 4 / 16);
+    uint32_t *d_mem_pat = carve.take<uint32_t>(members_cap);
+    uint32_t *d_mem_item = carve.take<uint32_t>(members_cap);
+    const uint64_t **d_mem_bits = carve.take<const uint64_t *>(members_cap);
+    const uint64_t arena_slots = d_mem_bits ? carve.left() / (stride * 8) : 0;
+    uint64_t *d_arena = arena_slots ? carve.take<uint64_t>(arena_slots * stride) : nullptr;
+    if (!d_frames || !d_queue || !d_root_cost || !d_mem_pat || !d_mem_item || !d_mem_bits || !d_arena ||
+        init.size() > queue_cap || roots.size() > frames_cap || arena_slots < 64)
+        return set_err(ctx, CPM_EINVAL, "%llu-word tidsets with %llu pairs exceed the %llu MiB static scratch",
+                       (unsigned long long)stride, (unsigned long long)P2, limit_mib);
+    CK(cudaMemcpyAsync(d_off, off.data(), (F + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    k_pair_emit<<<(unsigned)(((uint64_t)F * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+        d_C, F, ms, d_freq, d_off, d_bits, stride, d_parent, d_item, d_support, d_mem_pat, d_mem_item, d_mem_bits);
+    CK(cudaGetLastError());
+    if (roots.empty()) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        *n_patterns = F + P2;
+        return CPM_OK;
+    }
+    std::vector<uint32_t> hfreq(F);
+    CK(cudaMemcpyAsync(hfreq.data(), d_freq, (size_t)F * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<DFrame> frames(roots.size());
+    for (size_t k = 0; k < roots.size(); ++k) {
+        frames[k].mask = d_bits + (uint64_t)hfreq[roots[k]] * stride;
+        frames[k].mem_off = off[roots[k]];
+        frames[k].m = cnt[roots[k]];
+        frames[k].root = (uint32_t)k;
+    }
+    // Every call shares the scratch: reset what the kernel expects cleared.
+    CK(cudaMemcpyAsync(d_frames, frames.data(), frames.size() * sizeof(DFrame), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(d_queue, 0xff, queue_cap * 8, ctx->stream));
+    CK(cudaMemcpyAsync(d_queue, init.data(), init.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(d_root_cost, 0, std::max<size_t>(1, roots.size()) * 8, ctx->stream));
+    DeepState hs{};
+    hs.q_tail = init.size();
+    hs.pending = init.size();
+    hs.n_patterns = F + P2;
+    hs.n_frames = roots.size();
+    hs.n_members = P2;
+    CK(cudaMemcpyAsync(d_st, &hs, sizeof hs, cudaMemcpyHostToDevice, ctx->stream));
+    DeepParams P;
+    P.frames = d_frames; P.frames_cap = frames_cap;
+    P.mem_pat = d_mem_pat; P.mem_item = d_mem_item; P.mem_bits = d_mem_bits; P.members_cap = members_cap;
+    P.queue = d_queue; P.queue_cap = queue_cap;
+    P.arena = d_arena; P.arena_slots = arena_slots;
+    P.pat_parent = d_parent; P.pat_item = d_item; P.pat_sup = d_support; P.pat_cap = capacity;
+    P.root_cost = d_root_cost; P.st = d_st; P.stride = stride; P.minsup = ms; P.spin_limit = 1ull << 26;
+    // Each warp keeps one scratch tidset: leave at least half the arena to children.
+    const size_t prefix_bytes = stride * 8;
+    const bool smem_prefix = prefix_bytes <= 200 * 1024;
+    int per_sm = 1;
+    if (smem_prefix) {
+        CK(cudaFuncSetAttribute(k_deep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prefix_bytes));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_deep<true>, 256, prefix_bytes));
+    } else {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_deep<false>, 256, 0));
+    }
+    const uint64_t grid = std::max<uint64_t>(
+        1, std::min<uint64_t>((uint64_t)ctx->sms * std::max(1, per_sm), arena_slots / 16));
+    if (smem_prefix) k_deep<true><<<(unsigned)grid, 256, prefix_bytes, ctx->stream>>>(P);
+    else k_deep<false><<<(unsigned)grid, 256, 0, ctx->stream>>>(P);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(&hs, d_st, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (hs.error & DEEP_ERR_SPIN) return set_err(ctx, CPM_ETIMEOUT, "deep-level kernel wait ran out of spins");
+    if (hs.error & DEEP_ERR_PATTERNS)
+        return set_err(ctx, CPM_EOVERFLOW, "output capacity %llu is below the number of patterns",
+                       (unsigned long long)capacity);
+    if (hs.error)
+        return set_err(ctx, CPM_EOVERFLOW, "the search outgrew the %llu MiB static scratch (error 0x%x)", limit_mib,
+                       hs.error);
+    *n_patterns = hs.n_patterns;
     return CPM_OK;
 }

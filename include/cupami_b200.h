@@ -163,6 +163,35 @@ int cpm_intersect_extensions(cpm_ctx *ctx, const uint32_t *d_prefix,
 /* Waits for the context's stream. */
 int cpm_synchronize(cpm_ctx *ctx);
 
+/* ---- Eclat without device allocation ---------------------------------------
+ * No counterpart in the reference: cuPAMI allocates through CuPy's pool on
+ * every call.  This entry point is for callers that cannot allocate device
+ * memory while they mine -- their device memory is owned by another runtime's
+ * pool, or allocation is forbidden once they have started.  The caller passes
+ * the tidsets (d_bits: n_items rows of `stride` 64-bit words, stride even,
+ * base 16-byte aligned, bit r of row c set when transaction r holds column c,
+ * bits past n_transactions zero) and the outputs (pattern tree in device
+ * memory: pattern k = pattern d_parent[k] (0xffffffff: none) plus column
+ * d_item[k], support d_support[k], at most `capacity` patterns; the count goes
+ * to *n_patterns).  The patterns and supports are those cpm_mine(CPM_ECLAT)
+ * finds on the same tidsets; cpm_result_from_tree + cpm_result_copy order
+ * them as the reference does.
+ *
+ * No cudaMalloc, cudaFree or other allocating call is made: every
+ * intermediate buffer lives in one static device array of
+ * CPM_NOALLOC_SCRATCH_BYTES, held by every GPU that loads the library until
+ * the process exits.  Inputs needing more (a pair matrix or child tidsets that
+ * do not fit) are rejected with CPM_EINVAL or CPM_EOVERFLOW and a message in
+ * cpm_last_error.  The first call on each device looks up the array's device
+ * address, so make that first call before any stream capture.  All calls share
+ * the array, so calls that overlap on the GPU (two contexts, two threads) race
+ * and must be serialised by the caller. */
+#define CPM_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint64_t stride, uint32_t n_items,
+                           uint64_t n_transactions, int64_t min_sup, uint32_t *d_parent,
+                           uint32_t *d_item, uint32_t *d_support, uint64_t capacity,
+                           uint64_t *n_patterns);
+
 #ifdef __cplusplus
 }
 #endif
