@@ -10,6 +10,7 @@
 #include "k_pairs.cuh"
 #include "k_gram_tc.cuh"
 #include "k_deep.cuh"
+#include "k_apriori.cuh"
 
 #include <algorithm>
 #include <cstdarg>
@@ -35,7 +36,11 @@ struct cpm_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[8] = {};
     std::string err;
-    bool tc_ok = true;  // tensor-core Gram usable on this device
+    bool tc_ok = true;        // tensor-core Gram usable on this device
+    size_t mem_free = 0;      // free device memory when the context was made
+    int deep_occ_smem = -1;   // k_deep<true> CTAs per SM, for deep_occ_bytes of prefix
+    size_t deep_occ_bytes = 0;
+    int deep_occ_global = -1; // k_deep<false> CTAs per SM
 };
 
 struct cpm_db {
@@ -159,6 +164,12 @@ extern "C" int cpm_init(int device, cpm_ctx **out) {
         return CPM_ECUDA;
     }
     ctx->tc_ok = (major == 10 && minor == 0);
+    size_t total = 0;
+    cudaMemGetInfo(&ctx->mem_free, &total);
+    // The deep kernel stages prefixes of up to 200 KB in shared memory.
+    cudaFuncSetAttribute(k_deep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
+    cudaGetLastError();
     *out = ctx;
     return CPM_OK;
 }
@@ -413,11 +424,42 @@ static int pair_gram(cpm_ctx *ctx, cpm_db *db, const uint32_t *d_freq, uint32_t 
                      DevScope &ds, uint32_t **d_C, cpm_stats &st) {
     CKR(ds.alloc(d_C, (size_t)F * F));
     const bool use_tc = o.pair_engine == 1 || (o.pair_engine == 0 && ctx->tc_ok && gram_tc_worthwhile(F, db->n_tx));
+    CK(cudaEventRecord(ctx->ev[5], ctx->stream));
     if (use_tc) {
-        CKR(gram_tc_launch(ctx->stream, ctx->sms, db->d_bits, db->stride, d_freq, F, db->n_tx, *d_C, &st.pair_ops,
-                           &st.kernel_launches)
-                ? set_err(ctx, CPM_ECUDA, "tensor-core Gram launch failed: %s", cudaGetErrorString(cudaGetLastError()))
-                : CPM_OK);
+        if (!ctx->tc_ok) return set_err(ctx, CPM_EINVAL, "the tensor-core Gram needs an sm_100 device");
+        CK(cudaMemsetAsync(*d_C, 0, (size_t)F * F * 4, ctx->stream));
+        // Upper-triangle tiles: A block ti (128 rows) x B block tj (256 columns)
+        // whenever some column of the block lies right of some row.
+        std::vector<GramTile> tiles;
+        const uint32_t nti = (F + tc::BM - 1) / tc::BM, ntj = (F + tc::BN - 1) / tc::BN;
+        for (uint32_t ti = 0; ti < nti; ++ti)
+            for (uint32_t tj = 0; tj < ntj; ++tj)
+                if ((uint64_t)tj * tc::BN + tc::BN - 1 > (uint64_t)ti * tc::BM) tiles.push_back({ti, tj});
+        // K split (in pairs of words, one stage each) so the units cover the GPU.
+        const uint64_t kstages = db->stride / 2;
+        uint64_t ksplit = std::max<uint64_t>(1, ((uint64_t)ctx->sms * 2 + tiles.size() - 1) / tiles.size());
+        ksplit = std::min<uint64_t>(ksplit, std::max<uint64_t>(1, kstages / 8));
+        const uint64_t stages_per = (kstages + ksplit - 1) / ksplit;
+        ksplit = (kstages + stages_per - 1) / stages_per;
+        GramTile *d_tiles = nullptr;
+        unsigned int *d_err = nullptr;
+        CKR(ds.alloc(&d_tiles, tiles.size()));
+        CKR(ds.alloc(&d_err, 1));
+        CK(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(GramTile), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(cudaMemsetAsync(d_err, 0, 4, ctx->stream));
+        const uint64_t units = tiles.size() * ksplit;
+        k_gram_tc<<<(unsigned)units, tc::THREADS, tc::SMEM_BYTES, ctx->stream>>>(
+            db->d_bits, db->stride, d_freq, F, d_tiles, (uint32_t)tiles.size(), stages_per * 2, *d_C, d_err);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ctx->ev[6], ctx->stream));
+        unsigned int herr = 0;
+        CK(cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (herr) return set_err(ctx, CPM_ETIMEOUT, "tensor-core Gram pipeline wait ran out");
+        st.kernel_launches += 1;
+        // Work issued to the tensor cores: every tile is a full 128x256 block.
+        st.pair_ops += 2ull * (uint64_t)tc::BM * tc::BN * (kstages * 128) * tiles.size();
         return CPM_OK;
     }
     CK(cudaMemsetAsync(*d_C, 0, (size_t)F * F * 4, ctx->stream));
@@ -431,6 +473,7 @@ static int pair_gram(cpm_ctx *ctx, cpm_db *db, const uint32_t *d_freq, uint32_t 
     dim3 grid(tiles, (unsigned)ksplit);
     k_gram_simt<<<grid, 256, 0, ctx->stream>>>(db->d_bits, db->stride, d_freq, F, nt, k_chunk, *d_C);
     CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[6], ctx->stream));
     st.kernel_launches += 1;
     st.pair_ops += 2ull * db->n_tx * F * (uint64_t)F;
     return CPM_OK;
@@ -446,6 +489,10 @@ struct DeepBuffers {
     unsigned long long *root_cost = nullptr;
     DeepState *st = nullptr;
     uint64_t frames_cap = 0, members_cap = 0, queue_cap = 0, arena_slots = 0, pat_cap = 0;
+    cpm_ctx *owner = nullptr;  // released on every exit path
+    ~DeepBuffers() {
+        if (owner) release(owner);
+    }
     void release(cpm_ctx *ctx) {
         dfree(ctx, frames); dfree(ctx, mem_pat); dfree(ctx, mem_item); dfree(ctx, mem_bits);
         dfree(ctx, queue); dfree(ctx, arena); dfree(ctx, pat_parent); dfree(ctx, pat_item);
@@ -531,15 +578,14 @@ static int mine_eclat(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o,
     }
     const uint64_t stride = db->stride;
     DeepBuffers b;
+    b.owner = ctx;
     // First guesses scale with the pair level; a database that was mined
     // before starts from what it needed then.
     uint64_t frames_cap = std::max<uint64_t>({1024, roots.size() * 8 + P2 * 2, db->hint_frames});
     uint64_t members_cap = std::max<uint64_t>({4096, P2 * 16, db->hint_members});
     uint64_t queue_cap = std::max<uint64_t>({4096, init.size() * 8 + P2 * 4, db->hint_queue});
     uint64_t pat_cap = std::max<uint64_t>({4096, (F + P2) * 16, db->hint_patterns});
-    size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
-    const uint64_t arena_budget = (uint64_t)(free_b * 0.6) / (stride * 8);
+    const uint64_t arena_budget = (uint64_t)(ctx->mem_free * 0.6) / (stride * 8);
     uint64_t arena_slots = o.arena_bytes ? o.arena_bytes / (stride * 8)
                                          : std::min<uint64_t>(arena_budget, std::max<uint64_t>(
                                                {(uint64_t)ctx->sms * 8 * 4 + 1024, P2 * 8, db->hint_arena}));
@@ -548,16 +594,16 @@ static int mine_eclat(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o,
     // Shared-memory prefix when the tidset fits next to the static buffers.
     const size_t prefix_bytes = stride * 8;
     const bool smem_prefix = prefix_bytes <= 200 * 1024;
-    int cta_per_sm = 1;
-    if (smem_prefix) {
-        CK(cudaFuncSetAttribute(k_deep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prefix_bytes));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cta_per_sm, k_deep<true>, 256, prefix_bytes));
-    } else {
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cta_per_sm, k_deep<false>, 256, 0));
+    if (smem_prefix && (ctx->deep_occ_smem < 0 || ctx->deep_occ_bytes != prefix_bytes)) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_smem, k_deep<true>, 256, prefix_bytes));
+        ctx->deep_occ_bytes = prefix_bytes;
+    } else if (!smem_prefix && ctx->deep_occ_global < 0) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_global, k_deep<false>, 256, 0));
     }
-    cta_per_sm = std::max(1, cta_per_sm);
+    // Up to four CTAs per SM keep enough loads in flight; more only add
+    // contention on the queue head.
+    const int cta_per_sm = std::min(4, std::max(1, smem_prefix ? ctx->deep_occ_smem : ctx->deep_occ_global));
     const unsigned grid = (unsigned)(ctx->sms * cta_per_sm);
-    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
     DeepState hs{};
     for (int attempt = 0;; ++attempt) {
         CKR(grow(ctx, b, frames_cap, members_cap, queue_cap, arena_slots, pat_cap + F + P2, stride, roots.size()));
@@ -606,9 +652,11 @@ static int mine_eclat(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o,
         P.arena = b.arena; P.arena_slots = b.arena_slots;
         P.pat_parent = b.pat_parent; P.pat_item = b.pat_item; P.pat_sup = b.pat_sup; P.pat_cap = b.pat_cap;
         P.root_cost = b.root_cost; P.st = b.st; P.stride = stride; P.minsup = ms; P.spin_limit = spin;
+        CK(cudaEventRecord(ctx->ev[2], ctx->stream));
         if (smem_prefix) k_deep<true><<<grid, 256, prefix_bytes, ctx->stream>>>(P);
         else k_deep<false><<<grid, 256, 0, ctx->stream>>>(P);
         CK(cudaGetLastError());
+        CK(cudaEventRecord(ctx->ev[3], ctx->stream));
         st.kernel_launches++;
         CK(cudaMemcpyAsync(&hs, b.st, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
@@ -650,7 +698,6 @@ static int mine_eclat(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o,
     db->hint_queue = std::max<uint64_t>(db->hint_queue, hs.q_tail + hs.q_tail / 4 + 64);
     db->hint_patterns = std::max<uint64_t>(db->hint_patterns, hs.n_patterns + hs.n_patterns / 4 + 64);
     db->hint_arena = std::max<uint64_t>(db->hint_arena, hs.arena_next + hs.arena_next / 4 + 64);
-    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
     const uint64_t n = hs.n_patterns;
     res->parent.resize(n);
     res->item.resize(n);
@@ -668,16 +715,42 @@ static int mine_eclat(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o,
     st.work_items = hs.work_items;
     st.intersections = hs.intersections;
     st.bytes_alg = hs.bytes_alg;
-    st.ms_pairs = elapsed_ms(ctx, 1, 2);
-    st.ms_deep = elapsed_ms(ctx, 2, 3);
+    st.ms_pairs = F >= 2 ? elapsed_ms(ctx, 5, 6) : 0.0;
+    st.ms_deep = roots.empty() ? 0.0 : elapsed_ms(ctx, 2, 3);
     st.ms_total = elapsed_ms(ctx, 0, 4);
     st.deep_gbs = st.ms_deep > 0 ? st.bytes_alg / (st.ms_deep * 1e6) : 0.0;
     st.pair_tops = st.ms_pairs > 0 ? st.pair_ops / (st.ms_pairs * 1e9) : 0.0;
     return CPM_OK;
 }
 
-// Apriori (cuApriori.py:501-535): level 2 from the pair Gram, then prefix-join
-// candidates with full subset pruning, each counted by complete intersection.
+// Apriori (cuApriori.py:501-535): level 2 from the pair Gram, then each
+// level joined, pruned and counted on the device (k_apriori.cuh).  Two small
+// counts come back per level (candidates, survivors) to size the next.
+struct PatternArrays {
+    uint32_t *parent = nullptr, *item = nullptr, *sup = nullptr;
+    uint64_t cap = 0;
+};
+
+static int patterns_reserve(cpm_ctx *ctx, PatternArrays &pa, uint64_t used, uint64_t need) {
+    if (need <= pa.cap) return CPM_OK;
+    uint64_t cap = std::max<uint64_t>(need, pa.cap * 2);
+    PatternArrays nw;
+    nw.cap = cap;
+    CKR(dalloc(ctx, &nw.parent, cap));
+    CKR(dalloc(ctx, &nw.item, cap));
+    CKR(dalloc(ctx, &nw.sup, cap));
+    if (used) {
+        CK(cudaMemcpyAsync(nw.parent, pa.parent, used * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(nw.item, pa.item, used * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(nw.sup, pa.sup, used * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    dfree(ctx, pa.parent);
+    dfree(ctx, pa.item);
+    dfree(ctx, pa.sup);
+    pa = nw;
+    return CPM_OK;
+}
+
 static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o, cpm_result *res) {
     cpm_stats &st = res->stats;
     DevScope ds(ctx);
@@ -686,121 +759,126 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
     uint32_t F = 0;
     CKR(mine_singletons(ctx, db, ms, ds, &d_freq, F, st.kernel_launches));
     st.n_frequent_items = F;
-    std::vector<uint32_t> freq(F);
-    std::vector<uint32_t> sup1(db->n_items);
-    if (F) CK(cudaMemcpyAsync(freq.data(), d_freq, (size_t)F * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    if (db->n_items) CK(cudaMemcpyAsync(sup1.data(), db->d_support, (size_t)db->n_items * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    for (uint32_t i = 0; i < F; ++i) {
-        res->parent.push_back(0xffffffffu);
-        res->item.push_back(freq[i]);
-        res->support.push_back(sup1[freq[i]]);
-    }
-    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    // Level 2: the pair Gram over the frequent items.
-    std::vector<uint32_t> level;  // flattened patterns of the current level (frequent indices)
-    std::vector<uint32_t> level_id;
-    uint32_t k = 1;
-    for (uint32_t i = 0; i < F; ++i) { level.push_back(i); level_id.push_back(i); }
-    if (F >= 2) {
-        uint32_t *d_C = nullptr;
-        CKR(pair_gram(ctx, db, d_freq, F, o, ds, &d_C, st));
-        std::vector<uint32_t> C((size_t)F * F);
-        CK(cudaMemcpyAsync(C.data(), d_C, C.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        std::vector<uint32_t> nl, nid;
-        for (uint32_t i = 0; i < F; ++i)
-            for (uint32_t j = i + 1; j < F; ++j)
-                if ((long long)C[(size_t)i * F + j] >= ms) {
-                    nl.push_back(i); nl.push_back(j);
-                    nid.push_back((uint32_t)res->parent.size());
-                    res->parent.push_back(i);
-                    res->item.push_back(freq[j]);
-                    res->support.push_back(C[(size_t)i * F + j]);
-                }
-        st.n_frequent_pairs = nid.size();
-        level.swap(nl);
-        level_id.swap(nid);
-        k = 2;
-    } else {
-        level.clear();
-        level_id.clear();
-    }
-    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-    // Frequent index -> column for candidate rows.
-    uint32_t *d_cand = nullptr, *d_sup = nullptr;
-    size_t cand_cap = 0;
-    while (!level.empty()) {
-        const uint64_t n = level.size() / k;
-        // Hash set of the level for the subset test.
-        struct H {
-            size_t operator()(const std::string &s) const { return std::hash<std::string>()(s); }
-        };
-        std::unordered_set<std::string, H> seen;
-        seen.reserve(n * 2);
-        for (uint64_t a = 0; a < n; ++a) seen.insert(std::string((const char *)&level[a * k], k * 4));
-        std::vector<uint32_t> cand, cand_parent;
-        std::vector<uint32_t> sub(k);
-        for (uint64_t a = 0; a < n; ++a) {
-            const uint32_t *pa = &level[a * k];
-            for (uint64_t b2 = a + 1; b2 < n; ++b2) {
-                const uint32_t *pb = &level[b2 * k];
-                if (memcmp(pa, pb, (k - 1) * 4)) break;
-                // candidate = pa + pb[k-1]; all k-subsets must be frequent
-                bool ok = true;
-                for (uint32_t drop = 0; drop + 1 < k && ok; ++drop) {  // dropping the last two gives pa/pb
-                    uint32_t t = 0;
-                    for (uint32_t i = 0; i < k; ++i)
-                        if (i != drop) sub[t++] = pa[i];
-                    sub[t++] = pb[k - 1];
-                    ok = seen.count(std::string((const char *)sub.data(), k * 4)) > 0;
-                }
-                if (!ok) continue;
-                for (uint32_t i = 0; i < k; ++i) cand.push_back(pa[i]);
-                cand.push_back(pb[k - 1]);
-                cand_parent.push_back(level_id[a]);
-            }
-        }
-        const uint64_t nc = cand_parent.size();
-        if (!nc) break;
-        const uint32_t w = k + 1;
-        std::vector<uint32_t> rows(cand.size());
-        for (size_t i = 0; i < cand.size(); ++i) rows[i] = freq[cand[i]];
-        if (rows.size() > cand_cap) {
-            dfree(ctx, d_cand);
-            dfree(ctx, d_sup);
-            cand_cap = rows.size() * 2;
-            CKR(dalloc(ctx, &d_cand, cand_cap));
-            CKR(dalloc(ctx, &d_sup, cand_cap));
-        }
-        CK(cudaMemcpyAsync(d_cand, rows.data(), rows.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
-        k_count_kway<<<(unsigned)((nc * 32 + 255) / 256), 256, 0, ctx->stream>>>(db->d_bits, db->stride, d_cand, nc, w, d_sup);
+    PatternArrays pa;
+    struct Free {
+        cpm_ctx *c; PatternArrays *p;
+        ~Free() { dfree(c, p->parent); dfree(c, p->item); dfree(c, p->sup); }
+    } free_patterns{ctx, &pa};
+    uint64_t n_pat = 0;
+    CKR(patterns_reserve(ctx, pa, 0, std::max<uint64_t>(1024, (uint64_t)F * 4 + db->hint_patterns)));
+    if (F) {
+        k_emit_singletons<<<(F + 255) / 256, 256, 0, ctx->stream>>>(d_freq, F, db->d_support, pa.parent, pa.item,
+                                                                    pa.sup);
         CK(cudaGetLastError());
         st.kernel_launches++;
-        std::vector<uint32_t> sup(nc);
-        CK(cudaMemcpyAsync(sup.data(), d_sup, nc * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        st.intersections += nc * (w - 1);
-        st.bytes_alg += nc * w * db->stride * 8;
-        std::vector<uint32_t> nl, nid;
-        for (uint64_t c = 0; c < nc; ++c) {
-            if ((long long)sup[c] < ms) continue;
-            nl.insert(nl.end(), cand.begin() + c * w, cand.begin() + (c + 1) * w);
-            nid.push_back((uint32_t)res->parent.size());
-            res->parent.push_back(cand_parent[c]);
-            res->item.push_back(freq[cand[c * w + w - 1]]);
-            res->support.push_back(sup[c]);
-        }
-        level.swap(nl);
-        level_id.swap(nid);
-        k = w;
     }
-    dfree(ctx, d_cand);
-    dfree(ctx, d_sup);
+    n_pat = F;
+    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
+    CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+    uint64_t *d_total = nullptr;
+    CKR(ds.alloc(&d_total, 2));
+    if (F >= 2) {
+        uint32_t *d_C = nullptr, *d_cnt = nullptr;
+        uint64_t *d_off = nullptr;
+        CKR(pair_gram(ctx, db, d_freq, F, o, ds, &d_C, st));
+        CKR(ds.alloc(&d_cnt, F));
+        CKR(ds.alloc(&d_off, F + 1));
+        k_pair_count<<<(unsigned)(((uint64_t)F * 32 + 255) / 256), 256, 0, ctx->stream>>>(d_C, F, ms, d_cnt);
+        CK(cudaGetLastError());
+        k_scan_u32<<<1, 1024, 0, ctx->stream>>>(d_cnt, F, d_off, d_total);
+        CK(cudaGetLastError());
+        uint64_t P2 = 0;
+        CK(cudaMemcpyAsync(&P2, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        st.kernel_launches += 2;
+        st.n_frequent_pairs = P2;
+        CKR(patterns_reserve(ctx, pa, n_pat, n_pat + P2));
+        uint32_t *L = nullptr, *pid = nullptr;
+        CKR(dalloc(ctx, &L, 2 * P2));
+        CKR(dalloc(ctx, &pid, P2));
+        k_pairs_to_level<<<(unsigned)(((uint64_t)F * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+            d_C, F, ms, d_freq, d_off, n_pat, L, pid, pa.parent, pa.item, pa.sup);
+        CK(cudaGetLastError());
+        st.kernel_launches++;
+        n_pat += P2;
+        uint64_t n = P2;
+        uint32_t k = 2;
+        while (n >= 2) {
+            if (k + 1 > 64) {
+                dfree(ctx, L);
+                dfree(ctx, pid);
+                return set_err(ctx, CPM_EINVAL, "patterns longer than 64 items are not supported");
+            }
+            const uint32_t w = k + 1;
+            uint32_t *cnt = nullptr, *cand = nullptr, *left = nullptr, *sup = nullptr, *flag = nullptr;
+            uint64_t *off = nullptr, *pos = nullptr;
+            DevScope lvl(ctx);
+            CKR(lvl.alloc(&cnt, n));
+            CKR(lvl.alloc(&off, n));
+            const unsigned jb = (unsigned)((n + 127) / 128);
+            k_apriori_join<0><<<jb, 128, 0, ctx->stream>>>(L, n, k, cnt, nullptr, nullptr, nullptr);
+            CK(cudaGetLastError());
+            k_scan_u32<<<1, 1024, 0, ctx->stream>>>(cnt, n, off, d_total);
+            CK(cudaGetLastError());
+            uint64_t nc = 0;
+            CK(cudaMemcpyAsync(&nc, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            st.kernel_launches += 2;
+            if (!nc) break;
+            CKR(lvl.alloc(&cand, nc * w));
+            CKR(lvl.alloc(&left, nc));
+            CKR(lvl.alloc(&sup, nc));
+            CKR(lvl.alloc(&flag, nc));
+            CKR(lvl.alloc(&pos, nc));
+            k_apriori_join<1><<<jb, 128, 0, ctx->stream>>>(L, n, k, nullptr, off, cand, left);
+            CK(cudaGetLastError());
+            k_count_kway<<<(unsigned)((nc * 32 + 255) / 256), 256, 0, ctx->stream>>>(db->d_bits, db->stride, cand,
+                                                                                     nc, w, sup);
+            CK(cudaGetLastError());
+            k_apriori_flags<<<(unsigned)((nc + 255) / 256), 256, 0, ctx->stream>>>(sup, nc, ms, flag);
+            CK(cudaGetLastError());
+            k_scan_u32<<<1, 1024, 0, ctx->stream>>>(flag, nc, pos, d_total);
+            CK(cudaGetLastError());
+            uint64_t nk = 0;
+            CK(cudaMemcpyAsync(&nk, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            st.kernel_launches += 4;
+            st.intersections += nc * (w - 1);
+            st.bytes_alg += nc * w * db->stride * 8;
+            uint32_t *L2 = nullptr, *pid2 = nullptr;
+            CKR(patterns_reserve(ctx, pa, n_pat, n_pat + nk));
+            CKR(dalloc(ctx, &L2, std::max<uint64_t>(1, nk) * w));
+            CKR(dalloc(ctx, &pid2, std::max<uint64_t>(1, nk)));
+            if (nk) {
+                k_apriori_keep<<<(unsigned)((nc + 255) / 256), 256, 0, ctx->stream>>>(
+                    cand, left, sup, flag, pos, nc, w, pid, n_pat, L2, pid2, pa.parent, pa.item, pa.sup);
+                CK(cudaGetLastError());
+                st.kernel_launches++;
+            }
+            dfree(ctx, L);
+            dfree(ctx, pid);
+            L = L2;
+            pid = pid2;
+            n_pat += nk;
+            n = nk;
+            k = w;
+        }
+        dfree(ctx, L);
+        dfree(ctx, pid);
+    }
     CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    res->parent.resize(n_pat);
+    res->item.resize(n_pat);
+    res->support.resize(n_pat);
+    if (n_pat) {
+        CK(cudaMemcpyAsync(res->parent.data(), pa.parent, n_pat * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(res->item.data(), pa.item, n_pat * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(res->support.data(), pa.sup, n_pat * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    }
     CK(cudaStreamSynchronize(ctx->stream));
-    st.n_patterns = res->parent.size();
-    st.ms_pairs = elapsed_ms(ctx, 1, 2);
+    db->hint_patterns = std::max<uint64_t>(db->hint_patterns, n_pat + n_pat / 4);
+    st.n_patterns = n_pat;
+    st.ms_pairs = F >= 2 ? elapsed_ms(ctx, 5, 6) : 0.0;
     st.ms_deep = elapsed_ms(ctx, 2, 3);
     st.ms_total = elapsed_ms(ctx, 0, 3);
     st.deep_gbs = st.ms_deep > 0 ? st.bytes_alg / (st.ms_deep * 1e6) : 0.0;

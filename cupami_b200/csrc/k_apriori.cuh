@@ -1,0 +1,158 @@
+// Level-wise Apriori on the device (cuApriori.py:473-535).
+//
+// A level is a lexicographically sorted array of k-item rows (columns), with
+// the pattern id of every row.  Candidates of the next level join two rows
+// that share their first k-1 items (cuApriori.py:482-487) and survive only if
+// every k-subset is in the level (:488-490); the join runs in row order, so the
+// candidate list comes out sorted, as the reference's sorted(candidates).
+// Supports are complete intersections of the original tidsets (k_count_kway).
+#pragma once
+#include "common.cuh"
+
+namespace cpm {
+
+__device__ __forceinline__ int cmp_rows(const uint32_t *a, const uint32_t *b, uint32_t k) {
+    for (uint32_t i = 0; i < k; ++i)
+        if (a[i] != b[i]) return a[i] < b[i] ? -1 : 1;
+    return 0;
+}
+
+__device__ bool level_has(const uint32_t *L, uint64_t n, uint32_t k, const uint32_t *x) {
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        const int c = cmp_rows(L + mid * k, x, k);
+        if (!c) return true;
+        if (c < 0) lo = mid + 1; else hi = mid;
+    }
+    return false;
+}
+
+// Joins row a with every later row b of its prefix group; counts (mode 0) or
+// writes (mode 1) the candidates whose k-subsets are all frequent.
+template <int MODE>
+__global__ void k_apriori_join(const uint32_t *__restrict__ L, uint64_t n, uint32_t k,
+                               uint32_t *__restrict__ cnt, const uint64_t *__restrict__ off,
+                               uint32_t *__restrict__ cand, uint32_t *__restrict__ cand_left) {
+    const uint64_t a = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    const uint32_t *ra = L + a * k;
+    uint32_t sub[64];
+    uint32_t c = 0;
+    uint64_t pos = MODE ? off[a] : 0;
+    for (uint64_t b = a + 1; b < n; ++b) {
+        const uint32_t *rb = L + b * k;
+        if (cmp_rows(ra, rb, k - 1)) break;
+        const uint32_t last = rb[k - 1];
+        bool ok = true;
+        // Dropping item k-1 or k gives rows b or a, which are in the level.
+        for (uint32_t drop = 0; drop + 1 < k && ok; ++drop) {
+            uint32_t t = 0;
+            for (uint32_t i = 0; i < k; ++i)
+                if (i != drop) sub[t++] = ra[i];
+            sub[t] = last;
+            ok = level_has(L, n, k, sub);
+        }
+        if (!ok) continue;
+        if (MODE) {
+            uint32_t *dst = cand + pos * (k + 1);
+            for (uint32_t i = 0; i < k; ++i) dst[i] = ra[i];
+            dst[k] = last;
+            cand_left[pos] = (uint32_t)a;
+            ++pos;
+        } else {
+            ++c;
+        }
+    }
+    if (!MODE) cnt[a] = c;
+}
+
+// flag[c] = support passes (as 0/1 for the scan).
+__global__ void k_apriori_flags(const uint32_t *__restrict__ sup, uint64_t n, long long minsup,
+                                uint32_t *__restrict__ flag) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flag[i] = (long long)sup[i] >= minsup;
+}
+
+// Survivors, in candidate order, become the next level and pattern records.
+__global__ void k_apriori_keep(const uint32_t *__restrict__ cand, const uint32_t *__restrict__ cand_left,
+                               const uint32_t *__restrict__ sup, const uint32_t *__restrict__ flag,
+                               const uint64_t *__restrict__ pos, uint64_t n, uint32_t w,
+                               const uint32_t *__restrict__ pid_prev, uint64_t pid_base,
+                               uint32_t *__restrict__ L_next, uint32_t *__restrict__ pid_next,
+                               uint32_t *__restrict__ pat_parent, uint32_t *__restrict__ pat_item,
+                               uint32_t *__restrict__ pat_sup) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !flag[i]) return;
+    const uint64_t p = pos[i];
+    for (uint32_t j = 0; j < w; ++j) L_next[p * w + j] = cand[i * w + j];
+    const uint64_t pid = pid_base + p;
+    pid_next[p] = (uint32_t)pid;
+    pat_parent[pid] = pid_prev[cand_left[i]];
+    pat_item[pid] = cand[i * w + w - 1];
+    pat_sup[pid] = sup[i];
+}
+
+// Level 2 from the pair Gram: rows (f_i, f_j) in (i, j) order with pattern ids.
+__global__ void k_pairs_to_level(const uint32_t *__restrict__ C, uint32_t F, long long minsup,
+                                 const uint32_t *__restrict__ freq, const uint64_t *__restrict__ off,
+                                 uint64_t pid_base, uint32_t *__restrict__ L2, uint32_t *__restrict__ pid2,
+                                 uint32_t *__restrict__ pat_parent, uint32_t *__restrict__ pat_item,
+                                 uint32_t *__restrict__ pat_sup) {
+    const uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (i >= F) return;
+    uint64_t pos = off[i];
+    for (uint64_t j0 = i + 1; j0 < F; j0 += 32) {
+        const uint64_t j = j0 + lane;
+        const uint32_t s = j < F ? C[i * F + j] : 0u;
+        const bool pass = j < F && (long long)s >= minsup;
+        const unsigned bal = __ballot_sync(CPM_FULL, pass);
+        if (pass) {
+            const uint64_t k = pos + __popc(bal & ((1u << lane) - 1));
+            L2[2 * k] = freq[i];
+            L2[2 * k + 1] = freq[j];
+            const uint64_t pid = pid_base + k;
+            pid2[k] = (uint32_t)pid;
+            pat_parent[pid] = (uint32_t)i;
+            pat_item[pid] = freq[j];
+            pat_sup[pid] = s;
+        }
+        pos += __popc(bal);
+    }
+}
+
+// Exclusive prefix sum of n uint32 values into uint64 (one CTA, chunked);
+// *total receives the sum.  Levels hold at most a few million rows.
+__global__ void k_scan_u32(const uint32_t *__restrict__ in, uint64_t n, uint64_t *__restrict__ out,
+                           uint64_t *__restrict__ total) {
+    __shared__ unsigned long long warp_tot[32];
+    __shared__ unsigned long long base;
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    for (uint64_t start = 0; start < n; start += blockDim.x) {
+        const uint64_t i = start + threadIdx.x;
+        unsigned long long v = i < n ? in[i] : 0;
+        unsigned long long x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(CPM_FULL, x, o);
+            if (lane >= (unsigned)o) x += y;
+        }
+        if (lane == 31) warp_tot[wid] = x;
+        __syncthreads();
+        unsigned long long before = 0, all = 0;
+        for (unsigned w = 0; w < nw; ++w) {
+            if (w < wid) before += warp_tot[w];
+            all += warp_tot[w];
+        }
+        if (i < n) out[i] = base + before + x - v;
+        __syncthreads();
+        if (threadIdx.x == 0) base += all;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = base;
+}
+
+}  // namespace cpm

@@ -36,12 +36,25 @@ struct DFrame {
     uint32_t root;         // top-level class this frame descends from
 };
 
+// Every counter that CTAs update or poll sits on its own 128-byte line, so
+// that claims, allocations and statistics do not serialise on one L2 line.
+#define CPM_LINE(name) unsigned long long name; unsigned long long name##_pad[15]
 struct DeepState {
-    unsigned long long q_head, q_tail, pending;
-    unsigned long long n_patterns, arena_next, n_frames, n_members;
-    unsigned long long intersections, bytes_alg, work_items, survivors;
-    unsigned int error, pad;
+    CPM_LINE(q_head);       // next ticket to hand out
+    CPM_LINE(q_tail);       // entries reserved by producers
+    CPM_LINE(pending);      // units queued or running
+    CPM_LINE(n_patterns);
+    CPM_LINE(arena_next);
+    CPM_LINE(n_frames);
+    CPM_LINE(n_members);
+    CPM_LINE(intersections);
+    CPM_LINE(bytes_alg);
+    CPM_LINE(work_items);
+    CPM_LINE(survivors);
+    unsigned int error;
+    unsigned int pad[31];
 };
+#undef CPM_LINE
 
 struct DeepParams {
     DFrame *frames; uint64_t frames_cap;
@@ -58,28 +71,25 @@ struct DeepParams {
 
 __device__ __forceinline__ void deep_fail(DeepState *st, unsigned bit) { atomicOr(&st->error, bit); }
 
-// Thread 0 claims the next unit. Returns 0 with *item set, or 1 to stop.
+// Thread 0 claims the next unit with a ticket: one atomicAdd on the head,
+// then a wait on its own queue entry until a producer fills it, or until no
+// unit is queued or running (the ticket will never be filled), or an error.
+// Returns 0 with *item set, or 1 to stop.
 __device__ int deep_claim(const DeepParams &P, unsigned long long *item) {
     DeepState *st = P.st;
+    const unsigned long long h = atomicAdd(&st->q_head, 1ull);
+    unsigned backoff = 32;  // ns, doubled up to 2 us while waiting
     for (unsigned long long it = 0; it < P.spin_limit; ++it) {
-        if (ld_acquire_u32(&st->error)) return 1;
-        const unsigned long long h = ld_acquire_u64(&st->q_head);
-        const unsigned long long t = ld_acquire_u64(&st->q_tail);
-        if (h < t) {
-            // A producer that overflowed the queue bumped the tail before
-            // flagging the error: never read past the queue's end.
-            if (h >= P.queue_cap) return 1;
-            if (atomicCAS(&st->q_head, h, h + 1) != h) continue;
-            for (unsigned long long j = 0; j < P.spin_limit; ++j) {
-                const unsigned long long v = ld_acquire_u64(P.queue + h);
-                if (v != QUEUE_EMPTY) { *item = v; return 0; }
-                __nanosleep(32);
-            }
-            deep_fail(st, DEEP_ERR_SPIN);
-            return 1;
+        if (h < P.queue_cap) {
+            const unsigned long long v = ld_acquire_u64(P.queue + h);
+            if (v != QUEUE_EMPTY) { *item = v; return 0; }
         }
-        if (ld_acquire_u64(&st->pending) == 0) return 1;
-        __nanosleep(128);
+        if ((it & 7) == 0) {
+            if (ld_acquire_u32(&st->error)) return 1;
+            if (ld_acquire_u64(&st->pending) == 0) return 1;
+        }
+        __nanosleep(backoff);
+        backoff = min(backoff * 2, 2048u);
     }
     deep_fail(st, DEEP_ERR_SPIN);
     return 1;
@@ -95,12 +105,15 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
     __shared__ uint64_t s_pool[32];
     __shared__ int s_pool_n;
     __shared__ unsigned long long s_fid, s_qbase;
+    __shared__ int s_ok;
 
     const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const uint64_t n2 = P.stride / 2;
     DeepState *st = P.st;
     uint64_t my_slot = NO_SLOT;  // warp-uniform scratch slot (kept across units)
     if (threadIdx.x == 0) s_pool_n = 0;
+    // Per-CTA statistics (thread 0), added to the global counters at exit.
+    unsigned long long c_inter = 0, c_bytes = 0, c_units = 0, c_surv = 0;
 
     for (;;) {
         if (threadIdx.x == 0) s_stop = deep_claim(P, &s_item);
@@ -125,9 +138,10 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
             const unsigned long long mb = atomicAdd(&st->n_members, (unsigned long long)cnt);
             if (mb + cnt > P.members_cap) deep_fail(st, DEEP_ERR_MEMBERS);
             s_mem_base = mb;
+            s_ok = ld_acquire_u32(&st->error) == 0;
         }
         __syncthreads();
-        const bool ok = ld_acquire_u32(&st->error) == 0;
+        const bool ok = s_ok != 0;
         const uint32_t parent_pat = __ldcg(P.mem_pat + f.mem_off + p);
         for (uint32_t q = wid; ok && q < cnt; q += nw) {
             if (my_slot == NO_SLOT) {
@@ -239,14 +253,20 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            atomicAdd(&st->intersections, (unsigned long long)cnt);
-            atomicAdd(&st->bytes_alg, (unsigned long long)(8ull * P.stride * (1ull + cnt + ns)));
-            atomicAdd(&st->work_items, 1ull);
-            atomicAdd(&st->survivors, (unsigned long long)ns);
+            c_inter += cnt;
+            c_bytes += 8ull * P.stride * (1ull + cnt + ns);
+            c_units += 1;
+            c_surv += ns;
             if (P.root_cost) atomicAdd(P.root_cost + f.root, (unsigned long long)cnt);
             __threadfence();
             atomicAdd(&st->pending, ~0ull);  // pending -= 1
         }
+    }
+    if (threadIdx.x == 0 && c_units) {
+        atomicAdd(&st->intersections, c_inter);
+        atomicAdd(&st->bytes_alg, c_bytes);
+        atomicAdd(&st->work_items, c_units);
+        atomicAdd(&st->survivors, c_surv);
     }
 }
 

@@ -60,6 +60,11 @@ class cuApriori:
 
     #: Deep-level scheduler: "plain" (size ordered) or "learned" (cost model).
     scheduler = "plain"
+    #: Bound on every device wait (0: the library default).  A small value
+    #: makes a wait run out and mine() raise instead of waiting on.
+    _SPIN_LIMIT = 0
+    #: Pair-level engine: 0 automatic, 1 tensor-core Gram, 2 CUDA-core Gram.
+    _PAIR_ENGINE = 0
 
     def __init__(self, iFile, minSup, sep=None, use_gds="auto", use_gpu_io="auto"):
         loading_start = time.perf_counter()
@@ -244,6 +249,9 @@ class cuApriori:
         _native.library().cpm_default_opts(opts)
         opts.scheduler = (_native.CPM_SCHED_LEARNED if self.scheduler == "learned"
                           else _native.CPM_SCHED_PLAIN)
+        if self._SPIN_LIMIT:
+            opts.spin_limit = int(self._SPIN_LIMIT)
+        opts.pair_engine = int(self._PAIR_ENGINE)
         return opts
 
     def mine(self):

@@ -1,0 +1,107 @@
+"""GPU: the kernel-module drop-in, the hook-driven search and bounded waits."""
+from itertools import combinations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _rows(seed=3, n=600, n_items=12):
+    rng = np.random.default_rng(seed)
+    p = rng.uniform(0.2, 0.7, n_items)
+    return [[int(i) for i in np.nonzero(rng.random(n_items) < p)[0]] for _ in range(n)]
+
+
+def test_bitsets_module_matches_numpy():
+    import torch
+
+    from cupami_b200.frequentPattern import _bitsets
+
+    rng = np.random.default_rng(0)
+    n_tx, n_items, nnz = 1000, 37, 9000
+    rows = rng.integers(0, n_tx, nnz).astype(np.uint64)
+    cols = rng.integers(0, n_items, nnz).astype(np.uint32)
+    xp = _bitsets.array_module()
+    bits = _bitsets.build_bitsets(xp, xp.asarray(rows, dtype=xp.uint64), xp.asarray(cols, dtype=xp.uint32),
+                                  n_tx, n_items)
+    ref = np.zeros((n_items, (n_tx + 31) // 32), dtype=np.uint32)
+    np.bitwise_or.at(ref, (cols.astype(np.int64), (rows // 32).astype(np.int64)),
+                     np.left_shift(np.uint32(1), (rows % 32).astype(np.uint32)))
+    got = bits.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, ref)
+    cands = [[int(a), int(b), int(c)] for a, b, c in rng.integers(0, n_items, (500, 3))]
+    sup = _bitsets.count_supports(xp, bits, cands)
+    want = np.bitwise_count(ref[[c[0] for c in cands]] & ref[[c[1] for c in cands]]
+                            & ref[[c[2] for c in cands]]).sum(axis=1).tolist()
+    assert sup == want
+    children, sup = _bitsets.intersect_extensions(xp, bits[3], bits[5:20])
+    want_children = ref[5:20] & ref[3]
+    assert np.array_equal(children.cpu().numpy().view(np.uint32), want_children)
+    assert sup == np.bitwise_count(want_children).sum(axis=1).tolist()
+    assert _bitsets.count_supports(xp, bits, []) == []
+    assert isinstance(torch.cuda.current_device(), int)
+
+
+def test_hook_overrides_run_the_constrained_search(oracle_lib):
+    """A cuSpatialEclat-style subclass: only pairwise 'neighbour' itemsets."""
+    import cupami_b200
+
+    rows = _rows()
+    neighbours = {str(i): {str(j) for j in range(12) if abs(i - j) <= 3 and i != j} for i in range(12)}
+
+    class Constrained(cupami_b200.cuEclat):
+        def _candidatePairs(self, frequent, items):
+            for k, left in enumerate(frequent):
+                for right in frequent[k + 1:]:
+                    if items[right] in neighbours[items[left]]:
+                        yield left, right
+
+        def _extensionBatch(self, cp, prefix, labels, bitsets, start, stop):
+            allowed = set(neighbours[prefix[0]])
+            for item in prefix[1:]:
+                allowed &= neighbours[item]
+            keep = [i for i in range(start, stop) if labels[i] in allowed]
+            if not keep:
+                return [], None
+            return [labels[i] for i in keep], bitsets[cp.asarray(keep, dtype=cp.int64)]
+
+    miner = Constrained(rows, 30)
+    miner._PAIR_BATCH_SIZE = 7
+    miner._INTERSECTION_BATCH_BYTES = 64
+    miner.mine()
+    full = oracle_lib.mine_rows(rows, 30)
+    want = {k: v for k, v in full.items()
+            if all(b in neighbours[a] for a, b in combinations(k.split("\t"), 2))}
+    assert miner.getPatterns() == want
+    assert any(k.count("\t") >= 2 for k in want)
+
+
+def test_spin_limit_runs_out_and_context_survives(oracle_lib):
+    import cupami_b200
+    from cupami_b200._native import CPM_ETIMEOUT, NativeError
+
+    rows = _rows(seed=9, n=3000, n_items=18)
+    miner = cupami_b200.cuEclat(rows, 0.05)
+    miner._SPIN_LIMIT = 1
+    with pytest.raises(NativeError) as err:
+        miner.mine()
+    assert err.value.code == CPM_ETIMEOUT
+    miner._SPIN_LIMIT = 0
+    miner.mine()
+    assert miner.getPatterns() == oracle_lib.mine_rows(rows, 0.05)
+
+
+def test_cli_writes_reference_format(tmp_path):
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    src = tmp_path / "t.csv"
+    out = tmp_path / "p.txt"
+    src.write_text("1,2\n1\n2\n")
+    root = Path(__file__).resolve().parents[1]
+    res = subprocess.run([sys.executable, "-m", "cupami_b200.frequentPattern.cuEclat", str(src), str(out), "2"],
+                         capture_output=True, text=True, timeout=120, cwd=root)
+    assert res.returncode == 0, res.stderr
+    assert out.read_text() == "1 : 2\n2 : 2\n"
