@@ -45,6 +45,8 @@ WORKLOADS = {
     "dense-bernoulli-64k": ("dense_bernoulli", 0.6, ("eclat",)),
     "dense-fixed-64k": ("dense_fixed_length", 0.6, ("eclat",)),
     "sparse-zipf-1m": ("sparse_zipf", 0.001, ("eclat",)),
+    # 512 independent databases mined in one pass (cuEclat.mineBatch)
+    "batched-zipf-512": ("batched_zipf", 0.01, ("eclat-batch",)),
 }
 
 
@@ -57,6 +59,12 @@ def make_workload(name, rank):
 
     seed = inspect.signature(fn).parameters["seed"].default + rank
     return fn(seed=seed), minsup, algos, seed
+
+
+def n_transactions(csr):
+    if isinstance(csr, list):
+        return sum(n_transactions(c) for c in csr)
+    return int(np.count_nonzero(np.diff(csr.offsets.astype(np.int64)) > 0))
 
 
 def dist_setup():
@@ -134,41 +142,53 @@ def int8_peak_tops():
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
-def cpu_baseline(csr, minsup, algos, budget_s=30.0):
-    """The reference's host path (NumPy kernels) on one core, whole steps."""
+def _port_step(csr, minsup, algos):
     import oracle
     from oracle import numpy_port
 
     labels, rows, cols, n_tx = numpy_port.device_pairs_from_csr(csr.offsets, csr.items)
     ms = oracle.support_count(minsup, n_tx)
+    for a in algos:
+        (numpy_port.apriori if a == "apriori" else numpy_port.eclat)(labels, rows, cols, n_tx, ms)
+
+
+def cpu_step_seconds(csr, minsup, algos, budget_s=30.0):
+    """The reference's host path (NumPy kernels) on one core for one step.
+
+    Batched workloads run a sample of databases (first ones, up to the time
+    budget) and scale by transactions; returns (seconds, sample description)."""
+    if isinstance(csr, list):
+        t0 = time.perf_counter()
+        done_tx = 0
+        k = 0
+        for c in csr:
+            _port_step(c, minsup, algos)
+            done_tx += n_transactions(c)
+            k += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+        spent = time.perf_counter() - t0
+        total = n_transactions(csr)
+        return spent * total / max(1, done_tx), f"{k} of {len(csr)} databases ({done_tx} of {total} transactions), scaled by transactions"
     times = []
     t_end = time.perf_counter() + budget_s
     while not times or (time.perf_counter() < t_end and len(times) < 3):
         t0 = time.perf_counter()
-        labels, rows, cols, n_tx = numpy_port.device_pairs_from_csr(csr.offsets, csr.items)
-        for a in algos:
-            (numpy_port.eclat if a == "eclat" else numpy_port.apriori)(labels, rows, cols, n_tx, ms)
+        _port_step(csr, minsup, algos)
         times.append(time.perf_counter() - t0)
-    return statistics.median(times), len(times)
+    return statistics.median(times), f"whole step, median of {len(times)}"
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
     csr, minsup, algos, seed = make_workload(args.workload, 0)
-    cores = 1
-    times = []
-    import oracle
-    from oracle import numpy_port
-
+    budget = 20.0 if isinstance(csr, list) else 60.0
+    times, sample = [], ""
     for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        labels, rows, cols, n_tx = numpy_port.device_pairs_from_csr(csr.offsets, csr.items)
-        ms = oracle.support_count(minsup, n_tx)
-        for a in algos:
-            (numpy_port.eclat if a == "eclat" else numpy_port.apriori)(labels, rows, cols, n_tx, ms)
+        v, sample = cpu_step_seconds(csr, minsup, algos, budget_s=budget if isinstance(csr, list) else 0.0)
         if i >= args.warmup:
-            times.append(time.perf_counter() - t0)
+            times.append(v)
     v = statistics.mean(times)
     line = {
         "impl": "reference", "metric": "mine() seconds per step (" + "+".join(algos) + ")",
@@ -176,8 +196,8 @@ def run_reference(args, world, rank):
         "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "u64", "data": "synthetic",
         "config": {"workload": args.workload, "seed": seed, "minSup": minsup, "algorithms": list(algos)},
-        "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port",
-                         "sample": f"whole {args.workload} step (NumPy restatement of the reference host path)"},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "port",
+                         "sample": f"{sample} (NumPy restatement of the reference host path)"},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -186,12 +206,13 @@ def run_reference(args, world, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="planted-100k", choices=sorted(WORKLOADS))
     ap.add_argument("--scheduler", default="plain", choices=["plain", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ab", action="store_true", help="skip the learned-vs-plain scheduler comparison")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup()
@@ -211,65 +232,105 @@ def main():
                                 device_id=torch.device("cuda", local))
         pg = dist
     import cupami_b200
-    from cupami_b200 import _native
+    from cupami_b200 import _native, costmodel
 
     csr, minsup, algos, seed = make_workload(args.workload, rank)
-    n_tx = int(np.count_nonzero(np.diff(csr.offsets.astype(np.int64)) > 0))
-    ms_count = cupami_b200.cuApriori._getSupportCount(minsup, n_tx)
+    batched = isinstance(csr, list)
+    csrs = csr if batched else [csr]
+    n_tx = n_transactions(csr)
     ctx = _native.context(local)
-    db = _native.Database.from_ids(ctx, csr.offsets, csr.items)
-    opts = _native.Opts()
-    _native.library().cpm_default_opts(opts)
-    opts.scheduler = _native.CPM_SCHED_LEARNED if args.scheduler == "learned" else _native.CPM_SCHED_PLAIN
+    have_model = costmodel.ensure_default(ctx)
+    dbs = [_native.Database.from_ids(ctx, c.offsets, c.items) for c in csrs]
+    ms_counts = [cupami_b200.cuApriori._getSupportCount(minsup, n_transactions(c)) for c in csrs]
+
+    def options(sched):
+        o = _native.Opts()
+        _native.library().cpm_default_opts(o)
+        o.scheduler = _native.CPM_SCHED_LEARNED if sched == "learned" else _native.CPM_SCHED_PLAIN
+        return o
+
     algo_code = {"eclat": (_native.CPM_ECLAT, _native.CPM_ORDER_ECLAT),
                  "apriori": (_native.CPM_APRIORI, _native.CPM_ORDER_APRIORI)}
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
 
-    def device_step():
-        stats = []
+    def device_step(sched):
+        """[(algorithm, stats, results)] of one step with resident tidsets."""
+        out = []
         for a in algos:
-            code, order = algo_code[a]
-            res = db.mine(ms_count, code, opts, order)
-            stats.append(res.stats)
-        return stats
+            if a == "eclat-batch":
+                res = _native.mine_batch(ctx, dbs, ms_counts, options(sched))
+                out.append((a, res[0].stats, res))
+            else:
+                code, order = algo_code[a]
+                res = dbs[0].mine(ms_counts[0], code, options(sched), order)
+                out.append((a, res.stats, [res]))
+        return out
 
     def barrier():
         torch.cuda.synchronize()
         if pg:
             pg.barrier()
 
-    for _ in range(args.warmup):
-        device_step()
-    barrier()
+    def timed(sched, steps):
+        for _ in range(args.warmup):
+            device_step(sched)
+        barrier()
+        ms, kst, launches, last = [], [], 0, None
+        for _ in range(steps):
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            out = device_step(sched)
+            ms.append(sum(st["ms_total"] for _, st, _ in out))
+            kst.append(out)
+            launches += sum(int(st["kernel_launches"]) for _, st, _ in out)
+            last = out
+        barrier()
+        return ms, kst, launches, last
+
     sampler = ClockSampler(local)
-    step_ms, per_kernel = [], []
-    launches = 0
-    for _ in range(args.steps):
-        flush_l2(flush)
-        torch.cuda.synchronize()
-        stats = device_step()
-        step_ms.append(sum(s["ms_total"] for s in stats))
-        per_kernel.append(stats)
-        launches += sum(int(s["kernel_launches"]) for s in stats)
-    barrier()
+    step_ms, per_kernel, launches, last = timed(args.scheduler, args.steps)
     clocks = sampler.stop()
+    # Scheduler A/B on the same resident data (Eclat deep phase only).
+    ab = None
+    if not args.no_ab and have_model and any(a != "apriori" for a in algos):
+        other = "learned" if args.scheduler == "plain" else "plain"
+        o_ms, o_kst, _, o_last = timed(other, args.steps)
+        deep = lambda kst: statistics.mean(sum(st["ms_deep"] for a, st, _ in out if a != "apriori") for out in kst)
+        same = all(np.array_equal(r1.supports, r2.supports) and np.array_equal(r1.items, r2.items)
+                   for (_, _, a1), (_, _, a2) in zip(last, o_last) for r1, r2 in zip(a1, a2))
+        times = {args.scheduler: (statistics.mean(step_ms), deep(per_kernel)), other: (statistics.mean(o_ms), deep(o_kst))}
+        ab = {"plain_ms": times["plain"][0], "learned_ms": times["learned"][0],
+              "plain_deep_ms": times["plain"][1], "learned_deep_ms": times["learned"][1],
+              "speedup_step": times["plain"][0] / times["learned"][0],
+              "speedup_deep": times["plain"][1] / times["learned"][1] if times["learned"][1] else None,
+              "identical_output": bool(same)}
     # e2e through the public API from host arrays.
-    for _ in range(args.warmup):
+    def api_step():
+        t, d2h = 0.0, 0
         for a in algos:
-            (cupami_b200.cuEclat if a == "eclat" else cupami_b200.cuApriori)(csr, minsup).mine()
+            if a == "eclat-batch":
+                miners = cupami_b200.cuEclat.mineBatch(csrs, minsup)
+                t += miners[0].getMiningTime()
+                for m in miners:
+                    off, it, sup, _ = m.getPatternArrays()
+                    d2h += it.nbytes + sup.nbytes // 2 * 3
+            else:
+                m = (cupami_b200.cuEclat if a == "eclat" else cupami_b200.cuApriori)(csr, minsup)
+                m.scheduler = args.scheduler
+                m.mine()
+                t += m.getMiningTime()
+                off, it, sup, _ = m.getPatternArrays()
+                d2h += it.nbytes + sup.nbytes // 2 * 3
+        return t, d2h
+
+    for _ in range(args.warmup):
+        api_step()
     barrier()
-    e2e = []
-    d2h = 0
+    e2e, d2h = [], 0
     for _ in range(args.steps):
         flush_l2(flush)
         torch.cuda.synchronize()
-        t = 0.0
-        for a in algos:
-            m = (cupami_b200.cuEclat if a == "eclat" else cupami_b200.cuApriori)(csr, minsup)
-            m.mine()
-            t += m.getMiningTime()
-            off, it, sup, _ = m.getPatternArrays()
-            d2h = max(d2h, it.nbytes + sup.nbytes // 2 * 3)
+        t, d2h = api_step()
         e2e.append(t)
     barrier()
     value = statistics.mean(step_ms) / 1e3
@@ -278,24 +339,23 @@ def main():
         t = torch.tensor([value, e2e_v], device="cuda", dtype=torch.float64)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         value, e2e_v = t.tolist()
-    # Roofline of the dominant kernel, averaged over the timed steps.
-    deep_ms = statistics.mean(sum(s["ms_deep"] for s in st) for st in per_kernel)
-    pair_ms = statistics.mean(sum(s["ms_pairs"] for s in st) for st in per_kernel)
-    deep_bytes = statistics.mean(sum(s["bytes_alg"] for s in st) for st in per_kernel)
-    pair_ops = statistics.mean(sum(s["pair_ops"] for s in st) for st in per_kernel)
+    # Roofline of the deep-level intersection kernel (k_deep), the step's
+    # dominant kernel on Eclat workloads, from its own CUDA events.
     hbm, bf16, src = peaks()
-    if deep_ms >= pair_ms:
+    eclat_stats = [[st for a, st, _ in out if a != "apriori"] for out in per_kernel]
+    roof = None
+    if eclat_stats and eclat_stats[0]:
+        deep_ms = statistics.mean(sum(s["ms_deep"] for s in st) for st in eclat_stats)
+        deep_bytes = statistics.mean(sum(s["bytes_alg"] for s in st) for st in eclat_stats)
         achieved = deep_bytes / (deep_ms * 1e-3) / 1e9 if deep_ms else 0.0
-        roof = {"kernel": "deep-level intersection (k_deep)", "bound": "hbm", "achieved": achieved,
-                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-                "peak_source": src, "ms_per_step": deep_ms, "alg_bytes_per_step": deep_bytes}
-    else:
-        i8 = int8_peak_tops()
-        achieved = pair_ops / (pair_ms * 1e-3) / 1e12 if pair_ms else 0.0
-        roof = {"kernel": "pair Gram", "bound": "tensor", "achieved": achieved, "peak": i8,
-                "unit": "TOPS", "frac": achieved / i8, "traffic": None,
-                "peak_source": "torch._int_mm int8 8192^3 best of 12 on this box",
-                "ms_per_step": pair_ms, "alg_ops_per_step": pair_ops}
+        roof = {"kernel": "k_deep (deep-level AND+popcount, persistent)", "bound": "hbm", "achieved": achieved,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None, "peak_source": src,
+                "ms_per_launch": deep_ms, "alg_bytes_per_launch": deep_bytes,
+                "alg_bytes": "sum over units of 8*W*(1 + siblings + children written)"}
+    pair_ms = statistics.mean(sum(st["ms_pairs"] for _, st, _ in out) for out in per_kernel)
+    pair_ops = statistics.mean(sum(st["pair_ops"] for _, st, _ in out) for out in per_kernel)
+    gram = {"kernel": "pair Gram", "ms_per_step": pair_ms, "ops_per_step": pair_ops,
+            "tops": pair_ops / (pair_ms * 1e-3) / 1e12 if pair_ms else 0.0}
     if rank != 0:
         if pg:
             pg.barrier()
@@ -303,27 +363,29 @@ def main():
         return
     cpu = None
     if not args.no_cpu_baseline:
-        v, n = cpu_baseline(csr, minsup, algos)
+        v, sample = cpu_step_seconds(csr, minsup, algos)
         cpu = {"value": v, "unit": "s", "cores": 1, "kind": "port",
-               "sample": f"whole step, median of {n} (NumPy restatement of the reference host path)"}
-    h2d = int(csr.offsets.nbytes + csr.items.nbytes) * len(algos)
-    last = per_kernel[-1]
+               "sample": f"{sample} (NumPy restatement of the reference host path)"}
+    h2d = sum(int(c.offsets.nbytes + c.items.nbytes) for c in csrs) * len(algos)
+    last_stats = [st for _, st, _ in last]
     line = {
         "metric": "mine() seconds per step (" + "+".join(algos) + ")",
         "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "u64", "data": "synthetic",
         "config": {"workload": args.workload, "seed": seed, "minSup": minsup, "algorithms": list(algos),
-                   "transactions": n_tx, "scheduler": args.scheduler,
+                   "databases": len(csrs), "transactions": n_tx, "scheduler": args.scheduler,
                    "l2": "256 MB buffer rewritten before every timed step",
                    "parallelism": f"replicas{world}" if world > 1 else "single"},
         "e2e": {"value": e2e_v, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": roof,
+        "pair_gram": gram,
         "cpu_baseline": cpu,
+        "scheduler_ab": ab,
         "gpu_launches": launches,
         "clocks": clocks,
-        "patterns": [int(s["n_patterns"]) for s in last],
-        "kernel_stats": last,
+        "patterns": [int(st["n_patterns"]) for st in last_stats],
+        "kernel_stats": last_stats,
     }
     print(json.dumps(line), flush=True)
     if pg:

@@ -85,6 +85,8 @@ _SIGNATURES = {
     "cpm_db_free": (None, [_P]),
     "cpm_mine": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.c_int, ctypes.POINTER(Opts),
                                 ctypes.POINTER(_P)]),
+    "cpm_mine_batch": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.c_uint32, ctypes.POINTER(ctypes.c_int64),
+                                      ctypes.POINTER(Opts), ctypes.POINTER(_P)]),
     "cpm_result_size": (ctypes.c_int, [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
     "cpm_result_copy": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P]),
     "cpm_result_tree": (ctypes.c_int, [_P, _P, _P, _P]),
@@ -95,6 +97,12 @@ _SIGNATURES = {
     "cpm_count_supports": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, _P]),
     "cpm_intersect_extensions": (ctypes.c_int, [_P, _P, _P, _U64, _U64, _P, _P]),
     "cpm_synchronize": (ctypes.c_int, [_P]),
+    "cpm_costmodel_params": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
+    "cpm_costmodel_train": (ctypes.c_int, [_P, _P, _P, _U64, ctypes.c_uint32, ctypes.c_float, _U64, _P, _P]),
+    "cpm_costmodel_predict": (ctypes.c_int, [_P, _P, _P, _U64, _P]),
+    "cpm_costmodel_gradient": (ctypes.c_int, [_P, _P, _P, _P, _U64, _P, _P]),
+    "cpm_costmodel_set": (ctypes.c_int, [_P, _P]),
+    "cpm_result_trace": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(_U64)]),
     "cpm_mine_eclat_noalloc": (ctypes.c_int, [_P, _P, _U64, ctypes.c_uint32, _U64, ctypes.c_int64,
                                               _P, _P, _P, _U64, ctypes.POINTER(_U64)]),
 }
@@ -244,6 +252,28 @@ class Database:
             pass
 
 
+def mine_batch(ctx, databases, min_sups, opts=None, order=CPM_ORDER_ECLAT):
+    """Eclat over a list of Database objects in one pass; one Result each."""
+    n = len(databases)
+    if opts is None:
+        opts = Opts()
+        library().cpm_default_opts(ctypes.byref(opts))
+    handles = (_P * max(1, n))(*[db.handle for db in databases])
+    sups = (ctypes.c_int64 * max(1, n))(*[int(s) for s in min_sups])
+    outs = (_P * max(1, n))()
+    with ctx.lock:
+        ctx.check(library().cpm_mine_batch(ctx.handle, handles, n, sups, ctypes.byref(opts), outs))
+    results = []
+    try:
+        for k in range(n):
+            results.append(Result.collect(outs[k], order))
+    finally:
+        for k in range(n):
+            if outs[k]:
+                library().cpm_result_free(outs[k])
+    return results
+
+
 class Result:
     """Mined patterns as arrays: pattern k = items[offsets[k]:offsets[k+1]]."""
 
@@ -252,6 +282,7 @@ class Result:
         self.items = items
         self.supports = supports
         self.stats = stats
+        self.trace = None  # (features, log1p(subtree intersections)) per root unit, when traced
 
     @classmethod
     def collect(cls, handle, order):
@@ -268,7 +299,17 @@ class Result:
             raise NativeError(code, "result copy")
         st = Stats()
         lib.cpm_result_stats(handle, ctypes.byref(st))
-        return cls(offsets, items[:slots.value], supports[:n.value], st.as_dict())
+        out = cls(offsets, items[:slots.value], supports[:n.value], st.as_dict())
+        nt = _U64()
+        lib.cpm_result_trace(handle, None, None, ctypes.byref(nt))
+        if nt.value:
+            nf = ctypes.c_uint32()
+            lib.cpm_costmodel_params(ctypes.byref(nf), None)
+            X = np.zeros((nt.value, nf.value), dtype=np.float32)
+            y = np.zeros(nt.value, dtype=np.float32)
+            lib.cpm_result_trace(handle, X.ctypes.data, y.ctypes.data, ctypes.byref(nt))
+            out.trace = (X, y)
+        return out
 
     def __len__(self):
         return int(self.supports.size)

@@ -11,6 +11,11 @@
 #include "k_gram_tc.cuh"
 #include "k_deep.cuh"
 #include "k_apriori.cuh"
+#include "k_batch.cuh"
+#include "k_costmodel.cuh"
+
+#include <cub/device/device_scan.cuh>
+#include <thrust/iterator/transform_iterator.h>
 
 #include <algorithm>
 #include <cstdarg>
@@ -23,6 +28,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <mutex>
+#include <cmath>
 
 using namespace cpm;
 
@@ -41,6 +47,7 @@ struct cpm_ctx {
     int deep_occ_smem = -1;   // k_deep<true> CTAs per SM, for deep_occ_bytes of prefix
     size_t deep_occ_bytes = 0;
     int deep_occ_global = -1; // k_deep<false> CTAs per SM
+    std::vector<float> model;  // cost-model parameters (empty: none loaded)
 };
 
 struct cpm_db {
@@ -58,6 +65,8 @@ struct cpm_result {
     std::vector<uint32_t> parent, item, support;
     cpm_stats stats{};
     int algo = CPM_ECLAT;
+    // Per root unit, when traced: cost-model features and log1p(subtree intersections)
+    std::vector<float> trace_x, trace_y;
 };
 
 static int set_err(cpm_ctx *ctx, int code, const char *fmt, ...) {
@@ -419,6 +428,43 @@ static int mine_singletons(cpm_ctx *ctx, cpm_db *db, long long ms, DevScope &ds,
     return CPM_OK;
 }
 
+// Tensor-core Gram of F frequent rows into C (zeroed here); synchronous.
+static int gram_tc_run(cpm_ctx *ctx, DevScope &ds, const uint64_t *bits, uint64_t stride, const uint32_t *d_freq,
+                       uint32_t F, uint32_t *C, cpm_stats &st) {
+    CK(cudaMemsetAsync(C, 0, (size_t)F * F * 4, ctx->stream));
+    // Upper-triangle tiles: A block ti (128 rows) x B block tj (256 columns)
+    // whenever some column of the block lies right of some row.
+    std::vector<GramTile> tiles;
+    const uint32_t nti = (F + tc::BM - 1) / tc::BM, ntj = (F + tc::BN - 1) / tc::BN;
+    for (uint32_t ti = 0; ti < nti; ++ti)
+        for (uint32_t tj = 0; tj < ntj; ++tj)
+            if ((uint64_t)tj * tc::BN + tc::BN - 1 > (uint64_t)ti * tc::BM) tiles.push_back({ti, tj});
+    // K split (in pairs of words, one stage each) so the units cover the GPU.
+    const uint64_t kstages = stride / 2;
+    uint64_t ksplit = std::max<uint64_t>(1, ((uint64_t)ctx->sms * 2 + tiles.size() - 1) / tiles.size());
+    ksplit = std::min<uint64_t>(ksplit, std::max<uint64_t>(1, kstages / 8));
+    const uint64_t stages_per = (kstages + ksplit - 1) / ksplit;
+    ksplit = (kstages + stages_per - 1) / stages_per;
+    GramTile *d_tiles = nullptr;
+    unsigned int *d_err = nullptr;
+    CKR(ds.alloc(&d_tiles, tiles.size()));
+    CKR(ds.alloc(&d_err, 1));
+    CK(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(GramTile), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(d_err, 0, 4, ctx->stream));
+    const uint64_t units = tiles.size() * ksplit;
+    k_gram_tc<<<(unsigned)units, tc::THREADS, tc::SMEM_BYTES, ctx->stream>>>(
+        bits, stride, d_freq, F, d_tiles, (uint32_t)tiles.size(), stages_per * 2, C, d_err);
+    CK(cudaGetLastError());
+    unsigned int herr = 0;
+    CK(cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (herr) return set_err(ctx, CPM_ETIMEOUT, "tensor-core Gram pipeline wait ran out");
+    st.kernel_launches += 1;
+    // Work issued to the tensor cores: every tile is a full 128x256 block.
+    st.pair_ops += 2ull * (uint64_t)tc::BM * tc::BN * (kstages * 128) * tiles.size();
+    return CPM_OK;
+}
+
 // Pair Gram C[F][F] (upper triangle) on the tensor cores or the CUDA cores.
 static int pair_gram(cpm_ctx *ctx, cpm_db *db, const uint32_t *d_freq, uint32_t F, const cpm_opts &o,
                      DevScope &ds, uint32_t **d_C, cpm_stats &st) {
@@ -427,39 +473,8 @@ static int pair_gram(cpm_ctx *ctx, cpm_db *db, const uint32_t *d_freq, uint32_t 
     CK(cudaEventRecord(ctx->ev[5], ctx->stream));
     if (use_tc) {
         if (!ctx->tc_ok) return set_err(ctx, CPM_EINVAL, "the tensor-core Gram needs an sm_100 device");
-        CK(cudaMemsetAsync(*d_C, 0, (size_t)F * F * 4, ctx->stream));
-        // Upper-triangle tiles: A block ti (128 rows) x B block tj (256 columns)
-        // whenever some column of the block lies right of some row.
-        std::vector<GramTile> tiles;
-        const uint32_t nti = (F + tc::BM - 1) / tc::BM, ntj = (F + tc::BN - 1) / tc::BN;
-        for (uint32_t ti = 0; ti < nti; ++ti)
-            for (uint32_t tj = 0; tj < ntj; ++tj)
-                if ((uint64_t)tj * tc::BN + tc::BN - 1 > (uint64_t)ti * tc::BM) tiles.push_back({ti, tj});
-        // K split (in pairs of words, one stage each) so the units cover the GPU.
-        const uint64_t kstages = db->stride / 2;
-        uint64_t ksplit = std::max<uint64_t>(1, ((uint64_t)ctx->sms * 2 + tiles.size() - 1) / tiles.size());
-        ksplit = std::min<uint64_t>(ksplit, std::max<uint64_t>(1, kstages / 8));
-        const uint64_t stages_per = (kstages + ksplit - 1) / ksplit;
-        ksplit = (kstages + stages_per - 1) / stages_per;
-        GramTile *d_tiles = nullptr;
-        unsigned int *d_err = nullptr;
-        CKR(ds.alloc(&d_tiles, tiles.size()));
-        CKR(ds.alloc(&d_err, 1));
-        CK(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(GramTile), cudaMemcpyHostToDevice,
-                           ctx->stream));
-        CK(cudaMemsetAsync(d_err, 0, 4, ctx->stream));
-        const uint64_t units = tiles.size() * ksplit;
-        k_gram_tc<<<(unsigned)units, tc::THREADS, tc::SMEM_BYTES, ctx->stream>>>(
-            db->d_bits, db->stride, d_freq, F, d_tiles, (uint32_t)tiles.size(), stages_per * 2, *d_C, d_err);
-        CK(cudaGetLastError());
+        CKR(gram_tc_run(ctx, ds, db->d_bits, db->stride, d_freq, F, *d_C, st));
         CK(cudaEventRecord(ctx->ev[6], ctx->stream));
-        unsigned int herr = 0;
-        CK(cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        if (herr) return set_err(ctx, CPM_ETIMEOUT, "tensor-core Gram pipeline wait ran out");
-        st.kernel_launches += 1;
-        // Work issued to the tensor cores: every tile is a full 128x256 block.
-        st.pair_ops += 2ull * (uint64_t)tc::BM * tc::BN * (kstages * 128) * tiles.size();
         return CPM_OK;
     }
     CK(cudaMemsetAsync(*d_C, 0, (size_t)F * F * 4, ctx->stream));
@@ -485,10 +500,10 @@ struct DeepBuffers {
     const uint64_t **mem_bits = nullptr;
     unsigned long long *queue = nullptr;
     uint64_t *arena = nullptr;
-    uint32_t *pat_parent = nullptr, *pat_item = nullptr, *pat_sup = nullptr;
+    uint32_t *pat_parent = nullptr, *pat_item = nullptr, *pat_sup = nullptr, *pat_db = nullptr;
     unsigned long long *root_cost = nullptr;
     DeepState *st = nullptr;
-    uint64_t frames_cap = 0, members_cap = 0, queue_cap = 0, arena_slots = 0, pat_cap = 0;
+    uint64_t frames_cap = 0, members_cap = 0, queue_cap = 0, arena_words = 0, pat_cap = 0;
     cpm_ctx *owner = nullptr;  // released on every exit path
     ~DeepBuffers() {
         if (owner) release(owner);
@@ -496,103 +511,252 @@ struct DeepBuffers {
     void release(cpm_ctx *ctx) {
         dfree(ctx, frames); dfree(ctx, mem_pat); dfree(ctx, mem_item); dfree(ctx, mem_bits);
         dfree(ctx, queue); dfree(ctx, arena); dfree(ctx, pat_parent); dfree(ctx, pat_item);
-        dfree(ctx, pat_sup); dfree(ctx, root_cost); dfree(ctx, st);
+        dfree(ctx, pat_sup); dfree(ctx, pat_db); dfree(ctx, root_cost); dfree(ctx, st);
     }
 };
 
 static int grow(cpm_ctx *ctx, DeepBuffers &b, uint64_t frames_cap, uint64_t members_cap, uint64_t queue_cap,
-                uint64_t arena_slots, uint64_t pat_cap, uint64_t stride, uint64_t n_roots) {
+                uint64_t arena_words, uint64_t pat_cap, uint64_t n_roots, bool with_db) {
     b.release(ctx);
     b.frames_cap = frames_cap; b.members_cap = members_cap; b.queue_cap = queue_cap;
-    b.arena_slots = arena_slots; b.pat_cap = pat_cap;
+    b.arena_words = arena_words; b.pat_cap = pat_cap;
     CKR(dalloc(ctx, &b.frames, frames_cap));
     CKR(dalloc(ctx, &b.mem_pat, members_cap));
     CKR(dalloc(ctx, &b.mem_item, members_cap));
     CKR(dalloc(ctx, &b.mem_bits, members_cap));
     CKR(dalloc(ctx, &b.queue, queue_cap));
-    CKR(dalloc(ctx, &b.arena, arena_slots * stride));
+    CKR(dalloc(ctx, &b.arena, arena_words));
     CKR(dalloc(ctx, &b.pat_parent, pat_cap));
     CKR(dalloc(ctx, &b.pat_item, pat_cap));
     CKR(dalloc(ctx, &b.pat_sup, pat_cap));
+    if (with_db) CKR(dalloc(ctx, &b.pat_db, pat_cap));
     CKR(dalloc(ctx, &b.root_cost, std::max<uint64_t>(1, n_roots)));
     CKR(dalloc(ctx, &b.st, 1));
     return CPM_OK;
 }
 
-static int mine_eclat(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o, cpm_result *res) {
-    cpm_stats &st = res->stats;
+// One scheduling unit of the deep phase: position p of top-level frame k.
+struct RootUnit {
+    uint32_t frame, p;
+    double key;  // larger first
+};
+
+// Cost-model features of root unit (class with m members, position p).
+// sup[e] = support of member e (the pair {class item, e}); sa = the class
+// item's support; N = transactions; ms = threshold; stride = tidset words.
+static void unit_features(float *x, uint32_t m, uint32_t p, const std::vector<double> &sup, double sa, double N,
+                          double ms, uint32_t stride) {
+    const uint32_t cnt = m - p - 1;
+    const double sp = sup[p];
+    const double inv_n = N > 0 ? 1.0 / N : 0.0;
+    const double msp = std::max(ms, 0.0);
+    // Later siblings, every one when few, an even sample otherwise.
+    const uint32_t step = cnt > 256 ? (cnt + 255) / 256 : 1;
+    double hist[4] = {0, 0, 0, 0}, mean = 0, seen = 0, surv = 0;
+    for (uint32_t q = p + 1; q < m; q += step) {
+        const double r = sa > 0 ? sup[q] / sa : 0.0;
+        hist[std::min(3, (int)(r * 4))] += 1;
+        mean += r;
+        surv += sp * r >= msp ? 1 : 0;
+        seen += 1;
+    }
+    const double scale = seen > 0 ? cnt / seen : 0.0;
+    surv *= scale;
+    x[0] = (float)std::log1p((double)cnt);
+    x[1] = (float)std::log1p((double)m);
+    x[2] = (float)((double)p / m);
+    x[3] = (float)(sp * inv_n);
+    x[4] = (float)(sa * inv_n);
+    x[5] = (float)(msp * inv_n);
+    x[6] = (float)std::log1p(N);
+    x[7] = (float)std::log1p((double)stride);
+    for (int i = 0; i < 4; ++i) x[8 + i] = (float)(seen > 0 ? hist[i] / seen : 0.0);
+    x[12] = (float)(seen > 0 ? mean / seen : 0.0);
+    x[13] = (float)(surv / (cnt + 1.0));
+    x[14] = (float)std::log1p(surv);
+    x[15] = (float)std::log1p(surv * surv * sp * inv_n);
+}
+
+// Learned order: the cost model's predicted subtree intersections, weighted
+// by the tidset length, largest first (the plain order is the fallback).
+static int order_units_learned(cpm_ctx *ctx, DevScope &ds, std::vector<RootUnit> &units,
+                               const std::vector<DFrame> &frames, const std::vector<float> &features) {
+    const uint64_t n = units.size();
+    float *d_x = nullptr, *d_y = nullptr, *d_p = nullptr;
+    CKR(ds.alloc(&d_x, n * cm::NF));
+    CKR(ds.alloc(&d_y, n));
+    CKR(ds.alloc(&d_p, cm::N_PARAMS));
+    CK(cudaMemcpyAsync(d_x, features.data(), n * cm::NF * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_p, ctx->model.data(), cm::N_PARAMS * 4, cudaMemcpyHostToDevice, ctx->stream));
+    k_mlp_forward<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(d_p, d_x, n, d_y, 1);
+    CK(cudaGetLastError());
+    std::vector<float> y(n);
+    CK(cudaMemcpyAsync(y.data(), d_y, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (RootUnit &u : units) {
+        const uint64_t id = frames[u.frame].root + u.p;
+        u.key = std::expm1((double)y[id]) * frames[u.frame].stride + (double)(frames[u.frame].m - u.p - 1);
+    }
+    std::stable_sort(units.begin(), units.end(), [](const RootUnit &a, const RootUnit &b) { return a.key > b.key; });
+    return CPM_OK;
+}
+
+// Eclat over a batch of databases (a single database is a batch of one).
+// Host syncs: frequent counts; pair counts; end of the deep phase.
+static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const long long *ms, const cpm_opts &o,
+                            cpm_result **res) {
+    cpm_stats st{};
     DevScope ds(ctx);
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
-    uint32_t *d_freq = nullptr;
-    uint32_t F = 0;
-    CKR(mine_singletons(ctx, db, ms, ds, &d_freq, F, st.kernel_launches));
-    st.n_frequent_items = F;
-    CK(cudaEventRecord(ctx->ev[1], ctx->stream));
-    // Pair level.
-    std::vector<uint32_t> cnt(F, 0);
-    std::vector<uint64_t> off(F + 1, 0);
-    uint32_t *d_C = nullptr, *d_cnt = nullptr;
-    uint64_t *d_off = nullptr;
-    if (F >= 2) {
-        CKR(pair_gram(ctx, db, d_freq, F, o, ds, &d_C, st));
-        CKR(ds.alloc(&d_cnt, F));
-        k_pair_count<<<(unsigned)(((uint64_t)F * 32 + 255) / 256), 256, 0, ctx->stream>>>(d_C, F, ms, d_cnt);
-        CK(cudaGetLastError());
-        st.kernel_launches++;
-        CK(cudaMemcpyAsync(cnt.data(), d_cnt, (size_t)F * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        for (uint32_t i = 0; i < F; ++i) off[i + 1] = off[i] + cnt[i];
+    // ---- singletons ----
+    std::vector<DbDesc> h(n_db);
+    uint64_t items_total = 0, max_stride = 2;
+    for (uint32_t d = 0; d < n_db; ++d) items_total += dbs[d]->n_items;
+    uint32_t *freq_all = nullptr, *d_F = nullptr;
+    DbDesc *d_desc = nullptr;
+    CKR(ds.alloc(&freq_all, items_total));
+    CKR(ds.alloc(&d_F, n_db));
+    CKR(ds.alloc(&d_desc, n_db));
+    std::vector<uint64_t> item_off(n_db + 1, 0);
+    for (uint32_t d = 0; d < n_db; ++d) {
+        cpm_db *db = dbs[d];
+        h[d] = DbDesc{};
+        h[d].bits = db->d_bits;
+        h[d].support = db->d_support;
+        h[d].freq = freq_all + item_off[d];
+        h[d].stride = db->stride;
+        h[d].n_items = db->n_items;
+        h[d].minsup = ms[d];
+        item_off[d + 1] = item_off[d] + db->n_items;
+        max_stride = std::max<uint64_t>(max_stride, db->stride);
     }
-    const uint64_t P2 = off[F];
-    st.n_frequent_pairs = P2;
-    // Top-level classes (cuEclat.py:195-200): rows with at least two members.
-    std::vector<uint32_t> roots;
-    for (uint32_t i = 0; i < F; ++i)
-        if (cnt[i] >= 2) roots.push_back(i);
-    // Plain scheduler: largest class first (more members, more descendants).
-    std::stable_sort(roots.begin(), roots.end(), [&](uint32_t a, uint32_t b) { return cnt[a] > cnt[b]; });
-    std::vector<DFrame> frames(roots.size());
-    std::vector<unsigned long long> init;
-    for (size_t k = 0; k < roots.size(); ++k) {
-        const uint32_t i = roots[k];
-        frames[k].mask = nullptr;  // filled on the device side below
-        frames[k].mem_off = off[i];
-        frames[k].m = cnt[i];
-        frames[k].root = (uint32_t)k;
+    CK(cudaMemcpyAsync(d_desc, h.data(), n_db * sizeof(DbDesc), cudaMemcpyHostToDevice, ctx->stream));
+    k_compact_frequent_b<<<n_db, 1024, 0, ctx->stream>>>(d_desc, d_F);
+    CK(cudaGetLastError());
+    st.kernel_launches++;
+    std::vector<uint32_t> F(n_db);
+    CK(cudaMemcpyAsync(F.data(), d_F, n_db * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    // ---- pair Grams ----
+    uint64_t rows = 0, c_total = 0;
+    std::vector<uint64_t> c_off(n_db, 0);
+    for (uint32_t d = 0; d < n_db; ++d) {
+        h[d].F = F[d];
+        h[d].row_base = rows;
+        rows += F[d];
+        c_off[d] = c_total;
+        c_total += (uint64_t)F[d] * F[d];
+        st.n_frequent_items += F[d];
     }
-    // Units of all top-level classes, interleaved by position so that the
-    // long first positions of the largest classes start first.
-    {
-        std::vector<std::pair<uint32_t, uint32_t>> units;
-        for (size_t k = 0; k < roots.size(); ++k)
-            for (uint32_t p = 0; p + 1 < cnt[roots[k]]; ++p) units.push_back({cnt[roots[k]] - p - 1, (uint32_t)k});
-        std::vector<uint64_t> idx(units.size());
-        std::iota(idx.begin(), idx.end(), 0ull);
-        std::stable_sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) { return units[a].first > units[b].first; });
-        init.reserve(units.size());
-        for (uint64_t u : idx) {
-            const uint32_t k = units[u].second;
-            const uint32_t p = cnt[roots[k]] - 1 - units[u].first;
-            init.push_back(((unsigned long long)k << 32) | p);
+    uint32_t *C_all = nullptr, *cnt_all = nullptr;
+    uint64_t *off_all = nullptr;
+    CKR(ds.alloc(&C_all, c_total));
+    CKR(ds.alloc(&cnt_all, rows));
+    CKR(ds.alloc(&off_all, rows + 1));
+    if (c_total) CK(cudaMemsetAsync(C_all, 0, c_total * 4, ctx->stream));
+    for (uint32_t d = 0; d < n_db; ++d) h[d].C = C_all + c_off[d];
+    CK(cudaMemcpyAsync(d_desc, h.data(), n_db * sizeof(DbDesc), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaEventRecord(ctx->ev[5], ctx->stream));
+    std::vector<BTile> tiles;
+    for (uint32_t d = 0; d < n_db; ++d) {
+        if (F[d] < 2) continue;
+        const bool tc = o.pair_engine == 1 ||
+                        (o.pair_engine == 0 && ctx->tc_ok && gram_tc_worthwhile(F[d], dbs[d]->n_tx));
+        if (tc) {
+            if (!ctx->tc_ok) return set_err(ctx, CPM_EINVAL, "the tensor-core Gram needs an sm_100 device");
+            CKR(gram_tc_run(ctx, ds, h[d].bits, h[d].stride, h[d].freq, F[d], h[d].C, st));
+            continue;
+        }
+        const uint32_t nt = (F[d] + 63) / 64;
+        const uint64_t n_tri = (uint64_t)nt * (nt + 1) / 2;
+        // Split K so the batch covers the GPU a few times over.
+        const uint64_t words = h[d].stride;
+        uint64_t ksplit = std::max<uint64_t>(1, (uint64_t)ctx->sms * 4 / std::max<uint64_t>(1, n_tri * n_db));
+        ksplit = std::min<uint64_t>(ksplit, std::max<uint64_t>(1, words / 64));
+        const uint64_t chunk = ((words + ksplit - 1) / ksplit + 15) / 16 * 16;
+        for (uint32_t ti = 0; ti < nt; ++ti)
+            for (uint32_t tj = ti; tj < nt; ++tj)
+                for (uint64_t k = 0; k < words; k += chunk) tiles.push_back({d, ti, tj, 0, k, std::min(words, k + chunk)});
+        st.pair_ops += 2ull * dbs[d]->n_tx * F[d] * (uint64_t)F[d];
+    }
+    if (!tiles.empty()) {
+        BTile *d_tiles = nullptr;
+        CKR(ds.alloc(&d_tiles, tiles.size()));
+        CK(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(BTile), cudaMemcpyHostToDevice, ctx->stream));
+        for (size_t t0 = 0; t0 < tiles.size(); t0 += 1u << 30) {
+            const unsigned nb = (unsigned)std::min<size_t>(tiles.size() - t0, 1u << 30);
+            k_gram_simt_b<<<nb, 256, 0, ctx->stream>>>(d_desc, d_tiles + t0);
+            CK(cudaGetLastError());
+            st.kernel_launches++;
         }
     }
-    const uint64_t stride = db->stride;
+    CK(cudaEventRecord(ctx->ev[6], ctx->stream));
+    std::vector<uint32_t> cnt(rows), hfreq(items_total);
+    if (rows) {
+        k_pair_count_b<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, ctx->stream>>>(d_desc, n_db, rows, cnt_all);
+        CK(cudaGetLastError());
+        st.kernel_launches++;
+        CK(cudaMemcpyAsync(cnt.data(), cnt_all, rows * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(hfreq.data(), freq_all, items_total * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    // Pair numbering and pattern ids: per database, singletons then pairs.
+    std::vector<uint64_t> off(rows + 1, 0);
+    for (uint64_t r = 0; r < rows; ++r) off[r + 1] = off[r] + cnt[r];
+    const uint64_t P2_total = off[rows];
+    st.n_frequent_pairs = P2_total;
+    uint64_t pat_next = 0;
+    for (uint32_t d = 0; d < n_db; ++d) {
+        h[d].pat_base = pat_next;
+        h[d].pair_base = off[h[d].row_base];
+        const uint64_t p2 = off[h[d].row_base + F[d]] - off[h[d].row_base];
+        pat_next += F[d] + p2;
+    }
+    const uint64_t base_patterns = pat_next;
+    CK(cudaMemcpyAsync(d_desc, h.data(), n_db * sizeof(DbDesc), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(off_all, off.data(), (rows + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    // ---- top-level classes (cuEclat.py:195-200) ----
+    std::vector<DFrame> frames;
+    for (uint32_t d = 0; d < n_db; ++d)
+        for (uint32_t i = 0; i < F[d]; ++i) {
+            const uint64_t r = h[d].row_base + i;
+            if (cnt[r] < 2) continue;
+            DFrame f;
+            f.mask = h[d].bits + (uint64_t)hfreq[item_off[d] + i] * h[d].stride;
+            f.mem_off = off[r];
+            f.m = cnt[r];
+            f.root = (uint32_t)frames.size();
+            f.stride = (uint32_t)h[d].stride;
+            f.db = d;
+            f.minsup = ms[d];
+            frames.push_back(f);
+        }
+    // Root units: position p of top-level frame k has id frames[k].root + p.
+    std::vector<RootUnit> units;
+    for (uint32_t k = 0; k < frames.size(); ++k) {
+        frames[k].root = (uint32_t)units.size();
+        for (uint32_t p = 0; p + 1 < frames[k].m; ++p) units.push_back({k, p, (double)(frames[k].m - p - 1)});
+    }
+    const bool learned = o.scheduler == CPM_SCHED_LEARNED && !ctx->model.empty();
+    const bool need_features = (learned || o.collect_trace) && !units.empty();
+    if (!learned)
+        std::stable_sort(units.begin(), units.end(), [](const RootUnit &a, const RootUnit &b) { return a.key > b.key; });
+    // ---- deep phase, grown and rerun on overflow ----
+    cpm_db *db0 = dbs[0];
     DeepBuffers b;
     b.owner = ctx;
-    // First guesses scale with the pair level; a database that was mined
-    // before starts from what it needed then.
-    uint64_t frames_cap = std::max<uint64_t>({1024, roots.size() * 8 + P2 * 2, db->hint_frames});
-    uint64_t members_cap = std::max<uint64_t>({4096, P2 * 16, db->hint_members});
-    uint64_t queue_cap = std::max<uint64_t>({4096, init.size() * 8 + P2 * 4, db->hint_queue});
-    uint64_t pat_cap = std::max<uint64_t>({4096, (F + P2) * 16, db->hint_patterns});
-    const uint64_t arena_budget = (uint64_t)(ctx->mem_free * 0.6) / (stride * 8);
-    uint64_t arena_slots = o.arena_bytes ? o.arena_bytes / (stride * 8)
+    const bool with_db = n_db > 1;
+    uint64_t frames_cap = std::max<uint64_t>({1024, frames.size() * 8 + P2_total * 2, n_db == 1 ? db0->hint_frames : 0});
+    uint64_t members_cap = std::max<uint64_t>({4096, P2_total * 16, n_db == 1 ? db0->hint_members : 0});
+    uint64_t queue_cap = std::max<uint64_t>({4096, units.size() * 8 + P2_total * 4, n_db == 1 ? db0->hint_queue : 0});
+    uint64_t pat_cap = std::max<uint64_t>({4096, base_patterns * 16, n_db == 1 ? db0->hint_patterns : 0});
+    const uint64_t arena_budget = (uint64_t)(ctx->mem_free * 0.6) / 8;
+    uint64_t arena_words = o.arena_bytes ? o.arena_bytes / 8
                                          : std::min<uint64_t>(arena_budget, std::max<uint64_t>(
-                                               {(uint64_t)ctx->sms * 8 * 4 + 1024, P2 * 8, db->hint_arena}));
-    arena_slots = std::max<uint64_t>(arena_slots, (uint64_t)ctx->sms * 8 * 2 + 64);
+                                               {(uint64_t)4096 * max_stride, P2_total * 8 * max_stride,
+                                                n_db == 1 ? db0->hint_arena : 0}));
     const uint64_t spin = o.spin_limit ? o.spin_limit : (1ull << 26);
-    // Shared-memory prefix when the tidset fits next to the static buffers.
-    const size_t prefix_bytes = stride * 8;
+    const size_t prefix_bytes = max_stride * 8;
     const bool smem_prefix = prefix_bytes <= 200 * 1024;
     if (smem_prefix && (ctx->deep_occ_smem < 0 || ctx->deep_occ_bytes != prefix_bytes)) {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_smem, k_deep<true>, 256, prefix_bytes));
@@ -600,58 +764,70 @@ static int mine_eclat(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o,
     } else if (!smem_prefix && ctx->deep_occ_global < 0) {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_global, k_deep<false>, 256, 0));
     }
-    // Up to four CTAs per SM keep enough loads in flight; more only add
-    // contention on the queue head.
+    // Up to four CTAs per SM keep enough loads in flight.
     const int cta_per_sm = std::min(4, std::max(1, smem_prefix ? ctx->deep_occ_smem : ctx->deep_occ_global));
     const unsigned grid = (unsigned)(ctx->sms * cta_per_sm);
     DeepState hs{};
+    std::vector<float> features;  // per root unit (cost-model inputs)
+    std::vector<unsigned long long> init;
     for (int attempt = 0;; ++attempt) {
-        CKR(grow(ctx, b, frames_cap, members_cap, queue_cap, arena_slots, pat_cap + F + P2, stride, roots.size()));
-        // Singletons and pairs land in the pattern arrays; classes get their masks.
-        if (F) {
-            k_emit_singletons<<<(F + 255) / 256, 256, 0, ctx->stream>>>(d_freq, F, db->d_support, b.pat_parent,
-                                                                        b.pat_item, b.pat_sup);
+        CKR(grow(ctx, b, frames_cap, members_cap, queue_cap, arena_words, pat_cap + base_patterns, units.size(),
+                 with_db));
+        if (members_cap < P2_total) return set_err(ctx, CPM_EINTERNAL, "member table too small");
+        if (rows) {
+            k_emit_b<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+                d_desc, n_db, rows, off_all, b.pat_parent, b.pat_item, b.pat_sup, b.pat_db, b.mem_pat, b.mem_item,
+                b.mem_bits);
             CK(cudaGetLastError());
             st.kernel_launches++;
         }
-        if (P2) {
-            if (!d_off) CKR(ds.alloc(&d_off, F + 1));
-            CK(cudaMemcpyAsync(d_off, off.data(), (F + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
-            if (b.members_cap < P2) return set_err(ctx, CPM_EINTERNAL, "member table too small");
-            k_pair_emit<<<(unsigned)(((uint64_t)F * 32 + 255) / 256), 256, 0, ctx->stream>>>(
-                d_C, F, ms, d_freq, d_off, db->d_bits, stride, b.pat_parent, b.pat_item, b.pat_sup, b.mem_pat,
-                b.mem_item, b.mem_bits);
-            CK(cudaGetLastError());
-            st.kernel_launches++;
-        }
-        if (roots.empty()) {
+        if (frames.empty()) {
             hs = DeepState{};
-            hs.n_patterns = F + P2;
+            hs.n_patterns = base_patterns;
             break;
         }
-        // Frame masks point at the class item's tidset.
-        std::vector<uint32_t> hfreq(F);
-        CK(cudaMemcpyAsync(hfreq.data(), d_freq, (size_t)F * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        for (size_t k = 0; k < roots.size(); ++k) frames[k].mask = db->d_bits + (uint64_t)hfreq[roots[k]] * stride;
-        CK(cudaMemcpyAsync(b.frames, frames.data(), frames.size() * sizeof(DFrame), cudaMemcpyHostToDevice, ctx->stream));
+        if (need_features && features.empty()) {
+            // Features read the supports of every class's members (the pairs)
+            // and of the class items (the singletons).
+            std::vector<uint32_t> pat_sup_h(base_patterns);
+            CK(cudaMemcpyAsync(pat_sup_h.data(), b.pat_sup, base_patterns * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            features.assign(units.size() * cm::NF, 0.f);
+            for (uint32_t k = 0; k < frames.size(); ++k) {
+                const DFrame &f = frames[k];
+                const DbDesc &D = h[f.db];
+                const uint64_t row = std::upper_bound(off.begin(), off.end(), f.mem_off) - off.begin() - 1;
+                const double sa = pat_sup_h[D.pat_base + (row - D.row_base)];
+                std::vector<double> sup(f.m);
+                for (uint32_t e = 0; e < f.m; ++e) sup[e] = pat_sup_h[D.pat_base + D.F + (f.mem_off + e - D.pair_base)];
+                for (uint32_t p = 0; p + 1 < f.m; ++p)
+                    unit_features(&features[(uint64_t)(f.root + p) * cm::NF], f.m, p, sup, sa,
+                                  (double)dbs[f.db]->n_tx, (double)ms[f.db], f.stride);
+            }
+            if (learned) CKR(order_units_learned(ctx, ds, units, frames, features));
+        }
+        if (init.empty())
+            for (const RootUnit &u : units) init.push_back(((unsigned long long)u.frame << 32) | u.p);
+        CK(cudaMemcpyAsync(b.frames, frames.data(), frames.size() * sizeof(DFrame), cudaMemcpyHostToDevice,
+                           ctx->stream));
         CK(cudaMemsetAsync(b.queue, 0xff, b.queue_cap * 8, ctx->stream));
         CK(cudaMemcpyAsync(b.queue, init.data(), init.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemsetAsync(b.root_cost, 0, std::max<size_t>(1, roots.size()) * 8, ctx->stream));
+        CK(cudaMemsetAsync(b.root_cost, 0, std::max<size_t>(1, units.size()) * 8, ctx->stream));
         hs = DeepState{};
         hs.q_tail = init.size();
         hs.pending = init.size();
-        hs.n_patterns = F + P2;
-        hs.n_frames = roots.size();
-        hs.n_members = P2;
+        hs.n_patterns = base_patterns;
+        hs.n_frames = frames.size();
+        hs.n_members = P2_total;
         CK(cudaMemcpyAsync(b.st, &hs, sizeof hs, cudaMemcpyHostToDevice, ctx->stream));
         DeepParams P;
         P.frames = b.frames; P.frames_cap = b.frames_cap;
         P.mem_pat = b.mem_pat; P.mem_item = b.mem_item; P.mem_bits = b.mem_bits; P.members_cap = b.members_cap;
         P.queue = b.queue; P.queue_cap = b.queue_cap;
-        P.arena = b.arena; P.arena_slots = b.arena_slots;
-        P.pat_parent = b.pat_parent; P.pat_item = b.pat_item; P.pat_sup = b.pat_sup; P.pat_cap = b.pat_cap;
-        P.root_cost = b.root_cost; P.st = b.st; P.stride = stride; P.minsup = ms; P.spin_limit = spin;
+        P.arena = b.arena; P.arena_words = b.arena_words;
+        P.pat_parent = b.pat_parent; P.pat_item = b.pat_item; P.pat_sup = b.pat_sup; P.pat_db = b.pat_db;
+        P.pat_cap = b.pat_cap;
+        P.root_cost = b.root_cost; P.st = b.st; P.max_stride = max_stride; P.spin_limit = spin;
         CK(cudaEventRecord(ctx->ev[2], ctx->stream));
         if (smem_prefix) k_deep<true><<<grid, 256, prefix_bytes, ctx->stream>>>(P);
         else k_deep<false><<<grid, 256, 0, ctx->stream>>>(P);
@@ -670,14 +846,11 @@ static int mine_eclat(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o,
                            "members %llu/%llu, queue %llu/%llu, arena %llu/%llu, patterns %llu/%llu)",
                            hs.error, hs.n_frames, (unsigned long long)b.frames_cap, hs.n_members,
                            (unsigned long long)b.members_cap, hs.q_tail, (unsigned long long)b.queue_cap,
-                           hs.arena_next, (unsigned long long)b.arena_slots, hs.n_patterns,
+                           hs.arena_next, (unsigned long long)b.arena_words, hs.n_patterns,
                            (unsigned long long)b.pat_cap);
         if (getenv("CPM_DEBUG"))
-            fprintf(stderr, "cpm: deep retry %d error 0x%x frames %llu/%llu members %llu/%llu queue %llu/%llu "
-                    "arena %llu/%llu patterns %llu/%llu\n", attempt, hs.error, hs.n_frames,
-                    (unsigned long long)b.frames_cap, hs.n_members, (unsigned long long)b.members_cap, hs.q_tail,
-                    (unsigned long long)b.queue_cap, hs.arena_next, (unsigned long long)b.arena_slots,
-                    hs.n_patterns, (unsigned long long)b.pat_cap);
+            fprintf(stderr, "cpm: deep retry %d error 0x%x frames %llu members %llu queue %llu arena %llu patterns %llu\n",
+                    attempt, hs.error, hs.n_frames, hs.n_members, hs.q_tail, hs.arena_next, hs.n_patterns);
         st.retries++;
         // Counters at the failure are lower bounds of the final need: grow
         // every buffer past them (one overflow usually means several).
@@ -685,41 +858,110 @@ static int mine_eclat(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o,
         members_cap = std::max<uint64_t>(members_cap * 4, hs.n_members * 4);
         queue_cap = std::max<uint64_t>(queue_cap * 4, hs.q_tail * 4);
         pat_cap = std::max<uint64_t>(pat_cap * 4, hs.n_patterns * 4);
-        if (hs.error & DEEP_ERR_ARENA) {
-            if (arena_slots >= arena_budget)
-                return set_err(ctx, CPM_EOVERFLOW, "deep-level arena exceeds device memory (%llu slots)",
-                               (unsigned long long)arena_slots);
-        }
-        arena_slots = std::min<uint64_t>(arena_budget, std::max<uint64_t>(arena_slots * 4, hs.arena_next * 4));
+        if ((hs.error & DEEP_ERR_ARENA) && arena_words >= arena_budget)
+            return set_err(ctx, CPM_EOVERFLOW, "deep-level arena exceeds device memory (%llu words)",
+                           (unsigned long long)arena_words);
+        arena_words = std::min<uint64_t>(arena_budget, std::max<uint64_t>(arena_words * 4, hs.arena_next * 4));
     }
-    // Remember what this database needed so that the next mine() starts there.
-    db->hint_frames = std::max<uint64_t>(db->hint_frames, hs.n_frames + hs.n_frames / 4 + 64);
-    db->hint_members = std::max<uint64_t>(db->hint_members, hs.n_members + hs.n_members / 4 + 64);
-    db->hint_queue = std::max<uint64_t>(db->hint_queue, hs.q_tail + hs.q_tail / 4 + 64);
-    db->hint_patterns = std::max<uint64_t>(db->hint_patterns, hs.n_patterns + hs.n_patterns / 4 + 64);
-    db->hint_arena = std::max<uint64_t>(db->hint_arena, hs.arena_next + hs.arena_next / 4 + 64);
+    if (n_db == 1) {
+        // Remember what this database needed so that the next mine() starts there.
+        db0->hint_frames = std::max<uint64_t>(db0->hint_frames, hs.n_frames + hs.n_frames / 4 + 64);
+        db0->hint_members = std::max<uint64_t>(db0->hint_members, hs.n_members + hs.n_members / 4 + 64);
+        db0->hint_queue = std::max<uint64_t>(db0->hint_queue, hs.q_tail + hs.q_tail / 4 + 64);
+        db0->hint_patterns = std::max<uint64_t>(db0->hint_patterns, hs.n_patterns + hs.n_patterns / 4 + 64);
+        db0->hint_arena = std::max<uint64_t>(db0->hint_arena, hs.arena_next + hs.arena_next / 4 + 64);
+    }
     const uint64_t n = hs.n_patterns;
-    res->parent.resize(n);
-    res->item.resize(n);
-    res->support.resize(n);
+    std::vector<uint32_t> par(n), item(n), sup(n), pdb;
     if (n) {
-        CK(cudaMemcpyAsync(res->parent.data(), b.pat_parent, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(res->item.data(), b.pat_item, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(res->support.data(), b.pat_sup, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(par.data(), b.pat_parent, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(item.data(), b.pat_item, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(sup.data(), b.pat_sup, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        if (with_db) {
+            pdb.resize(n);
+            CK(cudaMemcpyAsync(pdb.data(), b.pat_db, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+    }
+    std::vector<unsigned long long> rc;
+    if (o.collect_trace && !units.empty()) {
+        rc.resize(units.size());
+        CK(cudaMemcpyAsync(rc.data(), b.root_cost, units.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
     }
     CK(cudaEventRecord(ctx->ev[4], ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    b.release(ctx);
-    st.n_patterns = n;
     st.frames = hs.n_frames;
     st.work_items = hs.work_items;
     st.intersections = hs.intersections;
     st.bytes_alg = hs.bytes_alg;
-    st.ms_pairs = F >= 2 ? elapsed_ms(ctx, 5, 6) : 0.0;
-    st.ms_deep = roots.empty() ? 0.0 : elapsed_ms(ctx, 2, 3);
+    st.ms_pairs = rows ? elapsed_ms(ctx, 5, 6) : 0.0;
+    st.ms_deep = frames.empty() ? 0.0 : elapsed_ms(ctx, 2, 3);
     st.ms_total = elapsed_ms(ctx, 0, 4);
     st.deep_gbs = st.ms_deep > 0 ? st.bytes_alg / (st.ms_deep * 1e6) : 0.0;
     st.pair_tops = st.ms_pairs > 0 ? st.pair_ops / (st.ms_pairs * 1e9) : 0.0;
+    st.n_patterns = n;
+    // ---- split the pattern tree per database (parents precede children) ----
+    if (n_db == 1) {
+        res[0]->parent.swap(par);
+        res[0]->item.swap(item);
+        res[0]->support.swap(sup);
+    } else {
+        std::vector<uint32_t> local(n);
+        for (uint32_t d = 0; d < n_db; ++d) {
+            res[d]->parent.clear(); res[d]->item.clear(); res[d]->support.clear();
+        }
+        for (uint64_t g = 0; g < n; ++g) {
+            cpm_result *r = res[pdb[g]];
+            local[g] = (uint32_t)r->parent.size();
+            r->parent.push_back(par[g] == 0xffffffffu ? 0xffffffffu : local[par[g]]);
+            r->item.push_back(item[g]);
+            r->support.push_back(sup[g]);
+        }
+    }
+    for (uint32_t d = 0; d < n_db; ++d) {
+        res[d]->stats = st;
+        res[d]->stats.n_patterns = res[d]->parent.size();
+        if (!rc.empty()) {
+            res[d]->trace_x.clear();
+            res[d]->trace_y.clear();
+            for (uint32_t k = 0; k < frames.size(); ++k) {
+                if (frames[k].db != d) continue;
+                for (uint32_t p = 0; p + 1 < frames[k].m; ++p) {
+                    const uint64_t u = frames[k].root + p;
+                    res[d]->trace_x.insert(res[d]->trace_x.end(), &features[u * cm::NF], &features[u * cm::NF] + cm::NF);
+                    res[d]->trace_y.push_back((float)std::log1p((double)rc[u]));
+                }
+            }
+        }
+    }
+    return CPM_OK;
+}
+
+static int mine_eclat(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o, cpm_result *res) {
+    return mine_eclat_batch(ctx, &db, 1, &ms, o, &res);
+}
+
+
+// Exclusive sum of n uint32 counts into uint64 offsets (CUB decoupled
+// look-back scan); *total gets the sum (one small read-back, synchronous).
+struct U32ToU64 {
+    __host__ __device__ uint64_t operator()(uint32_t v) const { return v; }
+};
+
+static int scan_u32(cpm_ctx *ctx, DevScope &ds, const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *total) {
+    *total = 0;
+    if (!n) return CPM_OK;
+    thrust::transform_iterator<U32ToU64, const uint32_t *, uint64_t> it(in, U32ToU64());
+    size_t bytes = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, it, out, (int64_t)n, ctx->stream));
+    void *tmp = nullptr;
+    CKR(ds.alloc(reinterpret_cast<unsigned char **>(&tmp), bytes));
+    CK(cub::DeviceScan::ExclusiveSum(tmp, bytes, it, out, (int64_t)n, ctx->stream));
+    uint64_t last_off = 0;
+    uint32_t last_in = 0;
+    CK(cudaMemcpyAsync(&last_off, out + n - 1, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&last_in, in + n - 1, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *total = last_off + last_in;
     return CPM_OK;
 }
 
@@ -810,48 +1052,55 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
                 return set_err(ctx, CPM_EINVAL, "patterns longer than 64 items are not supported");
             }
             const uint32_t w = k + 1;
-            uint32_t *cnt = nullptr, *cand = nullptr, *left = nullptr, *sup = nullptr, *flag = nullptr;
-            uint64_t *off = nullptr, *pos = nullptr;
             DevScope lvl(ctx);
-            CKR(lvl.alloc(&cnt, n));
-            CKR(lvl.alloc(&off, n));
-            const unsigned jb = (unsigned)((n + 127) / 128);
-            k_apriori_join<0><<<jb, 128, 0, ctx->stream>>>(L, n, k, cnt, nullptr, nullptr, nullptr);
+            // Prefix groups and join partners of every row.
+            uint32_t *gflag = nullptr, *partners = nullptr;
+            uint64_t *gid = nullptr, *gfirst = nullptr, *poff = nullptr;
+            CKR(lvl.alloc(&gflag, n));
+            CKR(lvl.alloc(&gid, n));
+            CKR(lvl.alloc(&partners, n));
+            CKR(lvl.alloc(&poff, n));
+            const unsigned nb = (unsigned)((n + 255) / 256);
+            k_group_start<<<nb, 256, 0, ctx->stream>>>(L, n, k, gflag);
             CK(cudaGetLastError());
-            k_scan_u32<<<1, 1024, 0, ctx->stream>>>(cnt, n, off, d_total);
+            uint64_t n_groups = 0;
+            CKR(scan_u32(ctx, lvl, gflag, gid, n, &n_groups));
+            CKR(lvl.alloc(&gfirst, n_groups));
+            k_group_first<<<nb, 256, 0, ctx->stream>>>(gflag, gid, n, gfirst);
             CK(cudaGetLastError());
-            uint64_t nc = 0;
-            CK(cudaMemcpyAsync(&nc, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
-            st.kernel_launches += 2;
-            if (!nc) break;
-            CKR(lvl.alloc(&cand, nc * w));
-            CKR(lvl.alloc(&left, nc));
-            CKR(lvl.alloc(&sup, nc));
-            CKR(lvl.alloc(&flag, nc));
-            CKR(lvl.alloc(&pos, nc));
-            k_apriori_join<1><<<jb, 128, 0, ctx->stream>>>(L, n, k, nullptr, off, cand, left);
+            k_partners<<<nb, 256, 0, ctx->stream>>>(gflag, gid, gfirst, n_groups, n, partners);
             CK(cudaGetLastError());
-            k_count_kway<<<(unsigned)((nc * 32 + 255) / 256), 256, 0, ctx->stream>>>(db->d_bits, db->stride, cand,
-                                                                                     nc, w, sup);
+            uint64_t n_pairs = 0;
+            CKR(scan_u32(ctx, lvl, partners, poff, n, &n_pairs));
+            st.kernel_launches += 7;
+            if (!n_pairs) break;
+            // Join, prune, count, keep.
+            uint32_t *cand = nullptr, *left = nullptr, *okf = nullptr, *sup = nullptr, *pass = nullptr;
+            uint64_t *pos = nullptr;
+            CKR(lvl.alloc(&cand, n_pairs * w));
+            CKR(lvl.alloc(&left, n_pairs));
+            CKR(lvl.alloc(&okf, n_pairs));
+            CKR(lvl.alloc(&sup, n_pairs));
+            CKR(lvl.alloc(&pass, n_pairs));
+            CKR(lvl.alloc(&pos, n_pairs));
+            k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, n, k, poff, n_pairs, cand,
+                                                                                     left, okf);
             CK(cudaGetLastError());
-            k_apriori_flags<<<(unsigned)((nc + 255) / 256), 256, 0, ctx->stream>>>(sup, nc, ms, flag);
-            CK(cudaGetLastError());
-            k_scan_u32<<<1, 1024, 0, ctx->stream>>>(flag, nc, pos, d_total);
+            k_count_pruned<<<(unsigned)((n_pairs * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+                db->d_bits, db->stride, cand, okf, n_pairs, w, ms, sup, pass);
             CK(cudaGetLastError());
             uint64_t nk = 0;
-            CK(cudaMemcpyAsync(&nk, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
+            CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, &nk));
             st.kernel_launches += 4;
-            st.intersections += nc * (w - 1);
-            st.bytes_alg += nc * w * db->stride * 8;
+            st.intersections += n_pairs * (w - 1);
+            st.bytes_alg += n_pairs * w * db->stride * 8;
             uint32_t *L2 = nullptr, *pid2 = nullptr;
             CKR(patterns_reserve(ctx, pa, n_pat, n_pat + nk));
             CKR(dalloc(ctx, &L2, std::max<uint64_t>(1, nk) * w));
             CKR(dalloc(ctx, &pid2, std::max<uint64_t>(1, nk)));
             if (nk) {
-                k_apriori_keep<<<(unsigned)((nc + 255) / 256), 256, 0, ctx->stream>>>(
-                    cand, left, sup, flag, pos, nc, w, pid, n_pat, L2, pid2, pa.parent, pa.item, pa.sup);
+                k_apriori_keep<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(
+                    cand, left, sup, pass, pos, n_pairs, w, pid, n_pat, L2, pid2, pa.parent, pa.item, pa.sup);
                 CK(cudaGetLastError());
                 st.kernel_launches++;
             }
@@ -912,6 +1161,36 @@ extern "C" int cpm_mine(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, int algo, con
     return CPM_OK;
 }
 
+extern "C" int cpm_mine_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const int64_t *min_sups,
+                              const cpm_opts *opts, cpm_result **out) {
+    if (!ctx || !out || (n_db && (!dbs || !min_sups))) return CPM_EINVAL;
+    for (uint32_t d = 0; d < n_db; ++d) {
+        out[d] = nullptr;
+        if (!dbs[d] || dbs[d]->ctx != ctx) return set_err(ctx, CPM_EINVAL, "database %u is not on this context", d);
+    }
+    if (!n_db) return CPM_OK;
+    CK(cudaSetDevice(ctx->device));
+    cpm_opts o;
+    if (opts) o = *opts;
+    else cpm_default_opts(&o);
+    std::vector<long long> ms(n_db);
+    std::vector<cpm_result *> res(n_db);
+    for (uint32_t d = 0; d < n_db; ++d) {
+        ms[d] = (long long)std::max<int64_t>(std::min<int64_t>(min_sups[d], (int64_t)1 << 40), -1);
+        res[d] = new cpm_result();
+        res[d]->algo = CPM_ECLAT;
+    }
+    const int r = mine_eclat_batch(ctx, dbs, n_db, ms.data(), o, res.data());
+    if (r != CPM_OK) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaGetLastError();
+        for (cpm_result *x : res) delete x;
+        return r;
+    }
+    for (uint32_t d = 0; d < n_db; ++d) out[d] = res[d];
+    return CPM_OK;
+}
+
 extern "C" int cpm_result_size(const cpm_result *res, uint64_t *n_patterns, uint64_t *n_item_slots) {
     if (!res) return CPM_EINVAL;
     const uint64_t n = res->parent.size();
@@ -967,7 +1246,64 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
     std::vector<uint64_t> idx(n);
     std::iota(idx.begin(), idx.end(), 0ull);
     auto pat = [&](uint64_t k) { return flat.data() + start[k]; };
-    if (order == CPM_ORDER_APRIORI) {
+    // A tree whose every pattern extends its parent by a larger item is the
+    // prefix tree of the patterns (the device builds it so); then both
+    // insertion orders are plain traversals.  Otherwise sort with the keys.
+    bool prefix_tree = true;
+    for (uint64_t k = 0; k < n && prefix_tree; ++k)
+        if (res->parent[k] != 0xffffffffu && res->item[k] <= res->item[res->parent[k]]) prefix_tree = false;
+    if (prefix_tree && order != CPM_ORDER_NONE) {
+        // children lists, each sorted by item
+        std::vector<uint64_t> coff(n + 2, 0), roots;
+        for (uint64_t k = 0; k < n; ++k)
+            if (res->parent[k] == 0xffffffffu) roots.push_back(k);
+            else coff[res->parent[k] + 1]++;
+        for (uint64_t k = 0; k < n; ++k) coff[k + 1] += coff[k];
+        std::vector<uint64_t> kids(coff[n]), fill(coff.begin(), coff.begin() + n);
+        for (uint64_t k = 0; k < n; ++k)
+            if (res->parent[k] != 0xffffffffu) kids[fill[res->parent[k]]++] = k;
+        auto by_item = [&](uint64_t a, uint64_t b) { return res->item[a] < res->item[b]; };
+        std::sort(roots.begin(), roots.end(), by_item);
+        for (uint64_t k = 0; k < n; ++k)
+            if (coff[k + 1] - coff[k] > 1) std::sort(kids.begin() + coff[k], kids.begin() + coff[k + 1], by_item);
+        uint64_t w = 0;
+        if (order == CPM_ORDER_APRIORI) {
+            // by length, then tuple: breadth first, children in item order
+            std::vector<uint64_t> level(roots), next;
+            while (!level.empty()) {
+                next.clear();
+                for (uint64_t v : level) {
+                    idx[w++] = v;
+                    next.insert(next.end(), kids.begin() + coff[v], kids.begin() + coff[v + 1]);
+                }
+                level.swap(next);
+            }
+        } else {
+            // singletons, pairs, then for every pair: its children, then each
+            // child's subtree in the same way (cuEclat.py:211-245)
+            for (uint64_t r : roots) idx[w++] = r;
+            std::vector<uint64_t> pairs;
+            for (uint64_t r : roots)
+                for (uint64_t c = coff[r]; c < coff[r + 1]; ++c) pairs.push_back(kids[c]);
+            for (uint64_t q : pairs) idx[w++] = q;
+            std::vector<std::pair<uint64_t, uint64_t>> stack;  // (node, next child to descend)
+            for (uint64_t q : pairs) {
+                for (uint64_t c = coff[q]; c < coff[q + 1]; ++c) idx[w++] = kids[c];
+                stack.push_back({q, coff[q]});
+                while (!stack.empty()) {
+                    auto &top = stack.back();
+                    if (top.second == coff[top.first + 1]) {
+                        stack.pop_back();
+                        continue;
+                    }
+                    const uint64_t child = kids[top.second++];
+                    for (uint64_t c = coff[child]; c < coff[child + 1]; ++c) idx[w++] = kids[c];
+                    stack.push_back({child, coff[child]});
+                }
+            }
+        }
+        if (w != n) return CPM_EINTERNAL;
+    } else if (order == CPM_ORDER_APRIORI) {
         std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
             if (depth[a] != depth[b]) return depth[a] < depth[b];
             return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
@@ -1069,6 +1405,160 @@ extern "C" int cpm_intersect_extensions(cpm_ctx *ctx, const uint32_t *d_prefix, 
     k_ref_intersect<<<(unsigned)((n_extensions * 32 + 255) / 256), 256, 0, ctx->stream>>>(
         d_prefix, d_extensions, words32, n_extensions, d_out, reinterpret_cast<unsigned long long *>(d_supports));
     CK(cudaGetLastError());
+    return CPM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// learned cost model (scheduler)
+// ---------------------------------------------------------------------------
+
+extern "C" int cpm_costmodel_params(uint32_t *n_features, uint32_t *n_params) {
+    if (n_features) *n_features = cm::NF;
+    if (n_params) *n_params = cm::N_PARAMS;
+    return CPM_OK;
+}
+
+extern "C" int cpm_costmodel_gradient(cpm_ctx *ctx, const float *params, const float *X, const float *y, uint64_t n,
+                                      float *grad, float *loss) {
+    if (!ctx || !params || !grad || (n && (!X || !y))) return CPM_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    DevScope ds(ctx);
+    float *d_p = nullptr, *d_x = nullptr, *d_t = nullptr, *d_g = nullptr, *d_l = nullptr;
+    CKR(ds.alloc(&d_p, cm::N_PARAMS));
+    CKR(ds.alloc(&d_x, std::max<uint64_t>(1, n) * cm::NF));
+    CKR(ds.alloc(&d_t, std::max<uint64_t>(1, n)));
+    CKR(ds.alloc(&d_g, cm::TRAIN_COUNT));
+    CKR(ds.alloc(&d_l, 1));
+    std::vector<float> t(n);
+    const float ysd = params[cm::OFF_YSD] != 0.f ? params[cm::OFF_YSD] : 1.f;
+    for (uint64_t i = 0; i < n; ++i) t[i] = (y[i] - params[cm::OFF_YMU]) / ysd;
+    CK(cudaMemcpyAsync(d_p, params, cm::N_PARAMS * 4, cudaMemcpyHostToDevice, ctx->stream));
+    if (n) {
+        CK(cudaMemcpyAsync(d_x, X, n * cm::NF * 4, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(d_t, t.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CK(cudaMemsetAsync(d_g, 0, cm::TRAIN_COUNT * 4, ctx->stream));
+    CK(cudaMemsetAsync(d_l, 0, 4, ctx->stream));
+    if (n) {
+        k_mlp_backward<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(d_p, d_x, d_t, n, d_g, d_l);
+        CK(cudaGetLastError());
+    }
+    std::vector<float> g(cm::TRAIN_COUNT);
+    float l = 0.f;
+    CK(cudaMemcpyAsync(g.data(), d_g, cm::TRAIN_COUNT * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&l, d_l, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    // d/dtheta of (1 / 2n) sum (f - t)^2
+    const float inv = n ? 1.f / (float)n : 0.f;
+    for (int i = 0; i < cm::N_PARAMS; ++i) grad[i] = 0.f;
+    for (int i = 0; i < cm::TRAIN_COUNT; ++i) grad[cm::TRAIN_FIRST + i] = g[i] * inv;
+    if (loss) *loss = 0.5f * l * inv;
+    return CPM_OK;
+}
+
+static uint64_t splitmix(uint64_t &s) {
+    uint64_t z = (s += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+static double gauss(uint64_t &s) {
+    const double u1 = ((splitmix(s) >> 11) + 1.0) / 9007199254740993.0;
+    const double u2 = (splitmix(s) >> 11) / 9007199254740992.0;
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+}
+
+extern "C" int cpm_costmodel_train(cpm_ctx *ctx, const float *X, const float *y, uint64_t n, uint32_t epochs,
+                                   float lr, uint64_t seed, float *params, float *loss_history) {
+    if (!ctx || !params || !n || !X || !y || !epochs) return CPM_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    // Standardisation from the training data; He-initialised weights.
+    std::vector<float> P(cm::N_PARAMS, 0.f);
+    for (int f = 0; f < cm::NF; ++f) {
+        double m = 0, v = 0;
+        for (uint64_t i = 0; i < n; ++i) m += X[i * cm::NF + f];
+        m /= n;
+        for (uint64_t i = 0; i < n; ++i) v += (X[i * cm::NF + f] - m) * (X[i * cm::NF + f] - m);
+        const double sd = std::sqrt(v / n);
+        P[cm::OFF_MU + f] = (float)m;
+        P[cm::OFF_IS + f] = (float)(sd > 1e-6 ? 1.0 / sd : 0.0);
+    }
+    double ym = 0, yv = 0;
+    for (uint64_t i = 0; i < n; ++i) ym += y[i];
+    ym /= n;
+    for (uint64_t i = 0; i < n; ++i) yv += (y[i] - ym) * (y[i] - ym);
+    const double ysd = std::max(std::sqrt(yv / n), 1e-6);
+    P[cm::OFF_YMU] = (float)ym;
+    P[cm::OFF_YSD] = (float)ysd;
+    uint64_t rng = seed * 0x2545F4914F6CDD1Dull + 1;
+    for (int i = 0; i < cm::H * cm::NF; ++i) P[cm::OFF_W1 + i] = (float)(gauss(rng) * std::sqrt(2.0 / cm::NF));
+    for (int i = 0; i < cm::H; ++i) P[cm::OFF_W2 + i] = (float)(gauss(rng) * std::sqrt(1.0 / cm::H));
+    std::vector<float> t(n);
+    for (uint64_t i = 0; i < n; ++i) t[i] = (float)((y[i] - ym) / ysd);
+    DevScope ds(ctx);
+    float *d_p = nullptr, *d_x = nullptr, *d_t = nullptr, *d_g = nullptr, *d_m1 = nullptr, *d_m2 = nullptr,
+          *d_l = nullptr;
+    CKR(ds.alloc(&d_p, cm::N_PARAMS));
+    CKR(ds.alloc(&d_x, n * cm::NF));
+    CKR(ds.alloc(&d_t, n));
+    CKR(ds.alloc(&d_g, cm::TRAIN_COUNT));
+    CKR(ds.alloc(&d_m1, cm::TRAIN_COUNT));
+    CKR(ds.alloc(&d_m2, cm::TRAIN_COUNT));
+    CKR(ds.alloc(&d_l, epochs));
+    CK(cudaMemcpyAsync(d_p, P.data(), cm::N_PARAMS * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_x, X, n * cm::NF * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_t, t.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(d_m1, 0, cm::TRAIN_COUNT * 4, ctx->stream));
+    CK(cudaMemsetAsync(d_m2, 0, cm::TRAIN_COUNT * 4, ctx->stream));
+    CK(cudaMemsetAsync(d_l, 0, epochs * 4, ctx->stream));
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    for (uint32_t e = 0; e < epochs; ++e) {
+        CK(cudaMemsetAsync(d_g, 0, cm::TRAIN_COUNT * 4, ctx->stream));
+        k_mlp_backward<<<blocks, 256, 0, ctx->stream>>>(d_p, d_x, d_t, n, d_g, d_l + e);
+        k_adam<<<(cm::TRAIN_COUNT + 255) / 256, 256, 0, ctx->stream>>>(d_p, d_g, d_m1, d_m2, lr, 1.f / (float)n,
+                                                                     (int)e + 1);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(params, d_p, cm::N_PARAMS * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<float> lh(epochs);
+    CK(cudaMemcpyAsync(lh.data(), d_l, epochs * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (loss_history)
+        for (uint32_t e = 0; e < epochs; ++e) loss_history[e] = 0.5f * lh[e] / (float)n;
+    return CPM_OK;
+}
+
+extern "C" int cpm_costmodel_predict(cpm_ctx *ctx, const float *params, const float *X, uint64_t n, float *y) {
+    if (!ctx || !params || (n && (!X || !y))) return CPM_EINVAL;
+    if (!n) return CPM_OK;
+    CK(cudaSetDevice(ctx->device));
+    DevScope ds(ctx);
+    float *d_p = nullptr, *d_x = nullptr, *d_y = nullptr;
+    CKR(ds.alloc(&d_p, cm::N_PARAMS));
+    CKR(ds.alloc(&d_x, n * cm::NF));
+    CKR(ds.alloc(&d_y, n));
+    CK(cudaMemcpyAsync(d_p, params, cm::N_PARAMS * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_x, X, n * cm::NF * 4, cudaMemcpyHostToDevice, ctx->stream));
+    k_mlp_forward<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(d_p, d_x, n, d_y, 1);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(y, d_y, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CPM_OK;
+}
+
+extern "C" int cpm_costmodel_set(cpm_ctx *ctx, const float *params) {
+    if (!ctx) return CPM_EINVAL;
+    if (!params) ctx->model.clear();
+    else ctx->model.assign(params, params + cm::N_PARAMS);
+    return CPM_OK;
+}
+
+extern "C" int cpm_result_trace(const cpm_result *res, float *X, float *y, uint64_t *n) {
+    if (!res || !n) return CPM_EINVAL;
+    *n = res->trace_y.size();
+    if (X) std::copy(res->trace_x.begin(), res->trace_x.end(), X);
+    if (y) std::copy(res->trace_y.begin(), res->trace_y.end(), y);
     return CPM_OK;
 }
 
@@ -1254,6 +1744,9 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
         frames[k].mem_off = off[roots[k]];
         frames[k].m = cnt[roots[k]];
         frames[k].root = (uint32_t)k;
+        frames[k].stride = (uint32_t)stride;
+        frames[k].db = 0;
+        frames[k].minsup = ms;
     }
     // Every call shares the scratch: reset what the kernel expects cleared.
     CK(cudaMemcpyAsync(d_frames, frames.data(), frames.size() * sizeof(DFrame), cudaMemcpyHostToDevice, ctx->stream));
@@ -1271,9 +1764,9 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     P.frames = d_frames; P.frames_cap = frames_cap;
     P.mem_pat = d_mem_pat; P.mem_item = d_mem_item; P.mem_bits = d_mem_bits; P.members_cap = members_cap;
     P.queue = d_queue; P.queue_cap = queue_cap;
-    P.arena = d_arena; P.arena_slots = arena_slots;
-    P.pat_parent = d_parent; P.pat_item = d_item; P.pat_sup = d_support; P.pat_cap = capacity;
-    P.root_cost = d_root_cost; P.st = d_st; P.stride = stride; P.minsup = ms; P.spin_limit = 1ull << 26;
+    P.arena = d_arena; P.arena_words = arena_slots * stride;
+    P.pat_parent = d_parent; P.pat_item = d_item; P.pat_sup = d_support; P.pat_db = nullptr; P.pat_cap = capacity;
+    P.root_cost = d_root_cost; P.st = d_st; P.max_stride = stride; P.spin_limit = 1ull << 26;
     // Each warp keeps one scratch tidset: leave at least half the arena to children.
     const size_t prefix_bytes = stride * 8;
     const bool smem_prefix = prefix_bytes <= 200 * 1024;

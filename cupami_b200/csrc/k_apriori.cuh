@@ -67,6 +67,90 @@ __global__ void k_apriori_join(const uint32_t *__restrict__ L, uint64_t n, uint3
     if (!MODE) cnt[a] = c;
 }
 
+// Row a starts a prefix group when its first k-1 items differ from row a-1.
+__global__ void k_group_start(const uint32_t *__restrict__ L, uint64_t n, uint32_t k, uint32_t *__restrict__ flag) {
+    const uint64_t a = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < n) flag[a] = (a == 0 || cmp_rows(L + (a - 1) * k, L + a * k, k - 1)) ? 1u : 0u;
+}
+
+// Exclusive group-start scan -> each group's first row (gfirst[g]) and, per
+// row, the number of later rows of its group (its join partners).
+__global__ void k_group_first(const uint32_t *__restrict__ flag, const uint64_t *__restrict__ gid_excl, uint64_t n,
+                              uint64_t *__restrict__ gfirst) {
+    const uint64_t a = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < n && flag[a]) gfirst[gid_excl[a]] = a;
+}
+
+__global__ void k_partners(const uint32_t *__restrict__ flag, const uint64_t *__restrict__ gid_excl,
+                           const uint64_t *__restrict__ gfirst, uint64_t n_groups, uint64_t n,
+                           uint32_t *__restrict__ partners) {
+    const uint64_t a = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    const uint64_t g = gid_excl[a] + flag[a] - 1;  // this row's group
+    const uint64_t end = g + 1 < n_groups ? gfirst[g + 1] : n;
+    partners[a] = (uint32_t)(end - a - 1);
+}
+
+// One thread per join pair t: row a = last row with poff[a] <= t, partner
+// b = a + 1 + t - poff[a].  Writes the candidate and whether every k-subset
+// is frequent (cuApriori.py:488-490).
+__global__ void k_join_pairs(const uint32_t *__restrict__ L, uint64_t n, uint32_t k,
+                             const uint64_t *__restrict__ poff, uint64_t n_pairs, uint32_t *__restrict__ cand,
+                             uint32_t *__restrict__ cand_left, uint32_t *__restrict__ ok_flag) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_pairs) return;
+    uint64_t lo = 0, hi = n;  // upper_bound(poff, t) - 1
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (poff[mid] <= t) lo = mid + 1; else hi = mid;
+    }
+    const uint64_t a = lo - 1;
+    const uint64_t b = a + 1 + (t - poff[a]);
+    const uint32_t *ra = L + a * k, *rb = L + b * k;
+    const uint32_t last = rb[k - 1];
+    uint32_t *dst = cand + t * (k + 1);
+    for (uint32_t i = 0; i < k; ++i) dst[i] = ra[i];
+    dst[k] = last;
+    cand_left[t] = (uint32_t)a;
+    uint32_t sub[64];
+    bool ok = true;
+    for (uint32_t drop = 0; drop + 1 < k && ok; ++drop) {
+        uint32_t m = 0;
+        for (uint32_t i = 0; i < k; ++i)
+            if (i != drop) sub[m++] = ra[i];
+        sub[m] = last;
+        ok = level_has(L, n, k, sub);
+    }
+    ok_flag[t] = ok ? 1u : 0u;
+}
+
+// Complete intersection of the candidates that passed pruning (warp each);
+// pass[t] = pruned-in and support >= minsup.
+__global__ void k_count_pruned(const uint64_t *__restrict__ bits, uint64_t stride, const uint32_t *__restrict__ cand,
+                               const uint32_t *__restrict__ ok_flag, uint64_t n, uint32_t width, long long minsup,
+                               uint32_t *__restrict__ support, uint32_t *__restrict__ pass) {
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    if (!ok_flag[warp]) {
+        if (!lane) { support[warp] = 0; pass[warp] = 0; }
+        return;
+    }
+    const uint32_t *cc = cand + warp * width;
+    uint32_t s = 0;
+    for (uint64_t v = lane; v < stride / 2; v += 32) {
+        ulonglong2 acc = make_ulonglong2(~0ull, ~0ull);
+        for (uint32_t j = 0; j < width; ++j)
+            acc = and2(acc, ld_stream(reinterpret_cast<const ulonglong2 *>(bits + (uint64_t)cc[j] * stride) + v));
+        s += popc2(acc);
+    }
+    s = warp_sum_u32(s);
+    if (!lane) {
+        support[warp] = s;
+        pass[warp] = (long long)s >= minsup ? 1u : 0u;
+    }
+}
+
 // flag[c] = support passes (as 0/1 for the scan).
 __global__ void k_apriori_flags(const uint32_t *__restrict__ sup, uint64_t n, long long minsup,
                                 uint32_t *__restrict__ flag) {

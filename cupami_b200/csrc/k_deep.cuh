@@ -7,15 +7,18 @@
 // work unit here.  Units run in a persistent kernel: each CTA pops a
 // (frame, position) unit from a queue in device memory, stages member p (the
 // prefix tidset, ANDed with the frame mask for top-level classes) in shared
-// memory, streams the later members with 128-bit loads, ANDs and popcounts
-// them with a warp reduction, writes surviving children into a device arena,
-// emits their patterns and, when two or more survive, appends a child frame
-// and its positions to the queue.  Non-surviving children are written to the
-// warp's reusable scratch slot only (overwritten in L2 before eviction).
+// memory and streams the later members with 128-bit loads, AND and popcount
+// per warp (pass 1).  Child tidsets are written only when a child frame will
+// exist (two or more survivors): one exact-size arena block per unit, filled
+// by a second pass over the survivors' siblings (pass 2, mostly L2 hits).  A
+// unit with one survivor writes nothing but its pattern record.
 //
-// Every wait is bounded by spin_limit; running out sets CPM_DEEP_ERR_SPIN and
-// the kernel returns.  Capacity overflow sets an error bit and stops all CTAs;
-// the host then grows the buffers and reruns the round, so output is exact.
+// Frames carry their database's tidset stride, threshold and id, so one launch
+// can mine many databases of different sizes at once.
+//
+// Every wait is bounded by spin_limit; running out sets DEEP_ERR_SPIN and the
+// kernel returns.  Capacity overflow sets an error bit and stops all CTAs; the
+// host then grows the buffers and reruns, so the output is exact.
 #pragma once
 #include "common.cuh"
 
@@ -27,13 +30,17 @@ enum : unsigned {
 };
 
 constexpr unsigned long long QUEUE_EMPTY = ~0ull;
-constexpr uint64_t NO_SLOT = ~0ull;
+constexpr uint32_t NO_PATTERN = 0xffffffffu;
 
 struct DFrame {
     const uint64_t *mask;  // top-level classes: tidset of the class item; else null
     uint64_t mem_off;      // first member entry
     uint32_t m;            // members
-    uint32_t root;         // top-level class this frame descends from
+    uint32_t root;         // top-level frames: id of their first root unit (unit p has id root + p);
+                           // deeper frames: the root unit whose subtree they belong to
+    uint32_t stride;       // words per tidset in this frame's database (even)
+    uint32_t db;           // database index within the batch
+    long long minsup;      // that database's threshold
 };
 
 // Every counter that CTAs update or poll sits on its own 128-byte line, so
@@ -44,7 +51,7 @@ struct DeepState {
     CPM_LINE(q_tail);       // entries reserved by producers
     CPM_LINE(pending);      // units queued or running
     CPM_LINE(n_patterns);
-    CPM_LINE(arena_next);
+    CPM_LINE(arena_next);   // words handed out
     CPM_LINE(n_frames);
     CPM_LINE(n_members);
     CPM_LINE(intersections);
@@ -60,12 +67,11 @@ struct DeepParams {
     DFrame *frames; uint64_t frames_cap;
     uint32_t *mem_pat; uint32_t *mem_item; const uint64_t **mem_bits; uint64_t members_cap;
     unsigned long long *queue; uint64_t queue_cap;
-    uint64_t *arena; uint64_t arena_slots;
-    uint32_t *pat_parent; uint32_t *pat_item; uint32_t *pat_sup; uint64_t pat_cap;
-    unsigned long long *root_cost;  // per top-level class: intersections in its subtree
+    uint64_t *arena; uint64_t arena_words;
+    uint32_t *pat_parent; uint32_t *pat_item; uint32_t *pat_sup; uint32_t *pat_db; uint64_t pat_cap;
+    unsigned long long *root_cost;  // per root unit: intersections in its subtree (null: not kept)
     DeepState *st;
-    uint64_t stride;                // words per tidset (even)
-    long long minsup;
+    uint64_t max_stride;            // largest frame stride (shared-memory prefix size)
     unsigned long long spin_limit;
 };
 
@@ -95,23 +101,21 @@ __device__ int deep_claim(const DeepParams &P, unsigned long long *item) {
     return 1;
 }
 
+__device__ __forceinline__ const ulonglong2 *ld_ptr(const uint64_t *const *p) {
+    return reinterpret_cast<const ulonglong2 *>(__ldcg(reinterpret_cast<const unsigned long long *>(p)));
+}
+
 template <bool SMEM_PREFIX>
 __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
     extern __shared__ ulonglong2 s_prefix[];
     __shared__ unsigned long long s_item;
-    __shared__ int s_stop;
+    __shared__ int s_stop, s_ok, s_grant;
     __shared__ uint32_t s_surv;
-    __shared__ unsigned long long s_mem_base;
-    __shared__ uint64_t s_pool[32];
-    __shared__ int s_pool_n;
-    __shared__ unsigned long long s_fid, s_qbase;
-    __shared__ int s_ok;
+    __shared__ unsigned long long s_mem_base, s_arena_base, s_fid, s_qbase;
+    __shared__ uint32_t s_wtot[32];
 
     const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const uint64_t n2 = P.stride / 2;
     DeepState *st = P.st;
-    uint64_t my_slot = NO_SLOT;  // warp-uniform scratch slot (kept across units)
-    if (threadIdx.x == 0) s_pool_n = 0;
     // Per-CTA statistics (thread 0), added to the global counters at exit.
     unsigned long long c_inter = 0, c_bytes = 0, c_units = 0, c_surv = 0;
 
@@ -120,15 +124,19 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
         __syncthreads();
         if (s_stop) break;
         const uint32_t fid = (uint32_t)(s_item >> 32), p = (uint32_t)s_item;
-        DFrame f;
-        f.mask = reinterpret_cast<const uint64_t *>(__ldcg(reinterpret_cast<const unsigned long long *>(&P.frames[fid].mask)));
-        f.mem_off = __ldcg(reinterpret_cast<const unsigned long long *>(&P.frames[fid].mem_off));
-        f.m = __ldcg(&P.frames[fid].m);
-        f.root = __ldcg(&P.frames[fid].root);
-        const uint32_t cnt = f.m - p - 1;
-        const ulonglong2 *pb = reinterpret_cast<const ulonglong2 *>(
-            __ldcg(reinterpret_cast<const unsigned long long *>(P.mem_bits + f.mem_off + p)));
-        const ulonglong2 *mk = reinterpret_cast<const ulonglong2 *>(f.mask);
+        const DFrame *fp = P.frames + fid;
+        const ulonglong2 *mk = reinterpret_cast<const ulonglong2 *>(
+            __ldcg(reinterpret_cast<const unsigned long long *>(&fp->mask)));
+        const uint64_t mem_off = __ldcg(reinterpret_cast<const unsigned long long *>(&fp->mem_off));
+        const uint32_t m = __ldcg(&fp->m), stride = __ldcg(&fp->stride);
+        // Root unit of this work: top-level frames (the ones with a mask) are
+        // split into one root unit per position.
+        const uint32_t root = __ldcg(&fp->root) + (mk ? p : 0u);
+        const uint32_t db = __ldcg(&fp->db);
+        const long long minsup = __ldcg(&fp->minsup);
+        const uint64_t n2 = stride / 2;
+        const uint32_t cnt = m - p - 1;
+        const ulonglong2 *pb = ld_ptr(P.mem_bits + mem_off + p);
         if (SMEM_PREFIX) {
             for (uint64_t v = threadIdx.x; v < n2; v += blockDim.x)
                 s_prefix[v] = mk ? and2(ld_cg(pb + v), ld_cg(mk + v)) : ld_cg(pb + v);
@@ -142,28 +150,12 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
         }
         __syncthreads();
         const bool ok = s_ok != 0;
-        const uint32_t parent_pat = __ldcg(P.mem_pat + f.mem_off + p);
+        const uint32_t parent_pat = __ldcg(P.mem_pat + mem_off + p);
+        // ---- pass 1: supports of every later member ----
         for (uint32_t q = wid; ok && q < cnt; q += nw) {
-            if (my_slot == NO_SLOT) {
-                uint64_t s = NO_SLOT;
-                if (lane == 0) {
-                    const int k = atomicSub(&s_pool_n, 1) - 1;
-                    if (k >= 0) {
-                        s = s_pool[k];
-                    } else {
-                        atomicAdd(&s_pool_n, 1);
-                        s = atomicAdd(&st->arena_next, 1ull);
-                        if (s >= P.arena_slots) { deep_fail(st, DEEP_ERR_ARENA); s = NO_SLOT; }
-                    }
-                }
-                my_slot = __shfl_sync(CPM_FULL, s, 0);
-                if (my_slot == NO_SLOT) break;
-            }
-            const uint64_t mi = f.mem_off + p + 1 + q;
-            const ulonglong2 *sb = reinterpret_cast<const ulonglong2 *>(
-                __ldcg(reinterpret_cast<const unsigned long long *>(P.mem_bits + mi)));
+            const uint64_t mi = mem_off + p + 1 + q;
+            const ulonglong2 *sb = ld_ptr(P.mem_bits + mi);
             const uint32_t sib_item = __ldcg(P.mem_item + mi);
-            ulonglong2 *dst = reinterpret_cast<ulonglong2 *>(P.arena + my_slot * P.stride);
             uint32_t s = 0;
             uint64_t v = lane;
             for (; v + 96 < n2; v += 128) {
@@ -180,7 +172,6 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
                         x2 = and2(x2, ld_cg(mk + v + 64)); x3 = and2(x3, ld_cg(mk + v + 96));
                     }
                 }
-                dst[v] = x0; dst[v + 32] = x1; dst[v + 64] = x2; dst[v + 96] = x3;
                 s += popc2(x0) + popc2(x1) + popc2(x2) + popc2(x3);
             }
             for (; v < n2; v += 32) {
@@ -191,14 +182,15 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
                     x = and2(x, ld_cg(pb + v));
                     if (mk) x = and2(x, ld_cg(mk + v));
                 }
-                dst[v] = x;
                 s += popc2(x);
             }
             s = warp_sum_u32(s);
-            if ((long long)s >= P.minsup) {
-                if (lane == 0) {
-                    const uint32_t idx = atomicAdd(&s_surv, 1u);
-                    const uint64_t m_out = s_mem_base + idx;
+            if (lane == 0) {
+                // Entry q of the unit's member block: the survivor (pattern,
+                // item, sibling tidset until pass 2) or a hole.
+                const uint64_t m_out = s_mem_base + q;
+                uint32_t pid32 = NO_PATTERN;
+                if ((long long)s >= minsup) {
                     const unsigned long long pid = atomicAdd(&st->n_patterns, 1ull);
                     if (pid >= P.pat_cap) {
                         deep_fail(st, DEEP_ERR_PATTERNS);
@@ -206,44 +198,110 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
                         P.pat_parent[pid] = parent_pat;
                         P.pat_item[pid] = sib_item;
                         P.pat_sup[pid] = s;
+                        if (P.pat_db) P.pat_db[pid] = db;
+                        pid32 = (uint32_t)pid;
                     }
-                    if (m_out < P.members_cap) {
-                        P.mem_pat[m_out] = (uint32_t)pid;
-                        P.mem_item[m_out] = sib_item;
-                        P.mem_bits[m_out] = P.arena + my_slot * P.stride;
-                    }
-                    __threadfence();
                 }
-                my_slot = NO_SLOT;
+                if (m_out < P.members_cap) {
+                    P.mem_pat[m_out] = pid32;
+                    P.mem_item[m_out] = sib_item;
+                    P.mem_bits[m_out] = reinterpret_cast<const uint64_t *>(sb);
+                }
             }
         }
         __syncthreads();
-        const uint32_t ns = s_surv;
-        if (threadIdx.x == 0) {
-            s_fid = ~0ull;
-            if (ns >= 2 && ld_acquire_u32(&st->error) == 0) {
-                const unsigned long long nf = atomicAdd(&st->n_frames, 1ull);
-                const unsigned long long qb = atomicAdd(&st->q_tail, (unsigned long long)(ns - 1));
-                if (nf >= P.frames_cap) deep_fail(st, DEEP_ERR_FRAMES);
-                else if (qb + ns - 1 > P.queue_cap) deep_fail(st, DEEP_ERR_QUEUE);
-                else {
-                    DFrame c;
-                    c.mask = nullptr;
-                    c.mem_off = s_mem_base;
-                    c.m = ns;
-                    c.root = f.root;
-                    P.frames[nf] = c;
-                    atomicAdd(&st->pending, (unsigned long long)(ns - 1));
-                    __threadfence();
-                    s_fid = nf;
-                    s_qbase = qb;
+        // Survivors move to the front of the block in member order, so every
+        // child frame keeps its members sorted by column (the pattern tree is
+        // then a prefix tree: a pattern's parent is itself minus its last item).
+        if (ok && s_mem_base + cnt <= P.members_cap) {
+            uint32_t base = 0;
+            for (uint32_t start = 0; start < cnt; start += blockDim.x) {
+                const uint32_t q = start + threadIdx.x;
+                const uint64_t src = s_mem_base + q;
+                uint32_t e_pat = NO_PATTERN, e_item = 0;
+                const uint64_t *e_bits = nullptr;
+                if (q < cnt) {
+                    e_pat = __ldcg(P.mem_pat + src);
+                    e_item = __ldcg(P.mem_item + src);
+                    e_bits = reinterpret_cast<const uint64_t *>(ld_ptr(P.mem_bits + src));
                 }
-            } else if (ns == 1 && s_mem_base < P.members_cap && ld_acquire_u32(&st->error) == 0) {
-                // The lone survivor's tidset is never read again: recycle it.
-                const uint64_t *b = reinterpret_cast<const uint64_t *>(
-                    __ldcg(reinterpret_cast<const unsigned long long *>(P.mem_bits + s_mem_base)));
-                const uint64_t slot = (uint64_t)(b - P.arena) / P.stride;
-                if (s_pool_n < 32) s_pool[s_pool_n++] = slot;
+                const bool keep = e_pat != NO_PATTERN;
+                const unsigned bal = __ballot_sync(CPM_FULL, keep);
+                if (lane == 0) s_wtot[wid] = __popc(bal);
+                __syncthreads();
+                uint32_t before = 0, total = 0;
+                for (unsigned w = 0; w < nw; ++w) {
+                    if (w < wid) before += s_wtot[w];
+                    total += s_wtot[w];
+                }
+                if (keep) {
+                    const uint64_t dst = s_mem_base + base + before + __popc(bal & ((1u << lane) - 1));
+                    P.mem_pat[dst] = e_pat;
+                    P.mem_item[dst] = e_item;
+                    P.mem_bits[dst] = e_bits;
+                }
+                base += total;
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) s_surv = base;
+        } else if (threadIdx.x == 0) {
+            s_surv = 0;
+        }
+        __syncthreads();
+        const uint32_t ns = s_surv;
+        const bool expand = ns >= 2;
+        if (threadIdx.x == 0) {
+            s_grant = 0;
+            s_fid = ~0ull;
+            if (expand && ld_acquire_u32(&st->error) == 0) {
+                const unsigned long long ab = atomicAdd(&st->arena_next, (unsigned long long)ns * stride);
+                if (ab + (unsigned long long)ns * stride > P.arena_words) deep_fail(st, DEEP_ERR_ARENA);
+                else s_grant = 1;
+                s_arena_base = ab;
+            }
+        }
+        __syncthreads();
+        // ---- pass 2: child tidsets of the survivors (only when they recurse) ----
+        if (s_grant) {
+            for (uint32_t idx = wid; idx < ns; idx += nw) {
+                const uint64_t m_out = s_mem_base + idx;
+                const ulonglong2 *sb = ld_ptr(P.mem_bits + m_out);
+                ulonglong2 *dst = reinterpret_cast<ulonglong2 *>(P.arena + s_arena_base + (uint64_t)idx * stride);
+                for (uint64_t v = lane; v < n2; v += 32) {
+                    ulonglong2 x = ld_cg(sb + v);
+                    if (SMEM_PREFIX) {
+                        x = and2(x, s_prefix[v]);
+                    } else {
+                        x = and2(x, ld_cg(pb + v));
+                        if (mk) x = and2(x, ld_cg(mk + v));
+                    }
+                    dst[v] = x;
+                }
+                __syncwarp();
+                if (lane == 0) P.mem_bits[m_out] = reinterpret_cast<const uint64_t *>(dst);
+            }
+            __threadfence();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && s_grant) {
+            const unsigned long long nf = atomicAdd(&st->n_frames, 1ull);
+            const unsigned long long qb = atomicAdd(&st->q_tail, (unsigned long long)(ns - 1));
+            if (nf >= P.frames_cap) deep_fail(st, DEEP_ERR_FRAMES);
+            else if (qb + ns - 1 > P.queue_cap) deep_fail(st, DEEP_ERR_QUEUE);
+            else {
+                DFrame c;
+                c.mask = nullptr;
+                c.mem_off = s_mem_base;
+                c.m = ns;
+                c.root = root;
+                c.stride = stride;
+                c.db = db;
+                c.minsup = minsup;
+                P.frames[nf] = c;
+                atomicAdd(&st->pending, (unsigned long long)(ns - 1));
+                __threadfence();
+                s_fid = nf;
+                s_qbase = qb;
             }
         }
         __syncthreads();
@@ -254,10 +312,10 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
         __syncthreads();
         if (threadIdx.x == 0) {
             c_inter += cnt;
-            c_bytes += 8ull * P.stride * (1ull + cnt + ns);
+            c_bytes += 8ull * stride * (1ull + cnt + (expand ? ns : 0));
             c_units += 1;
             c_surv += ns;
-            if (P.root_cost) atomicAdd(P.root_cost + f.root, (unsigned long long)cnt);
+            if (P.root_cost) atomicAdd(P.root_cost + root, (unsigned long long)cnt);
             __threadfence();
             atomicAdd(&st->pending, ~0ull);  // pending -= 1
         }

@@ -257,6 +257,10 @@ class cuApriori:
     def mine(self):
         self._startTime = time.perf_counter()
         ctx = self._getCudaModule()
+        if self.scheduler == "learned":
+            from .. import costmodel
+
+            costmodel.ensure_default(ctx)
         db, labels = self._deviceDatabase(ctx)
         try:
             result = db.mine(self._minSup, self._ALGORITHM, self._options(), self._ORDER)

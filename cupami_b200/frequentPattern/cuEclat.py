@@ -47,6 +47,39 @@ class cuEclat(cuApriori):
             return super().mine()
         self._mineWithHooks()
 
+    @classmethod
+    def mineBatch(cls, sources, minSup, **kwargs):
+        """Mine many independent databases in one device pass.
+
+        ``sources`` are anything the constructor accepts; ``minSup`` is one
+        threshold for all or a list.  Returns one miner per source with its
+        patterns in place, as if ``mine()`` had run on each.  Every miner's
+        mining time is the time of the whole batch.  (The reference mines one
+        database per call.)
+        """
+        sups = list(minSup) if isinstance(minSup, (list, tuple)) else [minSup] * len(sources)
+        miners = [cls(src, sup, **kwargs) for src, sup in zip(sources, sups)]
+        if not miners:
+            return miners
+        ctx = cls._getCudaModule()
+        mine_start = time.perf_counter()
+        if miners[0].scheduler == "learned":
+            from .. import costmodel
+
+            costmodel.ensure_default(ctx)
+        dbs, labels = zip(*(m._deviceDatabase(ctx) for m in miners))
+        try:
+            results = _native.mine_batch(ctx, list(dbs), [m._minSup for m in miners], miners[0]._options(),
+                                         cls._ORDER)
+        finally:
+            for db in dbs:
+                db.close()
+        end = time.perf_counter()
+        for m, res, lab in zip(miners, results, labels):
+            m._result, m._labels, m._patterns = res, lab, None
+            m._startTime, m._endTime = mine_start, end
+        return miners
+
     def _candidatePairs(self, frequent, items):
         return combinations(frequent, 2)
 

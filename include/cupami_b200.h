@@ -128,6 +128,13 @@ void cpm_db_free(cpm_db *db);
 /* ---- mining --------------------------------------------------------------- */
 int  cpm_mine(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, int algo,
               const cpm_opts *opts, cpm_result **out);
+/* Eclat over many independent databases in one pass: one launch per stage
+ * and one persistent deep-level launch for the whole batch.  out[d] is the
+ * result of dbs[d] at min_sups[d], equal to cpm_mine(dbs[d], min_sups[d],
+ * CPM_ECLAT); each result's statistics are those of the whole batch.  The
+ * reference mines one database per call (cuEclat.py:168-203). */
+int  cpm_mine_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const int64_t *min_sups,
+                    const cpm_opts *opts, cpm_result **out);
 int  cpm_result_size(const cpm_result *res, uint64_t *n_patterns, uint64_t *n_item_slots);
 /* Flattened patterns in the requested order: pattern k is
  * items[offsets[k] .. offsets[k+1]) (columns, increasing), support supports[k]. */
@@ -143,6 +150,28 @@ int  cpm_result_stats(const cpm_result *res, cpm_stats *stats);
 int  cpm_result_from_tree(const int64_t *parent, const uint32_t *item, const uint64_t *support,
                           uint64_t n, cpm_result **out);
 void cpm_result_free(cpm_result *res);
+
+/* ---- learned scheduler cost model -------------------------------------------
+ * No counterpart in the reference, whose class search runs in a fixed order
+ * (cuEclat.py:195-245).  A one-hidden-layer FP32 MLP predicts
+ * log(1 + subtree intersections) of every root unit (one position of a
+ * top-level class) from cheap features; with CPM_SCHED_LEARNED and a loaded
+ * model, root units are started in order of predicted cost (tidset length
+ * included), largest first.  The order never changes the patterns or their
+ * supports.  Traces (features and true costs) come from cpm_mine with
+ * opts.collect_trace = 1 via cpm_result_trace.  Training, prediction and
+ * gradients run in this library's CUDA kernels. */
+int cpm_costmodel_params(uint32_t *n_features, uint32_t *n_params);
+int cpm_costmodel_train(cpm_ctx *ctx, const float *X, const float *y, uint64_t n, uint32_t epochs, float lr,
+                        uint64_t seed, float *params, float *loss_history);
+int cpm_costmodel_predict(cpm_ctx *ctx, const float *params, const float *X, uint64_t n, float *y);
+/* Gradient of (1/2n) * sum (f(x_i) - t_i)^2 in the standardised target space,
+ * for every parameter (zero for the fixed standardisation entries). */
+int cpm_costmodel_gradient(cpm_ctx *ctx, const float *params, const float *X, const float *y, uint64_t n,
+                           float *grad, float *loss);
+/* Loads the model used by CPM_SCHED_LEARNED on this context (NULL unloads). */
+int cpm_costmodel_set(cpm_ctx *ctx, const float *params);
+int cpm_result_trace(const cpm_result *res, float *X, float *y, uint64_t *n);
 
 /* ---- reference kernel-module API (cupami/frequentPattern/_bitsets.py) ------- */
 /* d_bitsets: uint32[items][ceil(transactions/32)], zero-filled here, then one

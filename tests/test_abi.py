@@ -39,8 +39,11 @@ def test_no_device_raises_loudly():
         miner.mine()
 
 
-def _random_tree(patterns, rng):
-    """A valid pattern tree for ``patterns`` built in a random emission order."""
+def _random_tree(patterns, rng, prefix_tree=False):
+    """A valid pattern tree for ``patterns`` built in a random emission order.
+
+    With ``prefix_tree`` every parent is the pattern minus its largest item
+    (the device's trees); otherwise a random item is dropped."""
     by_set = {}
     order = list(range(len(patterns)))
     # parents must precede children: shuffle within lengths, shortest first
@@ -52,7 +55,7 @@ def _random_tree(patterns, rng):
             parent.append(-1)
             item.append(items[0])
         else:
-            drop = int(rng.integers(len(items)))
+            drop = len(items) - 1 if prefix_tree else int(rng.integers(len(items)))
             rest = frozenset(items[:drop] + items[drop + 1:])
             parent.append(by_set[rest])
             item.append(items[drop])
@@ -61,8 +64,9 @@ def _random_tree(patterns, rng):
     return parent, item, support
 
 
+@pytest.mark.parametrize("prefix_tree", [False, True])
 @pytest.mark.parametrize("algo,order", [("cuEclat", 0), ("cuApriori", 1)])
-def test_reference_insertion_order_from_shuffled_trees(golden, algo, order):
+def test_reference_insertion_order_from_shuffled_trees(golden, algo, order, prefix_tree):
     from cupami_b200._native import Result
 
     rng = np.random.default_rng(0)
@@ -75,7 +79,7 @@ def test_reference_insertion_order_from_shuffled_trees(golden, algo, order):
             labels = sorted({x for p in pats for x in p})
             col = {x: i for i, x in enumerate(labels)}
             patterns = [(tuple(sorted(col[x] for x in p)), s) for p, (_, s) in zip(pats, run["patterns"])]
-            parent, item, support = _random_tree(patterns, rng)
+            parent, item, support = _random_tree(patterns, rng, prefix_tree)
             res = Result.from_tree(parent, item, support, order)
             o = res.offsets.tolist()
             got = [("\t".join(labels[c] for c in res.items[o[k]:o[k + 1]].tolist()), int(res.supports[k]))

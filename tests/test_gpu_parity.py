@@ -112,3 +112,23 @@ def test_word_boundaries_dense(oracle_lib, count):
     csr = TransactionCSR.from_rows(rows, universe=10)
     _oracle_check(oracle_lib, csr, max(1, count // 6), "eclat")
     _oracle_check(oracle_lib, csr, max(1, count // 6), "apriori")
+
+
+def test_batch_of_databases_matches_single_mines(oracle_lib):
+    from cupami_b200 import _native, cuEclat, datasets
+
+    csrs = datasets.batched_zipf(limit=10)
+    miners = cuEclat.mineBatch(csrs, 0.01)
+    for csr, m in zip(csrs, miners):
+        single = cuEclat(csr, 0.01)
+        single.mine()
+        assert list(m.getPatterns().items()) == list(single.getPatterns().items())
+        labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, 0.01)
+        assert m.getPatterns() == oracle_lib.to_dict(labels, arrays)
+    # mixed sizes and thresholds, including an empty database
+    rows_a = [[1, 2, 3]] * 40 + [[2, 3]] * 10
+    rows_b = []
+    ms = cuEclat.mineBatch([rows_a, rows_b, csrs[0]], [5, 1, 0.02])
+    assert ms[1].getPatterns() == {}
+    assert ms[0].getPatterns() == oracle_lib.mine_rows(rows_a, 5)
+    assert ms[2].getPatterns() == oracle_lib.to_dict(*oracle_lib.mine_csr(csrs[0].offsets, csrs[0].items, 0.02))
