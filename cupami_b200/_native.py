@@ -61,7 +61,7 @@ class Opts(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "n_patterns", "n_frequent_items", "n_frequent_pairs", "frames", "work_items",
-        "intersections", "bytes_alg", "pair_ops", "kernel_launches", "retries")] + [
+        "intersections", "bytes_alg", "pair_ops", "kernel_launches", "retries", "deep_rounds")] + [
         (n, ctypes.c_double) for n in (
             "ms_pack", "ms_pairs", "ms_deep", "ms_total", "deep_gbs", "pair_tops")]
 
@@ -79,6 +79,8 @@ _SIGNATURES = {
     "cpm_default_opts": (ctypes.c_int, [ctypes.POINTER(Opts)]),
     "cpm_db_from_csr": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, ctypes.POINTER(_P)]),
     "cpm_db_from_ids": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.POINTER(_P)]),
+    "cpm_db_from_ids_batch": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(_P), ctypes.POINTER(_U64),
+                                             ctypes.POINTER(_P), ctypes.POINTER(_U64), ctypes.POINTER(_P)]),
     "cpm_db_info": (ctypes.c_int, [_P, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_uint32),
                                    ctypes.POINTER(_U64)]),
     "cpm_db_labels": (ctypes.c_int, [_P, _P]),
@@ -90,6 +92,7 @@ _SIGNATURES = {
     "cpm_result_size": (ctypes.c_int, [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
     "cpm_result_copy": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P]),
     "cpm_result_tree": (ctypes.c_int, [_P, _P, _P, _P]),
+    "cpm_results_copy": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_uint32, ctypes.c_int, _P, _P, _P, _P]),
     "cpm_result_stats": (ctypes.c_int, [_P, ctypes.POINTER(Stats)]),
     "cpm_result_from_tree": (ctypes.c_int, [_P, _P, _P, _U64, ctypes.POINTER(_P)]),
     "cpm_result_free": (None, [_P]),
@@ -227,6 +230,29 @@ class Database:
         db.labels = labels
         return db
 
+    @classmethod
+    def from_ids_batch(cls, ctx, sources):
+        """One Database per (offsets, ids) pair, loaded with one upload and one packing pass."""
+        n = len(sources)
+        offs = [np.ascontiguousarray(o, dtype=np.uint64) for o, _ in sources]
+        idss = [np.ascontiguousarray(i, dtype=np.uint32) for _, i in sources]
+        n_rows = (_U64 * max(1, n))(*[o.size - 1 for o in offs])
+        nnz = (_U64 * max(1, n))(*[i.size for i in idss])
+        p_off = (_P * max(1, n))(*[o.ctypes.data for o in offs])
+        p_ids = (_P * max(1, n))(*[i.ctypes.data for i in idss])
+        outs = (_P * max(1, n))()
+        with ctx.lock:
+            ctx.check(library().cpm_db_from_ids_batch(ctx.handle, n, p_off, n_rows, p_ids, nnz, outs))
+        dbs = []
+        for k in range(n):
+            db = cls(ctx, _P(outs[k]))
+            labels = np.zeros(db.n_items, dtype=np.uint32)
+            if db.n_items:
+                ctx.check(library().cpm_db_labels(db.handle, labels.ctypes.data))
+            db.labels = labels
+            dbs.append(db)
+        return dbs
+
     def mine(self, min_sup, algorithm, opts=None, order=None):
         if opts is None:
             opts = Opts()
@@ -263,10 +289,30 @@ def mine_batch(ctx, databases, min_sups, opts=None, order=CPM_ORDER_ECLAT):
     outs = (_P * max(1, n))()
     with ctx.lock:
         ctx.check(library().cpm_mine_batch(ctx.handle, handles, n, sups, ctypes.byref(opts), outs))
-    results = []
     try:
+        lib = library()
+        sizes = np.zeros(2 * max(1, n), dtype=np.uint64)
+        if lib.cpm_results_copy(outs, n, int(order), sizes.ctypes.data, None, None, None) != CPM_OK:
+            raise NativeError(CPM_EINTERNAL, "result sizes")
+        npat = sizes[0::2][:n].astype(np.int64)
+        nslot = sizes[1::2][:n].astype(np.int64)
+        offsets = np.zeros(max(1, int(npat.sum() + n)), dtype=np.uint64)
+        items = np.zeros(max(1, int(nslot.sum())), dtype=np.uint32)
+        supports = np.zeros(max(1, int(npat.sum())), dtype=np.uint64)
+        code = lib.cpm_results_copy(outs, n, int(order), sizes.ctypes.data, offsets.ctypes.data,
+                                    items.ctypes.data, supports.ctypes.data)
+        if code != CPM_OK:
+            raise NativeError(code, "result copy")
+        st = Stats()
+        lib.cpm_result_stats(outs[0], ctypes.byref(st))
+        stats = st.as_dict()
+        results, o, it, sp = [], 0, 0, 0
         for k in range(n):
-            results.append(Result.collect(outs[k], order))
+            results.append(Result(offsets[o:o + npat[k] + 1], items[it:it + nslot[k]], supports[sp:sp + npat[k]],
+                                  stats))
+            o += npat[k] + 1
+            it += nslot[k]
+            sp += npat[k]
     finally:
         for k in range(n):
             if outs[k]:
@@ -313,6 +359,13 @@ class Result:
 
     def __len__(self):
         return int(self.supports.size)
+
+    def patterns(self, labels):
+        """{tab-joined labels: support}, in result order."""
+        names = [str(v) for v in (labels.tolist() if hasattr(labels, "tolist") else labels)]
+        off, items = self.offsets.tolist(), self.items.tolist()
+        return {"\t".join(names[c] for c in items[off[k]:off[k + 1]]): int(s)
+                for k, s in enumerate(self.supports.tolist())}
 
     @classmethod
     def from_tree(cls, parent, item, support, order):

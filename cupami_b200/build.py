@@ -15,7 +15,7 @@ OUTPUT = PKG / "libcupami_b200.so"
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC,-O3", "-shared", "-Xptxas", "-O3",
+    "-Xcompiler", "-fPIC,-O3,-fopenmp", "-shared", "-Xptxas", "-O3", "-lgomp",
 ]
 
 

@@ -8,11 +8,14 @@
 #include "common.cuh"
 #include "k_basic.cuh"
 #include "k_pairs.cuh"
+#include "k_batch.cuh"
 #include "k_gram_tc.cuh"
 #include "k_deep.cuh"
 #include "k_apriori.cuh"
 #include "k_batch.cuh"
 #include "k_costmodel.cuh"
+#include "k_units.cuh"
+#include <cub/device/device_radix_sort.cuh>
 
 #include <cub/device/device_scan.cuh>
 #include <thrust/iterator/transform_iterator.h>
@@ -28,6 +31,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <mutex>
+#include <deque>
 #include <cmath>
 
 using namespace cpm;
@@ -47,7 +51,9 @@ struct cpm_ctx {
     int deep_occ_smem = -1;   // k_deep<true> CTAs per SM, for deep_occ_bytes of prefix
     size_t deep_occ_bytes = 0;
     int deep_occ_global = -1; // k_deep<false> CTAs per SM
+    unsigned deep_occ_block = 0;  // block size the occupancies above were taken for
     std::vector<float> model;  // cost-model parameters (empty: none loaded)
+    float last_deep_ms = 0.f;  // deep-phase kernel time of the last bounded-round run
 };
 
 struct cpm_db {
@@ -376,6 +382,149 @@ extern "C" int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n
     return CPM_OK;
 }
 
+extern "C" int cpm_db_from_ids_batch(cpm_ctx *ctx, uint32_t n_db, const uint64_t *const *offsets,
+                                     const uint64_t *n_rows, const uint32_t *const *ids, const uint64_t *nnz,
+                                     cpm_db **out) {
+    if (!ctx || !out || (n_db && (!offsets || !n_rows || !ids || !nnz))) return CPM_EINVAL;
+    for (uint32_t d = 0; d < n_db; ++d) out[d] = nullptr;
+    if (!n_db) return CPM_OK;
+    CK(cudaSetDevice(ctx->device));
+    // ---- host: compacted offsets and largest id of every database ----
+    std::vector<std::vector<uint64_t>> off(n_db);
+    std::vector<uint32_t> max_id(n_db, 0);
+    std::vector<int> bad(n_db, 0);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t d = 0; d < (int64_t)n_db; ++d) {
+        if ((!offsets[d] && n_rows[d]) || (!ids[d] && nnz[d])) { bad[d] = 1; continue; }
+        cpm_ctx tmp;  // errors are reported below
+        if (compact_offsets(&tmp, offsets[d], n_rows[d], nnz[d], off[d]) != CPM_OK) { bad[d] = 2; continue; }
+        uint32_t m = 0;
+        for (uint64_t k = 0; k < nnz[d]; ++k) m = std::max(m, ids[d][k]);
+        max_id[d] = m;
+    }
+    for (uint32_t d = 0; d < n_db; ++d) {
+        if (bad[d]) return set_err(ctx, CPM_EINVAL, "database %u: invalid CSR arrays", d);
+        if (max_id[d] >= (1u << 26)) {
+            // Ids this large take the one-database path (sorted ranks).
+            for (uint32_t e = 0; e < n_db; ++e) {
+                const int r = cpm_db_from_ids(ctx, offsets[e], n_rows[e], ids[e], nnz[e], &out[e]);
+                if (r != CPM_OK) {
+                    for (uint32_t f = 0; f < e; ++f) { cpm_db_free(out[f]); out[f] = nullptr; }
+                    return r;
+                }
+            }
+            return CPM_OK;
+        }
+    }
+    std::vector<uint64_t> row_base(n_db + 1, 0), occ_base(n_db + 1, 0), pres_base(n_db + 1, 0);
+    for (uint32_t d = 0; d < n_db; ++d) {
+        row_base[d + 1] = row_base[d] + off[d].size() - 1;
+        occ_base[d + 1] = occ_base[d] + nnz[d];
+        pres_base[d + 1] = pres_base[d] + (uint64_t)max_id[d] / 32 + 1;
+    }
+    const uint64_t R = row_base[n_db], NNZ = occ_base[n_db], PW = pres_base[n_db];
+    std::vector<uint64_t> h_off(R + 1);
+    std::vector<uint32_t> h_ids(NNZ);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t d = 0; d < (int64_t)n_db; ++d) {
+        for (uint64_t r = 0; r + 1 < off[d].size(); ++r) h_off[row_base[d] + r] = occ_base[d] + off[d][r];
+        if (nnz[d]) memcpy(h_ids.data() + occ_base[d], ids[d], nnz[d] * 4);
+    }
+    h_off[R] = NNZ;
+    DevScope tmp(ctx);
+    uint64_t *d_off = nullptr, *d_occ = nullptr, *d_pres_base = nullptr, *d_rows = nullptr, *d_items = nullptr;
+    uint32_t *d_ids = nullptr, *d_present = nullptr, *d_lut = nullptr;
+    CKR(tmp.alloc(&d_off, R + 1));
+    CKR(tmp.alloc(&d_ids, NNZ));
+    CKR(tmp.alloc(&d_occ, n_db));
+    CKR(tmp.alloc(&d_pres_base, n_db));
+    CKR(tmp.alloc(&d_present, PW));
+    CK(cudaMemcpyAsync(d_off, h_off.data(), (R + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (NNZ) CK(cudaMemcpyAsync(d_ids, h_ids.data(), NNZ * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_occ, occ_base.data(), n_db * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_pres_base, pres_base.data(), n_db * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(d_present, 0, PW * 4, ctx->stream));
+    if (NNZ) {
+        const unsigned blocks = (unsigned)std::min<uint64_t>((NNZ + 255) / 256, (uint64_t)ctx->sms * 16);
+        k_mark_ids_b<<<blocks, 256, 0, ctx->stream>>>(d_ids, NNZ, d_occ, d_pres_base, n_db, d_present);
+        CK(cudaGetLastError());
+    }
+    std::vector<uint32_t> present(PW);
+    CK(cudaMemcpyAsync(present.data(), d_present, PW * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    // ---- host: label order and id -> column table of every database ----
+    std::vector<uint64_t> lut_base(n_db + 1, 0);
+    for (uint32_t d = 0; d < n_db; ++d) lut_base[d + 1] = lut_base[d] + (uint64_t)max_id[d] + 1;
+    std::vector<uint32_t> h_lut(lut_base[n_db], 0);
+    std::vector<std::vector<uint32_t>> labels(n_db);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t d = 0; d < (int64_t)n_db; ++d) {
+        std::vector<uint32_t> uniq;
+        for (uint64_t w = pres_base[d]; w < pres_base[d + 1]; ++w)
+            for (uint32_t m = present[w]; m; m &= m - 1)
+                uniq.push_back((uint32_t)((w - pres_base[d]) * 32 + __builtin_ctz(m)));
+        std::vector<uint64_t> keys(uniq.size());
+        for (size_t i = 0; i < uniq.size(); ++i) keys[i] = decimal_key(uniq[i]);
+        std::vector<uint32_t> order(uniq.size());
+        std::iota(order.begin(), order.end(), 0u);
+        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return keys[a] < keys[b]; });
+        labels[d].resize(uniq.size());
+        for (size_t c = 0; c < order.size(); ++c) {
+            labels[d][c] = uniq[order[c]];
+            h_lut[lut_base[d] + uniq[order[c]]] = (uint32_t)c;
+        }
+    }
+    // ---- device: tidsets of every database, packed in one pass ----
+    std::vector<cpm_db *> dbs(n_db, nullptr);
+    auto cleanup = [&]() {
+        for (cpm_db *x : dbs)
+            if (x) cpm_db_free(x);
+    };
+    std::vector<PackDesc> pd(n_db);
+    std::vector<uint64_t> item_base(n_db + 1, 0);
+    for (uint32_t d = 0; d < n_db; ++d) {
+        cpm_db *db = new cpm_db();
+        dbs[d] = db;
+        db->ctx = ctx;
+        db->n_tx = off[d].size() - 1;
+        db->n_items = (uint32_t)labels[d].size();
+        db->labels = std::move(labels[d]);
+        const int r = db_alloc_bits(ctx, db);
+        if (r != CPM_OK) {
+            cleanup();
+            return r;
+        }
+        pd[d] = PackDesc{reinterpret_cast<uint32_t *>(db->d_bits), db->d_support, nullptr, db->stride,
+                         row_base[d], occ_base[d], pres_base[d], db->n_items, 0};
+        item_base[d + 1] = item_base[d] + db->n_items;
+    }
+    PackDesc *d_pd = nullptr;
+    int r = tmp.alloc(&d_lut, lut_base[n_db]);
+    if (r == CPM_OK) r = tmp.alloc(&d_pd, n_db);
+    if (r == CPM_OK) r = tmp.alloc(&d_rows, n_db);
+    if (r == CPM_OK) r = tmp.alloc(&d_items, n_db);
+    if (r != CPM_OK) {
+        cleanup();
+        return r;
+    }
+    for (uint32_t d = 0; d < n_db; ++d) pd[d].lut = d_lut + lut_base[d];
+    cudaMemcpyAsync(d_lut, h_lut.data(), lut_base[n_db] * 4, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(d_pd, pd.data(), n_db * sizeof(PackDesc), cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(d_rows, row_base.data(), n_db * 8, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(d_items, item_base.data(), n_db * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (R) k_pack_b<<<(unsigned)((R + 255) / 256), 256, 0, ctx->stream>>>(d_off, d_ids, R, d_pd, d_rows, n_db);
+    if (item_base[n_db])
+        k_item_support_b<<<(unsigned)((item_base[n_db] * 32 + 255) / 256), 256, 0, ctx->stream>>>(d_pd, d_items, n_db,
+                                                                                                 item_base[n_db]);
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+        cleanup();
+        return set_err(ctx, CPM_ECUDA, "batched pack failed: %s", cudaGetErrorString(e));
+    }
+    for (uint32_t d = 0; d < n_db; ++d) out[d] = dbs[d];
+    return CPM_OK;
+}
+
 extern "C" int cpm_db_info(const cpm_db *db, uint64_t *n_tx, uint32_t *n_items, uint64_t *words) {
     if (!db) return CPM_EINVAL;
     if (n_tx) *n_tx = db->n_tx;
@@ -428,40 +577,54 @@ static int mine_singletons(cpm_ctx *ctx, cpm_db *db, long long ms, DevScope &ds,
     return CPM_OK;
 }
 
-// Tensor-core Gram of F frequent rows into C (zeroed here); synchronous.
-static int gram_tc_run(cpm_ctx *ctx, DevScope &ds, const uint64_t *bits, uint64_t stride, const uint32_t *d_freq,
-                       uint32_t F, uint32_t *C, cpm_stats &st) {
-    CK(cudaMemsetAsync(C, 0, (size_t)F * F * 4, ctx->stream));
-    // Upper-triangle tiles: A block ti (128 rows) x B block tj (256 columns)
-    // whenever some column of the block lies right of some row.
-    std::vector<GramTile> tiles;
-    const uint32_t nti = (F + tc::BM - 1) / tc::BM, ntj = (F + tc::BN - 1) / tc::BN;
-    for (uint32_t ti = 0; ti < nti; ++ti)
-        for (uint32_t tj = 0; tj < ntj; ++tj)
-            if ((uint64_t)tj * tc::BN + tc::BN - 1 > (uint64_t)ti * tc::BM) tiles.push_back({ti, tj});
-    // K split (in pairs of words, one stage each) so the units cover the GPU.
-    const uint64_t kstages = stride / 2;
-    uint64_t ksplit = std::max<uint64_t>(1, ((uint64_t)ctx->sms * 2 + tiles.size() - 1) / tiles.size());
-    ksplit = std::min<uint64_t>(ksplit, std::max<uint64_t>(1, kstages / 8));
-    const uint64_t stages_per = (kstages + ksplit - 1) / ksplit;
-    ksplit = (kstages + stages_per - 1) / stages_per;
-    GramTile *d_tiles = nullptr;
+// Tensor-core Gram of the selected databases (C zeroed here) in one launch;
+// synchronous (reads the error word).  d_desc / h describe every database.
+static int gram_tc_run(cpm_ctx *ctx, DevScope &ds, const DbDesc *d_desc, const std::vector<DbDesc> &h,
+                       const std::vector<uint32_t> &sel, cpm_stats &st) {
+    // Upper-triangle tiles of each database: A block ti (128 rows) x B block
+    // tj (256 columns) whenever some column of the block lies right of some row.
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> tiles(sel.size());
+    uint64_t tile_stages = 0;
+    for (size_t s = 0; s < sel.size(); ++s) {
+        const DbDesc &D = h[sel[s]];
+        CK(cudaMemsetAsync(D.C, 0, (size_t)D.F * D.F * 4, ctx->stream));
+        const uint32_t nti = (D.F + tc::BM - 1) / tc::BM, ntj = (D.F + tc::BN - 1) / tc::BN;
+        for (uint32_t ti = 0; ti < nti; ++ti)
+            for (uint32_t tj = 0; tj < ntj; ++tj)
+                if ((uint64_t)tj * tc::BN + tc::BN - 1 > (uint64_t)ti * tc::BM) tiles[s].push_back({ti, tj});
+        tile_stages += tiles[s].size() * (D.stride / 2);
+    }
+    // K split: about four units per SM over the whole selection, and at
+    // least 32 stages per unit so the epilogue (one atomic per output) stays
+    // small next to the main loop.
+    const uint64_t per = std::max<uint64_t>(32, (tile_stages + (uint64_t)ctx->sms * 4 - 1) / ((uint64_t)ctx->sms * 4));
+    std::vector<GramUnit> units;
+    for (size_t s = 0; s < sel.size(); ++s) {
+        const DbDesc &D = h[sel[s]];
+        const uint64_t kstages = D.stride / 2;
+        for (auto &t : tiles[s])
+            for (uint64_t k = 0; k < kstages; k += per)
+                units.push_back({sel[s], t.first, t.second, 0, 2 * k, 2 * std::min(kstages, k + per)});
+        // Work issued to the tensor cores: every tile is a full 128x256 block.
+        st.pair_ops += 2ull * (uint64_t)tc::BM * tc::BN * (kstages * 128) * tiles[s].size();
+    }
+    if (units.empty()) return CPM_OK;
+    GramUnit *d_units = nullptr;
     unsigned int *d_err = nullptr;
-    CKR(ds.alloc(&d_tiles, tiles.size()));
+    CKR(ds.alloc(&d_units, units.size()));
     CKR(ds.alloc(&d_err, 1));
-    CK(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(GramTile), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_units, units.data(), units.size() * sizeof(GramUnit), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(d_err, 0, 4, ctx->stream));
-    const uint64_t units = tiles.size() * ksplit;
-    k_gram_tc<<<(unsigned)units, tc::THREADS, tc::SMEM_BYTES, ctx->stream>>>(
-        bits, stride, d_freq, F, d_tiles, (uint32_t)tiles.size(), stages_per * 2, C, d_err);
-    CK(cudaGetLastError());
+    for (size_t u0 = 0; u0 < units.size(); u0 += 1u << 30) {
+        const unsigned nb = (unsigned)std::min<size_t>(units.size() - u0, 1u << 30);
+        k_gram_tc<<<nb, tc::THREADS, tc::SMEM_BYTES, ctx->stream>>>(d_desc, d_units + u0, d_err);
+        CK(cudaGetLastError());
+        st.kernel_launches += 1;
+    }
     unsigned int herr = 0;
     CK(cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if (herr) return set_err(ctx, CPM_ETIMEOUT, "tensor-core Gram pipeline wait ran out");
-    st.kernel_launches += 1;
-    // Work issued to the tensor cores: every tile is a full 128x256 block.
-    st.pair_ops += 2ull * (uint64_t)tc::BM * tc::BN * (kstages * 128) * tiles.size();
     return CPM_OK;
 }
 
@@ -473,7 +636,18 @@ static int pair_gram(cpm_ctx *ctx, cpm_db *db, const uint32_t *d_freq, uint32_t 
     CK(cudaEventRecord(ctx->ev[5], ctx->stream));
     if (use_tc) {
         if (!ctx->tc_ok) return set_err(ctx, CPM_EINVAL, "the tensor-core Gram needs an sm_100 device");
-        CKR(gram_tc_run(ctx, ds, db->d_bits, db->stride, d_freq, F, *d_C, st));
+        std::vector<DbDesc> h(1);
+        h[0].bits = db->d_bits;
+        h[0].support = db->d_support;
+        h[0].freq = const_cast<uint32_t *>(d_freq);
+        h[0].C = *d_C;
+        h[0].stride = db->stride;
+        h[0].n_items = db->n_items;
+        h[0].F = F;
+        DbDesc *d_desc = nullptr;
+        CKR(ds.alloc(&d_desc, 1));
+        CK(cudaMemcpyAsync(d_desc, h.data(), sizeof(DbDesc), cudaMemcpyHostToDevice, ctx->stream));
+        CKR(gram_tc_run(ctx, ds, d_desc, h, std::vector<uint32_t>{0u}, st));
         CK(cudaEventRecord(ctx->ev[6], ctx->stream));
         return CPM_OK;
     }
@@ -535,69 +709,184 @@ static int grow(cpm_ctx *ctx, DeepBuffers &b, uint64_t frames_cap, uint64_t memb
     return CPM_OK;
 }
 
-// One scheduling unit of the deep phase: position p of top-level frame k.
-struct RootUnit {
-    uint32_t frame, p;
-    double key;  // larger first
-};
 
-// Cost-model features of root unit (class with m members, position p).
-// sup[e] = support of member e (the pair {class item, e}); sa = the class
-// item's support; N = transactions; ms = threshold; stride = tidset words.
-static void unit_features(float *x, uint32_t m, uint32_t p, const std::vector<double> &sup, double sa, double N,
-                          double ms, uint32_t stride) {
-    const uint32_t cnt = m - p - 1;
-    const double sp = sup[p];
-    const double inv_n = N > 0 ? 1.0 / N : 0.0;
-    const double msp = std::max(ms, 0.0);
-    // Later siblings, every one when few, an even sample otherwise.
-    const uint32_t step = cnt > 256 ? (cnt + 255) / 256 : 1;
-    double hist[4] = {0, 0, 0, 0}, mean = 0, seen = 0, surv = 0;
-    for (uint32_t q = p + 1; q < m; q += step) {
-        const double r = sa > 0 ? sup[q] / sa : 0.0;
-        hist[std::min(3, (int)(r * 4))] += 1;
-        mean += r;
-        surv += sp * r >= msp ? 1 : 0;
-        seen += 1;
+// Part of the arena kept free for frames that shallow expansion keeps.
+static inline uint64_t persist_cap_reserve(uint64_t arena_words) { return arena_words / 8; }
+
+// Memory-bounded deep phase.  Root units (in scheduler order: d_uid/d_key,
+// largest first) are admitted into rounds while their cost keys fit a share
+// of the arena; each round is one persistent launch with the arena reset to
+// the persistent region.  A round that overflows is discarded (its counters
+// rewound) and retried with half as many units; a single unit that still
+// overflows runs shallow -- only its own intersections -- and its child
+// frame, kept in the persistent region, contributes its positions as new
+// root units, processed next (depth first, so the region stays small).
+static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::vector<DFrame> &top_frames,
+                       const uint32_t *d_uid, const float *d_key, uint64_t n_units, uint64_t base_patterns,
+                       uint64_t P2_total, uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix,
+                       uint64_t spin,
+                       uint64_t pat_need, bool with_db, uint64_t arena_limit_words, bool keys_in_words,
+                       DeepState &hs, cpm_stats &st) {
+    const bool dbg = getenv("CPM_DEBUG") != nullptr;
+    // Fixed tables large enough for any round; the arena takes the rest.
+    const uint64_t frames_cap = 32ull << 20, members_cap = 256ull << 20, queue_cap = 64ull << 20;
+    const uint64_t pat_cap = std::max<uint64_t>(pat_need, 96ull << 20);
+    const uint64_t fixed = frames_cap * sizeof(DFrame) + members_cap * 16 + queue_cap * 8 + pat_cap * 16 + (1ull << 30);
+    uint64_t arena_words = ctx->mem_free > fixed * 2 ? (uint64_t)(ctx->mem_free * 0.75 - fixed) / 8 : 0;
+    if (arena_limit_words) arena_words = std::min(arena_words, arena_limit_words);
+    if (arena_words < 64 * max_stride) return set_err(ctx, CPM_ENOMEM, "no device memory left for deep rounds");
+    // Patterns, members and frames of the top level must survive the regrow.
+    std::vector<uint32_t> par(base_patterns), item(base_patterns), sup(base_patterns), pdb, mp(P2_total), mi(P2_total);
+    std::vector<const uint64_t *> mb(P2_total);
+    CK(cudaMemcpyAsync(par.data(), b.pat_parent, base_patterns * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(item.data(), b.pat_item, base_patterns * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(sup.data(), b.pat_sup, base_patterns * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (with_db) {
+        pdb.resize(base_patterns);
+        CK(cudaMemcpyAsync(pdb.data(), b.pat_db, base_patterns * 4, cudaMemcpyDeviceToHost, ctx->stream));
     }
-    const double scale = seen > 0 ? cnt / seen : 0.0;
-    surv *= scale;
-    x[0] = (float)std::log1p((double)cnt);
-    x[1] = (float)std::log1p((double)m);
-    x[2] = (float)((double)p / m);
-    x[3] = (float)(sp * inv_n);
-    x[4] = (float)(sa * inv_n);
-    x[5] = (float)(msp * inv_n);
-    x[6] = (float)std::log1p(N);
-    x[7] = (float)std::log1p((double)stride);
-    for (int i = 0; i < 4; ++i) x[8 + i] = (float)(seen > 0 ? hist[i] / seen : 0.0);
-    x[12] = (float)(seen > 0 ? mean / seen : 0.0);
-    x[13] = (float)(surv / (cnt + 1.0));
-    x[14] = (float)std::log1p(surv);
-    x[15] = (float)std::log1p(surv * surv * sp * inv_n);
-}
-
-// Learned order: the cost model's predicted subtree intersections, weighted
-// by the tidset length, largest first (the plain order is the fallback).
-static int order_units_learned(cpm_ctx *ctx, DevScope &ds, std::vector<RootUnit> &units,
-                               const std::vector<DFrame> &frames, const std::vector<float> &features) {
-    const uint64_t n = units.size();
-    float *d_x = nullptr, *d_y = nullptr, *d_p = nullptr;
-    CKR(ds.alloc(&d_x, n * cm::NF));
-    CKR(ds.alloc(&d_y, n));
-    CKR(ds.alloc(&d_p, cm::N_PARAMS));
-    CK(cudaMemcpyAsync(d_x, features.data(), n * cm::NF * 4, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(d_p, ctx->model.data(), cm::N_PARAMS * 4, cudaMemcpyHostToDevice, ctx->stream));
-    k_mlp_forward<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(d_p, d_x, n, d_y, 1);
-    CK(cudaGetLastError());
-    std::vector<float> y(n);
-    CK(cudaMemcpyAsync(y.data(), d_y, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(mp.data(), b.mem_pat, P2_total * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(mi.data(), b.mem_item, P2_total * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(mb.data(), b.mem_bits, P2_total * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<uint32_t> uid(n_units);
+    std::vector<float> key(n_units);
+    CK(cudaMemcpyAsync(uid.data(), d_uid, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(key.data(), d_key, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    for (RootUnit &u : units) {
-        const uint64_t id = frames[u.frame].root + u.p;
-        u.key = std::expm1((double)y[id]) * frames[u.frame].stride + (double)(frames[u.frame].m - u.p - 1);
+    CKR(grow(ctx, b, frames_cap, members_cap, queue_cap, arena_words, pat_cap, 1, with_db));
+    CK(cudaMemcpyAsync(b.pat_parent, par.data(), base_patterns * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(b.pat_item, item.data(), base_patterns * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(b.pat_sup, sup.data(), base_patterns * 4, cudaMemcpyHostToDevice, ctx->stream));
+    if (with_db) CK(cudaMemcpyAsync(b.pat_db, pdb.data(), base_patterns * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(b.mem_pat, mp.data(), P2_total * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(b.mem_item, mi.data(), P2_total * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(b.mem_bits, mb.data(), P2_total * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(b.frames, top_frames.data(), top_frames.size() * sizeof(DFrame), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    // Root units as (frame, position, key), front = next.
+    struct Root {
+        uint32_t frame, p;
+        double key;
+    };
+    std::deque<Root> roots;
+    for (uint64_t i = 0; i < n_units; ++i) {
+        uint32_t k = (uint32_t)(std::upper_bound(top_frames.begin(), top_frames.end(), uid[i],
+                                                 [](uint32_t u, const DFrame &f) { return u < f.root; }) -
+                                top_frames.begin()) - 1;
+        // Learned keys already estimate words touched; plain keys are member
+        // counts, scaled by the tidset length.
+        const double words = keys_in_words ? (double)key[i] : (double)key[i] * top_frames[k].stride;
+        roots.push_back({k, uid[i] - top_frames[k].root, std::max(1.0, words)});
     }
-    std::stable_sort(units.begin(), units.end(), [](const RootUnit &a, const RootUnit &b) { return a.key > b.key; });
+    uint64_t persist_frames = top_frames.size(), persist_members = P2_total, persist_arena = 0;
+    uint64_t committed = base_patterns;
+    const double budget = (double)(arena_words - persist_cap_reserve(arena_words)) * 0.8;
+    uint64_t limit = ~0ull;  // units per round
+    std::vector<unsigned long long> q;
+    DeepParams P;
+    P.frames = b.frames; P.frames_cap = b.frames_cap;
+    P.mem_pat = b.mem_pat; P.mem_item = b.mem_item; P.mem_bits = b.mem_bits; P.members_cap = b.members_cap;
+    P.queue = b.queue; P.queue_cap = b.queue_cap;
+    P.arena = b.arena; P.arena_words = b.arena_words;
+    P.pat_parent = b.pat_parent; P.pat_item = b.pat_item; P.pat_sup = b.pat_sup; P.pat_db = b.pat_db;
+    P.pat_cap = b.pat_cap;
+    P.root_cost = nullptr; P.st = b.st; P.max_stride = max_stride; P.spin_limit = spin; P.cta_time = nullptr;
+    const size_t prefix_bytes = max_stride * 8;
+    uint64_t rounds = 0, failed = 0, shallow = 0;
+    float deep_ms = 0.f;
+    auto launch = [&](size_t n_take, uint32_t shallow_mode) -> int {
+        q.clear();
+        for (size_t i = 0; i < n_take; ++i) q.push_back(((unsigned long long)roots[i].frame << 32) | roots[i].p);
+        CK(cudaMemsetAsync(b.queue, 0xff, std::min<uint64_t>(queue_cap, q.size() * 64 + (1u << 20)) * 8, ctx->stream));
+        CK(cudaMemcpyAsync(b.queue, q.data(), q.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+        DeepState s0{};
+        s0.q_tail = q.size();
+        s0.pending = q.size();
+        s0.n_patterns = committed;
+        s0.n_frames = persist_frames;
+        s0.n_members = persist_members;
+        s0.arena_next = persist_arena;
+        CK(cudaMemcpyAsync(b.st, &s0, sizeof s0, cudaMemcpyHostToDevice, ctx->stream));
+        P.shallow = shallow_mode;
+        // Queue entries beyond the memset stay stale: bound the round's queue.
+        P.queue_cap = std::min<uint64_t>(queue_cap, q.size() * 64 + (1u << 20));
+        CK(cudaEventRecord(ctx->ev[2], ctx->stream));
+        if (smem_prefix) k_deep<true><<<grid, block, prefix_bytes, ctx->stream>>>(P);
+        else k_deep<false><<<grid, block, 0, ctx->stream>>>(P);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+        CK(cudaMemcpyAsync(&hs, b.st, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        deep_ms += (float)elapsed_ms(ctx, 2, 3);
+        st.kernel_launches++;
+        st.intersections += hs.intersections;
+        st.bytes_alg += hs.bytes_alg;
+        st.work_items += hs.work_items;
+        ++rounds;
+        return CPM_OK;
+    };
+    // Arena words a round really used per unit of admitted key, measured on
+    // every successful round (keys are only relative estimates).
+    double words_per_key = 1.0;
+    while (!roots.empty()) {
+        size_t take = 0;
+        double est = 0;
+        while (take < roots.size() && take < limit &&
+               (take == 0 || (est + roots[take].key) * words_per_key <= budget))
+            est += roots[take++].key;
+        CKR(launch(take, 0));
+        if (!hs.error) {
+            committed = hs.n_patterns;
+            roots.erase(roots.begin(), roots.begin() + take);
+            limit = limit == ~0ull ? limit : limit * 2;
+            const double used = (double)(hs.arena_next - persist_arena);
+            if (est > 0 && take > 4) words_per_key = std::max(words_per_key * 0.5, std::min(used / est, words_per_key * 4));
+            continue;
+        }
+        if (hs.error & DEEP_ERR_SPIN) return set_err(ctx, CPM_ETIMEOUT, "deep-level kernel wait ran out of spins");
+        if (hs.error & DEEP_ERR_PATTERNS)
+            return set_err(ctx, CPM_EOVERFLOW, "more than %llu patterns", (unsigned long long)pat_cap);
+        ++failed;
+        if (take > 1) {
+            limit = std::max<size_t>(1, take / 2);
+            words_per_key *= 2;
+            continue;
+        }
+        // One root unit whose subtree does not fit: expand it by one level.
+        CKR(launch(1, 1));
+        if (hs.error)
+            return set_err(ctx, CPM_EOVERFLOW, "a single class of %u members exceeds the device arena (error 0x%x)",
+                           top_frames.size() > roots[0].frame ? top_frames[roots[0].frame].m : 0u, hs.error);
+        ++shallow;
+        committed = hs.n_patterns;
+        const Root parent = roots.front();
+        roots.pop_front();
+        if (hs.n_frames > persist_frames) {
+            DFrame c;
+            CK(cudaMemcpy(&c, b.frames + persist_frames, sizeof c, cudaMemcpyDeviceToHost));
+            const uint64_t cid = persist_frames;
+            persist_frames = hs.n_frames;
+            persist_members = hs.n_members;
+            persist_arena = hs.arena_next;
+            for (uint32_t p = c.m - 1; p-- > 0;)
+                roots.push_front({(uint32_t)cid, p, parent.key * (c.m - 1 - p) / std::max(1u, c.m)});
+        }
+        limit = ~0ull;
+    }
+    if (dbg)
+        fprintf(stderr, "cpm: deep rounds %llu (failed %llu, shallow %llu), persistent arena %.1f MB, %.3f ms\n",
+                (unsigned long long)rounds, (unsigned long long)failed, (unsigned long long)shallow,
+                persist_arena * 8 / 1e6, deep_ms);
+    st.retries += failed;
+    st.deep_rounds = rounds;
+    // The caller reads patterns up to hs.n_patterns and the deep time from
+    // these counters.
+    hs.n_patterns = committed;
+    hs.work_items = st.work_items;
+    hs.intersections = st.intersections;
+    hs.bytes_alg = st.bytes_alg;
+    hs.n_frames = persist_frames;
+    ctx->last_deep_ms = deep_ms;
     return CPM_OK;
 }
 
@@ -606,6 +895,15 @@ static int order_units_learned(cpm_ctx *ctx, DevScope &ds, std::vector<RootUnit>
 static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const long long *ms, const cpm_opts &o,
                             cpm_result **res) {
     cpm_stats st{};
+    const bool dbg = getenv("CPM_DEBUG") != nullptr;
+    auto t_start = std::chrono::steady_clock::now();
+    auto lap = [&](const char *what) {
+        if (!dbg) return;
+        const auto now = std::chrono::steady_clock::now();
+        fprintf(stderr, "cpm: host %-24s %.3f ms\n", what,
+                std::chrono::duration<double, std::milli>(now - t_start).count());
+        t_start = now;
+    };
     DevScope ds(ctx);
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     // ---- singletons ----
@@ -637,6 +935,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     std::vector<uint32_t> F(n_db);
     CK(cudaMemcpyAsync(F.data(), d_F, n_db * 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    lap("singletons");
     // ---- pair Grams ----
     uint64_t rows = 0, c_total = 0;
     std::vector<uint64_t> c_off(n_db, 0);
@@ -658,13 +957,14 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     CK(cudaMemcpyAsync(d_desc, h.data(), n_db * sizeof(DbDesc), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaEventRecord(ctx->ev[5], ctx->stream));
     std::vector<BTile> tiles;
+    std::vector<uint32_t> tc_dbs;
     for (uint32_t d = 0; d < n_db; ++d) {
         if (F[d] < 2) continue;
         const bool tc = o.pair_engine == 1 ||
                         (o.pair_engine == 0 && ctx->tc_ok && gram_tc_worthwhile(F[d], dbs[d]->n_tx));
         if (tc) {
             if (!ctx->tc_ok) return set_err(ctx, CPM_EINVAL, "the tensor-core Gram needs an sm_100 device");
-            CKR(gram_tc_run(ctx, ds, h[d].bits, h[d].stride, h[d].freq, F[d], h[d].C, st));
+            tc_dbs.push_back(d);
             continue;
         }
         const uint32_t nt = (F[d] + 63) / 64;
@@ -679,6 +979,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
                 for (uint64_t k = 0; k < words; k += chunk) tiles.push_back({d, ti, tj, 0, k, std::min(words, k + chunk)});
         st.pair_ops += 2ull * dbs[d]->n_tx * F[d] * (uint64_t)F[d];
     }
+    CKR(gram_tc_run(ctx, ds, d_desc, h, tc_dbs, st));
     if (!tiles.empty()) {
         BTile *d_tiles = nullptr;
         CKR(ds.alloc(&d_tiles, tiles.size()));
@@ -700,6 +1001,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         CK(cudaMemcpyAsync(hfreq.data(), freq_all, items_total * 4, cudaMemcpyDeviceToHost, ctx->stream));
     }
     CK(cudaStreamSynchronize(ctx->stream));
+    lap("pairs");
     // Pair numbering and pattern ids: per database, singletons then pairs.
     std::vector<uint64_t> off(rows + 1, 0);
     for (uint64_t r = 0; r < rows; ++r) off[r + 1] = off[r] + cnt[r];
@@ -717,6 +1019,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     CK(cudaMemcpyAsync(off_all, off.data(), (rows + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
     // ---- top-level classes (cuEclat.py:195-200) ----
     std::vector<DFrame> frames;
+    std::vector<FrameAux> aux;
     for (uint32_t d = 0; d < n_db; ++d)
         for (uint32_t i = 0; i < F[d]; ++i) {
             const uint64_t r = h[d].row_base + i;
@@ -725,32 +1028,34 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
             f.mask = h[d].bits + (uint64_t)hfreq[item_off[d] + i] * h[d].stride;
             f.mem_off = off[r];
             f.m = cnt[r];
-            f.root = (uint32_t)frames.size();
+            f.root = 0;
             f.stride = (uint32_t)h[d].stride;
             f.db = d;
             f.minsup = ms[d];
             frames.push_back(f);
+            aux.push_back({(uint32_t)(h[d].pat_base + i), (float)dbs[d]->n_tx, (float)ms[d], 0.f});
         }
-    // Root units: position p of top-level frame k has id frames[k].root + p.
-    std::vector<RootUnit> units;
-    for (uint32_t k = 0; k < frames.size(); ++k) {
-        frames[k].root = (uint32_t)units.size();
-        for (uint32_t p = 0; p + 1 < frames[k].m; ++p) units.push_back({k, p, (double)(frames[k].m - p - 1)});
+    // Root units: position p of top-level frame k has id frames[k].root + p;
+    // they are costed, ordered and queued on the device (k_units.cuh).
+    uint64_t n_units = 0;
+    for (DFrame &f : frames) {
+        f.root = (uint32_t)n_units;
+        n_units += f.m - 1;
     }
     const bool learned = o.scheduler == CPM_SCHED_LEARNED && !ctx->model.empty();
-    const bool need_features = (learned || o.collect_trace) && !units.empty();
-    if (!learned)
-        std::stable_sort(units.begin(), units.end(), [](const RootUnit &a, const RootUnit &b) { return a.key > b.key; });
+    lap("frames and units");
     // ---- deep phase, grown and rerun on overflow ----
     cpm_db *db0 = dbs[0];
     DeepBuffers b;
     b.owner = ctx;
     const bool with_db = n_db > 1;
     uint64_t frames_cap = std::max<uint64_t>({1024, frames.size() * 8 + P2_total * 2, n_db == 1 ? db0->hint_frames : 0});
-    uint64_t members_cap = std::max<uint64_t>({4096, P2_total * 16, n_db == 1 ? db0->hint_members : 0});
-    uint64_t queue_cap = std::max<uint64_t>({4096, units.size() * 8 + P2_total * 4, n_db == 1 ? db0->hint_queue : 0});
+    // Member entries are reserved for every sibling of every unit (~ the
+    // intersections), several times the pair count on deep lattices.
+    uint64_t members_cap = std::max<uint64_t>({4096, P2_total * 64, n_db == 1 ? db0->hint_members : 0});
+    uint64_t queue_cap = std::max<uint64_t>({4096, n_units * 8 + P2_total * 4, n_db == 1 ? db0->hint_queue : 0});
     uint64_t pat_cap = std::max<uint64_t>({4096, base_patterns * 16, n_db == 1 ? db0->hint_patterns : 0});
-    const uint64_t arena_budget = (uint64_t)(ctx->mem_free * 0.6) / 8;
+    const uint64_t arena_budget = o.arena_bytes ? o.arena_bytes / 8 : (uint64_t)(ctx->mem_free * 0.6) / 8;
     uint64_t arena_words = o.arena_bytes ? o.arena_bytes / 8
                                          : std::min<uint64_t>(arena_budget, std::max<uint64_t>(
                                                {(uint64_t)4096 * max_stride, P2_total * 8 * max_stride,
@@ -758,20 +1063,46 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     const uint64_t spin = o.spin_limit ? o.spin_limit : (1ull << 26);
     const size_t prefix_bytes = max_stride * 8;
     const bool smem_prefix = prefix_bytes <= 200 * 1024;
-    if (smem_prefix && (ctx->deep_occ_smem < 0 || ctx->deep_occ_bytes != prefix_bytes)) {
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_smem, k_deep<true>, 256, prefix_bytes));
+    // Long tidsets leave room for one CTA per SM: give it 16 warps so that
+    // enough loads stay in flight; short ones run up to four 8-warp CTAs.
+    const unsigned block = max_stride >= 2048 ? 512 : 256;
+    if (smem_prefix && (ctx->deep_occ_smem < 0 || ctx->deep_occ_bytes != prefix_bytes || ctx->deep_occ_block != block)) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_smem, k_deep<true>, block, prefix_bytes));
         ctx->deep_occ_bytes = prefix_bytes;
-    } else if (!smem_prefix && ctx->deep_occ_global < 0) {
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_global, k_deep<false>, 256, 0));
+        ctx->deep_occ_block = block;
+    } else if (!smem_prefix && (ctx->deep_occ_global < 0 || ctx->deep_occ_block != block)) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_global, k_deep<false>, block, 0));
+        ctx->deep_occ_block = block;
     }
-    // Up to four CTAs per SM keep enough loads in flight.
     const int cta_per_sm = std::min(4, std::max(1, smem_prefix ? ctx->deep_occ_smem : ctx->deep_occ_global));
     const unsigned grid = (unsigned)(ctx->sms * cta_per_sm);
     DeepState hs{};
-    std::vector<float> features;  // per root unit (cost-model inputs)
-    std::vector<unsigned long long> init;
+    bool rounds = false;
+    std::vector<float> features;  // per root unit, when traced (cost-model inputs)
+    FrameAux *d_aux = nullptr;
+    float *d_key = nullptr, *d_key2 = nullptr, *d_feat = nullptr, *d_model = nullptr;
+    uint32_t *d_uid = nullptr, *d_uid2 = nullptr;
+    void *d_sort_tmp = nullptr;
+    size_t sort_bytes = 0;
+    if (n_units) {
+        CKR(ds.alloc(&d_aux, aux.size()));
+        CKR(ds.alloc(&d_key, n_units));
+        CKR(ds.alloc(&d_key2, n_units));
+        CKR(ds.alloc(&d_uid, n_units));
+        CKR(ds.alloc(&d_uid2, n_units));
+        if (o.collect_trace) CKR(ds.alloc(&d_feat, n_units * cm::NF));
+        if (learned) {
+            CKR(ds.alloc(&d_model, cm::N_PARAMS));
+            CK(cudaMemcpyAsync(d_model, ctx->model.data(), cm::N_PARAMS * 4, cudaMemcpyHostToDevice, ctx->stream));
+        }
+        CK(cudaMemcpyAsync(d_aux, aux.data(), aux.size() * sizeof(FrameAux), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cub::DeviceRadixSort::SortPairsDescending(nullptr, sort_bytes, d_key, d_key2, d_uid, d_uid2,
+                                                     (int64_t)n_units, 0, 32, ctx->stream));
+        CKR(ds.alloc(reinterpret_cast<unsigned char **>(&d_sort_tmp), sort_bytes));
+    }
+
     for (int attempt = 0;; ++attempt) {
-        CKR(grow(ctx, b, frames_cap, members_cap, queue_cap, arena_words, pat_cap + base_patterns, units.size(),
+        CKR(grow(ctx, b, frames_cap, members_cap, queue_cap, arena_words, pat_cap + base_patterns, n_units,
                  with_db));
         if (members_cap < P2_total) return set_err(ctx, CPM_EINTERNAL, "member table too small");
         if (rows) {
@@ -786,36 +1117,43 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
             hs.n_patterns = base_patterns;
             break;
         }
-        if (need_features && features.empty()) {
-            // Features read the supports of every class's members (the pairs)
-            // and of the class items (the singletons).
-            std::vector<uint32_t> pat_sup_h(base_patterns);
-            CK(cudaMemcpyAsync(pat_sup_h.data(), b.pat_sup, base_patterns * 4, cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
-            features.assign(units.size() * cm::NF, 0.f);
-            for (uint32_t k = 0; k < frames.size(); ++k) {
-                const DFrame &f = frames[k];
-                const DbDesc &D = h[f.db];
-                const uint64_t row = std::upper_bound(off.begin(), off.end(), f.mem_off) - off.begin() - 1;
-                const double sa = pat_sup_h[D.pat_base + (row - D.row_base)];
-                std::vector<double> sup(f.m);
-                for (uint32_t e = 0; e < f.m; ++e) sup[e] = pat_sup_h[D.pat_base + D.F + (f.mem_off + e - D.pair_base)];
-                for (uint32_t p = 0; p + 1 < f.m; ++p)
-                    unit_features(&features[(uint64_t)(f.root + p) * cm::NF], f.m, p, sup, sa,
-                                  (double)dbs[f.db]->n_tx, (double)ms[f.db], f.stride);
-            }
-            if (learned) CKR(order_units_learned(ctx, ds, units, frames, features));
-        }
-        if (init.empty())
-            for (const RootUnit &u : units) init.push_back(((unsigned long long)u.frame << 32) | u.p);
         CK(cudaMemcpyAsync(b.frames, frames.data(), frames.size() * sizeof(DFrame), cudaMemcpyHostToDevice,
                            ctx->stream));
         CK(cudaMemsetAsync(b.queue, 0xff, b.queue_cap * 8, ctx->stream));
-        CK(cudaMemcpyAsync(b.queue, init.data(), init.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemsetAsync(b.root_cost, 0, std::max<size_t>(1, units.size()) * 8, ctx->stream));
+        // Key every root unit (size, or predicted cost), sort largest first
+        // (stable), write the queue -- all on the device.
+        k_unit_keys<<<(unsigned)((n_units + 127) / 128), 128, 0, ctx->stream>>>(
+            b.frames, (uint32_t)frames.size(), d_aux, (uint32_t)n_units, b.mem_pat, b.pat_sup, d_model, d_feat, d_key,
+            d_uid);
+        CK(cudaGetLastError());
+        CK(cub::DeviceRadixSort::SortPairsDescending(d_sort_tmp, sort_bytes, d_key, d_key2, d_uid, d_uid2,
+                                                     (int64_t)n_units, 0, 32, ctx->stream));
+        k_fill_queue<<<(unsigned)((n_units + 255) / 256), 256, 0, ctx->stream>>>(b.frames, (uint32_t)frames.size(),
+                                                                               d_uid2, (uint32_t)n_units, b.queue);
+        CK(cudaGetLastError());
+        st.kernel_launches += 3;
+        if (attempt == 0) {
+            // Estimated child-tidset words of the whole deep phase (learned
+            // keys estimate words touched; plain keys count later members).
+            std::vector<float> keys(n_units);
+            CK(cudaMemcpyAsync(keys.data(), d_key2, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            double est = 0;
+            for (float k : keys) est += learned ? (double)k : (double)k * max_stride;
+            if (est > (double)arena_budget) {
+                rounds = true;
+                break;
+            }
+        }
+        if (d_feat && features.empty()) {
+            features.resize(n_units * cm::NF);
+            CK(cudaMemcpyAsync(features.data(), d_feat, n_units * cm::NF * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        CK(cudaMemsetAsync(b.root_cost, 0, std::max<size_t>(1, n_units) * 8, ctx->stream));
+
         hs = DeepState{};
-        hs.q_tail = init.size();
-        hs.pending = init.size();
+        hs.q_tail = n_units;
+        hs.pending = n_units;
         hs.n_patterns = base_patterns;
         hs.n_frames = frames.size();
         hs.n_members = P2_total;
@@ -828,14 +1166,42 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         P.pat_parent = b.pat_parent; P.pat_item = b.pat_item; P.pat_sup = b.pat_sup; P.pat_db = b.pat_db;
         P.pat_cap = b.pat_cap;
         P.root_cost = b.root_cost; P.st = b.st; P.max_stride = max_stride; P.spin_limit = spin;
+        unsigned long long *d_ct = nullptr;
+        const bool timing = getenv("CPM_DEBUG") != nullptr;
+        if (timing) {
+            CKR(ds.alloc(&d_ct, 2ull * grid));
+            CK(cudaMemsetAsync(d_ct, 0, 16ull * grid, ctx->stream));
+        }
+        P.cta_time = d_ct;
+        P.shallow = 0;
         CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-        if (smem_prefix) k_deep<true><<<grid, 256, prefix_bytes, ctx->stream>>>(P);
-        else k_deep<false><<<grid, 256, 0, ctx->stream>>>(P);
+        if (smem_prefix) k_deep<true><<<grid, block, prefix_bytes, ctx->stream>>>(P);
+        else k_deep<false><<<grid, block, 0, ctx->stream>>>(P);
         CK(cudaGetLastError());
         CK(cudaEventRecord(ctx->ev[3], ctx->stream));
         st.kernel_launches++;
         CK(cudaMemcpyAsync(&hs, b.st, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        if (timing) {
+            std::vector<unsigned long long> ct(2ull * grid);
+            CK(cudaMemcpy(ct.data(), d_ct, 16ull * grid, cudaMemcpyDeviceToHost));
+            unsigned long long busy = 0, first = ~0ull, last = 0;
+            std::vector<unsigned long long> exits;
+            for (unsigned c = 0; c < grid; ++c) {
+                busy += ct[2 * c];
+                if (ct[2 * c + 1]) {
+                    first = std::min(first, ct[2 * c + 1]);
+                    last = std::max(last, ct[2 * c + 1]);
+                    exits.push_back(ct[2 * c + 1]);
+                }
+            }
+            std::sort(exits.begin(), exits.end());
+            const double span = (double)elapsed_ms(ctx, 2, 3) * 1e6;
+            fprintf(stderr, "cpm: deep %.3f ms, grid %u, busy %.1f%% of grid x span, exits: first %.3f ms before "
+                    "last, median %.3f ms before last, units %llu\n", span / 1e6, grid,
+                    100.0 * busy / (span * grid), (last - first) / 1e6,
+                    exits.empty() ? 0.0 : (last - exits[exits.size() / 2]) / 1e6, hs.work_items);
+        }
         if (!hs.error) break;
         if (hs.error & DEEP_ERR_SPIN)
             return set_err(ctx, CPM_ETIMEOUT, "deep-level kernel wait ran out of spins (limit %llu)",
@@ -854,15 +1220,20 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         st.retries++;
         // Counters at the failure are lower bounds of the final need: grow
         // every buffer past them (one overflow usually means several).
-        frames_cap = std::max<uint64_t>(frames_cap * 4, hs.n_frames * 4);
-        members_cap = std::max<uint64_t>(members_cap * 4, hs.n_members * 4);
-        queue_cap = std::max<uint64_t>(queue_cap * 4, hs.q_tail * 4);
-        pat_cap = std::max<uint64_t>(pat_cap * 4, hs.n_patterns * 4);
-        if ((hs.error & DEEP_ERR_ARENA) && arena_words >= arena_budget)
-            return set_err(ctx, CPM_EOVERFLOW, "deep-level arena exceeds device memory (%llu words)",
-                           (unsigned long long)arena_words);
+        frames_cap = std::max<uint64_t>(frames_cap * 8, hs.n_frames * 8);
+        members_cap = std::max<uint64_t>(members_cap * 8, hs.n_members * 8);
+        queue_cap = std::max<uint64_t>(queue_cap * 8, hs.q_tail * 8);
+        pat_cap = std::max<uint64_t>(pat_cap * 8, hs.n_patterns * 8);
+        if ((hs.error & DEEP_ERR_ARENA) && arena_words >= arena_budget) {
+            rounds = true;  // the child tidsets do not fit at once: bounded rounds below
+            break;
+        }
         arena_words = std::min<uint64_t>(arena_budget, std::max<uint64_t>(arena_words * 4, hs.arena_next * 4));
     }
+    if (rounds) CKR(deep_rounds(ctx, ds, b, frames, d_uid2, d_key2, n_units, base_patterns, P2_total, max_stride,
+                                grid, block, smem_prefix, spin, pat_cap + base_patterns, with_db,
+                                o.arena_bytes ? o.arena_bytes / 8 : 0, learned, hs, st));
+    lap("deep phase");
     if (n_db == 1) {
         // Remember what this database needed so that the next mine() starts there.
         db0->hint_frames = std::max<uint64_t>(db0->hint_frames, hs.n_frames + hs.n_frames / 4 + 64);
@@ -883,9 +1254,9 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         }
     }
     std::vector<unsigned long long> rc;
-    if (o.collect_trace && !units.empty()) {
-        rc.resize(units.size());
-        CK(cudaMemcpyAsync(rc.data(), b.root_cost, units.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if (o.collect_trace && n_units) {
+        rc.resize(n_units);
+        CK(cudaMemcpyAsync(rc.data(), b.root_cost, n_units * 8, cudaMemcpyDeviceToHost, ctx->stream));
     }
     CK(cudaEventRecord(ctx->ev[4], ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -894,11 +1265,12 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     st.intersections = hs.intersections;
     st.bytes_alg = hs.bytes_alg;
     st.ms_pairs = rows ? elapsed_ms(ctx, 5, 6) : 0.0;
-    st.ms_deep = frames.empty() ? 0.0 : elapsed_ms(ctx, 2, 3);
+    st.ms_deep = frames.empty() ? 0.0 : rounds ? ctx->last_deep_ms : elapsed_ms(ctx, 2, 3);
     st.ms_total = elapsed_ms(ctx, 0, 4);
     st.deep_gbs = st.ms_deep > 0 ? st.bytes_alg / (st.ms_deep * 1e6) : 0.0;
     st.pair_tops = st.ms_pairs > 0 ? st.pair_ops / (st.ms_pairs * 1e9) : 0.0;
     st.n_patterns = n;
+    lap("pattern download");
     // ---- split the pattern tree per database (parents precede children) ----
     if (n_db == 1) {
         res[0]->parent.swap(par);
@@ -1337,6 +1709,26 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
     return CPM_OK;
 }
 
+extern "C" int cpm_results_copy(cpm_result *const *res, uint32_t n, int order, uint64_t *sizes,
+                                uint64_t *offsets, uint32_t *items, uint64_t *supports) {
+    if (!res || !sizes) return CPM_EINVAL;
+    // sizes[2k], sizes[2k+1] = patterns and item slots of result k; with
+    // output arrays, result k's rows follow result k-1's (offsets restart at 0
+    // for every result and take n_k + 1 entries).
+    for (uint32_t k = 0; k < n; ++k)
+        if (!res[k] || cpm_result_size(res[k], &sizes[2 * k], &sizes[2 * k + 1]) != CPM_OK) return CPM_EINVAL;
+    if (!offsets || !supports) return CPM_OK;
+    uint64_t o = 0, it = 0, sp = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const int r = cpm_result_copy(res[k], order, offsets + o, items ? items + it : nullptr, supports + sp);
+        if (r != CPM_OK) return r;
+        o += sizes[2 * k] + 1;
+        it += sizes[2 * k + 1];
+        sp += sizes[2 * k];
+    }
+    return CPM_OK;
+}
+
 extern "C" int cpm_result_from_tree(const int64_t *parent, const uint32_t *item, const uint64_t *support,
                                     uint64_t n, cpm_result **out) {
     if (!out || (n && (!parent || !item || !support))) return CPM_EINVAL;
@@ -1767,6 +2159,8 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     P.arena = d_arena; P.arena_words = arena_slots * stride;
     P.pat_parent = d_parent; P.pat_item = d_item; P.pat_sup = d_support; P.pat_db = nullptr; P.pat_cap = capacity;
     P.root_cost = d_root_cost; P.st = d_st; P.max_stride = stride; P.spin_limit = 1ull << 26;
+    P.cta_time = nullptr;
+    P.shallow = 0;
     // Each warp keeps one scratch tidset: leave at least half the arena to children.
     const size_t prefix_bytes = stride * 8;
     const bool smem_prefix = prefix_bytes <= 200 * 1024;

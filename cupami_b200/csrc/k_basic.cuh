@@ -164,3 +164,91 @@ __global__ void k_ref_intersect(const uint32_t *__restrict__ prefix, const uint3
 }
 
 }  // namespace cpm
+
+namespace cpm {
+
+// Batched loading: databases concatenated, rows and occurrences numbered
+// globally.  One descriptor per database.
+struct PackDesc {
+    uint32_t *bits32;      // tidsets of this database (32-bit view)
+    uint32_t *support;     // per column
+    const uint32_t *lut;   // id -> column
+    uint64_t stride;       // 64-bit words per tidset
+    uint64_t row_base;     // first global row
+    uint64_t occ_base;     // first global occurrence (index into ids)
+    uint64_t present_base; // first word of this database's presence bitmap
+    uint32_t n_items, pad;
+};
+
+__device__ __forceinline__ uint32_t desc_of(const uint64_t *__restrict__ bases, uint32_t n, uint64_t x) {
+    uint32_t lo = 0, hi = n;  // last k with bases[k] <= x
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (bases[mid] <= x) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Presence bitmaps of every database (occ_bases[d] = first occurrence of d).
+__global__ void k_mark_ids_b(const uint32_t *__restrict__ ids, uint64_t nnz, const uint64_t *__restrict__ occ_bases,
+                             const uint64_t *__restrict__ present_bases, uint32_t n_db, uint32_t *__restrict__ present) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t d = desc_of(occ_bases, n_db, i);
+        const uint32_t v = ids[i];
+        atomicOr(present + present_bases[d] + (v >> 5), 1u << (v & 31));
+    }
+}
+
+// k_pack over all databases: one thread per global (non-empty) row; the
+// warp's 32 rows may span two databases, so lanes merge by (database, column).
+__global__ void k_pack_b(const uint64_t *__restrict__ offsets, const uint32_t *__restrict__ ids, uint64_t n_rows,
+                         const PackDesc *__restrict__ d, const uint64_t *__restrict__ row_bases, uint32_t n_db) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned lane = threadIdx.x & 31;
+    const bool valid = r < n_rows;
+    const uint32_t db = valid ? desc_of(row_bases, n_db, r) : 0;
+    const PackDesc D = d[db];
+    const uint64_t b = valid ? offsets[r] : 0;
+    const uint32_t len = valid ? (uint32_t)(offsets[r + 1] - b) : 0;
+    const uint32_t maxlen = warp_max_u32(len);
+    const uint64_t lr = r - D.row_base;  // row within its database
+    for (uint32_t k = 0; k < maxlen; ++k) {
+        uint64_t key = ~0ull;
+        uint32_t c = 0;
+        if (k < len) {
+            c = __ldg(D.lut + __ldg(ids + b + k));
+            key = ((uint64_t)db << 32) | c;
+        }
+        // Lanes of one database share the word only when they also share lr / 32.
+        key ^= (uint64_t)(lr >> 5) << 52;
+        const unsigned grp = __match_any_sync(CPM_FULL, key);
+        if (k < len && lane == (unsigned)(__ffs(grp) - 1)) {
+            // OR of 1 << (row % 32) over the group (rows are consecutive lanes)
+            uint32_t mask = 0;
+            for (unsigned g = grp; g; g &= g - 1) {
+                const unsigned l = __ffs(g) - 1;
+                mask |= 1u << ((lr + l - lane) & 31);
+            }
+            atomicOr(D.bits32 + (uint64_t)c * D.stride * 2 + (lr >> 5), mask);
+        }
+    }
+}
+
+// Singleton supports of every database: one warp per (database, column).
+__global__ void k_item_support_b(const PackDesc *__restrict__ d, const uint64_t *__restrict__ item_bases, uint32_t n_db,
+                                 uint64_t total_items) {
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (w >= total_items) return;
+    const uint32_t db = desc_of(item_bases, n_db, w);
+    const PackDesc D = d[db];
+    const uint64_t c = w - item_bases[db];
+    const ulonglong2 *row = reinterpret_cast<const ulonglong2 *>(reinterpret_cast<const uint64_t *>(D.bits32) + c * D.stride);
+    uint32_t s = 0;
+    for (uint64_t v = lane; v < D.stride / 2; v += 32) s += popc2(ld_stream(row + v));
+    s = warp_sum_u32(s);
+    if (!lane) D.support[c] = s;
+}
+
+}  // namespace cpm

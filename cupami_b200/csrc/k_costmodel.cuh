@@ -31,6 +31,23 @@ constexpr int TRAIN_COUNT = OFF_YMU - OFF_W1;  // W1, b1, w2, b2
 
 }  // namespace cm
 
+// Prediction (log-cost space) for one standardised-on-the-fly sample, with
+// the parameters already staged in shared memory.
+__device__ __forceinline__ float mlp_eval(const float *p, const float *xin) {
+    using namespace cm;
+    float x[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) x[f] = (xin[f] - p[OFF_MU + f]) * p[OFF_IS + f];
+    float out = p[OFF_B2];
+    for (int h = 0; h < H; ++h) {
+        float a = p[OFF_B1 + h];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) a += p[OFF_W1 + h * NF + f] * x[f];
+        out += p[OFF_W2 + h] * fmaxf(a, 0.f);
+    }
+    return out * p[OFF_YSD] + p[OFF_YMU];
+}
+
 // y[i] = prediction for sample i (standardised space when raw == 0, else
 // log-cost space).  One thread per sample, parameters staged in shared memory.
 __global__ void k_mlp_forward(const float *__restrict__ params, const float *__restrict__ X, uint64_t n,

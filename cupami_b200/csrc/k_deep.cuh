@@ -73,7 +73,15 @@ struct DeepParams {
     DeepState *st;
     uint64_t max_stride;            // largest frame stride (shared-memory prefix size)
     unsigned long long spin_limit;
+    unsigned long long *cta_time;   // optional [2 * grid]: busy ns, exit time (globaltimer)
+    uint32_t shallow;               // 1: child frames are recorded, not queued
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ void deep_fail(DeepState *st, unsigned bit) { atomicOr(&st->error, bit); }
 
@@ -106,7 +114,7 @@ __device__ __forceinline__ const ulonglong2 *ld_ptr(const uint64_t *const *p) {
 }
 
 template <bool SMEM_PREFIX>
-__global__ void __launch_bounds__(256) k_deep(DeepParams P) {
+__global__ void __launch_bounds__(512) k_deep(DeepParams P) {
     extern __shared__ ulonglong2 s_prefix[];
     __shared__ unsigned long long s_item;
     __shared__ int s_stop, s_ok, s_grant;
@@ -117,12 +125,13 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
     const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     DeepState *st = P.st;
     // Per-CTA statistics (thread 0), added to the global counters at exit.
-    unsigned long long c_inter = 0, c_bytes = 0, c_units = 0, c_surv = 0;
+    unsigned long long c_inter = 0, c_bytes = 0, c_units = 0, c_surv = 0, c_busy = 0, t_unit = 0;
 
     for (;;) {
         if (threadIdx.x == 0) s_stop = deep_claim(P, &s_item);
         __syncthreads();
         if (s_stop) break;
+        if (threadIdx.x == 0 && P.cta_time) t_unit = global_ns();
         const uint32_t fid = (uint32_t)(s_item >> 32), p = (uint32_t)s_item;
         const DFrame *fp = P.frames + fid;
         const ulonglong2 *mk = reinterpret_cast<const ulonglong2 *>(
@@ -158,21 +167,21 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
             const uint32_t sib_item = __ldcg(P.mem_item + mi);
             uint32_t s = 0;
             uint64_t v = lane;
-            for (; v + 96 < n2; v += 128) {
-                ulonglong2 x0 = ld_cg(sb + v), x1 = ld_cg(sb + v + 32);
-                ulonglong2 x2 = ld_cg(sb + v + 64), x3 = ld_cg(sb + v + 96);
-                if (SMEM_PREFIX) {
-                    x0 = and2(x0, s_prefix[v]); x1 = and2(x1, s_prefix[v + 32]);
-                    x2 = and2(x2, s_prefix[v + 64]); x3 = and2(x3, s_prefix[v + 96]);
-                } else {
-                    x0 = and2(x0, ld_cg(pb + v)); x1 = and2(x1, ld_cg(pb + v + 32));
-                    x2 = and2(x2, ld_cg(pb + v + 64)); x3 = and2(x3, ld_cg(pb + v + 96));
-                    if (mk) {
-                        x0 = and2(x0, ld_cg(mk + v)); x1 = and2(x1, ld_cg(mk + v + 32));
-                        x2 = and2(x2, ld_cg(mk + v + 64)); x3 = and2(x3, ld_cg(mk + v + 96));
+            // Eight 16-byte loads in flight per lane (4 KB per warp).
+            for (; v + 224 < n2; v += 256) {
+                ulonglong2 x[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) x[u] = ld_cg(sb + v + 32 * u);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (SMEM_PREFIX) {
+                        x[u] = and2(x[u], s_prefix[v + 32 * u]);
+                    } else {
+                        x[u] = and2(x[u], ld_cg(pb + v + 32 * u));
+                        if (mk) x[u] = and2(x[u], ld_cg(mk + v + 32 * u));
                     }
+                    s += popc2(x[u]);
                 }
-                s += popc2(x0) + popc2(x1) + popc2(x2) + popc2(x3);
             }
             for (; v < n2; v += 32) {
                 ulonglong2 x = ld_cg(sb + v);
@@ -285,9 +294,12 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
         __syncthreads();
         if (threadIdx.x == 0 && s_grant) {
             const unsigned long long nf = atomicAdd(&st->n_frames, 1ull);
-            const unsigned long long qb = atomicAdd(&st->q_tail, (unsigned long long)(ns - 1));
+            // Shallow launches keep the child frame for the host (its
+            // positions become root units of later rounds) instead of
+            // queueing them.
+            const unsigned long long qb = P.shallow ? 0ull : atomicAdd(&st->q_tail, (unsigned long long)(ns - 1));
             if (nf >= P.frames_cap) deep_fail(st, DEEP_ERR_FRAMES);
-            else if (qb + ns - 1 > P.queue_cap) deep_fail(st, DEEP_ERR_QUEUE);
+            else if (!P.shallow && qb + ns - 1 > P.queue_cap) deep_fail(st, DEEP_ERR_QUEUE);
             else {
                 DFrame c;
                 c.mask = nullptr;
@@ -298,10 +310,14 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
                 c.db = db;
                 c.minsup = minsup;
                 P.frames[nf] = c;
-                atomicAdd(&st->pending, (unsigned long long)(ns - 1));
-                __threadfence();
-                s_fid = nf;
-                s_qbase = qb;
+                if (!P.shallow) {
+                    atomicAdd(&st->pending, (unsigned long long)(ns - 1));
+                    __threadfence();
+                    s_fid = nf;
+                    s_qbase = qb;
+                } else {
+                    __threadfence();
+                }
             }
         }
         __syncthreads();
@@ -316,9 +332,14 @@ __global__ void __launch_bounds__(256) k_deep(DeepParams P) {
             c_units += 1;
             c_surv += ns;
             if (P.root_cost) atomicAdd(P.root_cost + root, (unsigned long long)cnt);
+            if (P.cta_time) c_busy += global_ns() - t_unit;
             __threadfence();
             atomicAdd(&st->pending, ~0ull);  // pending -= 1
         }
+    }
+    if (threadIdx.x == 0 && P.cta_time) {
+        P.cta_time[2 * blockIdx.x] = c_busy;
+        P.cta_time[2 * blockIdx.x + 1] = global_ns();
     }
     if (threadIdx.x == 0 && c_units) {
         atomicAdd(&st->intersections, c_inter);

@@ -18,6 +18,7 @@
 // the host sees the error word.
 #pragma once
 #include "common.cuh"
+#include "k_batch.cuh"
 
 namespace cpm {
 namespace tc {
@@ -95,16 +96,17 @@ __device__ __forceinline__ uint32_t expand4(uint32_t nib) {
 
 }  // namespace tc
 
-struct GramTile {
-    uint32_t ti, tj;  // A block (rows of 128 items), B block (rows of 256 items)
+// One unit: database db, A block ti (128 rows), B block tj (256 columns),
+// words [kw_begin, kw_end) of the tidsets (a whole number of 2-word stages).
+struct GramUnit {
+    uint32_t db, ti, tj, pad;
+    uint64_t kw_begin, kw_end;
 };
 
-// One unit = (tile, K split).  C must be zeroed.  *err gets a nonzero word if
-// any wait ran out.
+// C of every database must be zeroed.  *err gets a nonzero word if any wait
+// ran out.
 __global__ void __launch_bounds__(tc::THREADS, 1)
-    k_gram_tc(const uint64_t *__restrict__ bits, uint64_t stride, const uint32_t *__restrict__ freq, uint32_t F,
-              const GramTile *__restrict__ tiles, uint32_t n_tiles, uint64_t k_chunk_words,
-              uint32_t *__restrict__ C, unsigned int *__restrict__ err) {
+    k_gram_tc(const DbDesc *__restrict__ dbs, const GramUnit *__restrict__ units, unsigned int *__restrict__ err) {
     using namespace tc;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[STAGES];
@@ -114,12 +116,15 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
     __shared__ int abort_flag;
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t unit = blockIdx.x;
-    const uint32_t tile_idx = unit % n_tiles;
-    const uint32_t ksplit_idx = unit / n_tiles;
-    const GramTile tile = tiles[tile_idx];
-    const uint64_t kw_begin = (uint64_t)ksplit_idx * k_chunk_words;
-    const uint64_t kw_end = min(stride, kw_begin + k_chunk_words);
+    const GramUnit tile = units[blockIdx.x];
+    const DbDesc D = dbs[tile.db];
+    const uint64_t *__restrict__ bits = D.bits;
+    const uint64_t stride = D.stride;
+    const uint32_t *__restrict__ freq = D.freq;
+    const uint32_t F = D.F;
+    uint32_t *__restrict__ C = D.C;
+    const uint64_t kw_begin = tile.kw_begin;
+    const uint64_t kw_end = min(stride, tile.kw_end);
     const uint32_t n_k = kw_end > kw_begin ? (uint32_t)((kw_end - kw_begin + 1) / 2) : 0;  // 2 words per stage
 
     unsigned char *smem = reinterpret_cast<unsigned char *>(

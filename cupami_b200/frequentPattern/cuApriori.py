@@ -65,6 +65,9 @@ class cuApriori:
     _SPIN_LIMIT = 0
     #: Pair-level engine: 0 automatic, 1 tensor-core Gram, 2 CUDA-core Gram.
     _PAIR_ENGINE = 0
+    #: Device arena for child tidsets in bytes (0: as much as the GPU holds).
+    #: A small arena makes the deep levels run in memory-bounded rounds.
+    _ARENA_BYTES = 0
 
     def __init__(self, iFile, minSup, sep=None, use_gds="auto", use_gpu_io="auto"):
         loading_start = time.perf_counter()
@@ -252,6 +255,7 @@ class cuApriori:
         if self._SPIN_LIMIT:
             opts.spin_limit = int(self._SPIN_LIMIT)
         opts.pair_engine = int(self._PAIR_ENGINE)
+        opts.arena_bytes = int(self._ARENA_BYTES)
         return opts
 
     def mine(self):

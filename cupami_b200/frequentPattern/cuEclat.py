@@ -67,7 +67,12 @@ class cuEclat(cuApriori):
             from .. import costmodel
 
             costmodel.ensure_default(ctx)
-        dbs, labels = zip(*(m._deviceDatabase(ctx) for m in miners))
+        if all(m._csr is not None for m in miners):
+            # Integer-id sources: one upload and one packing pass for the whole batch.
+            dbs = _native.Database.from_ids_batch(ctx, [m._csr for m in miners])
+            labels = [[str(v) for v in db.labels.tolist()] for db in dbs]
+        else:
+            dbs, labels = zip(*(m._deviceDatabase(ctx) for m in miners))
         try:
             results = _native.mine_batch(ctx, list(dbs), [m._minSup for m in miners], miners[0]._options(),
                                          cls._ORDER)

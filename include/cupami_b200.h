@@ -90,7 +90,8 @@ typedef struct {
     uint64_t bytes_alg;            /* sum over units of 8*W*(1 + siblings + survivors) */
     uint64_t pair_ops;             /* tensor ops issued by the pair Gram (2*K*rows*cols) */
     uint64_t kernel_launches;
-    uint64_t retries;              /* arena/queue overflow retries */
+    uint64_t retries;              /* arena/queue overflow retries (failed rounds included) */
+    uint64_t deep_rounds;          /* memory-bounded rounds of the deep phase (0: one launch) */
     double   ms_pack;
     double   ms_pairs;
     double   ms_deep;
@@ -120,6 +121,13 @@ int cpm_db_from_csr(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows,
 int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows,
                     const uint32_t *ids, uint64_t nnz, cpm_db **out);
 
+/* Many integer-id databases at once (cpm_db_from_ids for each, with one
+ * upload, one presence pass and one packing pass for all of them); out[d]
+ * is the database built from offsets[d] / ids[d]. */
+int cpm_db_from_ids_batch(cpm_ctx *ctx, uint32_t n_db, const uint64_t *const *offsets,
+                          const uint64_t *n_rows, const uint32_t *const *ids, const uint64_t *nnz,
+                          cpm_db **out);
+
 int  cpm_db_info(const cpm_db *db, uint64_t *n_transactions, uint32_t *n_items,
                  uint64_t *words);
 int  cpm_db_labels(const cpm_db *db, uint32_t *ids_out);  /* n_items entries */
@@ -140,6 +148,12 @@ int  cpm_result_size(const cpm_result *res, uint64_t *n_patterns, uint64_t *n_it
  * items[offsets[k] .. offsets[k+1]) (columns, increasing), support supports[k]. */
 int  cpm_result_copy(const cpm_result *res, int order, uint64_t *offsets,
                      uint32_t *items, uint64_t *supports);
+/* Many results at once (e.g. from cpm_mine_batch): sizes[2k], sizes[2k+1] =
+ * patterns and item slots of res[k]; with the output arrays non-null, the
+ * results are written one after another, result k taking sizes[2k] + 1
+ * offsets (restarting at 0), sizes[2k+1] items and sizes[2k] supports. */
+int  cpm_results_copy(cpm_result *const *res, uint32_t n, int order, uint64_t *sizes,
+                      uint64_t *offsets, uint32_t *items, uint64_t *supports);
 /* Pattern tree form: pattern k = pattern parent[k] (or nothing when -1) plus item[k]. */
 int  cpm_result_tree(const cpm_result *res, int64_t *parent, uint32_t *item,
                      uint64_t *support);

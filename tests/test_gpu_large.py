@@ -1,0 +1,57 @@
+"""Full-size parity: 1,000,000 transactions x 20,000 items against the oracle's summary.
+
+The oracle's full answer (6.3 million patterns) is summarised in
+``golden/sparse_zipf_1m_summary.json`` by ``golden/make_sparse_summary.py``: the
+pattern count per length and two order-independent 64-bit hash sums over
+(sorted item ids, support).  The CUDA path must reproduce all of them, with
+the whole deep phase in one round and with the arena cut so that it runs in
+memory-bounded rounds.
+"""
+import json
+import sys
+from pathlib import Path
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).parent / "golden"
+sys.path.insert(0, str(GOLDEN))
+
+
+@pytest.fixture(scope="module")
+def workload():
+    from cupami_b200 import datasets
+
+    return datasets.sparse_zipf()
+
+
+@pytest.fixture(scope="module")
+def expected():
+    return json.loads((GOLDEN / "sparse_zipf_1m_summary.json").read_text())
+
+
+@pytest.mark.parametrize("scheduler,arena_bytes", [("plain", 0), ("learned", 3 << 30)])
+def test_sparse_1m_matches_oracle_summary(workload, expected, scheduler, arena_bytes):
+    from make_sparse_summary import summarize
+
+    from cupami_b200 import _native, costmodel
+    from cupami_b200.frequentPattern.cuApriori import cuApriori
+
+    ctx = _native.context(0)
+    if scheduler == "learned":
+        costmodel.ensure_default(ctx)
+    db = _native.Database.from_ids(ctx, workload.offsets, workload.items)
+    try:
+        opts = _native.Opts()
+        _native.library().cpm_default_opts(opts)
+        opts.scheduler = _native.CPM_SCHED_LEARNED if scheduler == "learned" else _native.CPM_SCHED_PLAIN
+        opts.arena_bytes = arena_bytes
+        res = db.mine(cuApriori._getSupportCount(expected["minSup"], db.n_transactions), _native.CPM_ECLAT, opts)
+        got = summarize(db.labels, res.offsets, res.items, res.supports)
+    finally:
+        db.close()
+    for key in ("patterns", "per_length", "hash_sum", "hash_xor_sum", "support_sum"):
+        assert got[key] == expected[key], key
+    if arena_bytes:
+        assert res.stats["deep_rounds"] > 1

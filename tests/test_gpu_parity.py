@@ -132,3 +132,43 @@ def test_batch_of_databases_matches_single_mines(oracle_lib):
     assert ms[1].getPatterns() == {}
     assert ms[0].getPatterns() == oracle_lib.mine_rows(rows_a, 5)
     assert ms[2].getPatterns() == oracle_lib.to_dict(*oracle_lib.mine_csr(csrs[0].offsets, csrs[0].items, 0.02))
+
+
+def test_batched_loader_matches_single_loads(oracle_lib):
+    """cpm_db_from_ids_batch: same shapes, labels and patterns as one cpm_db_from_ids per database,
+    with databases whose rows share a warp, empty databases and empty rows."""
+    from cupami_b200 import TransactionCSR, _native
+
+    rng = np.random.default_rng(11)
+    csrs = []
+    for n in [17, 0, 45, 3, 1, 64, 33, 500, 2, 129]:
+        rows = [[int(v) for v in rng.choice(40, size=rng.integers(0, 8), replace=False)] for _ in range(n)]
+        csrs.append(TransactionCSR.from_rows(rows))
+    csrs.append(TransactionCSR.from_rows([[], [], []]))
+    csrs.append(TransactionCSR.from_rows([[1 << 20, 5], [5], [1 << 20, 7, 5]]))
+    ctx = _native.context(0)
+    batch = _native.Database.from_ids_batch(ctx, [(c.offsets, c.items) for c in csrs])
+    try:
+        assert len(batch) == len(csrs)
+        for csr, db in zip(csrs, batch):
+            single = _native.Database.from_ids(ctx, csr.offsets, csr.items)
+            try:
+                assert (db.n_transactions, db.n_items) == (single.n_transactions, single.n_items)
+                assert db.labels.tolist() == single.labels.tolist()
+                a = db.mine(1, _native.CPM_ECLAT)
+                b = single.mine(1, _native.CPM_ECLAT)
+                assert a.patterns(db.labels) == b.patterns(single.labels)
+            finally:
+                single.close()
+            labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, 1)
+            assert a.patterns(db.labels) == oracle_lib.to_dict(labels, arrays)
+    finally:
+        for db in batch:
+            db.close()
+    # ids past the batched presence table fall back to the one-database loader
+    big = TransactionCSR.from_rows([[1 << 27, 3], [3]])
+    (db,) = _native.Database.from_ids_batch(ctx, [(big.offsets, big.items)])
+    try:
+        assert db.labels.tolist() == sorted([1 << 27, 3], key=str)
+    finally:
+        db.close()

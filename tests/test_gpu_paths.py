@@ -105,3 +105,22 @@ def test_cli_writes_reference_format(tmp_path):
                          capture_output=True, text=True, timeout=120, cwd=root)
     assert res.returncode == 0, res.stderr
     assert out.read_text() == "1 : 2\n2 : 2\n"
+
+
+@pytest.mark.parametrize("arena_kb", [64, 512])
+def test_memory_bounded_rounds_are_exact(oracle_lib, arena_kb):
+    """A small child-tidset arena forces bounded rounds, halving and shallow splits."""
+    import cupami_b200
+    from cupami_b200 import TransactionCSR
+
+    rng = np.random.default_rng(21)
+    p = rng.uniform(0.3, 0.85, 20)
+    rows = [[int(i) for i in np.nonzero(rng.random(20) < p)[0]] for _ in range(4000)]
+    csr = TransactionCSR.from_rows(rows, universe=20)
+    m = cupami_b200.cuEclat(csr, 0.2)
+    m._ARENA_BYTES = arena_kb * 1024
+    m.mine()
+    stats = m.getKernelStats()
+    assert stats["deep_rounds"] > 1
+    labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, 0.2)
+    assert list(m.getPatterns().items()) == list(oracle_lib.to_dict(labels, arrays).items())
