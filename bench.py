@@ -179,6 +179,64 @@ def cpu_step_seconds(csr, minsup, algos, budget_s=30.0):
     return statistics.median(times), f"whole step, median of {len(times)}"
 
 
+def reference_gpu_seconds(csr, minsup, algos, ours, device, budget_s=60.0):
+    """The reference's GPU path on this GPU for one step, warm (``oracle.ref_gpu``:
+    its own three kernels compiled from its source, its driver loops, torch
+    standing in for CuPy).  ``ours`` holds this engine's pattern dicts of the
+    same step, to check that both paths agree.
+
+    Batched workloads run the first databases up to the time budget and scale
+    by transactions; a single database that runs past the budget is scaled by
+    the patterns found by then (an estimate, and labelled as one)."""
+    from oracle import ref_gpu
+
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref/libref_bitsets.so not built"}
+    csrs = csr if isinstance(csr, list) else [csr]
+    algos = ["eclat" if a == "eclat-batch" else a for a in algos]
+    uploads = [ref_gpu.upload(c.offsets, c.items, device) for c in csrs]
+    k = ref_gpu.RefKernels(device)
+    # first call: module load and allocator warm-up (the reference's would also include NVRTC)
+    first = None
+    if n_transactions(csrs[0]) <= 200_000:
+        t0 = time.perf_counter()
+        for a in algos:
+            ref_gpu.mine(*uploads[0], minsup, a, k)
+        first = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    k.deadline = t0 + budget_s
+    done_tx, done_db, same, partial = 0, 0, True, None
+    try:
+        for i, (c, up) in enumerate(zip(csrs, uploads)):
+            for j, a in enumerate(algos):
+                out = {}
+                try:
+                    ref_gpu.mine(*up, minsup, a, k, out)
+                except TimeoutError:
+                    partial = (len(out), len(ours[i][j]))
+                    raise
+                got = [("\t".join(key), v) for key, v in out.items()]
+                same &= got == list(ours[i][j].items())
+            done_tx += n_transactions(c)
+            done_db += 1
+    except TimeoutError:
+        pass
+    spent = time.perf_counter() - t0
+    kind = ("reference kernels (cupami _bitsets source, nvcc sm_100a) + reference driver loops; "
+            "torch tensors in place of CuPy arrays")
+    if partial is not None and done_db == 0:
+        found, want = partial
+        return {"value": spent * want / max(1, found), "unit": "s", "first_call_s": first, "estimated": True,
+                "sample": f"stopped after {spent:.1f} s with {found} of {want} patterns; scaled by patterns",
+                "identical_output": None, "kind": kind}
+    total = n_transactions(csrs)
+    return {"value": spent * total / max(1, done_tx), "unit": "s", "first_call_s": first,
+            "estimated": done_db < len(csrs),
+            "sample": (f"{done_db} of {len(csrs)} databases, scaled by transactions" if len(csrs) > 1
+                       else "whole step, warm"),
+            "identical_output": bool(same), "kind": kind}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -213,6 +271,7 @@ def main():
     ap.add_argument("--scheduler", default="plain", choices=["plain", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ab", action="store_true", help="skip the learned-vs-plain scheduler comparison")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference-GPU-path leg")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup()
@@ -361,6 +420,11 @@ def main():
             pg.barrier()
             pg.destroy_process_group()
         return
+    ref_gpu_leg = None
+    if not args.no_ref_gpu:
+        ours = [[r.patterns(db.labels) for r in res] for db, res in
+                zip(dbs, zip(*[res for _, _, res in last]))]
+        ref_gpu_leg = reference_gpu_seconds(csr, minsup, algos, ours, local)
     cpu = None
     if not args.no_cpu_baseline:
         v, sample = cpu_step_seconds(csr, minsup, algos)
@@ -381,6 +445,7 @@ def main():
         "roofline": roof,
         "pair_gram": gram,
         "cpu_baseline": cpu,
+        "reference_gpu": ref_gpu_leg,
         "scheduler_ab": ab,
         "gpu_launches": launches,
         "clocks": clocks,

@@ -7,6 +7,10 @@ level-wise Apriori joins with subset pruning) over 32-bit word bitsets, with
 each kernel written as NumPy array arithmetic.  It is the CPU baseline the
 benchmark reports beside the CUDA path, never part of the product.
 
+The drivers take the kernels as an object (``NUMPY`` here); ``oracle.ref_gpu``
+passes the reference's own CUDA kernels instead, which makes the same drivers
+the reference's GPU path.
+
 Followed step by step:
   singletons + pairs + classes    cupami/frequentPattern/cuEclat.py:168-203
   class search                    cupami/frequentPattern/cuEclat.py:211-245
@@ -49,6 +53,33 @@ def intersect(prefix, ext):
     return child, np.bitwise_count(child).sum(axis=1, dtype=np.uint64).tolist()
 
 
+class NumpyKernels:
+    """The three reference kernels plus the array steps the drivers use, on host arrays."""
+
+    pack = staticmethod(pack)
+    supports = staticmethod(supports_of)
+    intersect = staticmethod(intersect)
+
+    @staticmethod
+    def vertical(bits, members, left):
+        return bits[np.asarray(members, dtype=np.int64)] & bits[left]
+
+    @staticmethod
+    def take(child, keep):
+        return child[np.asarray(keep, dtype=np.int64)]
+
+    @staticmethod
+    def concat(chunks):
+        return np.concatenate(chunks)
+
+    @staticmethod
+    def sync():
+        pass
+
+
+NUMPY = NumpyKernels()
+
+
 def device_pairs_from_csr(offsets, ids):
     """(labels, rows, cols) the way the reference's BIN bulk path builds them."""
     offsets = np.asarray(offsets, dtype=np.uint64)
@@ -65,11 +96,11 @@ def device_pairs_from_csr(offsets, ids):
     return labels, rows, cols, n_tx
 
 
-def eclat(labels, rows, cols, n_tx, minsup):
-    """``{tuple(labels): support}`` in the reference's insertion order."""
-    out = {}
-    bits = pack(rows, cols, n_tx, len(labels))
-    sup1 = supports_of(bits, [[i] for i in range(len(labels))])
+def eclat(labels, rows, cols, n_tx, minsup, k=NUMPY, out=None):
+    """``{tuple(labels): support}`` in the reference's insertion order (filled into ``out`` if given)."""
+    out = {} if out is None else out
+    bits = k.pack(rows, cols, n_tx, len(labels))
+    sup1 = k.supports(bits, [[i] for i in range(len(labels))])
     frequent = []
     for i, s in enumerate(sup1):
         if s >= minsup:
@@ -81,19 +112,20 @@ def eclat(labels, rows, cols, n_tx, minsup):
         batch = list(islice(pairs, PAIR_BATCH))
         if not batch:
             break
-        for (a, b), s in zip(batch, supports_of(bits, batch)):
+        for (a, b), s in zip(batch, k.supports(bits, batch)):
             if s >= minsup:
                 out[(labels[a], labels[b])] = int(s)
                 classes.setdefault(a, []).append(b)
     for a, members in classes.items():
         if len(members) < 2:
             continue
-        vertical = bits[np.asarray(members, dtype=np.int64)] & bits[a]
-        _search(out, (labels[a],), [labels[m] for m in members], vertical, minsup)
+        vertical = k.vertical(bits, members, a)
+        _search(out, (labels[a],), [labels[m] for m in members], vertical, minsup, k)
+    k.sync()
     return out
 
 
-def _search(out, prefix, names, vertical, minsup):
+def _search(out, prefix, names, vertical, minsup, k=NUMPY):
     stack = [[prefix, names, vertical, 0]]
     while stack:
         top = stack[-1]
@@ -107,24 +139,23 @@ def _search(out, prefix, names, vertical, minsup):
         kept_names, kept_bits = [], []
         for start in range(pos + 1, len(nm), step):
             stop = min(len(nm), start + step)
-            child, sups = intersect(vert[pos], vert[start:stop])
-            keep = [k for k, s in enumerate(sups) if s >= minsup]
-            for k in keep:
-                out[head + (nm[start + k],)] = int(sups[k])
-                kept_names.append(nm[start + k])
+            child, sups = k.intersect(vert[pos], vert[start:stop])
+            keep = [j for j, s in enumerate(sups) if s >= minsup]
+            for j in keep:
+                out[head + (nm[start + j],)] = int(sups[j])
+                kept_names.append(nm[start + j])
             if keep:
-                kept_bits.append(child[np.asarray(keep, dtype=np.int64)])
+                kept_bits.append(k.take(child, keep))
         if len(kept_names) > 1:
-            stack.append([head, kept_names,
-                          kept_bits[0] if len(kept_bits) == 1 else np.concatenate(kept_bits), 0])
+            stack.append([head, kept_names, kept_bits[0] if len(kept_bits) == 1 else k.concat(kept_bits), 0])
 
 
-def apriori(labels, rows, cols, n_tx, minsup):
-    out = {}
-    bits = pack(rows, cols, n_tx, len(labels))
+def apriori(labels, rows, cols, n_tx, minsup, k=NUMPY, out=None):
+    out = {} if out is None else out
+    bits = k.pack(rows, cols, n_tx, len(labels))
     index = {label: i for i, label in enumerate(labels)}
     level = []
-    for i, s in enumerate(supports_of(bits, [[i] for i in range(len(labels))])):
+    for i, s in enumerate(k.supports(bits, [[i] for i in range(len(labels))])):
         if s >= minsup:
             level.append((labels[i],))
             out[(labels[i],)] = int(s)
@@ -142,12 +173,13 @@ def apriori(labels, rows, cols, n_tx, minsup):
         cands = sorted(cands)
         if not cands:
             break
-        sups = supports_of(bits, [[index[x] for x in c] for c in cands])
+        sups = k.supports(bits, [[index[x] for x in c] for c in cands])
         level = []
         for c, s in zip(cands, sups):
             if s >= minsup:
                 level.append(c)
                 out[c] = int(s)
+    k.sync()
     return out
 
 
