@@ -54,17 +54,34 @@ def make_workload(name, rank):
     from cupami_b200 import datasets
 
     gen, minsup, algos = WORKLOADS[name]
-    fn = getattr(datasets, gen)
-    import inspect
-
-    seed = inspect.signature(fn).parameters["seed"].default + rank
-    return fn(seed=seed), minsup, algos, seed
+    seed = rank_seed(name, rank)
+    return getattr(datasets, gen)(seed=seed), minsup, algos, seed
 
 
 def n_transactions(csr):
     if isinstance(csr, list):
         return sum(n_transactions(c) for c in csr)
     return int(np.count_nonzero(np.diff(csr.offsets.astype(np.int64)) > 0))
+
+
+def max_over_ranks(values, device):
+    """Element-wise max of per-rank timings (the only collective: no data-path exchange)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(values, device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def rank_seed(name, rank):
+    """Seed of this rank's database: the workload's own seed plus the rank (weak scaling)."""
+    import inspect
+
+    from cupami_b200 import datasets
+
+    fn = getattr(datasets, WORKLOADS[name][0])
+    return inspect.signature(fn).parameters["seed"].default + rank
 
 
 def dist_setup():
@@ -395,9 +412,7 @@ def main():
     value = statistics.mean(step_ms) / 1e3
     e2e_v = statistics.mean(e2e)
     if pg:
-        t = torch.tensor([value, e2e_v], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        value, e2e_v = t.tolist()
+        value, e2e_v = max_over_ranks([value, e2e_v], "cuda")
     # Roofline of the deep-level intersection kernel (k_deep), the step's
     # dominant kernel on Eclat workloads, from its own CUDA events.
     hbm, bf16, src = peaks()

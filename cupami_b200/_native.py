@@ -54,7 +54,8 @@ class Opts(ctypes.Structure):
         ("scheduler", ctypes.c_int32), ("pair_engine", ctypes.c_int32),
         ("pair_batch", ctypes.c_uint64), ("intersection_bytes", ctypes.c_uint64),
         ("arena_bytes", ctypes.c_uint64), ("spin_limit", ctypes.c_uint64),
-        ("collect_trace", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7),
+        ("collect_trace", ctypes.c_int32), ("deep_block", ctypes.c_int32),
+        ("deep_ctas_per_sm", ctypes.c_int32), ("autotune", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4),
     ]
 
 
@@ -81,6 +82,8 @@ _SIGNATURES = {
     "cpm_db_from_ids": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.POINTER(_P)]),
     "cpm_db_from_ids_batch": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(_P), ctypes.POINTER(_U64),
                                              ctypes.POINTER(_P), ctypes.POINTER(_U64), ctypes.POINTER(_P)]),
+    "cpm_autotune": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.POINTER(Opts), ctypes.POINTER(ctypes.c_int32),
+                                    ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)]),
     "cpm_db_info": (ctypes.c_int, [_P, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_uint32),
                                    ctypes.POINTER(_U64)]),
     "cpm_db_labels": (ctypes.c_int, [_P, _P]),
@@ -276,6 +279,18 @@ class Database:
             self.close()
         except Exception:
             pass
+
+
+def autotune(ctx, db, min_sup, opts=None):
+    """cpm_autotune: fastest deep-level launch shape for this database, recorded in ctx."""
+    if opts is None:
+        opts = Opts()
+        library().cpm_default_opts(ctypes.byref(opts))
+    block, ctas, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+    with ctx.lock:
+        ctx.check(library().cpm_autotune(ctx.handle, db.handle, int(min_sup), ctypes.byref(opts),
+                                         ctypes.byref(block), ctypes.byref(ctas), ctypes.byref(ms)))
+    return {"block": block.value, "ctas_per_sm": ctas.value, "ms_deep": ms.value}
 
 
 def mine_batch(ctx, databases, min_sups, opts=None, order=CPM_ORDER_ECLAT):

@@ -28,6 +28,7 @@
 #include <string>
 #include <unordered_set>
 #include <vector>
+#include <map>
 #include <chrono>
 #include <cstdlib>
 #include <mutex>
@@ -54,6 +55,8 @@ struct cpm_ctx {
     unsigned deep_occ_block = 0;  // block size the occupancies above were taken for
     std::vector<float> model;  // cost-model parameters (empty: none loaded)
     float last_deep_ms = 0.f;  // deep-phase kernel time of the last bounded-round run
+    int last_deep_block = 0, last_deep_ctas = 0;  // launch shape of the last deep phase
+    std::map<int, std::pair<int, int>> tune;      // log2(stride) -> (threads per CTA, CTAs per SM), cpm_autotune
 };
 
 struct cpm_db {
@@ -1065,7 +1068,25 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     const bool smem_prefix = prefix_bytes <= 200 * 1024;
     // Long tidsets leave room for one CTA per SM: give it 16 warps so that
     // enough loads stay in flight; short ones run up to four 8-warp CTAs.
-    const unsigned block = max_stride >= 2048 ? 512 : 256;
+    unsigned block = max_stride >= 2048 ? 512 : 256;
+    int want_ctas = 4;
+    if (o.autotune) {
+        const auto it = ctx->tune.find(63 - __builtin_clzll(std::max<uint64_t>(1, max_stride)));
+        if (it != ctx->tune.end()) {
+            block = (unsigned)it->second.first;
+            want_ctas = it->second.second;
+        }
+    }
+    if (o.deep_block) {
+        if (o.deep_block != 128 && o.deep_block != 256 && o.deep_block != 512)
+            return set_err(ctx, CPM_EINVAL, "deep_block must be 128, 256 or 512 (got %d)", o.deep_block);
+        block = (unsigned)o.deep_block;
+    }
+    if (o.deep_ctas_per_sm) {
+        if (o.deep_ctas_per_sm < 1 || o.deep_ctas_per_sm > 4)
+            return set_err(ctx, CPM_EINVAL, "deep_ctas_per_sm must be 1-4 (got %d)", o.deep_ctas_per_sm);
+        want_ctas = o.deep_ctas_per_sm;
+    }
     if (smem_prefix && (ctx->deep_occ_smem < 0 || ctx->deep_occ_bytes != prefix_bytes || ctx->deep_occ_block != block)) {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_smem, k_deep<true>, block, prefix_bytes));
         ctx->deep_occ_bytes = prefix_bytes;
@@ -1074,8 +1095,10 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_global, k_deep<false>, block, 0));
         ctx->deep_occ_block = block;
     }
-    const int cta_per_sm = std::min(4, std::max(1, smem_prefix ? ctx->deep_occ_smem : ctx->deep_occ_global));
+    const int cta_per_sm = std::min(want_ctas, std::max(1, smem_prefix ? ctx->deep_occ_smem : ctx->deep_occ_global));
     const unsigned grid = (unsigned)(ctx->sms * cta_per_sm);
+    ctx->last_deep_block = (int)block;
+    ctx->last_deep_ctas = cta_per_sm;
     DeepState hs{};
     bool rounds = false;
     std::vector<float> features;  // per root unit, when traced (cost-model inputs)
@@ -1560,6 +1583,46 @@ extern "C" int cpm_mine_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const i
         return r;
     }
     for (uint32_t d = 0; d < n_db; ++d) out[d] = res[d];
+    return CPM_OK;
+}
+
+extern "C" int cpm_autotune(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, const cpm_opts *opts, int32_t *block,
+                            int32_t *ctas_per_sm, double *ms_deep) {
+    if (!ctx || !db) return CPM_EINVAL;
+    cpm_opts o;
+    if (opts) o = *opts;
+    else cpm_default_opts(&o);
+    o.autotune = 0;
+    o.collect_trace = 0;
+    static const int blocks[3] = {128, 256, 512};
+    double best = 1e300;
+    int best_block = 0, best_ctas = 0;
+    for (int bi = 0; bi < 3; ++bi) {
+        for (int c = 1; c <= 4; ++c) {
+            o.deep_block = blocks[bi];
+            o.deep_ctas_per_sm = c;
+            double t = 1e300;
+            int used = c;
+            for (int rep = 0; rep < 2; ++rep) {
+                cpm_result *r = nullptr;
+                const int rc = cpm_mine(ctx, db, min_sup, CPM_ECLAT, &o, &r);
+                if (rc != CPM_OK) return rc;
+                t = std::min(t, r->stats.ms_deep);
+                used = ctx->last_deep_ctas;
+                cpm_result_free(r);
+            }
+            if (t < best) {
+                best = t;
+                best_block = blocks[bi];
+                best_ctas = used;
+            }
+            if (used < c) break;  // occupancy allows no more CTAs of this size
+        }
+    }
+    ctx->tune[63 - __builtin_clzll(std::max<uint64_t>(1, db->stride))] = {best_block, best_ctas};
+    if (block) *block = best_block;
+    if (ctas_per_sm) *ctas_per_sm = best_ctas;
+    if (ms_deep) *ms_deep = best;
     return CPM_OK;
 }
 

@@ -68,6 +68,10 @@ class cuApriori:
     #: Device arena for child tidsets in bytes (0: as much as the GPU holds).
     #: A small arena makes the deep levels run in memory-bounded rounds.
     _ARENA_BYTES = 0
+    #: Deep-level launch shape: threads per CTA (128/256/512) and CTAs per SM
+    #: (1-4); 0 leaves each to the library (or to the autotuner's table).
+    _DEEP_BLOCK = 0
+    _DEEP_CTAS_PER_SM = 0
 
     def __init__(self, iFile, minSup, sep=None, use_gds="auto", use_gpu_io="auto"):
         loading_start = time.perf_counter()
@@ -256,7 +260,21 @@ class cuApriori:
             opts.spin_limit = int(self._SPIN_LIMIT)
         opts.pair_engine = int(self._PAIR_ENGINE)
         opts.arena_bytes = int(self._ARENA_BYTES)
+        opts.deep_block = int(self._DEEP_BLOCK)
+        opts.deep_ctas_per_sm = int(self._DEEP_CTAS_PER_SM)
+        opts.autotune = 1
         return opts
+
+    def autotune(self):
+        """Time the deep-level launch shapes on this database and keep the fastest
+        for databases with tidsets of this length (later mine() calls in this
+        process use it).  Returns {"block", "ctas_per_sm", "ms_deep"}."""
+        ctx = self._getCudaModule()
+        db, _ = self._deviceDatabase(ctx)
+        try:
+            return _native.autotune(ctx, db, self._minSup, self._options())
+        finally:
+            db.close()
 
     def mine(self):
         self._startTime = time.perf_counter()

@@ -77,7 +77,10 @@ typedef struct {
     uint64_t arena_bytes;          /* device arena for child tidsets; 0 = automatic */
     uint64_t spin_limit;           /* bounded device waits; 0 = default */
     int32_t  collect_trace;        /* 1: record per-frame features and costs for the cost model */
-    int32_t  reserved[7];
+    int32_t  deep_block;           /* deep-level kernel threads per CTA: 128, 256 or 512; 0 = automatic */
+    int32_t  deep_ctas_per_sm;     /* resident deep-level CTAs per SM, 1-4 (capped by occupancy); 0 = automatic */
+    int32_t  autotune;             /* 1: use the launch shape cpm_autotune found for this tidset length */
+    int32_t  reserved[4];
 } cpm_opts;
 
 typedef struct {
@@ -127,6 +130,17 @@ int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows,
 int cpm_db_from_ids_batch(cpm_ctx *ctx, uint32_t n_db, const uint64_t *const *offsets,
                           const uint64_t *n_rows, const uint32_t *const *ids, const uint64_t *nnz,
                           cpm_db **out);
+
+/* Autotuner of the deep-level launch shape.  Mines db (Eclat) once per
+ * shape -- threads per CTA in {128, 256, 512} x resident CTAs per SM in 1..4,
+ * as far as occupancy allows -- keeps the best of two deep-phase times each,
+ * and records the fastest shape in the context for tidsets of this length
+ * (power-of-two bucket of the row stride); mines whose opts set autotune = 1
+ * use it.  The shape never changes the output.  No reference counterpart: the
+ * reference launches one 256-thread block per candidate
+ * (cupami/frequentPattern/_bitsets.py:103-125). */
+int cpm_autotune(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, const cpm_opts *opts,
+                 int32_t *block, int32_t *ctas_per_sm, double *ms_deep);
 
 int  cpm_db_info(const cpm_db *db, uint64_t *n_transactions, uint32_t *n_items,
                  uint64_t *words);

@@ -124,3 +124,30 @@ def test_memory_bounded_rounds_are_exact(oracle_lib, arena_kb):
     assert stats["deep_rounds"] > 1
     labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, 0.2)
     assert list(m.getPatterns().items()) == list(oracle_lib.to_dict(labels, arrays).items())
+
+
+def test_launch_shapes_and_autotuner_keep_output():
+    """Every deep-level launch shape, and the autotuner's pick, mine the same patterns."""
+    import cupami_b200
+    from cupami_b200 import _native, datasets
+
+    csr = datasets.dense_bernoulli(n=16384, n_items=96, seed=3)
+    base = cupami_b200.cuEclat(csr, 0.6)
+    base.mine()
+    want = list(base.getPatterns().items())
+    assert len(want) > 1000
+    for block in (128, 256, 512):
+        for ctas in (1, 2, 4):
+            m = cupami_b200.cuEclat(csr, 0.6)
+            m._DEEP_BLOCK, m._DEEP_CTAS_PER_SM = block, ctas
+            m.mine()
+            assert list(m.getPatterns().items()) == want, (block, ctas)
+    tuned = cupami_b200.cuEclat(csr, 0.6).autotune()
+    assert tuned["block"] in (128, 256, 512) and 1 <= tuned["ctas_per_sm"] <= 4 and tuned["ms_deep"] > 0
+    m = cupami_b200.cuEclat(csr, 0.6)
+    m.mine()
+    assert list(m.getPatterns().items()) == want
+    bad = cupami_b200.cuEclat(csr, 0.6)
+    bad._DEEP_BLOCK = 96
+    with pytest.raises(_native.NativeError):
+        bad.mine()
