@@ -428,8 +428,13 @@ def main():
                 "alg_bytes": "sum over units of 8*W*(1 + siblings + children written)"}
     pair_ms = statistics.mean(sum(st["ms_pairs"] for _, st, _ in out) for out in per_kernel)
     pair_ops = statistics.mean(sum(st["pair_ops"] for _, st, _ in out) for out in per_kernel)
-    gram = {"kernel": "pair Gram", "ms_per_step": pair_ms, "ops_per_step": pair_ops,
-            "tops": pair_ops / (pair_ms * 1e-3) / 1e12 if pair_ms else 0.0}
+    int8_peak = int8_peak_tops()
+    gram_tops = pair_ops / (pair_ms * 1e-3) / 1e12 if pair_ms else 0.0
+    gram = {"kernel": "pair Gram (k_gram_tc when the tensor-core engine runs)", "ms_per_step": pair_ms,
+            "ops_per_step": pair_ops, "tops": gram_tops, "peak_int8_tops": int8_peak,
+            "peak_source": "torch._int_mm int8 8192^3, best of 12, measured in this run",
+            "frac": gram_tops / int8_peak if int8_peak else None,
+            "ops": "2*128*256*K per issued tile (full tiles of the upper triangle)"}
     if rank != 0:
         if pg:
             pg.barrier()

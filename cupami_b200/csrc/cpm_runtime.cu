@@ -216,6 +216,10 @@ extern "C" int cpm_synchronize(cpm_ctx *ctx) {
 
 // Offsets of the non-empty rows only (empty baskets are dropped and the rest
 // renumbered in order, cuApriori.py:391-392).
+// Presence bitmaps up to this many 32-bit words (id range 0..393,215) are
+// built in shared memory (48 KB, the default dynamic shared-memory limit).
+constexpr uint64_t CPM_MARK_SMEM_WORDS = 12288;
+
 static int compact_offsets(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows, uint64_t nnz,
                            std::vector<uint64_t> &out) {
     out.clear();
@@ -327,8 +331,13 @@ extern "C" int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n
     CKR(tmp.alloc(&d_present, pw));
     CK(cudaMemsetAsync(d_present, 0, pw * 4, ctx->stream));
     if (nnz) {
-        const unsigned blocks = (unsigned)std::min<uint64_t>((nnz + 255) / 256, (uint64_t)ctx->sms * 16);
-        k_mark_ids<<<blocks, 256, 0, ctx->stream>>>(d_ids, nnz, d_present);
+        if (pw <= CPM_MARK_SMEM_WORDS) {
+            const unsigned blocks = (unsigned)std::min<uint64_t>((nnz + 1023) / 1024, (uint64_t)ctx->sms * 2);
+            k_mark_ids_smem<<<blocks, 1024, pw * 4, ctx->stream>>>(d_ids, nnz, (uint32_t)pw, d_present);
+        } else {
+            const unsigned blocks = (unsigned)std::min<uint64_t>((nnz + 255) / 256, (uint64_t)ctx->sms * 16);
+            k_mark_ids<<<blocks, 256, 0, ctx->stream>>>(d_ids, nnz, d_present);
+        }
         CK(cudaGetLastError());
     }
     std::vector<uint32_t> present(pw);
@@ -449,7 +458,9 @@ extern "C" int cpm_db_from_ids_batch(cpm_ctx *ctx, uint32_t n_db, const uint64_t
     CK(cudaMemsetAsync(d_present, 0, PW * 4, ctx->stream));
     if (NNZ) {
         const unsigned blocks = (unsigned)std::min<uint64_t>((NNZ + 255) / 256, (uint64_t)ctx->sms * 16);
-        k_mark_ids_b<<<blocks, 256, 0, ctx->stream>>>(d_ids, NNZ, d_occ, d_pres_base, n_db, d_present);
+        const uint32_t spw = PW <= CPM_MARK_SMEM_WORDS ? (uint32_t)PW : 0u;
+        k_mark_ids_b<<<spw ? std::min(blocks, (unsigned)ctx->sms * 2) : blocks, 256, spw * 4, ctx->stream>>>(
+            d_ids, NNZ, d_occ, d_pres_base, n_db, d_present, spw);
         CK(cudaGetLastError());
     }
     std::vector<uint32_t> present(PW);
@@ -822,9 +833,11 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
         CK(cudaStreamSynchronize(ctx->stream));
         deep_ms += (float)elapsed_ms(ctx, 2, 3);
         st.kernel_launches++;
-        st.intersections += hs.intersections;
-        st.bytes_alg += hs.bytes_alg;
-        st.work_items += hs.work_items;
+        if (!hs.error) {  // a discarded round's work is not counted (its time is)
+            st.intersections += hs.intersections;
+            st.bytes_alg += hs.bytes_alg;
+            st.work_items += hs.work_items;
+        }
         ++rounds;
         return CPM_OK;
     };
@@ -842,8 +855,10 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
             committed = hs.n_patterns;
             roots.erase(roots.begin(), roots.begin() + take);
             limit = limit == ~0ull ? limit : limit * 2;
+            // Keys are relative: set the scale to what this round really used,
+            // with a margin (a round that still overflows halves and retries).
             const double used = (double)(hs.arena_next - persist_arena);
-            if (est > 0 && take > 4) words_per_key = std::max(words_per_key * 0.5, std::min(used / est, words_per_key * 4));
+            if (est > 0 && take > 4) words_per_key = std::max(1e-9, 1.25 * used / est);
             continue;
         }
         if (hs.error & DEEP_ERR_SPIN) return set_err(ctx, CPM_ETIMEOUT, "deep-level kernel wait ran out of spins");
@@ -1100,7 +1115,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     ctx->last_deep_block = (int)block;
     ctx->last_deep_ctas = cta_per_sm;
     DeepState hs{};
-    bool rounds = false;
+    bool rounds = false, arena_exceeded = false;
     std::vector<float> features;  // per root unit, when traced (cost-model inputs)
     FrameAux *d_aux = nullptr;
     float *d_key = nullptr, *d_key2 = nullptr, *d_feat = nullptr, *d_model = nullptr;
@@ -1156,14 +1171,37 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         CK(cudaGetLastError());
         st.kernel_launches += 3;
         if (attempt == 0) {
-            // Estimated child-tidset words of the whole deep phase (learned
-            // keys estimate words touched; plain keys count later members).
-            std::vector<float> keys(n_units);
-            CK(cudaMemcpyAsync(keys.data(), d_key2, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
-            double est = 0;
-            for (float k : keys) est += learned ? (double)k : (double)k * max_stride;
-            if (est > (double)arena_budget) {
+            // Go to bounded rounds at once only when one launch cannot fit:
+            // the arena this database needed before exceeds the budget, or,
+            // without that record, the estimated child-tidset words (learned
+            // keys estimate words touched; plain keys count later members,
+            // times the frame's tidset length) exceed it many times over --
+            // both estimates overshoot, so a moderate excess runs one launch
+            // and falls back to rounds only if its arena really overflows.
+            bool direct = false;
+            if (n_db == 1 && db0->hint_arena) {
+                direct = db0->hint_arena > arena_budget;
+            } else {
+                std::vector<float> keys(n_units);
+                std::vector<uint32_t> uids(n_units);
+                CK(cudaMemcpyAsync(keys.data(), d_key2, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
+                CK(cudaMemcpyAsync(uids.data(), d_uid2, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
+                CK(cudaStreamSynchronize(ctx->stream));
+                double est = 0;
+                for (uint64_t i = 0; i < n_units; ++i) {
+                    if (learned) {
+                        est += keys[i];
+                        continue;
+                    }
+                    const size_t k = (size_t)(std::upper_bound(frames.begin(), frames.end(), uids[i],
+                                                               [](uint32_t u, const DFrame &f) { return u < f.root; }) -
+                                              frames.begin()) - 1;
+                    est += (double)keys[i] * frames[k].stride;
+                }
+                direct = est > 16.0 * (double)arena_budget;
+                if (dbg) fprintf(stderr, "cpm: estimated arena %.3g words, budget %.3g words\n", est, (double)arena_budget);
+            }
+            if (direct) {
                 rounds = true;
                 break;
             }
@@ -1249,6 +1287,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         pat_cap = std::max<uint64_t>(pat_cap * 8, hs.n_patterns * 8);
         if ((hs.error & DEEP_ERR_ARENA) && arena_words >= arena_budget) {
             rounds = true;  // the child tidsets do not fit at once: bounded rounds below
+            arena_exceeded = true;
             break;
         }
         arena_words = std::min<uint64_t>(arena_budget, std::max<uint64_t>(arena_words * 4, hs.arena_next * 4));
@@ -1263,7 +1302,10 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         db0->hint_members = std::max<uint64_t>(db0->hint_members, hs.n_members + hs.n_members / 4 + 64);
         db0->hint_queue = std::max<uint64_t>(db0->hint_queue, hs.q_tail + hs.q_tail / 4 + 64);
         db0->hint_patterns = std::max<uint64_t>(db0->hint_patterns, hs.n_patterns + hs.n_patterns / 4 + 64);
-        db0->hint_arena = std::max<uint64_t>(db0->hint_arena, hs.arena_next + hs.arena_next / 4 + 64);
+        // After rounds the arena counter covers one round only; what is known
+        // then is whether one launch overflowed the whole budget.
+        if (!rounds) db0->hint_arena = std::max<uint64_t>(db0->hint_arena, hs.arena_next + hs.arena_next / 4 + 64);
+        else if (arena_exceeded) db0->hint_arena = std::max<uint64_t>(db0->hint_arena, arena_budget + 1);
     }
     const uint64_t n = hs.n_patterns;
     std::vector<uint32_t> par(n), item(n), sup(n), pdb;

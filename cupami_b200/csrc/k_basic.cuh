@@ -37,13 +37,33 @@ __global__ void k_pack(const uint64_t *__restrict__ offsets, const uint32_t *__r
     }
 }
 
-// Marks which raw ids occur (presence bitmap over the id universe).
+// Marks which raw ids occur (presence bitmap over the id universe).  A few
+// hundred distinct ids share a few dozen words, so the bits are tested before
+// the atomic: once a word is complete its readers stop issuing atomics (a
+// stale zero only costs one redundant atomicOr).
 __global__ void k_mark_ids(const uint32_t *__restrict__ ids, uint64_t nnz, uint32_t *__restrict__ present) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
          i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t v = ids[i];
-        atomicOr(present + (v >> 5), 1u << (v & 31));
+        const uint32_t v = ids[i], bit = 1u << (v & 31);
+        if (!(present[v >> 5] & bit)) atomicOr(present + (v >> 5), bit);
     }
+}
+
+// Same, with the bitmap (pw words) built per block in shared memory and OR-ed
+// into the global one once per non-zero word; for id ranges that fit.
+__global__ void k_mark_ids_smem(const uint32_t *__restrict__ ids, uint64_t nnz, uint32_t pw,
+                                uint32_t *__restrict__ present) {
+    extern __shared__ uint32_t s_present[];
+    for (uint32_t w = threadIdx.x; w < pw; w += blockDim.x) s_present[w] = 0;
+    __syncthreads();
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = ids[i], bit = 1u << (v & 31);
+        if (!(s_present[v >> 5] & bit)) atomicOr(s_present + (v >> 5), bit);
+    }
+    __syncthreads();
+    for (uint32_t w = threadIdx.x; w < pw; w += blockDim.x)
+        if (s_present[w]) atomicOr(present + w, s_present[w]);
 }
 
 // support[c] = popcount of row c; one warp per row, 128-bit loads.
@@ -190,14 +210,25 @@ __device__ __forceinline__ uint32_t desc_of(const uint64_t *__restrict__ bases, 
 }
 
 // Presence bitmaps of every database (occ_bases[d] = first occurrence of d).
+// With pw > 0 the whole bitmap (pw words) is staged in shared memory per
+// block (dynamic shared memory of pw words), as in k_mark_ids_smem.
 __global__ void k_mark_ids_b(const uint32_t *__restrict__ ids, uint64_t nnz, const uint64_t *__restrict__ occ_bases,
-                             const uint64_t *__restrict__ present_bases, uint32_t n_db, uint32_t *__restrict__ present) {
+                             const uint64_t *__restrict__ present_bases, uint32_t n_db, uint32_t *__restrict__ present,
+                             uint32_t pw) {
+    extern __shared__ uint32_t s_present[];
+    uint32_t *bm = pw ? s_present : present;
+    for (uint32_t w = threadIdx.x; w < pw; w += blockDim.x) s_present[w] = 0;
+    __syncthreads();
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t d = desc_of(occ_bases, n_db, i);
-        const uint32_t v = ids[i];
-        atomicOr(present + present_bases[d] + (v >> 5), 1u << (v & 31));
+        const uint32_t v = ids[i], bit = 1u << (v & 31);
+        const uint64_t w = present_bases[d] + (v >> 5);
+        if (!(bm[w] & bit)) atomicOr(bm + w, bit);
     }
+    __syncthreads();
+    for (uint32_t w = threadIdx.x; w < pw; w += blockDim.x)
+        if (s_present[w]) atomicOr(present + w, s_present[w]);
 }
 
 // k_pack over all databases: one thread per global (non-empty) row; the
