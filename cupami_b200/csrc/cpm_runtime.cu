@@ -725,7 +725,6 @@ static int grow(cpm_ctx *ctx, DeepBuffers &b, uint64_t frames_cap, uint64_t memb
 
 
 // Part of the arena kept free for frames that shallow expansion keeps.
-static inline uint64_t persist_cap_reserve(uint64_t arena_words) { return arena_words / 8; }
 
 // Memory-bounded deep phase.  Root units (in scheduler order: d_uid/d_key,
 // largest first) are admitted into rounds while their cost keys fit a share
@@ -794,7 +793,15 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
     }
     uint64_t persist_frames = top_frames.size(), persist_members = P2_total, persist_arena = 0;
     uint64_t committed = base_patterns;
-    const double budget = (double)(arena_words - persist_cap_reserve(arena_words)) * 0.8;
+    // Child frames kept by shallow expansions form a stack at the front of
+    // the arena: (frame id, arena start, root units still queued).  A frame's
+    // block is released once every root unit taken from it has run.
+    struct Kept {
+        uint32_t fid;
+        uint64_t arena_start;
+        uint64_t left;
+    };
+    std::vector<Kept> kept;
     uint64_t limit = ~0ull;  // units per round
     std::vector<unsigned long long> q;
     DeepParams P;
@@ -845,6 +852,8 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
     // every successful round (keys are only relative estimates).
     double words_per_key = 1.0;
     while (!roots.empty()) {
+        // Admission budget: what the kept frames leave of the arena.
+        const double budget = (double)(arena_words - persist_arena) * 0.8;
         size_t take = 0;
         double est = 0;
         while (take < roots.size() && take < limit &&
@@ -853,7 +862,14 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
         CKR(launch(take, 0));
         if (!hs.error) {
             committed = hs.n_patterns;
+            for (size_t i = 0; i < take; ++i)
+                for (Kept &k : kept)
+                    if (k.fid == roots[i].frame) --k.left;
             roots.erase(roots.begin(), roots.begin() + take);
+            while (!kept.empty() && kept.back().left == 0) {
+                persist_arena = kept.back().arena_start;
+                kept.pop_back();
+            }
             limit = limit == ~0ull ? limit : limit * 2;
             // Keys are relative: set the scale to what this round really used,
             // with a margin (a round that still overflows halves and retries).
@@ -873,21 +889,30 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
         // One root unit whose subtree does not fit: expand it by one level.
         CKR(launch(1, 1));
         if (hs.error)
-            return set_err(ctx, CPM_EOVERFLOW, "a single class of %u members exceeds the device arena (error 0x%x)",
-                           top_frames.size() > roots[0].frame ? top_frames[roots[0].frame].m : 0u, hs.error);
+            return set_err(ctx, CPM_EOVERFLOW,
+                           "the child tidsets of one class position exceed the device arena (%llu of %llu words "
+                           "free, error 0x%x)", (unsigned long long)(arena_words - persist_arena),
+                           (unsigned long long)arena_words, hs.error);
         ++shallow;
         committed = hs.n_patterns;
         const Root parent = roots.front();
         roots.pop_front();
+        for (Kept &k : kept)
+            if (k.fid == parent.frame) --k.left;
         if (hs.n_frames > persist_frames) {
             DFrame c;
             CK(cudaMemcpy(&c, b.frames + persist_frames, sizeof c, cudaMemcpyDeviceToHost));
             const uint64_t cid = persist_frames;
+            kept.push_back({(uint32_t)cid, persist_arena, (uint64_t)c.m - 1});
             persist_frames = hs.n_frames;
             persist_members = hs.n_members;
             persist_arena = hs.arena_next;
             for (uint32_t p = c.m - 1; p-- > 0;)
                 roots.push_front({(uint32_t)cid, p, parent.key * (c.m - 1 - p) / std::max(1u, c.m)});
+        }
+        while (!kept.empty() && kept.back().left == 0) {
+            persist_arena = kept.back().arena_start;
+            kept.pop_back();
         }
         limit = ~0ull;
     }
