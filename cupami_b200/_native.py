@@ -55,7 +55,8 @@ class Opts(ctypes.Structure):
         ("pair_batch", ctypes.c_uint64), ("intersection_bytes", ctypes.c_uint64),
         ("arena_bytes", ctypes.c_uint64), ("spin_limit", ctypes.c_uint64),
         ("collect_trace", ctypes.c_int32), ("deep_block", ctypes.c_int32),
-        ("deep_ctas_per_sm", ctypes.c_int32), ("autotune", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4),
+        ("deep_ctas_per_sm", ctypes.c_int32), ("autotune", ctypes.c_int32), ("tidsets", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
 

@@ -739,7 +739,7 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
                        uint64_t P2_total, uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix,
                        uint64_t spin,
                        uint64_t pat_need, bool with_db, uint64_t arena_limit_words, bool keys_in_words,
-                       DeepState &hs, cpm_stats &st) {
+                       bool lists, DeepState &hs, cpm_stats &st) {
     const bool dbg = getenv("CPM_DEBUG") != nullptr;
     // Fixed tables large enough for any round; the arena takes the rest.
     const uint64_t frames_cap = 32ull << 20, members_cap = 256ull << 20, queue_cap = 64ull << 20;
@@ -812,6 +812,8 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
     P.pat_parent = b.pat_parent; P.pat_item = b.pat_item; P.pat_sup = b.pat_sup; P.pat_db = b.pat_db;
     P.pat_cap = b.pat_cap;
     P.root_cost = nullptr; P.st = b.st; P.max_stride = max_stride; P.spin_limit = spin; P.cta_time = nullptr;
+    P.lists = lists ? 1u : 0u;
+    P.root_frames = 0; P.defer_words = 0; P.deferred = nullptr; P.deferred_cap = 0;
     const size_t prefix_bytes = max_stride * 8;
     uint64_t rounds = 0, failed = 0, shallow = 0;
     float deep_ms = 0.f;
@@ -848,45 +850,71 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
         ++rounds;
         return CPM_OK;
     };
-    // Arena words a round really used per unit of admitted key, measured on
-    // every successful round (keys are only relative estimates).
-    double words_per_key = 1.0;
+    // Each round queues the next root units (all of them unless a round
+    // overflowed) and lets the kernel defer root units once the round has
+    // filled `frac` of the free arena; deferred units return to the front.
+    // A round that still overflows is discarded and retried with half the
+    // units and half the fill level.
+    double frac = 0.5;
+    uint64_t deferred_total = 0;
+    unsigned long long *d_deferred = nullptr;
+    uint64_t deferred_cap = 0;
+    std::vector<unsigned long long> deferred_h;
     while (!roots.empty()) {
-        // Admission budget: what the kept frames leave of the arena.
-        const double budget = (double)(arena_words - persist_arena) * 0.8;
-        size_t take = 0;
-        double est = 0;
-        while (take < roots.size() && take < limit &&
-               (take == 0 || (est + roots[take].key) * words_per_key <= budget))
-            est += roots[take++].key;
+        const size_t take = (size_t)std::min<uint64_t>(roots.size(), limit);
+        if (take > deferred_cap) {
+            deferred_cap = std::max<uint64_t>(take, deferred_cap * 2);
+            CKR(ds.alloc(&d_deferred, deferred_cap));
+        }
+        P.root_frames = (uint32_t)persist_frames;
+        P.defer_words = persist_arena + std::max<uint64_t>(1, (uint64_t)(frac * (double)(arena_words - persist_arena)));
+        P.deferred = d_deferred;
+        P.deferred_cap = deferred_cap;
         CKR(launch(take, 0));
         if (!hs.error) {
             committed = hs.n_patterns;
-            for (size_t i = 0; i < take; ++i)
+            const uint64_t n_def = hs.n_deferred;
+            if (n_def >= take) return set_err(ctx, CPM_EINTERNAL, "a deep round deferred every root unit");
+            deferred_h.resize(n_def);
+            if (n_def) {
+                CK(cudaMemcpyAsync(deferred_h.data(), d_deferred, n_def * 8, cudaMemcpyDeviceToHost, ctx->stream));
+                CK(cudaStreamSynchronize(ctx->stream));
+            }
+            std::unordered_set<unsigned long long> def(deferred_h.begin(), deferred_h.end());
+            std::vector<Root> back;
+            for (size_t i = 0; i < take; ++i) {
+                if (def.count(((unsigned long long)roots[i].frame << 32) | roots[i].p)) {
+                    back.push_back(roots[i]);
+                    continue;
+                }
                 for (Kept &k : kept)
                     if (k.fid == roots[i].frame) --k.left;
+            }
             roots.erase(roots.begin(), roots.begin() + take);
+            roots.insert(roots.begin(), back.begin(), back.end());
             while (!kept.empty() && kept.back().left == 0) {
                 persist_arena = kept.back().arena_start;
                 kept.pop_back();
             }
-            limit = limit == ~0ull ? limit : limit * 2;
-            // Keys are relative: set the scale to what this round really used,
-            // with a margin (a round that still overflows halves and retries).
-            const double used = (double)(hs.arena_next - persist_arena);
-            if (est > 0 && take > 4) words_per_key = std::max(1e-9, 1.25 * used / est);
+            deferred_total += n_def;
+            if (limit != ~0ull) limit *= 2;
+            frac = std::min(0.5, frac * 1.25);
             continue;
         }
         if (hs.error & DEEP_ERR_SPIN) return set_err(ctx, CPM_ETIMEOUT, "deep-level kernel wait ran out of spins");
+        if (hs.error & DEEP_ERR_INTERNAL)
+            return set_err(ctx, CPM_EINTERNAL, "deep-level kernel: a child list disagrees with its support");
         if (hs.error & DEEP_ERR_PATTERNS)
             return set_err(ctx, CPM_EOVERFLOW, "more than %llu patterns", (unsigned long long)pat_cap);
         ++failed;
         if (take > 1) {
             limit = std::max<size_t>(1, take / 2);
-            words_per_key *= 2;
+            frac = std::max(0.05, frac / 2);
             continue;
         }
         // One root unit whose subtree does not fit: expand it by one level.
+        P.root_frames = 0;
+        P.defer_words = 0;
         CKR(launch(1, 1));
         if (hs.error)
             return set_err(ctx, CPM_EOVERFLOW,
@@ -917,9 +945,9 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
         limit = ~0ull;
     }
     if (dbg)
-        fprintf(stderr, "cpm: deep rounds %llu (failed %llu, shallow %llu), persistent arena %.1f MB, %.3f ms\n",
-                (unsigned long long)rounds, (unsigned long long)failed, (unsigned long long)shallow,
-                persist_arena * 8 / 1e6, deep_ms);
+        fprintf(stderr, "cpm: deep rounds %llu (failed %llu, shallow %llu, deferred units %llu), arena %.1f GB, "
+                "%.3f ms\n", (unsigned long long)rounds, (unsigned long long)failed, (unsigned long long)shallow,
+                (unsigned long long)deferred_total, arena_words * 8 / 1e9, deep_ms);
     st.retries += failed;
     st.deep_rounds = rounds;
     // The caller reads patterns up to hs.n_patterns and the deep time from
@@ -971,6 +999,8 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         item_off[d + 1] = item_off[d] + db->n_items;
         max_stride = std::max<uint64_t>(max_stride, db->stride);
     }
+    // Transaction-id lists need the prefix bitmap in shared memory (k_deep.cuh).
+    const bool use_lists = o.tidsets != 1 && max_stride * 8 <= 200 * 1024;
     CK(cudaMemcpyAsync(d_desc, h.data(), n_db * sizeof(DbDesc), cudaMemcpyHostToDevice, ctx->stream));
     k_compact_frequent_b<<<n_db, 1024, 0, ctx->stream>>>(d_desc, d_F);
     CK(cudaGetLastError());
@@ -1036,15 +1066,46 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     }
     CK(cudaEventRecord(ctx->ev[6], ctx->stream));
     std::vector<uint32_t> cnt(rows), hfreq(items_total);
+    std::vector<uint64_t> list_words_h;
+    uint64_t *d_list_words = nullptr;
     if (rows) {
         k_pair_count_b<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, ctx->stream>>>(d_desc, n_db, rows, cnt_all);
         CK(cudaGetLastError());
         st.kernel_launches++;
         CK(cudaMemcpyAsync(cnt.data(), cnt_all, rows * 4, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaMemcpyAsync(hfreq.data(), freq_all, items_total * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        if (use_lists) {
+            CKR(ds.alloc(&d_list_words, rows));
+            k_list_plan<<<(unsigned)((rows + 255) / 256), 256, 0, ctx->stream>>>(d_desc, n_db, rows, d_list_words);
+            CK(cudaGetLastError());
+            st.kernel_launches++;
+            list_words_h.resize(rows);
+            CK(cudaMemcpyAsync(list_words_h.data(), d_list_words, rows * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        }
     }
     CK(cudaStreamSynchronize(ctx->stream));
     lap("pairs");
+    // Transaction-id lists of the sparse frequent items (members of the top-level classes).
+    unsigned long long *d_row_list = nullptr;
+    if (!list_words_h.empty()) {
+        std::vector<uint64_t> loff(rows);
+        uint64_t lw_total = 0;
+        for (uint64_t r = 0; r < rows; ++r) {
+            loff[r] = lw_total;
+            lw_total += list_words_h[r];
+        }
+        if (lw_total) {
+            uint64_t *d_lbuf = nullptr, *d_loff = nullptr;
+            CKR(ds.alloc(&d_lbuf, lw_total));
+            CKR(ds.alloc(&d_loff, rows));
+            CKR(ds.alloc(&d_row_list, rows));
+            CK(cudaMemcpyAsync(d_loff, loff.data(), rows * 8, cudaMemcpyHostToDevice, ctx->stream));
+            k_item_lists<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, ctx->stream>>>(d_desc, n_db, rows, d_list_words,
+                                                                                     d_loff, d_lbuf, d_row_list);
+            CK(cudaGetLastError());
+            st.kernel_launches++;
+        }
+    }
     // Pair numbering and pattern ids: per database, singletons then pairs.
     std::vector<uint64_t> off(rows + 1, 0);
     for (uint64_t r = 0; r < rows; ++r) off[r + 1] = off[r] + cnt[r];
@@ -1171,7 +1232,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         if (rows) {
             k_emit_b<<<(unsigned)((rows * 32 + 255) / 256), 256, 0, ctx->stream>>>(
                 d_desc, n_db, rows, off_all, b.pat_parent, b.pat_item, b.pat_sup, b.pat_db, b.mem_pat, b.mem_item,
-                b.mem_bits);
+                b.mem_bits, d_row_list);
             CK(cudaGetLastError());
             st.kernel_launches++;
         }
@@ -1260,6 +1321,8 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         }
         P.cta_time = d_ct;
         P.shallow = 0;
+        P.lists = use_lists ? 1u : 0u;
+        P.root_frames = 0; P.defer_words = 0; P.deferred = nullptr; P.deferred_cap = 0;
         CK(cudaEventRecord(ctx->ev[2], ctx->stream));
         if (smem_prefix) k_deep<true><<<grid, block, prefix_bytes, ctx->stream>>>(P);
         else k_deep<false><<<grid, block, 0, ctx->stream>>>(P);
@@ -1292,6 +1355,8 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         if (hs.error & DEEP_ERR_SPIN)
             return set_err(ctx, CPM_ETIMEOUT, "deep-level kernel wait ran out of spins (limit %llu)",
                            (unsigned long long)spin);
+        if (hs.error & DEEP_ERR_INTERNAL)
+            return set_err(ctx, CPM_EINTERNAL, "deep-level kernel: a child list disagrees with its support");
         if (attempt >= 12)
             return set_err(ctx, CPM_EOVERFLOW,
                            "deep-level buffers still too small after retries (error 0x%x, frames %llu/%llu, "
@@ -1319,7 +1384,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     }
     if (rounds) CKR(deep_rounds(ctx, ds, b, frames, d_uid2, d_key2, n_units, base_patterns, P2_total, max_stride,
                                 grid, block, smem_prefix, spin, pat_cap + base_patterns, with_db,
-                                o.arena_bytes ? o.arena_bytes / 8 : 0, learned, hs, st));
+                                o.arena_bytes ? o.arena_bytes / 8 : 0, learned, use_lists, hs, st));
     lap("deep phase");
     if (n_db == 1) {
         // Remember what this database needed so that the next mine() starts there.
@@ -2291,6 +2356,8 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     P.root_cost = d_root_cost; P.st = d_st; P.max_stride = stride; P.spin_limit = 1ull << 26;
     P.cta_time = nullptr;
     P.shallow = 0;
+    P.lists = 0;
+    P.root_frames = 0; P.defer_words = 0; P.deferred = nullptr; P.deferred_cap = 0;
     // Each warp keeps one scratch tidset: leave at least half the arena to children.
     const size_t prefix_bytes = stride * 8;
     const bool smem_prefix = prefix_bytes <= 200 * 1024;

@@ -127,7 +127,8 @@ __global__ void k_emit_b(const DbDesc *__restrict__ d, uint32_t n_db, uint64_t n
                          const uint64_t *__restrict__ off, uint32_t *__restrict__ pat_parent,
                          uint32_t *__restrict__ pat_item, uint32_t *__restrict__ pat_sup,
                          uint32_t *__restrict__ pat_db, uint32_t *__restrict__ mem_pat,
-                         uint32_t *__restrict__ mem_item, const uint64_t **__restrict__ mem_bits) {
+                         uint32_t *__restrict__ mem_item, const uint64_t **__restrict__ mem_bits,
+                         const unsigned long long *__restrict__ row_list) {
     const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     if (r >= n_rows) return;
@@ -158,9 +159,66 @@ __global__ void k_emit_b(const DbDesc *__restrict__ d, uint32_t n_db, uint64_t n
             if (pat_db) pat_db[pid] = db;
             mem_pat[k] = (uint32_t)pid;
             mem_item[k] = item;
-            mem_bits[k] = D.bits + (uint64_t)item * D.stride;
+            // The item's transaction-id list where one was built (bit 0 set), else its bitset.
+            const unsigned long long lp = row_list ? row_list[D.row_base + j] : 0ull;
+            mem_bits[k] = lp ? reinterpret_cast<const uint64_t *>(lp) : D.bits + (uint64_t)item * D.stride;
         }
         pos += __popc(bal);
+    }
+}
+
+// Transaction-id lists of sparse frequent items (the list form of k_deep.cuh:
+// 16-byte header {count, 0, 0, 0}, ascending ids, zero padding to 16 bytes).
+// words[r] = 64-bit words of row r's list, or 0 when the item stays dense
+// (list not at most half the bitset).
+__global__ void k_list_plan(const DbDesc *__restrict__ d, uint32_t n_db, uint64_t n_rows, uint64_t *__restrict__ words) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows) return;
+    const DbDesc &D = d[db_of_row(d, n_db, r)];
+    const uint32_t sup = D.support[D.freq[r - D.row_base]];
+    const uint64_t lw = ((uint64_t)sup + 7) / 4 * 2;
+    words[r] = lw * 2 <= D.stride ? lw : 0;
+}
+
+// One warp per frequent row with a list: extracts the row's set bits in order.
+// row_list[r] gets the tagged pointer (bit 0 set) or 0.
+__global__ void k_item_lists(const DbDesc *__restrict__ d, uint32_t n_db, uint64_t n_rows,
+                             const uint64_t *__restrict__ words, const uint64_t *__restrict__ offs,
+                             uint64_t *__restrict__ buf, unsigned long long *__restrict__ row_list) {
+    const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (r >= n_rows) return;
+    if (!words[r]) {
+        if (lane == 0) row_list[r] = 0ull;
+        return;
+    }
+    const DbDesc &D = d[db_of_row(d, n_db, r)];
+    const uint32_t item = D.freq[r - D.row_base];
+    const ulonglong2 *row = reinterpret_cast<const ulonglong2 *>(D.bits + (uint64_t)item * D.stride);
+    uint32_t *o32 = reinterpret_cast<uint32_t *>(buf + offs[r]);
+    const uint64_t n2 = D.stride / 2;
+    uint32_t written = 0;
+    for (uint64_t v0 = 0; v0 < n2; v0 += 32) {
+        const uint64_t v = v0 + lane;
+        const ulonglong2 x = v < n2 ? ld_stream(row + v) : make_ulonglong2(0ull, 0ull);
+        const uint32_t c = (uint32_t)(__popcll(x.x) + __popcll(x.y));
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(CPM_FULL, incl, o);
+            if (lane >= (unsigned)o) incl += y;
+        }
+        uint32_t pos = 4 + written + incl - c;
+        for (unsigned long long b = x.x; b; b &= b - 1) o32[pos++] = (uint32_t)(v * 128 + __ffsll((long long)b) - 1);
+        for (unsigned long long b = x.y; b; b &= b - 1) o32[pos++] = (uint32_t)(v * 128 + 64 + __ffsll((long long)b) - 1);
+        written += __shfl_sync(CPM_FULL, incl, 31);
+    }
+    const uint32_t end = 4 + written, pad_end = (uint32_t)(((uint64_t)written + 7) / 4 * 4);
+    if (lane < pad_end - end) o32[end + lane] = 0u;
+    if (lane == 0) {
+        o32[0] = written;
+        o32[1] = o32[2] = o32[3] = 0u;
+        row_list[r] = reinterpret_cast<unsigned long long>(o32) | 1ull;
     }
 }
 

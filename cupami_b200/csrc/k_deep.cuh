@@ -16,6 +16,18 @@
 // Frames carry their database's tidset stride, threshold and id, so one launch
 // can mine many databases of different sizes at once.
 //
+// Tidsets come in two forms, told apart by bit 0 of the member pointer.
+// Dense: `stride` 64-bit words, bit r of word r/64 set when transaction r
+// holds the pattern.  List (bit 0 set): a 16-byte header whose first uint32 is
+// the count n, then the n transaction ids in ascending order, padded to a
+// 16-byte multiple.  At one bit per transaction a bitset is the smaller form
+// until fewer than one transaction in 32 holds the pattern; below that (list
+// at most half the dense size) children are written as lists, and frequent
+// items that sparse serve as list members of the top-level classes.  The
+// prefix of a unit is always staged as a dense bitmap in shared memory; a
+// list sibling is intersected by testing its ids against that bitmap.  Lists
+// are used only when the prefix fits in shared memory (P.lists).
+//
 // Every wait is bounded by spin_limit; running out sets DEEP_ERR_SPIN and the
 // kernel returns.  Capacity overflow sets an error bit and stops all CTAs; the
 // host then grows the buffers and reruns, so the output is exact.
@@ -26,8 +38,11 @@ namespace cpm {
 
 enum : unsigned {
     DEEP_ERR_QUEUE = 1u, DEEP_ERR_ARENA = 2u, DEEP_ERR_MEMBERS = 4u, DEEP_ERR_FRAMES = 8u,
-    DEEP_ERR_PATTERNS = 16u, DEEP_ERR_SPIN = 32u,
+    DEEP_ERR_PATTERNS = 16u, DEEP_ERR_SPIN = 32u, DEEP_ERR_INTERNAL = 64u,
 };
+
+// 64-bit words of a list of n transaction ids (16-byte header, 16-byte padding).
+__host__ __device__ __forceinline__ uint64_t list_words(uint64_t n) { return (n + 7) / 4 * 2; }
 
 constexpr unsigned long long QUEUE_EMPTY = ~0ull;
 constexpr uint32_t NO_PATTERN = 0xffffffffu;
@@ -58,6 +73,7 @@ struct DeepState {
     CPM_LINE(bytes_alg);
     CPM_LINE(work_items);
     CPM_LINE(survivors);
+    CPM_LINE(n_deferred);   // root units handed back to the host (memory-bounded rounds)
     unsigned int error;
     unsigned int pad[31];
 };
@@ -75,7 +91,48 @@ struct DeepParams {
     unsigned long long spin_limit;
     unsigned long long *cta_time;   // optional [2 * grid]: busy ns, exit time (globaltimer)
     uint32_t shallow;               // 1: child frames are recorded, not queued
+    uint32_t lists;                 // 1: list-form tidsets allowed (needs SMEM_PREFIX)
+    // Memory-bounded rounds: a unit of a frame below root_frames (a root
+    // unit) claimed while arena_next >= defer_words is not run but handed
+    // back in deferred[] for a later round (defer_words 0: never).
+    uint32_t root_frames;
+    unsigned long long defer_words;
+    unsigned long long *deferred;
+    uint64_t deferred_cap;
 };
+
+// Child tidset form: a list when it takes at most half the dense words.
+__device__ __forceinline__ bool as_list(const DeepParams &P, uint64_t n, uint32_t stride) {
+    return P.lists && list_words(n) * 2 <= stride;
+}
+
+__device__ __forceinline__ unsigned long long ld_raw_ptr(const uint64_t *const *p) {
+    return __ldcg(reinterpret_cast<const unsigned long long *>(p));
+}
+
+__device__ __forceinline__ uint32_t bit_of(const uint32_t *bm, uint32_t t) { return (bm[t >> 5] >> (t & 31)) & 1u; }
+
+// Exclusive prefix sum over the block (every thread calls it); *total gets
+// the block's sum.  s_w holds 32 partial sums.
+__device__ __forceinline__ uint64_t block_excl_scan_u64(uint64_t v, uint64_t *s_w, uint64_t *total) {
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint64_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(CPM_FULL, incl, o);
+        if (lane >= (unsigned)o) incl += y;
+    }
+    if (lane == 31) s_w[wid] = incl;
+    __syncthreads();
+    uint64_t before = 0, tot = 0;
+    for (unsigned w = 0; w < nw; ++w) {
+        if (w < wid) before += s_w[w];
+        tot += s_w[w];
+    }
+    __syncthreads();
+    *total = tot;
+    return before + incl - v;
+}
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -117,10 +174,14 @@ template <bool SMEM_PREFIX>
 __global__ void __launch_bounds__(512) k_deep(DeepParams P) {
     extern __shared__ ulonglong2 s_prefix[];
     __shared__ unsigned long long s_item;
-    __shared__ int s_stop, s_ok, s_grant;
+    __shared__ int s_stop, s_ok, s_grant, s_skip;
     __shared__ uint32_t s_surv;
     __shared__ unsigned long long s_mem_base, s_arena_base, s_fid, s_qbase;
     __shared__ uint32_t s_wtot[32];
+    __shared__ uint64_t s_w64[32];
+    __shared__ uint64_t s_off[512];      // child offsets of one chunk of survivors
+    __shared__ unsigned long long s_bytes;
+    uint32_t *const s_p32 = reinterpret_cast<uint32_t *>(s_prefix);
 
     const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     DeepState *st = P.st;
@@ -128,9 +189,26 @@ __global__ void __launch_bounds__(512) k_deep(DeepParams P) {
     unsigned long long c_inter = 0, c_bytes = 0, c_units = 0, c_surv = 0, c_busy = 0, t_unit = 0;
 
     for (;;) {
-        if (threadIdx.x == 0) s_stop = deep_claim(P, &s_item);
+        if (threadIdx.x == 0) {
+            s_stop = deep_claim(P, &s_item);
+            s_skip = 0;
+            if (!s_stop && P.defer_words && (uint32_t)(s_item >> 32) < P.root_frames &&
+                ld_acquire_u64(&st->arena_next) >= P.defer_words) {
+                // The round's arena is filling up: leave this root unit to the next round.
+                const unsigned long long di = atomicAdd(&st->n_deferred, 1ull);
+                if (di < P.deferred_cap) P.deferred[di] = s_item;
+                else deep_fail(st, DEEP_ERR_QUEUE);
+                __threadfence();
+                atomicAdd(&st->pending, ~0ull);  // pending -= 1
+                s_skip = 1;
+            }
+        }
         __syncthreads();
         if (s_stop) break;
+        if (s_skip) {
+            __syncthreads();  // every thread has read s_skip before thread 0 claims again
+            continue;
+        }
         if (threadIdx.x == 0 && P.cta_time) t_unit = global_ns();
         const uint32_t fid = (uint32_t)(s_item >> 32), p = (uint32_t)s_item;
         const DFrame *fp = P.frames + fid;
@@ -145,12 +223,29 @@ __global__ void __launch_bounds__(512) k_deep(DeepParams P) {
         const long long minsup = __ldcg(&fp->minsup);
         const uint64_t n2 = stride / 2;
         const uint32_t cnt = m - p - 1;
-        const ulonglong2 *pb = ld_ptr(P.mem_bits + mem_off + p);
-        if (SMEM_PREFIX) {
+        const unsigned long long praw = ld_raw_ptr(P.mem_bits + mem_off + p);
+        const ulonglong2 *pb = reinterpret_cast<const ulonglong2 *>(praw);
+        uint64_t prefix_bytes = 8ull * stride;
+        if (SMEM_PREFIX && (praw & 1ull)) {
+            // List prefix: clear the bitmap, set its transactions, then apply the mask.
+            const uint32_t *L = reinterpret_cast<const uint32_t *>(praw & ~1ull);
+            const uint32_t n = __ldcg(L);
+            prefix_bytes = 8ull * list_words(n);
+            for (uint64_t v = threadIdx.x; v < n2; v += blockDim.x) s_prefix[v] = make_ulonglong2(0ull, 0ull);
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const uint32_t t = __ldcg(L + 4 + i);
+                atomicOr(s_p32 + (t >> 5), 1u << (t & 31));
+            }
+            __syncthreads();
+            if (mk)
+                for (uint64_t v = threadIdx.x; v < n2; v += blockDim.x) s_prefix[v] = and2(s_prefix[v], ld_cg(mk + v));
+        } else if (SMEM_PREFIX) {
             for (uint64_t v = threadIdx.x; v < n2; v += blockDim.x)
                 s_prefix[v] = mk ? and2(ld_cg(pb + v), ld_cg(mk + v)) : ld_cg(pb + v);
         }
         if (threadIdx.x == 0) {
+            s_bytes = prefix_bytes;
             s_surv = 0;
             const unsigned long long mb = atomicAdd(&st->n_members, (unsigned long long)cnt);
             if (mb + cnt > P.members_cap) deep_fail(st, DEEP_ERR_MEMBERS);
@@ -163,10 +258,41 @@ __global__ void __launch_bounds__(512) k_deep(DeepParams P) {
         // ---- pass 1: supports of every later member ----
         for (uint32_t q = wid; ok && q < cnt; q += nw) {
             const uint64_t mi = mem_off + p + 1 + q;
-            const ulonglong2 *sb = ld_ptr(P.mem_bits + mi);
+            const unsigned long long sraw = ld_raw_ptr(P.mem_bits + mi);
+            const ulonglong2 *sb = reinterpret_cast<const ulonglong2 *>(sraw);
             const uint32_t sib_item = __ldcg(P.mem_item + mi);
             uint32_t s = 0;
             uint64_t v = lane;
+            if (SMEM_PREFIX && (sraw & 1ull)) {
+                // List sibling: test its ids against the prefix bitmap (four
+                // 16-byte loads of ids in flight per lane).
+                const uint32_t *L = reinterpret_cast<const uint32_t *>(sraw & ~1ull);
+                const uint32_t n = __ldcg(L);
+                const uint4 *T = reinterpret_cast<const uint4 *>(L + 4);
+                const uint32_t nv = (n + 3) / 4, nfull = n / 4;
+                uint32_t w = lane;
+                for (; w + 96 < nfull; w += 128) {  // four complete groups of four ids
+                    uint4 t[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) t[u] = __ldcg(T + w + 32 * u);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        s += bit_of(s_p32, t[u].x) + bit_of(s_p32, t[u].y) + bit_of(s_p32, t[u].z) +
+                             bit_of(s_p32, t[u].w);
+                }
+                for (; w < nv; w += 32) {
+                    const uint4 t = __ldcg(T + w);
+                    const uint32_t i0 = 4 * w;
+                    s += bit_of(s_p32, t.x);
+                    if (i0 + 1 < n) s += bit_of(s_p32, t.y);
+                    if (i0 + 2 < n) s += bit_of(s_p32, t.z);
+                    if (i0 + 3 < n) s += bit_of(s_p32, t.w);
+                }
+                if (lane == 0) atomicAdd(&s_bytes, 8ull * list_words(n));
+                v = n2;  // the dense loops below do nothing
+            } else if (lane == 0) {
+                atomicAdd(&s_bytes, 8ull * stride);
+            }
             // Eight 16-byte loads in flight per lane (4 KB per warp).
             for (; v + 224 < n2; v += 256) {
                 ulonglong2 x[8];
@@ -232,7 +358,7 @@ __global__ void __launch_bounds__(512) k_deep(DeepParams P) {
                 if (q < cnt) {
                     e_pat = __ldcg(P.mem_pat + src);
                     e_item = __ldcg(P.mem_item + src);
-                    e_bits = reinterpret_cast<const uint64_t *>(ld_ptr(P.mem_bits + src));
+                    e_bits = reinterpret_cast<const uint64_t *>(ld_raw_ptr(P.mem_bits + src));
                 }
                 const bool keep = e_pat != NO_PATTERN;
                 const unsigned bal = __ballot_sync(CPM_FULL, keep);
@@ -259,12 +385,24 @@ __global__ void __launch_bounds__(512) k_deep(DeepParams P) {
         __syncthreads();
         const uint32_t ns = s_surv;
         const bool expand = ns >= 2;
+        // Words of the survivors' child tidsets (each dense or a list, by its support).
+        uint64_t child_words = (uint64_t)ns * stride;
+        if (expand && P.lists) {
+            uint64_t part = 0;
+            for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) {
+                const uint32_t sc = __ldcg(P.pat_sup + __ldcg(P.mem_pat + s_mem_base + i));
+                part += as_list(P, sc, stride) ? list_words(sc) : stride;
+            }
+            uint64_t tot = 0;
+            block_excl_scan_u64(part, s_w64, &tot);
+            child_words = tot;
+        }
         if (threadIdx.x == 0) {
             s_grant = 0;
             s_fid = ~0ull;
             if (expand && ld_acquire_u32(&st->error) == 0) {
-                const unsigned long long ab = atomicAdd(&st->arena_next, (unsigned long long)ns * stride);
-                if (ab + (unsigned long long)ns * stride > P.arena_words) deep_fail(st, DEEP_ERR_ARENA);
+                const unsigned long long ab = atomicAdd(&st->arena_next, (unsigned long long)child_words);
+                if (ab + (unsigned long long)child_words > P.arena_words) deep_fail(st, DEEP_ERR_ARENA);
                 else s_grant = 1;
                 s_arena_base = ab;
             }
@@ -272,22 +410,99 @@ __global__ void __launch_bounds__(512) k_deep(DeepParams P) {
         __syncthreads();
         // ---- pass 2: child tidsets of the survivors (only when they recurse) ----
         if (s_grant) {
-            for (uint32_t idx = wid; idx < ns; idx += nw) {
-                const uint64_t m_out = s_mem_base + idx;
-                const ulonglong2 *sb = ld_ptr(P.mem_bits + m_out);
-                ulonglong2 *dst = reinterpret_cast<ulonglong2 *>(P.arena + s_arena_base + (uint64_t)idx * stride);
-                for (uint64_t v = lane; v < n2; v += 32) {
-                    ulonglong2 x = ld_cg(sb + v);
-                    if (SMEM_PREFIX) {
-                        x = and2(x, s_prefix[v]);
+            uint64_t chunk_base = 0;
+            for (uint32_t start = 0; start < ns; start += blockDim.x) {
+                // Offsets of this chunk's children within the unit's block.
+                const uint32_t i = start + threadIdx.x;
+                uint64_t sz = 0;
+                if (i < ns) {
+                    if (P.lists) {
+                        const uint32_t sc = __ldcg(P.pat_sup + __ldcg(P.mem_pat + s_mem_base + i));
+                        sz = as_list(P, sc, stride) ? list_words(sc) : stride;
                     } else {
-                        x = and2(x, ld_cg(pb + v));
-                        if (mk) x = and2(x, ld_cg(mk + v));
+                        sz = stride;
                     }
-                    dst[v] = x;
                 }
-                __syncwarp();
-                if (lane == 0) P.mem_bits[m_out] = reinterpret_cast<const uint64_t *>(dst);
+                uint64_t chunk_total = 0;
+                const uint64_t excl = block_excl_scan_u64(sz, s_w64, &chunk_total);
+                s_off[threadIdx.x] = chunk_base + excl;
+                __syncthreads();
+                const uint32_t stop = min(ns, start + blockDim.x);
+                for (uint32_t idx = start + wid; idx < stop; idx += nw) {
+                    const uint64_t m_out = s_mem_base + idx;
+                    const unsigned long long sraw = ld_raw_ptr(P.mem_bits + m_out);
+                    const ulonglong2 *sb = reinterpret_cast<const ulonglong2 *>(sraw);
+                    uint64_t *out = P.arena + s_arena_base + s_off[idx - start];
+                    const uint32_t sc = P.lists ? __ldcg(P.pat_sup + __ldcg(P.mem_pat + m_out)) : 0u;
+                    unsigned long long tagged;
+                    if (SMEM_PREFIX && as_list(P, sc, stride)) {
+                        // List child: the ids of the sibling's transactions that the
+                        // prefix holds, in ascending order.
+                        uint32_t *o32 = reinterpret_cast<uint32_t *>(out);
+                        uint32_t written = 0;
+                        if (sraw & 1ull) {
+                            const uint32_t *L = reinterpret_cast<const uint32_t *>(sraw & ~1ull);
+                            const uint32_t n = __ldcg(L);
+                            for (uint32_t j0 = 0; j0 < n; j0 += 32) {
+                                const uint32_t j = j0 + lane;
+                                const uint32_t t = j < n ? __ldcg(L + 4 + j) : 0u;
+                                const bool keep = j < n && bit_of(s_p32, t);
+                                const unsigned bal = __ballot_sync(CPM_FULL, keep);
+                                const uint32_t at = written + __popc(bal & ((1u << lane) - 1));
+                                if (keep && at < sc) o32[4 + at] = t;
+                                written += __popc(bal);
+                            }
+                        } else {
+                            for (uint64_t v0 = 0; v0 < n2; v0 += 32) {
+                                const uint64_t v = v0 + lane;
+                                ulonglong2 x = make_ulonglong2(0ull, 0ull);
+                                if (v < n2) x = and2(ld_cg(sb + v), s_prefix[v]);
+                                const uint32_t c = (uint32_t)(__popcll(x.x) + __popcll(x.y));
+                                uint32_t incl = c;
+#pragma unroll
+                                for (int o = 1; o < 32; o <<= 1) {
+                                    const uint32_t y = __shfl_up_sync(CPM_FULL, incl, o);
+                                    if (lane >= (unsigned)o) incl += y;
+                                }
+                                uint32_t at = written + incl - c;  // stays below sc unless counts disagree
+                                for (unsigned long long b = x.x; b; b &= b - 1, ++at)
+                                    if (at < sc) o32[4 + at] = (uint32_t)(v * 128 + __ffsll((long long)b) - 1);
+                                for (unsigned long long b = x.y; b; b &= b - 1, ++at)
+                                    if (at < sc) o32[4 + at] = (uint32_t)(v * 128 + 64 + __ffsll((long long)b) - 1);
+                                written += __shfl_sync(CPM_FULL, incl, 31);
+                            }
+                        }
+                        if (lane == 0) {
+                            o32[0] = sc;
+                            o32[1] = o32[2] = o32[3] = 0u;
+                            if (written != sc) deep_fail(st, DEEP_ERR_INTERNAL);
+                        }
+                        // Ids the count promised but the pass did not find (only when the
+                        // counts disagree, an error) become 0, an in-range id.
+                        for (uint32_t j = written + lane; j < sc; j += 32) o32[4 + j] = 0u;
+                        // Zero the padding after the last id.
+                        const uint32_t end = 4 + sc, pad_end = (uint32_t)(list_words(sc) * 2);
+                        if (lane < pad_end - end) o32[end + lane] = 0u;
+                        tagged = reinterpret_cast<unsigned long long>(out) | 1ull;
+                    } else {
+                        ulonglong2 *dst = reinterpret_cast<ulonglong2 *>(out);
+                        for (uint64_t v = lane; v < n2; v += 32) {
+                            ulonglong2 x = ld_cg(sb + v);
+                            if (SMEM_PREFIX) {
+                                x = and2(x, s_prefix[v]);
+                            } else {
+                                x = and2(x, ld_cg(pb + v));
+                                if (mk) x = and2(x, ld_cg(mk + v));
+                            }
+                            dst[v] = x;
+                        }
+                        tagged = reinterpret_cast<unsigned long long>(out);
+                    }
+                    __syncwarp();
+                    if (lane == 0) P.mem_bits[m_out] = reinterpret_cast<const uint64_t *>(tagged);
+                }
+                chunk_base += chunk_total;
+                __syncthreads();
             }
             __threadfence();
         }
@@ -328,7 +543,7 @@ __global__ void __launch_bounds__(512) k_deep(DeepParams P) {
         __syncthreads();
         if (threadIdx.x == 0) {
             c_inter += cnt;
-            c_bytes += 8ull * stride * (1ull + cnt + (expand ? ns : 0));
+            c_bytes += s_bytes + (s_grant ? 8ull * child_words : 0ull);
             c_units += 1;
             c_surv += ns;
             if (P.root_cost) atomicAdd(P.root_cost + root, (unsigned long long)cnt);

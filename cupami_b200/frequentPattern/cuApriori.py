@@ -72,6 +72,9 @@ class cuApriori:
     #: (1-4); 0 leaves each to the library (or to the autotuner's table).
     _DEEP_BLOCK = 0
     _DEEP_CTAS_PER_SM = 0
+    #: Tidset forms of the deep levels: 0 bitsets plus transaction-id lists for
+    #: tidsets held by under 1/32 of the transactions; 1 bitsets only.
+    _TIDSETS = 0
 
     def __init__(self, iFile, minSup, sep=None, use_gds="auto", use_gpu_io="auto"):
         loading_start = time.perf_counter()
@@ -263,6 +266,7 @@ class cuApriori:
         opts.deep_block = int(self._DEEP_BLOCK)
         opts.deep_ctas_per_sm = int(self._DEEP_CTAS_PER_SM)
         opts.autotune = 1
+        opts.tidsets = int(self._TIDSETS)
         return opts
 
     def autotune(self):

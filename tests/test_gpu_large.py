@@ -31,7 +31,7 @@ def expected():
     return json.loads((GOLDEN / "sparse_zipf_1m_summary.json").read_text())
 
 
-@pytest.mark.parametrize("scheduler,arena_bytes", [("plain", 0), ("learned", 3 << 30)])
+@pytest.mark.parametrize("scheduler,arena_bytes", [("plain", 0), ("learned", 2 << 30)])
 def test_sparse_1m_matches_oracle_summary(workload, expected, scheduler, arena_bytes):
     from make_sparse_summary import summarize
 

@@ -151,3 +151,43 @@ def test_launch_shapes_and_autotuner_keep_output():
     bad._DEEP_BLOCK = 96
     with pytest.raises(_native.NativeError):
         bad.mine()
+
+
+@pytest.mark.parametrize("name,minsup", [("planted_zipf", 0.005), ("uniform_poisson", 0.01),
+                                         ("dense_bernoulli", 0.6)])
+def test_list_and_bitset_tidsets_agree(oracle_lib, name, minsup):
+    """Deep levels with transaction-id lists for sparse tidsets (the default) and
+    with bitsets only give the same patterns, in order, as the oracle."""
+    import cupami_b200
+    from cupami_b200 import datasets
+
+    csr = getattr(datasets, name)()
+    out = []
+    for tidsets in (0, 1):
+        m = cupami_b200.cuEclat(csr, minsup)
+        m._TIDSETS = tidsets
+        m.mine()
+        out.append((list(m.getPatterns().items()), m.getKernelStats()))
+    assert out[0][0] == out[1][0]
+    labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, minsup)
+    assert dict(out[0][0]) == oracle_lib.to_dict(labels, arrays)
+    if name == "planted_zipf":  # sparse deep levels: the lists move fewer bytes
+        assert out[0][1]["bytes_alg"] < out[1][1]["bytes_alg"]
+
+
+def test_lists_in_memory_bounded_rounds_and_batches(oracle_lib):
+    from cupami_b200 import _native, cuEclat, datasets
+
+    csr = datasets.planted_zipf(n=60000, seed=21)
+    m = cuEclat(csr, 0.004)
+    m._ARENA_BYTES = 256 << 10
+    m.mine()
+    assert m.getKernelStats()["deep_rounds"] > 1
+    labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, 0.004)
+    assert m.getPatterns() == oracle_lib.to_dict(labels, arrays)
+    csrs = datasets.batched_zipf(limit=12)
+    for tidsets in (0, 1):
+        cls = type("E", (cuEclat,), {"_TIDSETS": tidsets})
+        for csr, m in zip(csrs, cls.mineBatch(csrs, 0.01)):
+            labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, 0.01)
+            assert m.getPatterns() == oracle_lib.to_dict(labels, arrays)
