@@ -178,13 +178,23 @@ def test_list_and_bitset_tidsets_agree(oracle_lib, name, minsup):
 def test_lists_in_memory_bounded_rounds_and_batches(oracle_lib):
     from cupami_b200 import _native, cuEclat, datasets
 
-    csr = datasets.planted_zipf(n=60000, seed=21)
-    m = cuEclat(csr, 0.004)
-    m._ARENA_BYTES = 256 << 10
-    m.mine()
-    assert m.getKernelStats()["deep_rounds"] > 1
-    labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, 0.004)
-    assert m.getPatterns() == oracle_lib.to_dict(labels, arrays)
+    from cupami_b200 import TransactionCSR
+
+    # Sparse items (p up to 0.3) at a low threshold: the deeper children are
+    # held by under 1/32 of the 4000 transactions, so they become lists.
+    rng = np.random.default_rng(22)
+    p = rng.uniform(0.02, 0.3, 30)
+    rows = [[int(i) for i in np.nonzero(rng.random(30) < p)[0]] for _ in range(4000)]
+    csr = TransactionCSR.from_rows(rows, universe=30)
+    labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, 0.005)
+    want = oracle_lib.to_dict(labels, arrays)
+    for arena in (64 << 10, 0):
+        m = cuEclat(csr, 0.005)
+        m._ARENA_BYTES = arena
+        m.mine()
+        assert m.getPatterns() == want
+        if arena:
+            assert m.getKernelStats()["deep_rounds"] > 1
     csrs = datasets.batched_zipf(limit=12)
     for tidsets in (0, 1):
         cls = type("E", (cuEclat,), {"_TIDSETS": tidsets})
