@@ -56,6 +56,7 @@ struct cpm_ctx {
     std::vector<float> model;  // cost-model parameters (empty: none loaded)
     float last_deep_ms = 0.f;  // deep-phase kernel time of the last bounded-round run
     int last_deep_block = 0, last_deep_ctas = 0;  // launch shape of the last deep phase
+    size_t l2_bytes = 126ull << 20;               // device L2 size (cpm_init)
     std::map<int, std::pair<int, int>> tune;      // log2(stride) -> (threads per CTA, CTAs per SM), cpm_autotune
 };
 
@@ -165,6 +166,9 @@ extern "C" int cpm_init(int device, cpm_ctx **out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&ctx->ev[i]);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+    int l2 = 0;
+    if (e == cudaSuccess && cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device) == cudaSuccess && l2 > 0)
+        ctx->l2_bytes = (size_t)l2;
     int major = 0, minor = 0;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device);
@@ -734,13 +738,21 @@ static int grow(cpm_ctx *ctx, DeepBuffers &b, uint64_t frames_cap, uint64_t memb
 // overflows runs shallow -- only its own intersections -- and its child
 // frame, kept in the persistent region, contributes its positions as new
 // root units, processed next (depth first, so the region stays small).
+static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::vector<DFrame> &top_frames,
+                           const uint32_t *d_uid, const float *d_key, uint64_t n_units, uint64_t P2_total,
+                           uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix, uint64_t spin,
+                           bool keys_in_words, bool lists, const std::vector<unsigned long long> *cont,
+                           uint64_t arena_words, uint64_t pat_cap, DeepState &hs, cpm_stats &st);
+
 static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::vector<DFrame> &top_frames,
                        const uint32_t *d_uid, const float *d_key, uint64_t n_units, uint64_t base_patterns,
                        uint64_t P2_total, uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix,
                        uint64_t spin,
                        uint64_t pat_need, bool with_db, uint64_t arena_limit_words, bool keys_in_words,
-                       bool lists, DeepState &hs, cpm_stats &st) {
+                       bool lists, const std::vector<unsigned long long> *cont, DeepState &hs, cpm_stats &st) {
     const bool dbg = getenv("CPM_DEBUG") != nullptr;
+    if (cont) return deep_rounds_run(ctx, ds, b, top_frames, nullptr, nullptr, 0, P2_total, max_stride, grid, block,
+                                     smem_prefix, spin, keys_in_words, lists, cont, b.arena_words, b.pat_cap, hs, st);
     // Fixed tables large enough for any round; the arena takes the rest.
     const uint64_t frames_cap = 32ull << 20, members_cap = 256ull << 20, queue_cap = 64ull << 20;
     const uint64_t pat_cap = std::max<uint64_t>(pat_need, 96ull << 20);
@@ -761,11 +773,8 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
     CK(cudaMemcpyAsync(mp.data(), b.mem_pat, P2_total * 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(mi.data(), b.mem_item, P2_total * 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaMemcpyAsync(mb.data(), b.mem_bits, P2_total * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    std::vector<uint32_t> uid(n_units);
-    std::vector<float> key(n_units);
-    CK(cudaMemcpyAsync(uid.data(), d_uid, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(key.data(), d_key, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    // The unit order (d_uid / d_key) lives in the caller's scratch, not in b.
     CKR(grow(ctx, b, frames_cap, members_cap, queue_cap, arena_words, pat_cap, 1, with_db));
     CK(cudaMemcpyAsync(b.pat_parent, par.data(), base_patterns * 4, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(b.pat_item, item.data(), base_patterns * 4, cudaMemcpyHostToDevice, ctx->stream));
@@ -776,12 +785,38 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
     CK(cudaMemcpyAsync(b.mem_bits, mb.data(), P2_total * 8, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(b.frames, top_frames.data(), top_frames.size() * sizeof(DFrame), cudaMemcpyHostToDevice,
                        ctx->stream));
+    hs = DeepState{};
+    hs.n_patterns = base_patterns;
+    return deep_rounds_run(ctx, ds, b, top_frames, d_uid, d_key, n_units, P2_total, max_stride, grid, block,
+                           smem_prefix, spin, keys_in_words, lists, nullptr, arena_words, pat_cap, hs, st);
+}
+
+// The rounds themselves.  Fresh start (cont null): every root unit d_uid /
+// d_key, largest first, after the top level was rebuilt in b.  Continuation
+// (cont): the root units a first launch deferred, in queue order, with the
+// top level and the patterns found so far (hs.n_patterns) kept in b.
+static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::vector<DFrame> &top_frames,
+                           const uint32_t *d_uid, const float *d_key, uint64_t n_units, uint64_t P2_total,
+                           uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix, uint64_t spin,
+                           bool keys_in_words, bool lists, const std::vector<unsigned long long> *cont,
+                           uint64_t arena_words, uint64_t pat_cap, DeepState &hs, cpm_stats &st) {
+    const bool dbg = getenv("CPM_DEBUG") != nullptr;
+    const uint64_t queue_cap = b.queue_cap;
+    std::vector<uint32_t> uid(n_units);
+    std::vector<float> key(n_units);
+    if (n_units) {
+        CK(cudaMemcpyAsync(uid.data(), d_uid, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(key.data(), d_key, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     // Root units as (frame, position, key), front = next.
     struct Root {
         uint32_t frame, p;
         double key;
     };
     std::deque<Root> roots;
+    if (cont)
+        for (unsigned long long it : *cont) roots.push_back({(uint32_t)(it >> 32), (uint32_t)it, 1.0});
     for (uint64_t i = 0; i < n_units; ++i) {
         uint32_t k = (uint32_t)(std::upper_bound(top_frames.begin(), top_frames.end(), uid[i],
                                                  [](uint32_t u, const DFrame &f) { return u < f.root; }) -
@@ -792,7 +827,7 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
         roots.push_back({k, uid[i] - top_frames[k].root, std::max(1.0, words)});
     }
     uint64_t persist_frames = top_frames.size(), persist_members = P2_total, persist_arena = 0;
-    uint64_t committed = base_patterns;
+    uint64_t committed = hs.n_patterns;
     // Child frames kept by shallow expansions form a stack at the front of
     // the arena: (frame id, arena start, root units still queued).  A frame's
     // block is released once every root unit taken from it has run.
@@ -904,8 +939,25 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
         if (hs.error & DEEP_ERR_SPIN) return set_err(ctx, CPM_ETIMEOUT, "deep-level kernel wait ran out of spins");
         if (hs.error & DEEP_ERR_INTERNAL)
             return set_err(ctx, CPM_EINTERNAL, "deep-level kernel: a child list disagrees with its support");
-        if (hs.error & DEEP_ERR_PATTERNS)
-            return set_err(ctx, CPM_EOVERFLOW, "more than %llu patterns", (unsigned long long)pat_cap);
+        if (hs.error & DEEP_ERR_PATTERNS) {
+            // Grow the pattern records (keeping the committed ones) and rerun the round.
+            const uint64_t cap = std::max<uint64_t>(b.pat_cap * 2, committed + (hs.n_patterns - committed) * 2);
+            uint32_t *np_[4] = {nullptr, nullptr, nullptr, nullptr};
+            uint32_t **old_[4] = {&b.pat_parent, &b.pat_item, &b.pat_sup, &b.pat_db};
+            for (int a = 0; a < 4; ++a) {
+                if (!*old_[a]) continue;
+                CKR(dalloc(ctx, &np_[a], cap));
+                if (committed)
+                    CK(cudaMemcpyAsync(np_[a], *old_[a], committed * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+                dfree(ctx, *old_[a]);
+                *old_[a] = np_[a];
+            }
+            b.pat_cap = cap;
+            P.pat_parent = b.pat_parent; P.pat_item = b.pat_item; P.pat_sup = b.pat_sup; P.pat_db = b.pat_db;
+            P.pat_cap = b.pat_cap;
+            ++failed;
+            continue;
+        }
         ++failed;
         if (take > 1) {
             limit = std::max<size_t>(1, take / 2);
@@ -999,8 +1051,9 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         item_off[d + 1] = item_off[d] + db->n_items;
         max_stride = std::max<uint64_t>(max_stride, db->stride);
     }
-    // Transaction-id lists need the prefix bitmap in shared memory (k_deep.cuh).
-    const bool use_lists = o.tidsets != 1 && max_stride * 8 <= 200 * 1024;
+    // Transaction-id lists need the prefix bitmap in shared memory (k_deep.cuh);
+    // decided once the frequent items are known (below).
+    bool use_lists = false;
     CK(cudaMemcpyAsync(d_desc, h.data(), n_db * sizeof(DbDesc), cudaMemcpyHostToDevice, ctx->stream));
     k_compact_frequent_b<<<n_db, 1024, 0, ctx->stream>>>(d_desc, d_F);
     CK(cudaGetLastError());
@@ -1009,6 +1062,15 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     CK(cudaMemcpyAsync(F.data(), d_F, n_db * 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     lap("singletons");
+    // Lists halve the bytes of sparse tidsets but cost more instructions per
+    // byte: they pay where the deep phase streams from HBM, i.e. where one
+    // database's frequent tidsets exceed half the L2 (126 MB on B200).
+    {
+        uint64_t biggest = 0;
+        for (uint32_t d = 0; d < n_db; ++d) biggest = std::max<uint64_t>(biggest, (uint64_t)F[d] * dbs[d]->stride * 8);
+        use_lists = o.tidsets != 1 && max_stride * 8 <= 200 * 1024 &&
+                    (o.tidsets == 2 || biggest > (uint64_t)ctx->l2_bytes / 2);
+    }
     // ---- pair Grams ----
     uint64_t rows = 0, c_total = 0;
     std::vector<uint64_t> c_off(n_db, 0);
@@ -1160,9 +1222,12 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     uint64_t queue_cap = std::max<uint64_t>({4096, n_units * 8 + P2_total * 4, n_db == 1 ? db0->hint_queue : 0});
     uint64_t pat_cap = std::max<uint64_t>({4096, base_patterns * 16, n_db == 1 ? db0->hint_patterns : 0});
     const uint64_t arena_budget = o.arena_bytes ? o.arena_bytes / 8 : (uint64_t)(ctx->mem_free * 0.6) / 8;
+    // First arena: what the database needed before, else a guess capped at
+    // 16 GB (a launch that fills it hands the rest to rounds).
     uint64_t arena_words = o.arena_bytes ? o.arena_bytes / 8
                                          : std::min<uint64_t>(arena_budget, std::max<uint64_t>(
-                                               {(uint64_t)4096 * max_stride, P2_total * 8 * max_stride,
+                                               {(uint64_t)4096 * max_stride,
+                                                std::min<uint64_t>(P2_total * 8 * max_stride, 2ull << 30),
                                                 n_db == 1 ? db0->hint_arena : 0}));
     const uint64_t spin = o.spin_limit ? o.spin_limit : (1ull << 26);
     const size_t prefix_bytes = max_stride * 8;
@@ -1225,6 +1290,8 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         CKR(ds.alloc(reinterpret_cast<unsigned char **>(&d_sort_tmp), sort_bytes));
     }
 
+    unsigned long long *d_deferred = nullptr;
+    if (n_units) CKR(ds.alloc(&d_deferred, n_units));
     for (int attempt = 0;; ++attempt) {
         CKR(grow(ctx, b, frames_cap, members_cap, queue_cap, arena_words, pat_cap + base_patterns, n_units,
                  with_db));
@@ -1256,41 +1323,10 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
                                                                                d_uid2, (uint32_t)n_units, b.queue);
         CK(cudaGetLastError());
         st.kernel_launches += 3;
-        if (attempt == 0) {
-            // Go to bounded rounds at once only when one launch cannot fit:
-            // the arena this database needed before exceeds the budget, or,
-            // without that record, the estimated child-tidset words (learned
-            // keys estimate words touched; plain keys count later members,
-            // times the frame's tidset length) exceed it many times over --
-            // both estimates overshoot, so a moderate excess runs one launch
-            // and falls back to rounds only if its arena really overflows.
-            bool direct = false;
-            if (n_db == 1 && db0->hint_arena) {
-                direct = db0->hint_arena > arena_budget;
-            } else {
-                std::vector<float> keys(n_units);
-                std::vector<uint32_t> uids(n_units);
-                CK(cudaMemcpyAsync(keys.data(), d_key2, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
-                CK(cudaMemcpyAsync(uids.data(), d_uid2, n_units * 4, cudaMemcpyDeviceToHost, ctx->stream));
-                CK(cudaStreamSynchronize(ctx->stream));
-                double est = 0;
-                for (uint64_t i = 0; i < n_units; ++i) {
-                    if (learned) {
-                        est += keys[i];
-                        continue;
-                    }
-                    const size_t k = (size_t)(std::upper_bound(frames.begin(), frames.end(), uids[i],
-                                                               [](uint32_t u, const DFrame &f) { return u < f.root; }) -
-                                              frames.begin()) - 1;
-                    est += (double)keys[i] * frames[k].stride;
-                }
-                direct = est > 16.0 * (double)arena_budget;
-                if (dbg) fprintf(stderr, "cpm: estimated arena %.3g words, budget %.3g words\n", est, (double)arena_budget);
-            }
-            if (direct) {
-                rounds = true;
-                break;
-            }
+        if (attempt == 0 && n_db == 1 && db0->hint_arena > arena_budget) {
+            // This database's child tidsets did not fit in one launch before.
+            rounds = true;
+            break;
         }
         if (d_feat && features.empty()) {
             features.resize(n_units * cm::NF);
@@ -1322,7 +1358,12 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         P.cta_time = d_ct;
         P.shallow = 0;
         P.lists = use_lists ? 1u : 0u;
-        P.root_frames = 0; P.defer_words = 0; P.deferred = nullptr; P.deferred_cap = 0;
+        // Root units claimed once the arena is three-quarters full are handed
+        // back and finished in memory-bounded rounds after this launch.
+        P.root_frames = (uint32_t)frames.size();
+        P.defer_words = std::max<uint64_t>(1, b.arena_words / 4 * 3);
+        P.deferred = d_deferred;
+        P.deferred_cap = n_units;
         CK(cudaEventRecord(ctx->ev[2], ctx->stream));
         if (smem_prefix) k_deep<true><<<grid, block, prefix_bytes, ctx->stream>>>(P);
         else k_deep<false><<<grid, block, 0, ctx->stream>>>(P);
@@ -1382,9 +1423,27 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         }
         arena_words = std::min<uint64_t>(arena_budget, std::max<uint64_t>(arena_words * 4, hs.arena_next * 4));
     }
-    if (rounds) CKR(deep_rounds(ctx, ds, b, frames, d_uid2, d_key2, n_units, base_patterns, P2_total, max_stride,
-                                grid, block, smem_prefix, spin, pat_cap + base_patterns, with_db,
-                                o.arena_bytes ? o.arena_bytes / 8 : 0, learned, use_lists, hs, st));
+    float first_ms = 0.f;
+    bool continued = false;
+    if (!rounds && !frames.empty() && hs.n_deferred) {
+        // The first launch filled its arena and handed root units back: finish
+        // them in rounds over the same buffers.
+        std::vector<unsigned long long> cont(hs.n_deferred);
+        CK(cudaMemcpyAsync(cont.data(), d_deferred, cont.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        first_ms = (float)elapsed_ms(ctx, 2, 3);
+        st.intersections = hs.intersections;
+        st.bytes_alg = hs.bytes_alg;
+        st.work_items = hs.work_items;
+        CKR(deep_rounds(ctx, ds, b, frames, nullptr, nullptr, 0, base_patterns, P2_total, max_stride, grid, block,
+                        smem_prefix, spin, 0, with_db, 0, learned, use_lists, &cont, hs, st));
+        rounds = continued = true;
+        ++st.deep_rounds;  // the first launch
+    } else if (rounds) {
+        CKR(deep_rounds(ctx, ds, b, frames, d_uid2, d_key2, n_units, base_patterns, P2_total, max_stride, grid, block,
+                        smem_prefix, spin, pat_cap + base_patterns, with_db, o.arena_bytes ? o.arena_bytes / 8 : 0,
+                        learned, use_lists, nullptr, hs, st));
+    }
     lap("deep phase");
     if (n_db == 1) {
         // Remember what this database needed so that the next mine() starts there.
@@ -1396,6 +1455,8 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         // then is whether one launch overflowed the whole budget.
         if (!rounds) db0->hint_arena = std::max<uint64_t>(db0->hint_arena, hs.arena_next + hs.arena_next / 4 + 64);
         else if (arena_exceeded) db0->hint_arena = std::max<uint64_t>(db0->hint_arena, arena_budget + 1);
+        else if (continued && !o.arena_bytes)
+            db0->hint_arena = std::max<uint64_t>(db0->hint_arena, std::min<uint64_t>(arena_budget, b.arena_words * 2));
     }
     const uint64_t n = hs.n_patterns;
     std::vector<uint32_t> par(n), item(n), sup(n), pdb;
@@ -1420,7 +1481,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     st.intersections = hs.intersections;
     st.bytes_alg = hs.bytes_alg;
     st.ms_pairs = rows ? elapsed_ms(ctx, 5, 6) : 0.0;
-    st.ms_deep = frames.empty() ? 0.0 : rounds ? ctx->last_deep_ms : elapsed_ms(ctx, 2, 3);
+    st.ms_deep = frames.empty() ? 0.0 : rounds ? first_ms + ctx->last_deep_ms : elapsed_ms(ctx, 2, 3);
     st.ms_total = elapsed_ms(ctx, 0, 4);
     st.deep_gbs = st.ms_deep > 0 ? st.bytes_alg / (st.ms_deep * 1e6) : 0.0;
     st.pair_tops = st.ms_pairs > 0 ? st.pair_ops / (st.ms_pairs * 1e9) : 0.0;

@@ -72,8 +72,9 @@ class cuApriori:
     #: (1-4); 0 leaves each to the library (or to the autotuner's table).
     _DEEP_BLOCK = 0
     _DEEP_CTAS_PER_SM = 0
-    #: Tidset forms of the deep levels: 0 bitsets plus transaction-id lists for
-    #: tidsets held by under 1/32 of the transactions; 1 bitsets only.
+    #: Tidset forms of the deep levels: 0 automatic (bitsets, plus transaction-id
+    #: lists for sparse tidsets of databases too big for the L2); 1 bitsets
+    #: only; 2 lists wherever possible.
     _TIDSETS = 0
 
     def __init__(self, iFile, minSup, sep=None, use_gds="auto", use_gpu_io="auto"):

@@ -80,8 +80,11 @@ typedef struct {
     int32_t  deep_block;           /* deep-level kernel threads per CTA: 128, 256 or 512; 0 = automatic */
     int32_t  deep_ctas_per_sm;     /* resident deep-level CTAs per SM, 1-4 (capped by occupancy); 0 = automatic */
     int32_t  autotune;             /* 1: use the launch shape cpm_autotune found for this tidset length */
-    int32_t  tidsets;              /* 0: bitsets, and transaction-id lists for tidsets held by under 1/32 of
-                                      the transactions (when a bitset fits in shared memory); 1: bitsets only */
+    int32_t  tidsets;              /* deep-level tidset forms.  0: bitsets, plus transaction-id lists for
+                                      tidsets held by under 1/64 of the transactions when a database's
+                                      frequent bitsets exceed half the L2 and one bitset fits in shared
+                                      memory; 1: bitsets only; 2: lists wherever a bitset fits in shared
+                                      memory */
     int32_t  reserved[3];
 } cpm_opts;
 

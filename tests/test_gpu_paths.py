@@ -156,14 +156,14 @@ def test_launch_shapes_and_autotuner_keep_output():
 @pytest.mark.parametrize("name,minsup", [("planted_zipf", 0.005), ("uniform_poisson", 0.01),
                                          ("dense_bernoulli", 0.6)])
 def test_list_and_bitset_tidsets_agree(oracle_lib, name, minsup):
-    """Deep levels with transaction-id lists for sparse tidsets (the default) and
-    with bitsets only give the same patterns, in order, as the oracle."""
+    """Deep levels with transaction-id lists for sparse tidsets and with bitsets
+    only give the same patterns, in order, as the oracle."""
     import cupami_b200
     from cupami_b200 import datasets
 
     csr = getattr(datasets, name)()
     out = []
-    for tidsets in (0, 1):
+    for tidsets in (2, 1):
         m = cupami_b200.cuEclat(csr, minsup)
         m._TIDSETS = tidsets
         m.mine()
@@ -191,12 +191,13 @@ def test_lists_in_memory_bounded_rounds_and_batches(oracle_lib):
     for arena in (64 << 10, 0):
         m = cuEclat(csr, 0.005)
         m._ARENA_BYTES = arena
+        m._TIDSETS = 2
         m.mine()
         assert m.getPatterns() == want
         if arena:
             assert m.getKernelStats()["deep_rounds"] > 1
     csrs = datasets.batched_zipf(limit=12)
-    for tidsets in (0, 1):
+    for tidsets in (2, 1):
         cls = type("E", (cuEclat,), {"_TIDSETS": tidsets})
         for csr, m in zip(csrs, cls.mineBatch(csrs, 0.01)):
             labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, 0.01)
