@@ -45,6 +45,8 @@ WORKLOADS = {
     "dense-bernoulli-64k": ("dense_bernoulli", 0.6, ("eclat",)),
     "dense-fixed-64k": ("dense_fixed_length", 0.6, ("eclat",)),
     "sparse-zipf-1m": ("sparse_zipf", 0.001, ("eclat",)),
+    # the same generator at a quarter of the transactions (profiling-sized)
+    "sparse-zipf-250k": ("sparse_zipf_250k", 0.001, ("eclat",)),
     # 512 independent databases mined in one pass (cuEclat.mineBatch)
     "batched-zipf-512": ("batched_zipf", 0.01, ("eclat-batch",)),
 }
@@ -289,6 +291,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ab", action="store_true", help="skip the learned-vs-plain scheduler comparison")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference-GPU-path leg")
+    ap.add_argument("--arena-mb", type=int, default=0,
+                    help="cap the deep-level arena (memory-bounded rounds past it); 0 = automatic")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup()
@@ -323,6 +327,7 @@ def main():
         o = _native.Opts()
         _native.library().cpm_default_opts(o)
         o.scheduler = _native.CPM_SCHED_LEARNED if sched == "learned" else _native.CPM_SCHED_PLAIN
+        o.arena_bytes = args.arena_mb << 20
         return o
 
     algo_code = {"eclat": (_native.CPM_ECLAT, _native.CPM_ORDER_ECLAT),

@@ -237,6 +237,11 @@ def sparse_zipf(n=1_000_000, n_items=20_000, mean=40, s=1.0, seed=3) -> Transact
     return TransactionCSR(offsets, items, n_items)
 
 
+def sparse_zipf_250k(seed=3) -> TransactionCSR:
+    """``sparse_zipf`` at 250,000 transactions (a profiling-sized case of the same shape)."""
+    return sparse_zipf(n=250_000, seed=seed)
+
+
 def batched_zipf(n_db=512, low=1_000, high=200_000, n_items=200, mean=8, s=1.1,
                  seed=19, limit=None) -> list[TransactionCSR]:
     """``n_db`` independent databases with log-uniform transaction counts.
