@@ -56,7 +56,7 @@ class Opts(ctypes.Structure):
         ("arena_bytes", ctypes.c_uint64), ("spin_limit", ctypes.c_uint64),
         ("collect_trace", ctypes.c_int32), ("deep_block", ctypes.c_int32),
         ("deep_ctas_per_sm", ctypes.c_int32), ("autotune", ctypes.c_int32), ("tidsets", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 3),
+        ("list_div", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -84,7 +84,8 @@ _SIGNATURES = {
     "cpm_db_from_ids_batch": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.POINTER(_P), ctypes.POINTER(_U64),
                                              ctypes.POINTER(_P), ctypes.POINTER(_U64), ctypes.POINTER(_P)]),
     "cpm_autotune": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.POINTER(Opts), ctypes.POINTER(ctypes.c_int32),
-                                    ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)]),
+                                    ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                    ctypes.POINTER(ctypes.c_double)]),
     "cpm_db_info": (ctypes.c_int, [_P, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_uint32),
                                    ctypes.POINTER(_U64)]),
     "cpm_db_labels": (ctypes.c_int, [_P, _P]),
@@ -287,11 +288,12 @@ def autotune(ctx, db, min_sup, opts=None):
     if opts is None:
         opts = Opts()
         library().cpm_default_opts(ctypes.byref(opts))
-    block, ctas, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
+    block, ctas, div, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
     with ctx.lock:
         ctx.check(library().cpm_autotune(ctx.handle, db.handle, int(min_sup), ctypes.byref(opts),
-                                         ctypes.byref(block), ctypes.byref(ctas), ctypes.byref(ms)))
-    return {"block": block.value, "ctas_per_sm": ctas.value, "ms_deep": ms.value}
+                                         ctypes.byref(block), ctypes.byref(ctas), ctypes.byref(div),
+                                         ctypes.byref(ms)))
+    return {"block": block.value, "ctas_per_sm": ctas.value, "list_div": div.value, "ms_deep": ms.value}
 
 
 def mine_batch(ctx, databases, min_sups, opts=None, order=CPM_ORDER_ECLAT):

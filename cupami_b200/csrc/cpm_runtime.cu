@@ -58,6 +58,7 @@ struct cpm_ctx {
     int last_deep_block = 0, last_deep_ctas = 0;  // launch shape of the last deep phase
     size_t l2_bytes = 126ull << 20;               // device L2 size (cpm_init)
     std::map<int, std::pair<int, int>> tune;      // log2(stride) -> (threads per CTA, CTAs per SM), cpm_autotune
+    std::map<int, int> tune_lists;                // log2(stride) -> list divisor (0: bitsets only), cpm_autotune
 };
 
 struct cpm_db {
@@ -741,7 +742,7 @@ static int grow(cpm_ctx *ctx, DeepBuffers &b, uint64_t frames_cap, uint64_t memb
 static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::vector<DFrame> &top_frames,
                            const uint32_t *d_uid, const float *d_key, uint64_t n_units, uint64_t P2_total,
                            uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix, uint64_t spin,
-                           bool keys_in_words, bool lists, const std::vector<unsigned long long> *cont,
+                           bool keys_in_words, uint32_t lists, const std::vector<unsigned long long> *cont,
                            uint64_t arena_words, uint64_t pat_cap, DeepState &hs, cpm_stats &st);
 
 static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::vector<DFrame> &top_frames,
@@ -749,7 +750,7 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
                        uint64_t P2_total, uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix,
                        uint64_t spin,
                        uint64_t pat_need, bool with_db, uint64_t arena_limit_words, bool keys_in_words,
-                       bool lists, const std::vector<unsigned long long> *cont, DeepState &hs, cpm_stats &st) {
+                       uint32_t lists, const std::vector<unsigned long long> *cont, DeepState &hs, cpm_stats &st) {
     const bool dbg = getenv("CPM_DEBUG") != nullptr;
     if (cont) return deep_rounds_run(ctx, ds, b, top_frames, nullptr, nullptr, 0, P2_total, max_stride, grid, block,
                                      smem_prefix, spin, keys_in_words, lists, cont, b.arena_words, b.pat_cap, hs, st);
@@ -798,7 +799,7 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
 static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::vector<DFrame> &top_frames,
                            const uint32_t *d_uid, const float *d_key, uint64_t n_units, uint64_t P2_total,
                            uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix, uint64_t spin,
-                           bool keys_in_words, bool lists, const std::vector<unsigned long long> *cont,
+                           bool keys_in_words, uint32_t lists, const std::vector<unsigned long long> *cont,
                            uint64_t arena_words, uint64_t pat_cap, DeepState &hs, cpm_stats &st) {
     const bool dbg = getenv("CPM_DEBUG") != nullptr;
     const uint64_t queue_cap = b.queue_cap;
@@ -847,7 +848,7 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
     P.pat_parent = b.pat_parent; P.pat_item = b.pat_item; P.pat_sup = b.pat_sup; P.pat_db = b.pat_db;
     P.pat_cap = b.pat_cap;
     P.root_cost = nullptr; P.st = b.st; P.max_stride = max_stride; P.spin_limit = spin; P.cta_time = nullptr;
-    P.lists = lists ? 1u : 0u;
+    P.lists = lists;
     P.root_frames = 0; P.defer_words = 0; P.deferred = nullptr; P.deferred_cap = 0;
     const size_t prefix_bytes = max_stride * 8;
     uint64_t rounds = 0, failed = 0, shallow = 0;
@@ -1071,6 +1072,16 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         use_lists = o.tidsets != 1 && max_stride * 8 <= 200 * 1024 &&
                     (o.tidsets == 2 || biggest > (uint64_t)ctx->l2_bytes / 2);
     }
+    // A tidset becomes a list when its list takes at most 1/list_div of its
+    // bitset (set by the options or the autotuner; 2 by default).
+    uint32_t list_div = o.list_div > 0 ? (uint32_t)o.list_div : 2u;
+    if (o.tidsets == 0 && !o.list_div && o.autotune) {
+        const auto it = ctx->tune_lists.find(63 - __builtin_clzll(std::max<uint64_t>(1, max_stride)));
+        if (it != ctx->tune_lists.end()) {
+            use_lists = it->second > 0 && max_stride * 8 <= 200 * 1024;
+            if (it->second > 0) list_div = (uint32_t)it->second;
+        }
+    }
     // ---- pair Grams ----
     uint64_t rows = 0, c_total = 0;
     std::vector<uint64_t> c_off(n_db, 0);
@@ -1138,7 +1149,8 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         CK(cudaMemcpyAsync(hfreq.data(), freq_all, items_total * 4, cudaMemcpyDeviceToHost, ctx->stream));
         if (use_lists) {
             CKR(ds.alloc(&d_list_words, rows));
-            k_list_plan<<<(unsigned)((rows + 255) / 256), 256, 0, ctx->stream>>>(d_desc, n_db, rows, d_list_words);
+            k_list_plan<<<(unsigned)((rows + 255) / 256), 256, 0, ctx->stream>>>(d_desc, n_db, rows, list_div,
+                                                                               d_list_words);
             CK(cudaGetLastError());
             st.kernel_launches++;
             list_words_h.resize(rows);
@@ -1357,7 +1369,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         }
         P.cta_time = d_ct;
         P.shallow = 0;
-        P.lists = use_lists ? 1u : 0u;
+        P.lists = use_lists ? list_div : 0u;
         // Root units claimed once the arena is three-quarters full are handed
         // back and finished in memory-bounded rounds after this launch.
         P.root_frames = (uint32_t)frames.size();
@@ -1436,13 +1448,13 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         st.bytes_alg = hs.bytes_alg;
         st.work_items = hs.work_items;
         CKR(deep_rounds(ctx, ds, b, frames, nullptr, nullptr, 0, base_patterns, P2_total, max_stride, grid, block,
-                        smem_prefix, spin, 0, with_db, 0, learned, use_lists, &cont, hs, st));
+                        smem_prefix, spin, 0, with_db, 0, learned, use_lists ? list_div : 0u, &cont, hs, st));
         rounds = continued = true;
         ++st.deep_rounds;  // the first launch
     } else if (rounds) {
         CKR(deep_rounds(ctx, ds, b, frames, d_uid2, d_key2, n_units, base_patterns, P2_total, max_stride, grid, block,
                         smem_prefix, spin, pat_cap + base_patterns, with_db, o.arena_bytes ? o.arena_bytes / 8 : 0,
-                        learned, use_lists, nullptr, hs, st));
+                        learned, use_lists ? list_div : 0u, nullptr, hs, st));
     }
     lap("deep phase");
     if (n_db == 1) {
@@ -1780,7 +1792,7 @@ extern "C" int cpm_mine_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const i
 }
 
 extern "C" int cpm_autotune(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, const cpm_opts *opts, int32_t *block,
-                            int32_t *ctas_per_sm, double *ms_deep) {
+                            int32_t *ctas_per_sm, int32_t *list_div, double *ms_deep) {
     if (!ctx || !db) return CPM_EINVAL;
     cpm_opts o;
     if (opts) o = *opts;
@@ -1812,9 +1824,40 @@ extern "C" int cpm_autotune(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, const cpm
             if (used < c) break;  // occupancy allows no more CTAs of this size
         }
     }
-    ctx->tune[63 - __builtin_clzll(std::max<uint64_t>(1, db->stride))] = {best_block, best_ctas};
+    const int bucket = 63 - __builtin_clzll(std::max<uint64_t>(1, db->stride));
+    ctx->tune[bucket] = {best_block, best_ctas};
+    // Tidset forms at that shape: bitsets only, or lists below 1/1 .. 1/8 of the bitset.
+    if (db->stride * 8 <= 200 * 1024) {
+        o.deep_block = best_block;
+        o.deep_ctas_per_sm = best_ctas;
+        int best_div = -1;
+        double best_l = 1e300;
+        static const int divs[5] = {0, 1, 2, 4, 8};
+        for (int di = 0; di < 5; ++di) {
+            o.tidsets = divs[di] ? 2 : 1;
+            o.list_div = divs[di];
+            double t = 1e300;
+            for (int rep = 0; rep < 2; ++rep) {
+                cpm_result *r = nullptr;
+                const int rc = cpm_mine(ctx, db, min_sup, CPM_ECLAT, &o, &r);
+                if (rc != CPM_OK) return rc;
+                t = std::min(t, r->stats.ms_deep);
+                cpm_result_free(r);
+            }
+            if (t < best_l) {
+                best_l = t;
+                best_div = divs[di];
+            }
+        }
+        ctx->tune_lists[bucket] = best_div;
+        best = std::min(best, best_l);
+    }
     if (block) *block = best_block;
     if (ctas_per_sm) *ctas_per_sm = best_ctas;
+    if (list_div) {
+        const auto it = ctx->tune_lists.find(bucket);
+        *list_div = it == ctx->tune_lists.end() ? 0 : it->second;
+    }
     if (ms_deep) *ms_deep = best;
     return CPM_OK;
 }

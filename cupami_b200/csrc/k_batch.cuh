@@ -170,14 +170,15 @@ __global__ void k_emit_b(const DbDesc *__restrict__ d, uint32_t n_db, uint64_t n
 // Transaction-id lists of sparse frequent items (the list form of k_deep.cuh:
 // 16-byte header {count, 0, 0, 0}, ascending ids, zero padding to 16 bytes).
 // words[r] = 64-bit words of row r's list, or 0 when the item stays dense
-// (list not at most half the bitset).
-__global__ void k_list_plan(const DbDesc *__restrict__ d, uint32_t n_db, uint64_t n_rows, uint64_t *__restrict__ words) {
+// (list above 1/list_div of the bitset).
+__global__ void k_list_plan(const DbDesc *__restrict__ d, uint32_t n_db, uint64_t n_rows, uint32_t list_div,
+                            uint64_t *__restrict__ words) {
     const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_rows) return;
     const DbDesc &D = d[db_of_row(d, n_db, r)];
     const uint32_t sup = D.support[D.freq[r - D.row_base]];
     const uint64_t lw = ((uint64_t)sup + 7) / 4 * 2;
-    words[r] = lw * 2 <= D.stride ? lw : 0;
+    words[r] = lw * list_div <= D.stride ? lw : 0;
 }
 
 // One warp per frequent row with a list: extracts the row's set bits in order.

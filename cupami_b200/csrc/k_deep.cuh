@@ -91,7 +91,7 @@ struct DeepParams {
     unsigned long long spin_limit;
     unsigned long long *cta_time;   // optional [2 * grid]: busy ns, exit time (globaltimer)
     uint32_t shallow;               // 1: child frames are recorded, not queued
-    uint32_t lists;                 // 1: list-form tidsets allowed (needs SMEM_PREFIX)
+    uint32_t lists;                 // list-form threshold divisor (0: bitsets only; needs SMEM_PREFIX)
     // Memory-bounded rounds: a unit of a frame below root_frames (a root
     // unit) claimed while arena_next >= defer_words is not run but handed
     // back in deferred[] for a later round (defer_words 0: never).
@@ -101,9 +101,10 @@ struct DeepParams {
     uint64_t deferred_cap;
 };
 
-// Child tidset form: a list when it takes at most half the dense words.
+// Child tidset form: a list when it takes at most 1/P.lists of the dense
+// words (P.lists = 0: bitsets only).
 __device__ __forceinline__ bool as_list(const DeepParams &P, uint64_t n, uint32_t stride) {
-    return P.lists && list_words(n) * 2 <= stride;
+    return P.lists && list_words(n) * P.lists <= stride;
 }
 
 __device__ __forceinline__ unsigned long long ld_raw_ptr(const uint64_t *const *p) {

@@ -273,7 +273,8 @@ class cuApriori:
     def autotune(self):
         """Time the deep-level launch shapes on this database and keep the fastest
         for databases with tidsets of this length (later mine() calls in this
-        process use it).  Returns {"block", "ctas_per_sm", "ms_deep"}."""
+        process use it), and the tidset form at that shape (``list_div`` 0:
+        bitsets only).  Returns {"block", "ctas_per_sm", "list_div", "ms_deep"}."""
         ctx = self._getCudaModule()
         db, _ = self._deviceDatabase(ctx)
         try:

@@ -85,7 +85,9 @@ typedef struct {
                                       frequent bitsets exceed half the L2 and one bitset fits in shared
                                       memory; 1: bitsets only; 2: lists wherever a bitset fits in shared
                                       memory */
-    int32_t  reserved[3];
+    int32_t  list_div;             /* a tidset is stored as a list when its list takes at most 1/list_div
+                                      of its bitset; 0 = the autotuner's choice, else 2 */
+    int32_t  reserved[2];
 } cpm_opts;
 
 typedef struct {
@@ -136,16 +138,18 @@ int cpm_db_from_ids_batch(cpm_ctx *ctx, uint32_t n_db, const uint64_t *const *of
                           const uint64_t *n_rows, const uint32_t *const *ids, const uint64_t *nnz,
                           cpm_db **out);
 
-/* Autotuner of the deep-level launch shape.  Mines db (Eclat) once per
- * shape -- threads per CTA in {128, 256, 512} x resident CTAs per SM in 1..4,
- * as far as occupancy allows -- keeps the best of two deep-phase times each,
- * and records the fastest shape in the context for tidsets of this length
- * (power-of-two bucket of the row stride); mines whose opts set autotune = 1
- * use it.  The shape never changes the output.  No reference counterpart: the
+/* Autotuner of the deep level.  Mines db (Eclat) once per launch shape --
+ * threads per CTA in {128, 256, 512} x resident CTAs per SM in 1..4, as far as
+ * occupancy allows -- then, at the fastest shape, once per tidset form
+ * (bitsets only, or lists at divisors 1, 2, 4, 8), keeping the best of two
+ * deep-phase times each, and records the fastest shape and form in the
+ * context for tidsets of this length (power-of-two bucket of the row stride);
+ * mines whose opts set autotune = 1 (and leave tidsets and list_div at 0) use
+ * them.  Neither changes the output.  No reference counterpart: the
  * reference launches one 256-thread block per candidate
  * (cupami/frequentPattern/_bitsets.py:103-125). */
 int cpm_autotune(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, const cpm_opts *opts,
-                 int32_t *block, int32_t *ctas_per_sm, double *ms_deep);
+                 int32_t *block, int32_t *ctas_per_sm, int32_t *list_div, double *ms_deep);
 
 int  cpm_db_info(const cpm_db *db, uint64_t *n_transactions, uint32_t *n_items,
                  uint64_t *words);

@@ -144,6 +144,7 @@ def test_launch_shapes_and_autotuner_keep_output():
             assert list(m.getPatterns().items()) == want, (block, ctas)
     tuned = cupami_b200.cuEclat(csr, 0.6).autotune()
     assert tuned["block"] in (128, 256, 512) and 1 <= tuned["ctas_per_sm"] <= 4 and tuned["ms_deep"] > 0
+    assert tuned["list_div"] in (0, 1, 2, 4, 8)
     m = cupami_b200.cuEclat(csr, 0.6)
     m.mine()
     assert list(m.getPatterns().items()) == want
