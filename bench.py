@@ -141,6 +141,17 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def deep_traffic(workload, tidsets, arena_mb):
+    """DRAM bytes of one k_deep launch of this workload, from a committed ncu capture (None if none)."""
+    p = ROOT / "profiles" / "k_deep_traffic.json"
+    if not p.exists() or arena_mb:
+        return None
+    d = json.loads(p.read_text()).get(workload)
+    if not d or d.get("tidsets", 0) != tidsets:
+        return None
+    return d["dram_bytes_per_launch"]
+
+
 def flush_l2(buf):
     buf.add_(1)
 
@@ -292,7 +303,9 @@ def main():
     ap.add_argument("--no-ab", action="store_true", help="skip the learned-vs-plain scheduler comparison")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference-GPU-path leg")
     ap.add_argument("--arena-mb", type=int, default=0,
-                    help="cap the deep-level arena (memory-bounded rounds past it); 0 = automatic")
+                    help="deep-level arena size (memory-bounded rounds past it); 0 = automatic")
+    ap.add_argument("--tidsets", type=int, default=0, choices=[0, 1, 2],
+                    help="deep-level tidset forms: 0 automatic, 1 bitsets only, 2 lists wherever possible")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup()
@@ -328,6 +341,7 @@ def main():
         _native.library().cpm_default_opts(o)
         o.scheduler = _native.CPM_SCHED_LEARNED if sched == "learned" else _native.CPM_SCHED_PLAIN
         o.arena_bytes = args.arena_mb << 20
+        o.tidsets = args.tidsets
         return o
 
     algo_code = {"eclat": (_native.CPM_ECLAT, _native.CPM_ORDER_ECLAT),
@@ -427,8 +441,11 @@ def main():
         deep_ms = statistics.mean(sum(s["ms_deep"] for s in st) for st in eclat_stats)
         deep_bytes = statistics.mean(sum(s["bytes_alg"] for s in st) for st in eclat_stats)
         achieved = deep_bytes / (deep_ms * 1e-3) / 1e9 if deep_ms else 0.0
+        traffic = deep_traffic(args.workload, args.tidsets, args.arena_mb)
         roof = {"kernel": "k_deep (deep-level AND+popcount, persistent)", "bound": "hbm", "achieved": achieved,
-                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None, "peak_source": src,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_source": src,
+                "traffic_source": "profiles/k_deep_traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                  "of one launch)" if traffic is not None else None,
                 "ms_per_launch": deep_ms, "alg_bytes_per_launch": deep_bytes,
                 "alg_bytes": "sum over units of 8*W*(1 + siblings + children written)"}
     pair_ms = statistics.mean(sum(st["ms_pairs"] for _, st, _ in out) for out in per_kernel)

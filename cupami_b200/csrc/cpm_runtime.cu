@@ -323,7 +323,8 @@ extern "C" int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n
     std::vector<uint64_t> off;
     CKR(compact_offsets(ctx, offsets, n_rows, nnz, off));
     uint32_t max_id = 0;
-    for (uint64_t k = 0; k < nnz; ++k) max_id = std::max(max_id, ids[k]);
+#pragma omp parallel for reduction(max : max_id) schedule(static) if (nnz > (1u << 18))
+    for (int64_t k = 0; k < (int64_t)nnz; ++k) max_id = std::max(max_id, ids[k]);
     DevScope tmp(ctx);
     uint64_t *d_off = nullptr;
     uint32_t *d_ids = nullptr, *d_lut = nullptr, *d_present = nullptr;
@@ -1468,7 +1469,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         if (!rounds) db0->hint_arena = std::max<uint64_t>(db0->hint_arena, hs.arena_next + hs.arena_next / 4 + 64);
         else if (arena_exceeded) db0->hint_arena = std::max<uint64_t>(db0->hint_arena, arena_budget + 1);
         else if (continued && !o.arena_bytes)
-            db0->hint_arena = std::max<uint64_t>(db0->hint_arena, std::min<uint64_t>(arena_budget, b.arena_words * 2));
+            db0->hint_arena = std::max<uint64_t>(db0->hint_arena, arena_budget);  // did not fit: take the budget next time
     }
     const uint64_t n = hs.n_patterns;
     std::vector<uint32_t> par(n), item(n), sup(n), pdb;
@@ -1889,53 +1890,44 @@ extern "C" int cpm_result_tree(const cpm_result *res, int64_t *parent, uint32_t 
     return CPM_OK;
 }
 
+// Patterns of a result in the requested order.  A pattern is its parent's
+// items plus its own.  The device builds a prefix tree (every pattern extends
+// its parent by a larger item), so both insertion orders are traversals of
+// that tree; any other tree is ordered by comparing item lists.
 extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offsets, uint32_t *items,
                                uint64_t *supports) {
     if (!res || !offsets || !supports) return CPM_EINVAL;
     if (order != CPM_ORDER_ECLAT && order != CPM_ORDER_APRIORI && order != CPM_ORDER_NONE) return CPM_EINVAL;
     const uint64_t n = res->parent.size();
-    // Patterns in device order, items sorted ascending within each.
+    const uint32_t *par = res->parent.data(), *itm = res->item.data();
     std::vector<uint32_t> depth(n);
-    std::vector<uint64_t> start(n + 1, 0);
     for (uint64_t k = 0; k < n; ++k) {
-        const uint32_t p = res->parent[k];
+        const uint32_t p = par[k];
         if (p != 0xffffffffu && p >= k) return CPM_EINTERNAL;
         depth[k] = p == 0xffffffffu ? 1 : depth[p] + 1;
-        start[k + 1] = start[k] + depth[k];
     }
-    // Parents precede children, so a parent's list is already sorted when a
-    // child copies it; the child's own item is then moved into place.
-    std::vector<uint32_t> flat(start[n]);
-    for (uint64_t k = 0; k < n; ++k) {
-        uint32_t *a = flat.data() + start[k];
-        const uint32_t p = res->parent[k];
-        const uint32_t d = depth[k];
-        if (p != 0xffffffffu) memcpy(a, flat.data() + start[p], (d - 1) * 4);
-        a[d - 1] = res->item[k];
-        for (uint32_t i = d - 1; i > 0 && a[i] < a[i - 1]; --i) std::swap(a[i], a[i - 1]);
-    }
-    std::vector<uint64_t> idx(n);
-    std::iota(idx.begin(), idx.end(), 0ull);
-    auto pat = [&](uint64_t k) { return flat.data() + start[k]; };
-    // A tree whose every pattern extends its parent by a larger item is the
-    // prefix tree of the patterns (the device builds it so); then both
-    // insertion orders are plain traversals.  Otherwise sort with the keys.
     bool prefix_tree = true;
     for (uint64_t k = 0; k < n && prefix_tree; ++k)
-        if (res->parent[k] != 0xffffffffu && res->item[k] <= res->item[res->parent[k]]) prefix_tree = false;
+        if (par[k] != 0xffffffffu && itm[k] <= itm[par[k]]) prefix_tree = false;
+    std::vector<uint64_t> idx(n);
+    std::iota(idx.begin(), idx.end(), 0ull);
+    std::vector<uint64_t> start;  // item lists in device order (only for non-prefix trees)
+    std::vector<uint32_t> flat;
+    auto pat = [&](uint64_t k) { return flat.data() + start[k]; };
     if (prefix_tree && order != CPM_ORDER_NONE) {
-        // children lists, each sorted by item
+        // children lists (counting sort by parent), each sorted by item
         std::vector<uint64_t> coff(n + 2, 0), roots;
         for (uint64_t k = 0; k < n; ++k)
-            if (res->parent[k] == 0xffffffffu) roots.push_back(k);
-            else coff[res->parent[k] + 1]++;
+            if (par[k] == 0xffffffffu) roots.push_back(k);
+            else coff[par[k] + 1]++;
         for (uint64_t k = 0; k < n; ++k) coff[k + 1] += coff[k];
         std::vector<uint64_t> kids(coff[n]), fill(coff.begin(), coff.begin() + n);
         for (uint64_t k = 0; k < n; ++k)
-            if (res->parent[k] != 0xffffffffu) kids[fill[res->parent[k]]++] = k;
-        auto by_item = [&](uint64_t a, uint64_t b) { return res->item[a] < res->item[b]; };
+            if (par[k] != 0xffffffffu) kids[fill[par[k]]++] = k;
+        auto by_item = [&](uint64_t a, uint64_t b) { return itm[a] < itm[b]; };
         std::sort(roots.begin(), roots.end(), by_item);
-        for (uint64_t k = 0; k < n; ++k)
+#pragma omp parallel for schedule(dynamic, 4096)
+        for (int64_t k = 0; k < (int64_t)n; ++k)
             if (coff[k + 1] - coff[k] > 1) std::sort(kids.begin() + coff[k], kids.begin() + coff[k + 1], by_item);
         uint64_t w = 0;
         if (order == CPM_ORDER_APRIORI) {
@@ -1974,36 +1966,58 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
             }
         }
         if (w != n) return CPM_EINTERNAL;
-    } else if (order == CPM_ORDER_APRIORI) {
-        std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
-            if (depth[a] != depth[b]) return depth[a] < depth[b];
-            return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
-        });
-    } else if (order == CPM_ORDER_ECLAT) {
-        // cuEclat inserts singletons, then pairs, then every deeper pattern in
-        // the order of its class search: key (x1..x_{k-1}, -1, x_k).
-        std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
-            const uint32_t ga = std::min<uint32_t>(depth[a], 3), gb = std::min<uint32_t>(depth[b], 3);
-            if (ga != gb) return ga < gb;
-            if (ga < 3) return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
-            const uint32_t *x = pat(a), *y = pat(b);
-            const int64_t la = depth[a] + 1, lb = depth[b] + 1;
-            for (int64_t i = 0; i < std::min(la, lb); ++i) {
-                const int64_t u = i < la - 2 ? (int64_t)x[i] : (i == la - 2 ? (int64_t)-1 : (int64_t)x[la - 2]);
-                const int64_t v = i < lb - 2 ? (int64_t)y[i] : (i == lb - 2 ? (int64_t)-1 : (int64_t)y[lb - 2]);
-                if (u != v) return u < v;
-            }
-            return la < lb;
-        });
+    } else if (order != CPM_ORDER_NONE || !prefix_tree) {
+        // Item lists, sorted ascending within each pattern (parents precede
+        // children, so a parent's list is sorted when a child copies it).
+        start.assign(n + 1, 0);
+        for (uint64_t k = 0; k < n; ++k) start[k + 1] = start[k] + depth[k];
+        flat.resize(start[n]);
+        for (uint64_t k = 0; k < n; ++k) {
+            uint32_t *a = flat.data() + start[k];
+            const uint32_t p = par[k];
+            const uint32_t d = depth[k];
+            if (p != 0xffffffffu) memcpy(a, flat.data() + start[p], (d - 1) * 4);
+            a[d - 1] = itm[k];
+            for (uint32_t i = d - 1; i > 0 && a[i] < a[i - 1]; --i) std::swap(a[i], a[i - 1]);
+        }
+        if (order == CPM_ORDER_APRIORI) {
+            std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+                if (depth[a] != depth[b]) return depth[a] < depth[b];
+                return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
+            });
+        } else if (order == CPM_ORDER_ECLAT) {
+            // cuEclat inserts singletons, then pairs, then every deeper pattern in
+            // the order of its class search: key (x1..x_{k-1}, -1, x_k).
+            std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+                const uint32_t ga = std::min<uint32_t>(depth[a], 3), gb = std::min<uint32_t>(depth[b], 3);
+                if (ga != gb) return ga < gb;
+                if (ga < 3) return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
+                const uint32_t *x = pat(a), *y = pat(b);
+                const int64_t la = depth[a] + 1, lb = depth[b] + 1;
+                for (int64_t i = 0; i < std::min(la, lb); ++i) {
+                    const int64_t u = i < la - 2 ? (int64_t)x[i] : (i == la - 2 ? (int64_t)-1 : (int64_t)x[la - 2]);
+                    const int64_t v = i < lb - 2 ? (int64_t)y[i] : (i == lb - 2 ? (int64_t)-1 : (int64_t)y[lb - 2]);
+                    if (u != v) return u < v;
+                }
+                return la < lb;
+            });
+        }
     }
-    uint64_t pos = 0;
     offsets[0] = 0;
-    for (uint64_t r = 0; r < n; ++r) {
+    for (uint64_t r = 0; r < n; ++r) offsets[r + 1] = offsets[r] + depth[idx[r]];
+#pragma omp parallel for schedule(static, 65536)
+    for (int64_t r = 0; r < (int64_t)n; ++r) {
         const uint64_t k = idx[r];
-        if (items) memcpy(items + pos, pat(k), depth[k] * 4);
-        pos += depth[k];
-        offsets[r + 1] = pos;
         supports[r] = res->support[k];
+        if (!items) continue;
+        uint32_t *a = items + offsets[r];
+        if (!flat.empty()) {
+            memcpy(a, pat(k), depth[k] * 4);
+        } else {
+            // prefix tree: walk up the parents, last item first (already ascending)
+            uint64_t v = k;
+            for (uint32_t i = depth[k]; i-- > 0; v = par[v]) a[i] = itm[v];
+        }
     }
     return CPM_OK;
 }
