@@ -1245,9 +1245,9 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     const uint64_t spin = o.spin_limit ? o.spin_limit : (1ull << 26);
     const size_t prefix_bytes = max_stride * 8;
     const bool smem_prefix = prefix_bytes <= 200 * 1024;
-    // Long tidsets leave room for one CTA per SM: give it 16 warps so that
-    // enough loads stay in flight; short ones run up to four 8-warp CTAs.
-    unsigned block = max_stride >= 2048 ? 512 : 256;
+    // Long tidsets leave room for one CTA per SM: give it 16 or 32 warps so
+    // that enough loads stay in flight; short ones run up to four 8-warp CTAs.
+    unsigned block = max_stride >= 8192 ? 1024 : max_stride >= 2048 ? 512 : 256;
     int want_ctas = 4;
     if (o.autotune) {
         const auto it = ctx->tune.find(63 - __builtin_clzll(std::max<uint64_t>(1, max_stride)));
@@ -1257,8 +1257,8 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         }
     }
     if (o.deep_block) {
-        if (o.deep_block != 128 && o.deep_block != 256 && o.deep_block != 512)
-            return set_err(ctx, CPM_EINVAL, "deep_block must be 128, 256 or 512 (got %d)", o.deep_block);
+        if (o.deep_block != 128 && o.deep_block != 256 && o.deep_block != 512 && o.deep_block != 1024)
+            return set_err(ctx, CPM_EINVAL, "deep_block must be 128, 256, 512 or 1024 (got %d)", o.deep_block);
         block = (unsigned)o.deep_block;
     }
     if (o.deep_ctas_per_sm) {
@@ -1800,10 +1800,10 @@ extern "C" int cpm_autotune(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, const cpm
     else cpm_default_opts(&o);
     o.autotune = 0;
     o.collect_trace = 0;
-    static const int blocks[3] = {128, 256, 512};
+    static const int blocks[4] = {128, 256, 512, 1024};
     double best = 1e300;
     int best_block = 0, best_ctas = 0;
-    for (int bi = 0; bi < 3; ++bi) {
+    for (int bi = 0; bi < 4; ++bi) {
         for (int c = 1; c <= 4; ++c) {
             o.deep_block = blocks[bi];
             o.deep_ctas_per_sm = c;

@@ -171,8 +171,77 @@ __device__ __forceinline__ const ulonglong2 *ld_ptr(const uint64_t *const *p) {
     return reinterpret_cast<const ulonglong2 *>(__ldcg(reinterpret_cast<const unsigned long long *>(p)));
 }
 
+// This lane's share of |prefix & sibling| over part `part` of `parts` equal
+// slices of the sibling (dense words or list ids); *bytes gets the sibling's
+// size in its own form.  Eight 16-byte loads in flight per lane.
 template <bool SMEM_PREFIX>
-__global__ void __launch_bounds__(512) k_deep(DeepParams P) {
+__device__ __forceinline__ uint32_t sibling_count(unsigned long long sraw, uint32_t part, uint32_t parts, uint64_t n2,
+                                                  const ulonglong2 *s_prefix, const uint32_t *s_p32,
+                                                  const ulonglong2 *pb, const ulonglong2 *mk, unsigned lane,
+                                                  uint64_t *bytes) {
+    uint32_t s = 0;
+    if (SMEM_PREFIX && (sraw & 1ull)) {
+        // List sibling: test its ids against the prefix bitmap.
+        const uint32_t *L = reinterpret_cast<const uint32_t *>(sraw & ~1ull);
+        const uint32_t n = __ldcg(L);
+        const uint4 *T = reinterpret_cast<const uint4 *>(L + 4);
+        const uint32_t nv = (n + 3) / 4, nfull = n / 4;
+        const uint32_t lo = (uint32_t)((uint64_t)nv * part / parts), hi = (uint32_t)((uint64_t)nv * (part + 1) / parts);
+        const uint32_t hi_full = min(hi, nfull);
+        uint32_t w = lo + lane;
+        for (; w + 224 < hi_full; w += 256) {  // eight complete groups of four ids
+            uint4 t[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) t[u] = __ldcg(T + w + 32 * u);
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                s += bit_of(s_p32, t[u].x) + bit_of(s_p32, t[u].y) + bit_of(s_p32, t[u].z) + bit_of(s_p32, t[u].w);
+        }
+        for (; w < hi; w += 32) {
+            const uint4 t = __ldcg(T + w);
+            const uint32_t i0 = 4 * w;
+            s += bit_of(s_p32, t.x);
+            if (i0 + 1 < n) s += bit_of(s_p32, t.y);
+            if (i0 + 2 < n) s += bit_of(s_p32, t.z);
+            if (i0 + 3 < n) s += bit_of(s_p32, t.w);
+        }
+        *bytes = 8ull * list_words(n);
+        return s;
+    }
+    const ulonglong2 *sb = reinterpret_cast<const ulonglong2 *>(sraw);
+    const uint64_t lo = n2 * part / parts, hi = n2 * (part + 1) / parts;
+    uint64_t v = lo + lane;
+    for (; v + 224 < hi; v += 256) {
+        ulonglong2 x[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) x[u] = ld_cg(sb + v + 32 * u);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (SMEM_PREFIX) {
+                x[u] = and2(x[u], s_prefix[v + 32 * u]);
+            } else {
+                x[u] = and2(x[u], ld_cg(pb + v + 32 * u));
+                if (mk) x[u] = and2(x[u], ld_cg(mk + v + 32 * u));
+            }
+            s += popc2(x[u]);
+        }
+    }
+    for (; v < hi; v += 32) {
+        ulonglong2 x = ld_cg(sb + v);
+        if (SMEM_PREFIX) {
+            x = and2(x, s_prefix[v]);
+        } else {
+            x = and2(x, ld_cg(pb + v));
+            if (mk) x = and2(x, ld_cg(mk + v));
+        }
+        s += popc2(x);
+    }
+    *bytes = 16ull * n2;
+    return s;
+}
+
+template <bool SMEM_PREFIX>
+__global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     extern __shared__ ulonglong2 s_prefix[];
     __shared__ unsigned long long s_item;
     __shared__ int s_stop, s_ok, s_grant, s_skip;
@@ -180,8 +249,9 @@ __global__ void __launch_bounds__(512) k_deep(DeepParams P) {
     __shared__ unsigned long long s_mem_base, s_arena_base, s_fid, s_qbase;
     __shared__ uint32_t s_wtot[32];
     __shared__ uint64_t s_w64[32];
-    __shared__ uint64_t s_off[512];      // child offsets of one chunk of survivors
+    __shared__ uint64_t s_off[1024];     // child offsets of one chunk of survivors
     __shared__ unsigned long long s_bytes;
+    __shared__ uint32_t s_part[32];      // per-sibling sums when siblings are split over warps
     uint32_t *const s_p32 = reinterpret_cast<uint32_t *>(s_prefix);
 
     const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -257,92 +327,63 @@ __global__ void __launch_bounds__(512) k_deep(DeepParams P) {
         const bool ok = s_ok != 0;
         const uint32_t parent_pat = __ldcg(P.mem_pat + mem_off + p);
         // ---- pass 1: supports of every later member ----
-        for (uint32_t q = wid; ok && q < cnt; q += nw) {
-            const uint64_t mi = mem_off + p + 1 + q;
-            const unsigned long long sraw = ld_raw_ptr(P.mem_bits + mi);
-            const ulonglong2 *sb = reinterpret_cast<const ulonglong2 *>(sraw);
-            const uint32_t sib_item = __ldcg(P.mem_item + mi);
-            uint32_t s = 0;
-            uint64_t v = lane;
-            if (SMEM_PREFIX && (sraw & 1ull)) {
-                // List sibling: test its ids against the prefix bitmap (four
-                // 16-byte loads of ids in flight per lane).
-                const uint32_t *L = reinterpret_cast<const uint32_t *>(sraw & ~1ull);
-                const uint32_t n = __ldcg(L);
-                const uint4 *T = reinterpret_cast<const uint4 *>(L + 4);
-                const uint32_t nv = (n + 3) / 4, nfull = n / 4;
-                uint32_t w = lane;
-                for (; w + 96 < nfull; w += 128) {  // four complete groups of four ids
-                    uint4 t[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) t[u] = __ldcg(T + w + 32 * u);
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                        s += bit_of(s_p32, t[u].x) + bit_of(s_p32, t[u].y) + bit_of(s_p32, t[u].z) +
-                             bit_of(s_p32, t[u].w);
-                }
-                for (; w < nv; w += 32) {
-                    const uint4 t = __ldcg(T + w);
-                    const uint32_t i0 = 4 * w;
-                    s += bit_of(s_p32, t.x);
-                    if (i0 + 1 < n) s += bit_of(s_p32, t.y);
-                    if (i0 + 2 < n) s += bit_of(s_p32, t.z);
-                    if (i0 + 3 < n) s += bit_of(s_p32, t.w);
-                }
-                if (lane == 0) atomicAdd(&s_bytes, 8ull * list_words(n));
-                v = n2;  // the dense loops below do nothing
-            } else if (lane == 0) {
-                atomicAdd(&s_bytes, 8ull * stride);
-            }
-            // Eight 16-byte loads in flight per lane (4 KB per warp).
-            for (; v + 224 < n2; v += 256) {
-                ulonglong2 x[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) x[u] = ld_cg(sb + v + 32 * u);
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    if (SMEM_PREFIX) {
-                        x[u] = and2(x[u], s_prefix[v + 32 * u]);
-                    } else {
-                        x[u] = and2(x[u], ld_cg(pb + v + 32 * u));
-                        if (mk) x[u] = and2(x[u], ld_cg(mk + v + 32 * u));
-                    }
-                    s += popc2(x[u]);
-                }
-            }
-            for (; v < n2; v += 32) {
-                ulonglong2 x = ld_cg(sb + v);
-                if (SMEM_PREFIX) {
-                    x = and2(x, s_prefix[v]);
+        // Entry q of the unit's member block: the survivor (pattern, item,
+        // sibling tidset until pass 2) or a hole.
+        auto emit = [&](uint32_t q, uint32_t s, uint32_t sib_item, unsigned long long sraw) {
+            const uint64_t m_out = s_mem_base + q;
+            uint32_t pid32 = NO_PATTERN;
+            if ((long long)s >= minsup) {
+                const unsigned long long pid = atomicAdd(&st->n_patterns, 1ull);
+                if (pid >= P.pat_cap) {
+                    deep_fail(st, DEEP_ERR_PATTERNS);
                 } else {
-                    x = and2(x, ld_cg(pb + v));
-                    if (mk) x = and2(x, ld_cg(mk + v));
+                    P.pat_parent[pid] = parent_pat;
+                    P.pat_item[pid] = sib_item;
+                    P.pat_sup[pid] = s;
+                    if (P.pat_db) P.pat_db[pid] = db;
+                    pid32 = (uint32_t)pid;
                 }
-                s += popc2(x);
             }
-            s = warp_sum_u32(s);
-            if (lane == 0) {
-                // Entry q of the unit's member block: the survivor (pattern,
-                // item, sibling tidset until pass 2) or a hole.
-                const uint64_t m_out = s_mem_base + q;
-                uint32_t pid32 = NO_PATTERN;
-                if ((long long)s >= minsup) {
-                    const unsigned long long pid = atomicAdd(&st->n_patterns, 1ull);
-                    if (pid >= P.pat_cap) {
-                        deep_fail(st, DEEP_ERR_PATTERNS);
-                    } else {
-                        P.pat_parent[pid] = parent_pat;
-                        P.pat_item[pid] = sib_item;
-                        P.pat_sup[pid] = s;
-                        if (P.pat_db) P.pat_db[pid] = db;
-                        pid32 = (uint32_t)pid;
-                    }
+            if (m_out < P.members_cap) {
+                P.mem_pat[m_out] = pid32;
+                P.mem_item[m_out] = sib_item;
+                P.mem_bits[m_out] = reinterpret_cast<const uint64_t *>(sraw);
+            }
+        };
+        // Fewer siblings than warps: split every sibling into equal slices
+        // (at least 4 KB of bitset each) so that every warp has work.
+        const uint32_t parts = (cnt && cnt < nw) ? max(1u, min(nw / cnt, (uint32_t)(n2 >> 8))) : 1u;
+        if (parts == 1) {
+            for (uint32_t q = wid; ok && q < cnt; q += nw) {
+                const uint64_t mi = mem_off + p + 1 + q;
+                const unsigned long long sraw = ld_raw_ptr(P.mem_bits + mi);
+                const uint32_t sib_item = __ldcg(P.mem_item + mi);
+                uint64_t b = 0;
+                uint32_t s = sibling_count<SMEM_PREFIX>(sraw, 0, 1, n2, s_prefix, s_p32, pb, mk, lane, &b);
+                s = warp_sum_u32(s);
+                if (lane == 0) {
+                    atomicAdd(&s_bytes, (unsigned long long)b);
+                    emit(q, s, sib_item, sraw);
                 }
-                if (m_out < P.members_cap) {
-                    P.mem_pat[m_out] = pid32;
-                    P.mem_item[m_out] = sib_item;
-                    P.mem_bits[m_out] = reinterpret_cast<const uint64_t *>(sb);
+            }
+        } else {
+            if (threadIdx.x < 32) s_part[threadIdx.x] = 0;
+            __syncthreads();
+            for (uint32_t it = wid; ok && it < cnt * parts; it += nw) {
+                const uint32_t q = it / parts, j = it - q * parts;
+                const unsigned long long sraw = ld_raw_ptr(P.mem_bits + mem_off + p + 1 + q);
+                uint64_t b = 0;
+                uint32_t s = sibling_count<SMEM_PREFIX>(sraw, j, parts, n2, s_prefix, s_p32, pb, mk, lane, &b);
+                s = warp_sum_u32(s);
+                if (lane == 0) {
+                    atomicAdd(&s_part[q], s);
+                    if (j == 0) atomicAdd(&s_bytes, (unsigned long long)b);
                 }
+            }
+            __syncthreads();
+            if (ok && threadIdx.x < cnt) {
+                const uint64_t mi = mem_off + p + 1 + threadIdx.x;
+                emit(threadIdx.x, s_part[threadIdx.x], __ldcg(P.mem_item + mi), ld_raw_ptr(P.mem_bits + mi));
             }
         }
         __syncthreads();

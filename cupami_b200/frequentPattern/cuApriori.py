@@ -68,7 +68,7 @@ class cuApriori:
     #: Device arena for child tidsets in bytes (0: as much as the GPU holds).
     #: A small arena makes the deep levels run in memory-bounded rounds.
     _ARENA_BYTES = 0
-    #: Deep-level launch shape: threads per CTA (128/256/512) and CTAs per SM
+    #: Deep-level launch shape: threads per CTA (128/256/512/1024) and CTAs per SM
     #: (1-4); 0 leaves each to the library (or to the autotuner's table).
     _DEEP_BLOCK = 0
     _DEEP_CTAS_PER_SM = 0

@@ -77,7 +77,7 @@ typedef struct {
     uint64_t arena_bytes;          /* device arena for child tidsets; 0 = automatic */
     uint64_t spin_limit;           /* bounded device waits; 0 = default */
     int32_t  collect_trace;        /* 1: record per-frame features and costs for the cost model */
-    int32_t  deep_block;           /* deep-level kernel threads per CTA: 128, 256 or 512; 0 = automatic */
+    int32_t  deep_block;           /* deep-level kernel threads per CTA: 128, 256, 512 or 1024; 0 = automatic */
     int32_t  deep_ctas_per_sm;     /* resident deep-level CTAs per SM, 1-4 (capped by occupancy); 0 = automatic */
     int32_t  autotune;             /* 1: use the launch shape cpm_autotune found for this tidset length */
     int32_t  tidsets;              /* deep-level tidset forms.  0: bitsets, plus transaction-id lists for
@@ -139,7 +139,7 @@ int cpm_db_from_ids_batch(cpm_ctx *ctx, uint32_t n_db, const uint64_t *const *of
                           cpm_db **out);
 
 /* Autotuner of the deep level.  Mines db (Eclat) once per launch shape --
- * threads per CTA in {128, 256, 512} x resident CTAs per SM in 1..4, as far as
+ * threads per CTA in {128, 256, 512, 1024} x resident CTAs per SM in 1..4, as far as
  * occupancy allows -- then, at the fastest shape, once per tidset form
  * (bitsets only, or lists at divisors 1, 2, 4, 8), keeping the best of two
  * deep-phase times each, and records the fastest shape and form in the

@@ -136,14 +136,14 @@ def test_launch_shapes_and_autotuner_keep_output():
     base.mine()
     want = list(base.getPatterns().items())
     assert len(want) > 1000
-    for block in (128, 256, 512):
+    for block in (128, 256, 512, 1024):
         for ctas in (1, 2, 4):
             m = cupami_b200.cuEclat(csr, 0.6)
             m._DEEP_BLOCK, m._DEEP_CTAS_PER_SM = block, ctas
             m.mine()
             assert list(m.getPatterns().items()) == want, (block, ctas)
     tuned = cupami_b200.cuEclat(csr, 0.6).autotune()
-    assert tuned["block"] in (128, 256, 512) and 1 <= tuned["ctas_per_sm"] <= 4 and tuned["ms_deep"] > 0
+    assert tuned["block"] in (128, 256, 512, 1024) and 1 <= tuned["ctas_per_sm"] <= 4 and tuned["ms_deep"] > 0
     assert tuned["list_div"] in (0, 1, 2, 4, 8)
     m = cupami_b200.cuEclat(csr, 0.6)
     m.mine()
