@@ -4,8 +4,9 @@ The reference compiles its three bitset kernels at run time from a CUDA source
 string (``_SOURCE`` in cupami/frequentPattern/_bitsets.py:19-78, NVRTC, cached
 per device).  This recipe compiles the same string ahead of time for sm_100a:
 it reads the string out of the reference file with ``ast`` (the module is not
-imported or executed), writes it to ``oracle/_ref/ref_bitsets.cu`` and builds
-``oracle/ref_launch.cu`` (host launchers written here) around it with nvcc.
+imported or executed), writes it to a temporary file under ``oracle/_ref/``
+(deleted after the compile) and builds ``oracle/ref_launch.cu`` (host
+launchers written here) around it with nvcc.
 Outputs go to ``oracle/_ref/`` only; that folder is git-ignored and ships with
 the built library.  Without the reference sources (as on a machine that only
 has the prebuilt files) it does nothing.
@@ -45,11 +46,14 @@ def build(root: Path = DEFAULT_ROOT, force: bool = False) -> Path | None:
     if not force and LIB.exists() and LIB.stat().st_mtime >= max(shim.stat().st_mtime, ref_file.stat().st_mtime):
         return LIB
     OUT.mkdir(exist_ok=True)
-    cu = OUT / "ref_bitsets.cu"
+    cu = OUT / ("ref_bitsets.%d.cu" % os.getpid())  # build intermediate, removed below
     cu.write_text(reference_source(root))
     tmp = LIB.with_suffix(".so.tmp%d" % os.getpid())
-    subprocess.check_call([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
-                           "-Xcompiler", "-fPIC", "-shared", f'-DREF_KERNELS="{cu}"', "-o", str(tmp), str(shim)])
+    try:
+        subprocess.check_call([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
+                               "-Xcompiler", "-fPIC", "-shared", f'-DREF_KERNELS="{cu}"', "-o", str(tmp), str(shim)])
+    finally:
+        cu.unlink(missing_ok=True)
     os.replace(tmp, LIB)
     return LIB
 

@@ -4,7 +4,7 @@
 //
 // The kernels are not restated here: oracle/build_ref.py extracts the
 // reference's CUDA source string (cupami/frequentPattern/_bitsets.py:19-78)
-// into oracle/_ref/ref_bitsets.cu and compiles this file with
+// into a temporary file under oracle/_ref/ and compiles this file with
 // -DREF_KERNELS=<that path>.  Each launcher uses the reference wrapper's launch
 // shape: build_bitsets one thread per occurrence in blocks of 256
 // (_bitsets.py:91-100); count_supports and intersect_extensions one block of
