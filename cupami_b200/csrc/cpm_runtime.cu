@@ -850,7 +850,8 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
     P.pat_cap = b.pat_cap;
     P.root_cost = nullptr; P.st = b.st; P.max_stride = max_stride; P.spin_limit = spin; P.cta_time = nullptr;
     P.lists = lists;
-    P.root_frames = 0; P.defer_words = 0; P.deferred = nullptr; P.deferred_cap = 0;
+    P.root_frames = 0; P.defer_words = 0; P.defer_members = 0; P.defer_frames = 0; P.defer_queue = 0;
+    P.deferred = nullptr; P.deferred_cap = 0;
     const size_t prefix_bytes = max_stride * 8;
     uint64_t rounds = 0, failed = 0, shallow = 0;
     float deep_ms = 0.f;
@@ -877,7 +878,12 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
         CK(cudaEventRecord(ctx->ev[3], ctx->stream));
         CK(cudaMemcpyAsync(&hs, b.st, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
-        deep_ms += (float)elapsed_ms(ctx, 2, 3);
+        const float round_ms = (float)elapsed_ms(ctx, 2, 3);
+        deep_ms += round_ms;
+        if (dbg)
+            fprintf(stderr, "cpm: round %llu: %zu units, %.3f ms, %.3g bytes, %.0f GB/s, deferred %llu, error 0x%x\n",
+                    (unsigned long long)rounds, n_take, round_ms, (double)hs.bytes_alg,
+                    round_ms > 0 ? hs.bytes_alg / (round_ms * 1e6) : 0.0, (unsigned long long)hs.n_deferred, hs.error);
         st.kernel_launches++;
         if (!hs.error) {  // a discarded round's work is not counted (its time is)
             st.intersections += hs.intersections;
@@ -905,6 +911,9 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
         }
         P.root_frames = (uint32_t)persist_frames;
         P.defer_words = persist_arena + std::max<uint64_t>(1, (uint64_t)(frac * (double)(arena_words - persist_arena)));
+        P.defer_members = persist_members + (uint64_t)(frac * (double)(b.members_cap - persist_members));
+        P.defer_frames = persist_frames + (uint64_t)(frac * (double)(b.frames_cap - persist_frames));
+        P.defer_queue = take + (uint64_t)(frac * (double)(std::min<uint64_t>(queue_cap, take * 64 + (1u << 20)) - take));
         P.deferred = d_deferred;
         P.deferred_cap = deferred_cap;
         CKR(launch(take, 0));
@@ -1231,7 +1240,11 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     uint64_t frames_cap = std::max<uint64_t>({1024, frames.size() * 8 + P2_total * 2, n_db == 1 ? db0->hint_frames : 0});
     // Member entries are reserved for every sibling of every unit (~ the
     // intersections), several times the pair count on deep lattices.
-    uint64_t members_cap = std::max<uint64_t>({4096, P2_total * 64, n_db == 1 ? db0->hint_members : 0});
+    // Every unit reserves an entry per sibling: the third level alone takes
+    // sum m(m-1)/2 over the top-level classes; deeper levels add to it.
+    uint64_t level3 = 0;
+    for (const DFrame &f : frames) level3 += (uint64_t)f.m * (f.m - 1) / 2;
+    uint64_t members_cap = std::max<uint64_t>({4096, P2_total * 64, level3 * 4, n_db == 1 ? db0->hint_members : 0});
     uint64_t queue_cap = std::max<uint64_t>({4096, n_units * 8 + P2_total * 4, n_db == 1 ? db0->hint_queue : 0});
     uint64_t pat_cap = std::max<uint64_t>({4096, base_patterns * 16, n_db == 1 ? db0->hint_patterns : 0});
     const uint64_t arena_budget = o.arena_bytes ? o.arena_bytes / 8 : (uint64_t)(ctx->mem_free * 0.6) / 8;
@@ -1375,6 +1388,9 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         // back and finished in memory-bounded rounds after this launch.
         P.root_frames = (uint32_t)frames.size();
         P.defer_words = std::max<uint64_t>(1, b.arena_words / 4 * 3);
+        P.defer_members = P2_total + (b.members_cap - P2_total) / 4 * 3;
+        P.defer_frames = frames.size() + (b.frames_cap - frames.size()) / 4 * 3;
+        P.defer_queue = n_units + (b.queue_cap - n_units) / 4 * 3;
         P.deferred = d_deferred;
         P.deferred_cap = n_units;
         CK(cudaEventRecord(ctx->ev[2], ctx->stream));
@@ -2475,7 +2491,8 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     P.cta_time = nullptr;
     P.shallow = 0;
     P.lists = 0;
-    P.root_frames = 0; P.defer_words = 0; P.deferred = nullptr; P.deferred_cap = 0;
+    P.root_frames = 0; P.defer_words = 0; P.defer_members = 0; P.defer_frames = 0; P.defer_queue = 0;
+    P.deferred = nullptr; P.deferred_cap = 0;
     // Each warp keeps one scratch tidset: leave at least half the arena to children.
     const size_t prefix_bytes = stride * 8;
     const bool smem_prefix = prefix_bytes <= 200 * 1024;

@@ -93,10 +93,11 @@ struct DeepParams {
     uint32_t shallow;               // 1: child frames are recorded, not queued
     uint32_t lists;                 // list-form threshold divisor (0: bitsets only; needs SMEM_PREFIX)
     // Memory-bounded rounds: a unit of a frame below root_frames (a root
-    // unit) claimed while arena_next >= defer_words is not run but handed
-    // back in deferred[] for a later round (defer_words 0: never).
+    // unit) claimed while the arena, the member table or the frame table has
+    // (or the queue) has reached its hand-back level is not run but handed back in deferred[]
+    // for a later round (defer_words 0: never).
     uint32_t root_frames;
-    unsigned long long defer_words;
+    unsigned long long defer_words, defer_members, defer_frames, defer_queue;
     unsigned long long *deferred;
     uint64_t deferred_cap;
 };
@@ -264,7 +265,9 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             s_stop = deep_claim(P, &s_item);
             s_skip = 0;
             if (!s_stop && P.defer_words && (uint32_t)(s_item >> 32) < P.root_frames &&
-                ld_acquire_u64(&st->arena_next) >= P.defer_words) {
+                (ld_acquire_u64(&st->arena_next) >= P.defer_words ||
+                 ld_acquire_u64(&st->n_members) >= P.defer_members || ld_acquire_u64(&st->n_frames) >= P.defer_frames ||
+                 ld_acquire_u64(&st->q_tail) >= P.defer_queue)) {
                 // The round's arena is filling up: leave this root unit to the next round.
                 const unsigned long long di = atomicAdd(&st->n_deferred, 1ull);
                 if (di < P.deferred_cap) P.deferred[di] = s_item;
