@@ -11,6 +11,7 @@ from __future__ import annotations
 import atexit
 import ctypes
 import threading
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -157,6 +158,7 @@ class Context:
         self.handle = handle
         self.device = device
         self.lock = threading.Lock()
+        self.databases = weakref.WeakSet()  # freed before the context (they point to it)
 
     def check(self, code):
         if code != CPM_OK:
@@ -165,6 +167,8 @@ class Context:
 
     def close(self):
         if self.handle:
+            for db in list(self.databases):
+                db.close()
             library().cpm_shutdown(self.handle)
             self.handle = None
 
@@ -201,6 +205,7 @@ class Database:
     def __init__(self, ctx: Context, handle, labels=None):
         self.ctx = ctx
         self.handle = handle
+        ctx.databases.add(self)
         n_tx, n_items, words = _U64(), ctypes.c_uint32(), _U64()
         ctx.check(library().cpm_db_info(handle, ctypes.byref(n_tx), ctypes.byref(n_items),
                                         ctypes.byref(words)))
@@ -272,9 +277,10 @@ class Database:
             library().cpm_result_free(res)
 
     def close(self):
-        if self.handle:
+        # A database outliving its context (interpreter teardown) was freed with it.
+        if self.handle and self.ctx.handle:
             library().cpm_db_free(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:

@@ -112,8 +112,19 @@ static int dalloc(cpm_ctx *ctx, T **p, size_t count) {
     *p = nullptr;
     if (count == 0) count = 1;
     cudaError_t e = cudaMallocAsync((void **)p, count * sizeof(T), ctx->stream);
+    if (e == cudaErrorMemoryAllocation) {
+        // Blocks freed earlier stay reserved by the stream-ordered pool: once
+        // the stream has passed their frees, hand them back and try again.
+        cudaGetLastError();
+        cudaMemPool_t pool;
+        if (cudaStreamSynchronize(ctx->stream) == cudaSuccess &&
+            cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess)
+            cudaMemPoolTrimTo(pool, 0);
+        e = cudaMallocAsync((void **)p, count * sizeof(T), ctx->stream);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
+        *p = nullptr;
         return set_err(ctx, CPM_ENOMEM, "device allocation of %zu bytes failed: %s",
                        count * sizeof(T), cudaGetErrorString(e));
     }
@@ -197,6 +208,7 @@ extern "C" int cpm_init(int device, cpm_ctx **out) {
     return CPM_OK;
 }
 
+// Databases made on the context must be freed first (they point to it).
 extern "C" void cpm_shutdown(cpm_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);

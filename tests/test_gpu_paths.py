@@ -203,3 +203,26 @@ def test_lists_in_memory_bounded_rounds_and_batches(oracle_lib):
         for csr, m in zip(csrs, cls.mineBatch(csrs, 0.01)):
             labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, 0.01)
             assert m.getPatterns() == oracle_lib.to_dict(labels, arrays)
+
+
+def test_interpreter_exit_with_live_databases():
+    """A process that ends with databases still alive (a global, a traceback)
+    exits cleanly: the context frees its databases before itself."""
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    code = (
+        "import numpy as np, cupami_b200._native as n\n"
+        "ctx = n.context(0)\n"
+        "off = np.array([0, 2, 3], np.uint64); ids = np.array([1, 2, 2], np.uint32)\n"
+        "KEEP = n.Database.from_ids(ctx, off, ids)\n"
+        "def f():\n"
+        "    db = n.Database.from_ids(ctx, off, ids)\n"
+        "    raise RuntimeError('left with a live database')\n"
+        "f()\n"
+    )
+    root = Path(__file__).resolve().parents[1]
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=240)
+    assert r.returncode == 1, (r.returncode, r.stderr[-2000:])
+    assert "left with a live database" in r.stderr
