@@ -29,6 +29,7 @@
 #include <unordered_set>
 #include <vector>
 #include <map>
+#include <array>
 #include <chrono>
 #include <cstdlib>
 #include <mutex>
@@ -59,6 +60,10 @@ struct cpm_ctx {
     size_t l2_bytes = 126ull << 20;               // device L2 size (cpm_init)
     std::map<int, std::pair<int, int>> tune;      // log2(stride) -> (threads per CTA, CTAs per SM), cpm_autotune
     std::map<int, int> tune_lists;                // log2(stride) -> list divisor (0: bitsets only), cpm_autotune
+    // Deep-level buffer sizes the last Eclat mine of a database of this shape
+    // needed (transactions, items, frequent pairs, threshold), so that a
+    // database loaded again (the drop-in reloads per mine()) starts there.
+    std::map<std::array<uint64_t, 4>, std::array<uint64_t, 5>> plan_hints;
 };
 
 struct cpm_db {
@@ -1249,7 +1254,19 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     DeepBuffers b;
     b.owner = ctx;
     const bool with_db = n_db > 1;
-    uint64_t frames_cap = std::max<uint64_t>({1024, frames.size() * 8 + P2_total * 2, n_db == 1 ? db0->hint_frames : 0});
+    const std::array<uint64_t, 4> plan_key{db0->n_tx, db0->n_items, P2_total, (uint64_t)ms[0]};
+    if (n_db == 1 && !db0->hint_members) {
+        const auto it = ctx->plan_hints.find(plan_key);
+        if (it != ctx->plan_hints.end()) {
+            db0->hint_frames = it->second[0];
+            db0->hint_members = it->second[1];
+            db0->hint_queue = it->second[2];
+            db0->hint_patterns = it->second[3];
+            db0->hint_arena = it->second[4];
+        }
+    }
+    uint64_t frames_cap = std::max<uint64_t>({1024, frames.size() * 8 + P2_total * 2,
+                                              n_db == 1 ? db0->hint_frames : 0});
     // Member entries are reserved for every sibling of every unit (~ the
     // intersections), several times the pair count on deep lattices.
     // Every unit reserves an entry per sibling: the third level alone takes
@@ -1257,7 +1274,9 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     uint64_t level3 = 0;
     for (const DFrame &f : frames) level3 += (uint64_t)f.m * (f.m - 1) / 2;
     uint64_t members_cap = std::max<uint64_t>({4096, P2_total * 64, level3 * 4, n_db == 1 ? db0->hint_members : 0});
-    uint64_t queue_cap = std::max<uint64_t>({4096, n_units * 8 + P2_total * 4, n_db == 1 ? db0->hint_queue : 0});
+    uint64_t queue_cap = std::max<uint64_t>({4096, n_units * 8 + P2_total * 4, level3,
+                                             n_db == 1 ? db0->hint_queue : 0});
+    frames_cap = std::max<uint64_t>(frames_cap, level3 / 8);
     uint64_t pat_cap = std::max<uint64_t>({4096, base_patterns * 16, n_db == 1 ? db0->hint_patterns : 0});
     const uint64_t arena_budget = o.arena_bytes ? o.arena_bytes / 8 : (uint64_t)(ctx->mem_free * 0.6) / 8;
     // First arena: what the database needed before, else a guess capped at
@@ -1498,6 +1517,8 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         else if (arena_exceeded) db0->hint_arena = std::max<uint64_t>(db0->hint_arena, arena_budget + 1);
         else if (continued && !o.arena_bytes)
             db0->hint_arena = std::max<uint64_t>(db0->hint_arena, arena_budget);  // did not fit: take the budget next time
+        ctx->plan_hints[plan_key] = {db0->hint_frames, db0->hint_members, db0->hint_queue, db0->hint_patterns,
+                                     db0->hint_arena};
     }
     const uint64_t n = hs.n_patterns;
     std::vector<uint32_t> par(n), item(n), sup(n), pdb;

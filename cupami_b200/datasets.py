@@ -289,6 +289,12 @@ def reference_uniform_baskets(transactions, items, avg_length=None, seed=None):
     return rows
 
 
+def quickstart(seed=42) -> TransactionCSR:
+    """The reference's quickstart dataset (10,000 baskets over items 1..50, mean
+    length 6, seed 42), rebuilt with the reference's own sampler."""
+    return TransactionCSR.from_rows(reference_uniform_baskets(10_000, 50, avg_length=6, seed=seed), universe=51)
+
+
 _WORKLOADS = {
     "uniform-10k": (uniform_poisson, 0.01),
     "planted-100k": (planted_zipf, 0.005),
