@@ -336,9 +336,18 @@ extern "C" int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n
                                const uint32_t *ids, uint64_t nnz, cpm_db **out) {
     if (!ctx || !out || (!offsets && n_rows) || (!ids && nnz)) return CPM_EINVAL;
     *out = nullptr;
+    const bool dbg = getenv("CPM_DEBUG") != nullptr;
+    auto t0 = std::chrono::steady_clock::now();
+    auto lap = [&](const char *what) {
+        if (!dbg) return;
+        const auto now = std::chrono::steady_clock::now();
+        fprintf(stderr, "cpm: load %-20s %.3f ms\n", what, std::chrono::duration<double, std::milli>(now - t0).count());
+        t0 = now;
+    };
     CK(cudaSetDevice(ctx->device));
     std::vector<uint64_t> off;
     CKR(compact_offsets(ctx, offsets, n_rows, nnz, off));
+    lap("offsets");
     uint32_t max_id = 0;
 #pragma omp parallel for reduction(max : max_id) schedule(static) if (nnz > (1u << 18))
     for (int64_t k = 0; k < (int64_t)nnz; ++k) max_id = std::max(max_id, ids[k]);
@@ -363,9 +372,11 @@ extern "C" int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n
         }
         CK(cudaGetLastError());
     }
+    lap("max id, upload, mark");
     std::vector<uint32_t> present(pw);
     CK(cudaMemcpyAsync(present.data(), d_present, pw * 4, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    lap("presence sync");
     std::vector<uint32_t> uniq;
     for (uint64_t w = 0; w < pw; ++w)
         for (uint32_t m = present[w]; m; m &= m - 1) uniq.push_back((uint32_t)(w * 32 + __builtin_ctz(m)));
@@ -413,6 +424,7 @@ extern "C" int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n
         cpm_db_free(db);
         return r;
     }
+    lap("labels, table, pack");
     *out = db;
     return CPM_OK;
 }
@@ -1597,8 +1609,10 @@ struct U32ToU64 {
     __host__ __device__ uint64_t operator()(uint32_t v) const { return v; }
 };
 
+// Exclusive sum of n counts into out; with total, also its sum (one
+// device-to-host copy and a sync), without it nothing leaves the device.
 static int scan_u32(cpm_ctx *ctx, DevScope &ds, const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *total) {
-    *total = 0;
+    if (total) *total = 0;
     if (!n) return CPM_OK;
     thrust::transform_iterator<U32ToU64, const uint32_t *, uint64_t> it(in, U32ToU64());
     size_t bytes = 0;
@@ -1606,6 +1620,7 @@ static int scan_u32(cpm_ctx *ctx, DevScope &ds, const uint32_t *in, uint64_t *ou
     void *tmp = nullptr;
     CKR(ds.alloc(reinterpret_cast<unsigned char **>(&tmp), bytes));
     CK(cub::DeviceScan::ExclusiveSum(tmp, bytes, it, out, (int64_t)n, ctx->stream));
+    if (!total) return CPM_OK;
     uint64_t last_off = 0;
     uint32_t last_in = 0;
     CK(cudaMemcpyAsync(&last_off, out + n - 1, 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1713,12 +1728,11 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
             const unsigned nb = (unsigned)((n + 255) / 256);
             k_group_start<<<nb, 256, 0, ctx->stream>>>(L, n, k, gflag);
             CK(cudaGetLastError());
-            uint64_t n_groups = 0;
-            CKR(scan_u32(ctx, lvl, gflag, gid, n, &n_groups));
-            CKR(lvl.alloc(&gfirst, n_groups));
+            CKR(scan_u32(ctx, lvl, gflag, gid, n, nullptr));
+            CKR(lvl.alloc(&gfirst, n + 1));
             k_group_first<<<nb, 256, 0, ctx->stream>>>(gflag, gid, n, gfirst);
             CK(cudaGetLastError());
-            k_partners<<<nb, 256, 0, ctx->stream>>>(gflag, gid, gfirst, n_groups, n, partners);
+            k_partners<<<nb, 256, 0, ctx->stream>>>(gflag, gid, gfirst, n, partners);
             CK(cudaGetLastError());
             uint64_t n_pairs = 0;
             CKR(scan_u32(ctx, lvl, partners, poff, n, &n_pairs));

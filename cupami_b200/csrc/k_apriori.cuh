@@ -75,20 +75,21 @@ __global__ void k_group_start(const uint32_t *__restrict__ L, uint64_t n, uint32
 
 // Exclusive group-start scan -> each group's first row (gfirst[g]) and, per
 // row, the number of later rows of its group (its join partners).
+// gfirst[g] = first row of group g; the entry after the last group holds n,
+// so a row's group always ends at gfirst[g + 1] (gfirst has n + 1 entries).
 __global__ void k_group_first(const uint32_t *__restrict__ flag, const uint64_t *__restrict__ gid_excl, uint64_t n,
                               uint64_t *__restrict__ gfirst) {
     const uint64_t a = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (a < n && flag[a]) gfirst[gid_excl[a]] = a;
+    if (a + 1 == n) gfirst[gid_excl[a] + flag[a]] = n;
 }
 
 __global__ void k_partners(const uint32_t *__restrict__ flag, const uint64_t *__restrict__ gid_excl,
-                           const uint64_t *__restrict__ gfirst, uint64_t n_groups, uint64_t n,
-                           uint32_t *__restrict__ partners) {
+                           const uint64_t *__restrict__ gfirst, uint64_t n, uint32_t *__restrict__ partners) {
     const uint64_t a = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n) return;
     const uint64_t g = gid_excl[a] + flag[a] - 1;  // this row's group
-    const uint64_t end = g + 1 < n_groups ? gfirst[g + 1] : n;
-    partners[a] = (uint32_t)(end - a - 1);
+    partners[a] = (uint32_t)(gfirst[g + 1] - a - 1);
 }
 
 // One thread per join pair t: row a = last row with poff[a] <= t, partner
