@@ -241,85 +241,6 @@ __device__ __forceinline__ uint32_t sibling_count(unsigned long long sraw, uint3
     return s;
 }
 
-// Work per chunk in pass 1: 256 16-byte loads (4 KB) of a sibling -- bitset
-// words, or groups of four list ids.
-constexpr uint32_t DEEP_CHUNK = 256;
-
-// Chunks of a sibling and its size in bytes (its own form).
-template <bool SMEM_PREFIX>
-__device__ __forceinline__ uint32_t sibling_chunks(unsigned long long sraw, uint64_t n2, uint64_t *bytes) {
-    if (SMEM_PREFIX && (sraw & 1ull)) {
-        const uint32_t n = __ldcg(reinterpret_cast<const uint32_t *>(sraw & ~1ull));
-        *bytes = 8ull * list_words(n);
-        return ((n + 3) / 4 + DEEP_CHUNK - 1) / DEEP_CHUNK;
-    }
-    *bytes = 16ull * n2;
-    return (uint32_t)((n2 + DEEP_CHUNK - 1) / DEEP_CHUNK);
-}
-
-// This lane's share of |prefix & sibling| over chunk j of the sibling.
-template <bool SMEM_PREFIX>
-__device__ __forceinline__ uint32_t chunk_count(unsigned long long sraw, uint32_t j, uint64_t n2,
-                                                const ulonglong2 *s_prefix, const uint32_t *s_p32,
-                                                const ulonglong2 *pb, const ulonglong2 *mk, unsigned lane) {
-    uint32_t s = 0;
-    if (SMEM_PREFIX && (sraw & 1ull)) {
-        const uint32_t *L = reinterpret_cast<const uint32_t *>(sraw & ~1ull);
-        const uint32_t n = __ldcg(L);
-        const uint4 *T = reinterpret_cast<const uint4 *>(L + 4);
-        const uint32_t nv = (n + 3) / 4;
-        const uint32_t lo = j * DEEP_CHUNK, hi = min(nv, lo + DEEP_CHUNK);
-        if (hi == lo + DEEP_CHUNK && 4 * hi <= n) {  // a full chunk of complete groups
-            uint4 t[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) t[u] = __ldcg(T + lo + lane + 32 * u);
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-                s += bit_of(s_p32, t[u].x) + bit_of(s_p32, t[u].y) + bit_of(s_p32, t[u].z) + bit_of(s_p32, t[u].w);
-            return s;
-        }
-        for (uint32_t w = lo + lane; w < hi; w += 32) {
-            const uint4 t = __ldcg(T + w);
-            const uint32_t i0 = 4 * w;
-            s += bit_of(s_p32, t.x);
-            if (i0 + 1 < n) s += bit_of(s_p32, t.y);
-            if (i0 + 2 < n) s += bit_of(s_p32, t.z);
-            if (i0 + 3 < n) s += bit_of(s_p32, t.w);
-        }
-        return s;
-    }
-    const ulonglong2 *sb = reinterpret_cast<const ulonglong2 *>(sraw);
-    const uint64_t lo = (uint64_t)j * DEEP_CHUNK, hi = min(n2, lo + DEEP_CHUNK);
-    if (hi == lo + DEEP_CHUNK) {
-        ulonglong2 x[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) x[u] = ld_cg(sb + lo + lane + 32 * u);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const uint64_t v = lo + lane + 32 * u;
-            if (SMEM_PREFIX) {
-                x[u] = and2(x[u], s_prefix[v]);
-            } else {
-                x[u] = and2(x[u], ld_cg(pb + v));
-                if (mk) x[u] = and2(x[u], ld_cg(mk + v));
-            }
-            s += popc2(x[u]);
-        }
-        return s;
-    }
-    for (uint64_t v = lo + lane; v < hi; v += 32) {
-        ulonglong2 x = ld_cg(sb + v);
-        if (SMEM_PREFIX) {
-            x = and2(x, s_prefix[v]);
-        } else {
-            x = and2(x, ld_cg(pb + v));
-            if (mk) x = and2(x, ld_cg(mk + v));
-        }
-        s += popc2(x);
-    }
-    return s;
-}
-
 template <bool SMEM_PREFIX>
 __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     extern __shared__ ulonglong2 s_prefix[];
@@ -331,9 +252,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     __shared__ uint64_t s_w64[32];
     __shared__ uint64_t s_off[1024];     // child offsets of one chunk of survivors
     __shared__ unsigned long long s_bytes;
-    __shared__ uint32_t s_cnt[1024];     // pass 1: per-sibling sums (units of at most blockDim siblings)
-    __shared__ uint32_t s_choff[1024];   // pass 1: first chunk of every sibling
-    __shared__ uint32_t s_next;          // pass 1: next chunk to take
+    __shared__ uint32_t s_part[32];      // per-sibling sums when siblings are split over warps
     uint32_t *const s_p32 = reinterpret_cast<uint32_t *>(s_prefix);
 
     const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -434,8 +353,10 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 P.mem_bits[m_out] = reinterpret_cast<const uint64_t *>(sraw);
             }
         };
-        if (cnt > blockDim.x) {
-            // Many siblings: one warp per sibling.
+        // Fewer siblings than warps: split every sibling into equal slices
+        // (at least 4 KB of bitset each) so that every warp has work.
+        const uint32_t parts = (cnt && cnt < nw) ? max(1u, min(nw / cnt, (uint32_t)(n2 >> 8))) : 1u;
+        if (parts == 1) {
             for (uint32_t q = wid; ok && q < cnt; q += nw) {
                 const uint64_t mi = mem_off + p + 1 + q;
                 const unsigned long long sraw = ld_raw_ptr(P.mem_bits + mi);
@@ -448,41 +369,24 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                     emit(q, s, sib_item, sraw);
                 }
             }
-        } else if (ok) {
-            // At most one sibling per thread: cut every sibling into 4 KB
-            // chunks and let the warps take chunks in turn, so that a few
-            // large bitsets among small lists do not leave warps idle.
-            uint32_t nch = 0;
-            if (threadIdx.x < cnt) {
+        } else {
+            if (threadIdx.x < 32) s_part[threadIdx.x] = 0;
+            __syncthreads();
+            for (uint32_t it = wid; ok && it < cnt * parts; it += nw) {
+                const uint32_t q = it / parts, j = it - q * parts;
+                const unsigned long long sraw = ld_raw_ptr(P.mem_bits + mem_off + p + 1 + q);
                 uint64_t b = 0;
-                nch = sibling_chunks<SMEM_PREFIX>(ld_raw_ptr(P.mem_bits + mem_off + p + 1 + threadIdx.x), n2, &b);
-                atomicAdd(&s_bytes, (unsigned long long)b);
-                s_cnt[threadIdx.x] = 0;
-            }
-            uint64_t total = 0;
-            const uint64_t first = block_excl_scan_u64(nch, s_w64, &total);
-            if (threadIdx.x < cnt) s_choff[threadIdx.x] = (uint32_t)first;
-            if (threadIdx.x == 0) s_next = 0;
-            __syncthreads();
-            for (;;) {
-                uint32_t it = 0;
-                if (lane == 0) it = atomicAdd(&s_next, 1u);
-                it = __shfl_sync(CPM_FULL, it, 0);
-                if (it >= total) break;
-                uint32_t lo = 0, hi = cnt;  // last sibling whose first chunk is <= it
-                while (hi - lo > 1) {
-                    const uint32_t mid = (lo + hi) >> 1;
-                    if (s_choff[mid] <= it) lo = mid; else hi = mid;
-                }
-                const unsigned long long sraw = ld_raw_ptr(P.mem_bits + mem_off + p + 1 + lo);
-                uint32_t s = chunk_count<SMEM_PREFIX>(sraw, it - s_choff[lo], n2, s_prefix, s_p32, pb, mk, lane);
+                uint32_t s = sibling_count<SMEM_PREFIX>(sraw, j, parts, n2, s_prefix, s_p32, pb, mk, lane, &b);
                 s = warp_sum_u32(s);
-                if (lane == 0 && s) atomicAdd(&s_cnt[lo], s);
+                if (lane == 0) {
+                    atomicAdd(&s_part[q], s);
+                    if (j == 0) atomicAdd(&s_bytes, (unsigned long long)b);
+                }
             }
             __syncthreads();
-            if (threadIdx.x < cnt) {
+            if (ok && threadIdx.x < cnt) {
                 const uint64_t mi = mem_off + p + 1 + threadIdx.x;
-                emit(threadIdx.x, s_cnt[threadIdx.x], __ldcg(P.mem_item + mi), ld_raw_ptr(P.mem_bits + mi));
+                emit(threadIdx.x, s_part[threadIdx.x], __ldcg(P.mem_item + mi), ld_raw_ptr(P.mem_bits + mi));
             }
         }
         __syncthreads();
