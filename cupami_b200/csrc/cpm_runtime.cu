@@ -58,6 +58,8 @@ struct cpm_ctx {
     float last_deep_ms = 0.f;  // deep-phase kernel time of the last bounded-round run
     int last_deep_block = 0, last_deep_ctas = 0;  // launch shape of the last deep phase
     size_t l2_bytes = 126ull << 20;               // device L2 size (cpm_init)
+    void *pinned = nullptr;                       // host staging for uploads (stage_upload)
+    size_t pinned_bytes = 0;
     std::map<int, std::pair<int, int>> tune;      // log2(stride) -> (threads per CTA, CTAs per SM), cpm_autotune
     std::map<int, int> tune_lists;                // log2(stride) -> list divisor (0: bitsets only), cpm_autotune
     // Deep-level buffer sizes the last Eclat mine of a database of this shape
@@ -221,6 +223,7 @@ extern "C" void cpm_shutdown(cpm_ctx *ctx) {
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
     delete ctx;
 }
 
@@ -257,6 +260,73 @@ static int compact_offsets(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_row
     for (uint64_t r = 0; r < n_rows; ++r) {
         if (offsets[r + 1] < offsets[r]) return set_err(ctx, CPM_EINVAL, "offsets must be nondecreasing");
         if (offsets[r + 1] > offsets[r]) out.push_back(offsets[r + 1]);
+    }
+    return CPM_OK;
+}
+
+// The offsets as uploaded: the caller's own array when no basket is empty
+// (checked in parallel), else the compacted copy in `storage`.
+static int offsets_view(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows, uint64_t nnz,
+                        std::vector<uint64_t> &storage, const uint64_t **view, uint64_t *n_view) {
+    if (n_rows && offsets[0] == 0 && offsets[n_rows] == nnz) {
+        int bad = 0, empty = 0;
+#pragma omp parallel for reduction(| : bad, empty) schedule(static) if (n_rows > (1u << 16))
+        for (int64_t r = 0; r < (int64_t)n_rows; ++r) {
+            bad |= offsets[r + 1] < offsets[r];
+            empty |= offsets[r + 1] == offsets[r];
+        }
+        if (bad) return set_err(ctx, CPM_EINVAL, "offsets must be nondecreasing");
+        if (!empty) {
+            *view = offsets;
+            *n_view = n_rows + 1;
+            return CPM_OK;
+        }
+    }
+    CKR(compact_offsets(ctx, offsets, n_rows, nnz, storage));
+    *view = storage.data();
+    *n_view = storage.size();
+    return CPM_OK;
+}
+
+// Uploads through pinned memory the context keeps (up to 256 MB; larger
+// inputs are copied from pageable memory).  The staging buffer is reused
+// only after the caller has synchronised the stream (every loader does).
+static int stage_upload(cpm_ctx *ctx, const std::vector<std::pair<void *, std::pair<const void *, size_t>>> &parts) {
+    size_t total = 0;
+    for (auto &pt : parts) total += (pt.second.second + 255) & ~(size_t)255;
+    if (total == 0) return CPM_OK;
+    if (total > (256ull << 20)) {
+        for (auto &pt : parts)
+            if (pt.second.second)
+                CK(cudaMemcpyAsync(pt.first, pt.second.first, pt.second.second, cudaMemcpyHostToDevice, ctx->stream));
+        return CPM_OK;
+    }
+    if (ctx->pinned_bytes < total) {
+        if (ctx->pinned) cudaFreeHost(ctx->pinned);
+        ctx->pinned = nullptr;
+        ctx->pinned_bytes = 0;
+        const size_t want = std::max<size_t>(total, 16ull << 20);
+        if (cudaHostAlloc(&ctx->pinned, want, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            ctx->pinned = nullptr;
+            for (auto &pt : parts)
+                if (pt.second.second)
+                    CK(cudaMemcpyAsync(pt.first, pt.second.first, pt.second.second, cudaMemcpyHostToDevice,
+                                       ctx->stream));
+            return CPM_OK;
+        }
+        ctx->pinned_bytes = want;
+    }
+    size_t at = 0;
+    for (auto &pt : parts) {
+        unsigned char *dst = static_cast<unsigned char *>(ctx->pinned) + at;
+        const unsigned char *src = static_cast<const unsigned char *>(pt.second.first);
+        const size_t n = pt.second.second, chunk = 1u << 20;
+#pragma omp parallel for schedule(static) if (n > (4u << 20))
+        for (int64_t c = 0; c < (int64_t)((n + chunk - 1) / chunk); ++c)
+            memcpy(dst + c * chunk, src + c * chunk, std::min(chunk, n - c * chunk));
+        if (n) CK(cudaMemcpyAsync(pt.first, dst, n, cudaMemcpyHostToDevice, ctx->stream));
+        at += (n + 255) & ~(size_t)255;
     }
     return CPM_OK;
 }
@@ -345,8 +415,10 @@ extern "C" int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n
         t0 = now;
     };
     CK(cudaSetDevice(ctx->device));
-    std::vector<uint64_t> off;
-    CKR(compact_offsets(ctx, offsets, n_rows, nnz, off));
+    std::vector<uint64_t> off_store;
+    const uint64_t *offv = nullptr;
+    uint64_t n_off = 0;
+    CKR(offsets_view(ctx, offsets, n_rows, nnz, off_store, &offv, &n_off));
     lap("offsets");
     uint32_t max_id = 0;
 #pragma omp parallel for reduction(max : max_id) schedule(static) if (nnz > (1u << 18))
@@ -354,10 +426,9 @@ extern "C" int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n
     DevScope tmp(ctx);
     uint64_t *d_off = nullptr;
     uint32_t *d_ids = nullptr, *d_lut = nullptr, *d_present = nullptr;
-    CKR(tmp.alloc(&d_off, off.size()));
+    CKR(tmp.alloc(&d_off, n_off));
     CKR(tmp.alloc(&d_ids, nnz));
-    CK(cudaMemcpyAsync(d_off, off.data(), off.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
-    if (nnz) CK(cudaMemcpyAsync(d_ids, ids, nnz * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CKR(stage_upload(ctx, {{d_off, {offv, n_off * 8}}, {d_ids, {ids, nnz * 4}}}));
     // Distinct ids: a presence bitmap over [0, max_id] built on the device.
     const uint64_t pw = (uint64_t)max_id / 32 + 1;
     CKR(tmp.alloc(&d_present, pw));
@@ -387,7 +458,7 @@ extern "C" int cpm_db_from_ids(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n
     std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return keys[a] < keys[b]; });
     cpm_db *db = new cpm_db();
     db->ctx = ctx;
-    db->n_tx = off.size() - 1;
+    db->n_tx = n_off - 1;
     db->n_items = (uint32_t)uniq.size();
     db->labels.resize(uniq.size());
     // Column lookup: dense table over the id range when it is small enough,
