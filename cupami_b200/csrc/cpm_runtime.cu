@@ -288,14 +288,16 @@ static int offsets_view(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows, 
     return CPM_OK;
 }
 
-// Uploads through pinned memory the context keeps (up to 256 MB; larger
-// inputs are copied from pageable memory).  The staging buffer is reused
+// Uploads of 16-256 MB go through pinned memory the context keeps, filled by
+// a parallel copy; smaller and larger ones are copied from pageable memory.  The staging buffer is reused
 // only after the caller has synchronised the stream (every loader does).
 static int stage_upload(cpm_ctx *ctx, const std::vector<std::pair<void *, std::pair<const void *, size_t>>> &parts) {
     size_t total = 0;
     for (auto &pt : parts) total += (pt.second.second + 255) & ~(size_t)255;
     if (total == 0) return CPM_OK;
-    if (total > (256ull << 20)) {
+    // Small uploads: the driver's own pageable path is as fast (measured);
+    // very large ones would pin too much host memory.
+    if (total < (16ull << 20) || total > (256ull << 20)) {
         for (auto &pt : parts)
             if (pt.second.second)
                 CK(cudaMemcpyAsync(pt.first, pt.second.first, pt.second.second, cudaMemcpyHostToDevice, ctx->stream));
@@ -322,7 +324,7 @@ static int stage_upload(cpm_ctx *ctx, const std::vector<std::pair<void *, std::p
         unsigned char *dst = static_cast<unsigned char *>(ctx->pinned) + at;
         const unsigned char *src = static_cast<const unsigned char *>(pt.second.first);
         const size_t n = pt.second.second, chunk = 1u << 20;
-#pragma omp parallel for schedule(static) if (n > (4u << 20))
+#pragma omp parallel for schedule(static) if (n > (1u << 20))
         for (int64_t c = 0; c < (int64_t)((n + chunk - 1) / chunk); ++c)
             memcpy(dst + c * chunk, src + c * chunk, std::min(chunk, n - c * chunk));
         if (n) CK(cudaMemcpyAsync(pt.first, dst, n, cudaMemcpyHostToDevice, ctx->stream));
