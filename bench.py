@@ -439,6 +439,9 @@ def main():
     e2e_v = statistics.mean(e2e)
     if pg:
         value, e2e_v = max_over_ranks([value, e2e_v], "cuda")
+        # The last collective: rank 0's baselines below run on its own, so no
+        # rank waits on a barrier while they do.
+        pg.destroy_process_group()
     # Roofline of the deep-level intersection kernel (k_deep), the step's
     # dominant kernel on Eclat workloads, from its own CUDA events.
     hbm, bf16, src = peaks()
@@ -465,9 +468,6 @@ def main():
             "frac": gram_tops / int8_peak if int8_peak else None,
             "ops": "2*128*256*K per issued tile (full tiles of the upper triangle)"}
     if rank != 0:
-        if pg:
-            pg.barrier()
-            pg.destroy_process_group()
         return
     ref_gpu_leg = None
     if not args.no_ref_gpu:
@@ -503,9 +503,6 @@ def main():
         "kernel_stats": last_stats,
     }
     print(json.dumps(line), flush=True)
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
 
 
 if __name__ == "__main__":
