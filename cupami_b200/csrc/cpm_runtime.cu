@@ -29,6 +29,7 @@
 #include <unordered_set>
 #include <vector>
 #include <map>
+#include <memory>
 #include <array>
 #include <chrono>
 #include <cstdlib>
@@ -2036,7 +2037,20 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
     if (order != CPM_ORDER_ECLAT && order != CPM_ORDER_APRIORI && order != CPM_ORDER_NONE) return CPM_EINVAL;
     const uint64_t n = res->parent.size();
     const uint32_t *par = res->parent.data(), *itm = res->item.data();
-    std::vector<uint32_t> depth(n);
+    const bool dbg = getenv("CPM_DEBUG") != nullptr;
+    auto t0 = std::chrono::steady_clock::now();
+    auto lap = [&](const char *what) {
+        if (!dbg) return;
+        const auto now = std::chrono::steady_clock::now();
+        fprintf(stderr, "cpm: order %-16s %.3f ms\n", what, std::chrono::duration<double, std::milli>(now - t0).count());
+        t0 = now;
+    };
+    // Scratch kept per thread across calls: large fresh allocations cost a
+    // page fault per 4 KB on first touch, which dominated this function.
+    static thread_local std::vector<uint32_t> depth_s;
+    static thread_local std::vector<uint64_t> idx_s, coff_s, kids_s, fill_s;
+    if (depth_s.size() < n) depth_s.resize(n);
+    uint32_t *depth = depth_s.data();
     for (uint64_t k = 0; k < n; ++k) {
         const uint32_t p = par[k];
         if (p != 0xffffffffu && p >= k) return CPM_EINTERNAL;
@@ -2045,26 +2059,36 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
     bool prefix_tree = true;
     for (uint64_t k = 0; k < n && prefix_tree; ++k)
         if (par[k] != 0xffffffffu && itm[k] <= itm[par[k]]) prefix_tree = false;
-    std::vector<uint64_t> idx(n);
-    std::iota(idx.begin(), idx.end(), 0ull);
+    lap("depth, check");
+    if (idx_s.size() < n) idx_s.resize(n);
+    uint64_t *idx = idx_s.data();
+    std::iota(idx, idx + n, 0ull);
     std::vector<uint64_t> start;  // item lists in device order (only for non-prefix trees)
     std::vector<uint32_t> flat;
     auto pat = [&](uint64_t k) { return flat.data() + start[k]; };
     if (prefix_tree && order != CPM_ORDER_NONE) {
         // children lists (counting sort by parent), each sorted by item
-        std::vector<uint64_t> coff(n + 2, 0), roots;
+        if (coff_s.size() < n + 2) coff_s.resize(n + 2);
+        uint64_t *coff = coff_s.data();
+        std::fill(coff, coff + n + 2, 0ull);
+        std::vector<uint64_t> roots;
         for (uint64_t k = 0; k < n; ++k)
             if (par[k] == 0xffffffffu) roots.push_back(k);
             else coff[par[k] + 1]++;
         for (uint64_t k = 0; k < n; ++k) coff[k + 1] += coff[k];
-        std::vector<uint64_t> kids(coff[n]), fill(coff.begin(), coff.begin() + n);
+        if (kids_s.size() < coff[n] + 1) kids_s.resize(coff[n] + 1);
+        if (fill_s.size() < n + 1) fill_s.resize(n + 1);
+        uint64_t *kids = kids_s.data(), *fill = fill_s.data();
+        std::copy(coff, coff + n, fill);
         for (uint64_t k = 0; k < n; ++k)
             if (par[k] != 0xffffffffu) kids[fill[par[k]]++] = k;
+        lap("children");
         auto by_item = [&](uint64_t a, uint64_t b) { return itm[a] < itm[b]; };
         std::sort(roots.begin(), roots.end(), by_item);
 #pragma omp parallel for schedule(dynamic, 4096)
         for (int64_t k = 0; k < (int64_t)n; ++k)
-            if (coff[k + 1] - coff[k] > 1) std::sort(kids.begin() + coff[k], kids.begin() + coff[k + 1], by_item);
+            if (coff[k + 1] - coff[k] > 1) std::sort(kids + coff[k], kids + coff[k + 1], by_item);
+        lap("sort children");
         uint64_t w = 0;
         if (order == CPM_ORDER_APRIORI) {
             // by length, then tuple: breadth first, children in item order
@@ -2073,7 +2097,7 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
                 next.clear();
                 for (uint64_t v : level) {
                     idx[w++] = v;
-                    next.insert(next.end(), kids.begin() + coff[v], kids.begin() + coff[v + 1]);
+                    next.insert(next.end(), kids + coff[v], kids + coff[v + 1]);
                 }
                 level.swap(next);
             }
@@ -2117,14 +2141,14 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
             for (uint32_t i = d - 1; i > 0 && a[i] < a[i - 1]; --i) std::swap(a[i], a[i - 1]);
         }
         if (order == CPM_ORDER_APRIORI) {
-            std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+            std::sort(idx, idx + n, [&](uint64_t a, uint64_t b) {
                 if (depth[a] != depth[b]) return depth[a] < depth[b];
                 return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
             });
         } else if (order == CPM_ORDER_ECLAT) {
             // cuEclat inserts singletons, then pairs, then every deeper pattern in
             // the order of its class search: key (x1..x_{k-1}, -1, x_k).
-            std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+            std::sort(idx, idx + n, [&](uint64_t a, uint64_t b) {
                 const uint32_t ga = std::min<uint32_t>(depth[a], 3), gb = std::min<uint32_t>(depth[b], 3);
                 if (ga != gb) return ga < gb;
                 if (ga < 3) return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
@@ -2139,8 +2163,10 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
             });
         }
     }
+    lap("order");
     offsets[0] = 0;
     for (uint64_t r = 0; r < n; ++r) offsets[r + 1] = offsets[r] + depth[idx[r]];
+    lap("offsets");
 #pragma omp parallel for schedule(static, 65536)
     for (int64_t r = 0; r < (int64_t)n; ++r) {
         const uint64_t k = idx[r];
@@ -2155,6 +2181,7 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
             for (uint32_t i = depth[k]; i-- > 0; v = par[v]) a[i] = itm[v];
         }
     }
+    lap("items");
     return CPM_OK;
 }
 
