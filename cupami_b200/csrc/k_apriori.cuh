@@ -5,7 +5,7 @@
 // that share their first k-1 items (cuApriori.py:482-487) and survive only if
 // every k-subset is in the level (:488-490); the join runs in row order, so the
 // candidate list comes out sorted, as the reference's sorted(candidates).
-// Supports are complete intersections of the original tidsets (k_count_kway).
+// Supports are complete intersections of the original tidsets (k_count_pruned).
 #pragma once
 #include "common.cuh"
 
@@ -26,45 +26,6 @@ __device__ bool level_has(const uint32_t *L, uint64_t n, uint32_t k, const uint3
         if (c < 0) lo = mid + 1; else hi = mid;
     }
     return false;
-}
-
-// Joins row a with every later row b of its prefix group; counts (mode 0) or
-// writes (mode 1) the candidates whose k-subsets are all frequent.
-template <int MODE>
-__global__ void k_apriori_join(const uint32_t *__restrict__ L, uint64_t n, uint32_t k,
-                               uint32_t *__restrict__ cnt, const uint64_t *__restrict__ off,
-                               uint32_t *__restrict__ cand, uint32_t *__restrict__ cand_left) {
-    const uint64_t a = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= n) return;
-    const uint32_t *ra = L + a * k;
-    uint32_t sub[64];
-    uint32_t c = 0;
-    uint64_t pos = MODE ? off[a] : 0;
-    for (uint64_t b = a + 1; b < n; ++b) {
-        const uint32_t *rb = L + b * k;
-        if (cmp_rows(ra, rb, k - 1)) break;
-        const uint32_t last = rb[k - 1];
-        bool ok = true;
-        // Dropping item k-1 or k gives rows b or a, which are in the level.
-        for (uint32_t drop = 0; drop + 1 < k && ok; ++drop) {
-            uint32_t t = 0;
-            for (uint32_t i = 0; i < k; ++i)
-                if (i != drop) sub[t++] = ra[i];
-            sub[t] = last;
-            ok = level_has(L, n, k, sub);
-        }
-        if (!ok) continue;
-        if (MODE) {
-            uint32_t *dst = cand + pos * (k + 1);
-            for (uint32_t i = 0; i < k; ++i) dst[i] = ra[i];
-            dst[k] = last;
-            cand_left[pos] = (uint32_t)a;
-            ++pos;
-        } else {
-            ++c;
-        }
-    }
-    if (!MODE) cnt[a] = c;
 }
 
 // Row a starts a prefix group when its first k-1 items differ from row a-1.
@@ -150,13 +111,6 @@ __global__ void k_count_pruned(const uint64_t *__restrict__ bits, uint64_t strid
         support[warp] = s;
         pass[warp] = (long long)s >= minsup ? 1u : 0u;
     }
-}
-
-// flag[c] = support passes (as 0/1 for the scan).
-__global__ void k_apriori_flags(const uint32_t *__restrict__ sup, uint64_t n, long long minsup,
-                                uint32_t *__restrict__ flag) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) flag[i] = (long long)sup[i] >= minsup;
 }
 
 // Survivors, in candidate order, become the next level and pattern records.

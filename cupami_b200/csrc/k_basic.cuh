@@ -119,26 +119,6 @@ __global__ void k_emit_singletons(const uint32_t *__restrict__ freq, uint32_t F,
     pat_sup[i] = support[freq[i]];
 }
 
-// k-way complete intersection (GPApriori counting, _bitsets.py:30-53): one
-// warp per candidate, candidate c = rows cand[c*width .. +width).
-__global__ void k_count_kway(const uint64_t *__restrict__ bits, uint64_t stride,
-                             const uint32_t *__restrict__ cand, uint64_t n, uint32_t width,
-                             uint32_t *__restrict__ support) {
-    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const unsigned lane = threadIdx.x & 31;
-    if (warp >= n) return;
-    const uint32_t *cc = cand + warp * width;
-    uint32_t s = 0;
-    for (uint64_t v = lane; v < stride / 2; v += 32) {
-        ulonglong2 acc = make_ulonglong2(~0ull, ~0ull);
-        for (uint32_t j = 0; j < width; ++j)
-            acc = and2(acc, ld_stream(reinterpret_cast<const ulonglong2 *>(bits + (uint64_t)cc[j] * stride) + v));
-        s += popc2(acc);
-    }
-    s = warp_sum_u32(s);
-    if (!lane) support[warp] = s;
-}
-
 // ---- reference kernel-module API (32-bit word layout of _bitsets.py) ------
 
 __global__ void k_ref_build(const uint64_t *__restrict__ rows, const uint32_t *__restrict__ cols,

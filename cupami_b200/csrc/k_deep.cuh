@@ -168,10 +168,6 @@ __device__ int deep_claim(const DeepParams &P, unsigned long long *item) {
     return 1;
 }
 
-__device__ __forceinline__ const ulonglong2 *ld_ptr(const uint64_t *const *p) {
-    return reinterpret_cast<const ulonglong2 *>(__ldcg(reinterpret_cast<const unsigned long long *>(p)));
-}
-
 // This lane's share of |prefix & sibling| over part `part` of `parts` equal
 // slices of the sibling (dense words or list ids); *bytes gets the sibling's
 // size in its own form.  Eight 16-byte loads in flight per lane.
