@@ -1786,9 +1786,16 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
         CK(cudaGetLastError());
         st.kernel_launches++;
         n_pat += P2;
-        uint64_t n = P2;
+        // Row and pattern counts stay on the device (d_cnt2[0], d_cnt2[1]);
+        // the host keeps upper bounds (n_ub, pat_ub) for grids and buffers
+        // and learns the true counts with each level's one round trip.
+        uint64_t *d_cnt2 = nullptr;
+        CKR(ds.alloc(&d_cnt2, 2));
+        k_set_u64x2<<<1, 1, 0, ctx->stream>>>(d_cnt2, P2, d_cnt2 + 1, n_pat);
+        CK(cudaGetLastError());
+        uint64_t n_ub = P2, pat_ub = n_pat;
         uint32_t k = 2;
-        while (n >= 2) {
+        while (n_ub >= 2) {
             if (k + 1 > 64) {
                 dfree(ctx, L);
                 dfree(ctx, pid);
@@ -1799,21 +1806,24 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
             // Prefix groups and join partners of every row.
             uint32_t *gflag = nullptr, *partners = nullptr;
             uint64_t *gid = nullptr, *gfirst = nullptr, *poff = nullptr;
-            CKR(lvl.alloc(&gflag, n));
-            CKR(lvl.alloc(&gid, n));
-            CKR(lvl.alloc(&partners, n));
-            CKR(lvl.alloc(&poff, n));
-            const unsigned nb = (unsigned)((n + 255) / 256);
-            k_group_start<<<nb, 256, 0, ctx->stream>>>(L, n, k, gflag);
+            CKR(lvl.alloc(&gflag, n_ub));
+            CKR(lvl.alloc(&gid, n_ub));
+            CKR(lvl.alloc(&partners, n_ub));
+            CKR(lvl.alloc(&poff, n_ub));
+            CKR(lvl.alloc(&gfirst, n_ub + 1));
+            const unsigned nb = (unsigned)((n_ub + 255) / 256);
+            k_group_start<<<nb, 256, 0, ctx->stream>>>(L, n_ub, d_cnt2, k, gflag);
             CK(cudaGetLastError());
-            CKR(scan_u32(ctx, lvl, gflag, gid, n, nullptr));
-            CKR(lvl.alloc(&gfirst, n + 1));
-            k_group_first<<<nb, 256, 0, ctx->stream>>>(gflag, gid, n, gfirst);
+            CKR(scan_u32(ctx, lvl, gflag, gid, n_ub, nullptr));
+            k_group_first<<<nb, 256, 0, ctx->stream>>>(gflag, gid, d_cnt2, gfirst);
             CK(cudaGetLastError());
-            k_partners<<<nb, 256, 0, ctx->stream>>>(gflag, gid, gfirst, n, partners);
+            k_partners<<<nb, 256, 0, ctx->stream>>>(gflag, gid, gfirst, n_ub, d_cnt2, partners);
             CK(cudaGetLastError());
+            uint64_t counts[2] = {0, 0};
+            CK(cudaMemcpyAsync(counts, d_cnt2, 16, cudaMemcpyDeviceToHost, ctx->stream));
             uint64_t n_pairs = 0;
-            CKR(scan_u32(ctx, lvl, partners, poff, n, &n_pairs));
+            CKR(scan_u32(ctx, lvl, partners, poff, n_ub, &n_pairs));  // synchronises: counts are in
+            n_pat = counts[1];
             st.kernel_launches += 7;
             if (!n_pairs) break;
             // Join, prune, count, keep.
@@ -1825,35 +1835,39 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
             CKR(lvl.alloc(&sup, n_pairs));
             CKR(lvl.alloc(&pass, n_pairs));
             CKR(lvl.alloc(&pos, n_pairs));
-            k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, n, k, poff, n_pairs, cand,
-                                                                                     left, okf);
+            k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, n_ub, k, poff, n_pairs,
+                                                                                     cand, left, okf);
             CK(cudaGetLastError());
             k_count_pruned<<<(unsigned)((n_pairs * 32 + 255) / 256), 256, 0, ctx->stream>>>(
                 db->d_bits, db->stride, cand, okf, n_pairs, w, ms, sup, pass);
             CK(cudaGetLastError());
-            uint64_t nk = 0;
-            CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, &nk));
+            CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, nullptr));
             st.kernel_launches += 4;
             st.intersections += n_pairs * (w - 1);
             st.bytes_alg += n_pairs * w * db->stride * 8;
+            // Survivors: at most n_pairs rows and patterns.
             uint32_t *L2 = nullptr, *pid2 = nullptr;
-            CKR(patterns_reserve(ctx, pa, n_pat, n_pat + nk));
-            CKR(dalloc(ctx, &L2, std::max<uint64_t>(1, nk) * w));
-            CKR(dalloc(ctx, &pid2, std::max<uint64_t>(1, nk)));
-            if (nk) {
-                k_apriori_keep<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(
-                    cand, left, sup, pass, pos, n_pairs, w, pid, n_pat, L2, pid2, pa.parent, pa.item, pa.sup);
-                CK(cudaGetLastError());
-                st.kernel_launches++;
-            }
+            CKR(patterns_reserve(ctx, pa, n_pat, pat_ub + n_pairs));
+            CKR(dalloc(ctx, &L2, n_pairs * w));
+            CKR(dalloc(ctx, &pid2, n_pairs));
+            k_apriori_keep<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(
+                cand, left, sup, pass, pos, n_pairs, w, pid, d_cnt2 + 1, L2, pid2, pa.parent, pa.item, pa.sup);
+            CK(cudaGetLastError());
+            k_level_close<<<1, 1, 0, ctx->stream>>>(pos, pass, n_pairs, d_cnt2, d_cnt2 + 1);
+            CK(cudaGetLastError());
+            st.kernel_launches += 2;
             dfree(ctx, L);
             dfree(ctx, pid);
             L = L2;
             pid = pid2;
-            n_pat += nk;
-            n = nk;
+            pat_ub += n_pairs;
+            n_ub = n_pairs;
             k = w;
         }
+        uint64_t final_pat = 0;
+        CK(cudaMemcpyAsync(&final_pat, d_cnt2 + 1, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        n_pat = final_pat;
         dfree(ctx, L);
         dfree(ctx, pid);
     }

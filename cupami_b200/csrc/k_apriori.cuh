@@ -29,26 +29,38 @@ __device__ bool level_has(const uint32_t *L, uint64_t n, uint32_t k, const uint3
 }
 
 // Row a starts a prefix group when its first k-1 items differ from row a-1.
-__global__ void k_group_start(const uint32_t *__restrict__ L, uint64_t n, uint32_t k, uint32_t *__restrict__ flag) {
+// Levels run with their row count on the device (*d_n) and grids sized by an
+// upper bound n_ub on the host, so that no level waits for its own count:
+// rows at or past *d_n flag nothing and have no partners.
+__global__ void k_group_start(const uint32_t *__restrict__ L, uint64_t n_ub, const uint64_t *__restrict__ d_n,
+                              uint32_t k, uint32_t *__restrict__ flag) {
     const uint64_t a = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (a < n) flag[a] = (a == 0 || cmp_rows(L + (a - 1) * k, L + a * k, k - 1)) ? 1u : 0u;
+    if (a >= n_ub) return;
+    const uint64_t n = *d_n;
+    flag[a] = a < n && (a == 0 || cmp_rows(L + (a - 1) * k, L + a * k, k - 1)) ? 1u : 0u;
 }
 
 // Exclusive group-start scan -> each group's first row (gfirst[g]) and, per
 // row, the number of later rows of its group (its join partners).
 // gfirst[g] = first row of group g; the entry after the last group holds n,
 // so a row's group always ends at gfirst[g + 1] (gfirst has n + 1 entries).
-__global__ void k_group_first(const uint32_t *__restrict__ flag, const uint64_t *__restrict__ gid_excl, uint64_t n,
-                              uint64_t *__restrict__ gfirst) {
+__global__ void k_group_first(const uint32_t *__restrict__ flag, const uint64_t *__restrict__ gid_excl,
+                              const uint64_t *__restrict__ d_n, uint64_t *__restrict__ gfirst) {
     const uint64_t a = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t n = *d_n;
     if (a < n && flag[a]) gfirst[gid_excl[a]] = a;
     if (a + 1 == n) gfirst[gid_excl[a] + flag[a]] = n;
 }
 
 __global__ void k_partners(const uint32_t *__restrict__ flag, const uint64_t *__restrict__ gid_excl,
-                           const uint64_t *__restrict__ gfirst, uint64_t n, uint32_t *__restrict__ partners) {
+                           const uint64_t *__restrict__ gfirst, uint64_t n_ub, const uint64_t *__restrict__ d_n,
+                           uint32_t *__restrict__ partners) {
     const uint64_t a = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= n) return;
+    if (a >= n_ub) return;
+    if (a >= *d_n) {
+        partners[a] = 0;
+        return;
+    }
     const uint64_t g = gid_excl[a] + flag[a] - 1;  // this row's group
     partners[a] = (uint32_t)(gfirst[g + 1] - a - 1);
 }
@@ -117,7 +129,7 @@ __global__ void k_count_pruned(const uint64_t *__restrict__ bits, uint64_t strid
 __global__ void k_apriori_keep(const uint32_t *__restrict__ cand, const uint32_t *__restrict__ cand_left,
                                const uint32_t *__restrict__ sup, const uint32_t *__restrict__ flag,
                                const uint64_t *__restrict__ pos, uint64_t n, uint32_t w,
-                               const uint32_t *__restrict__ pid_prev, uint64_t pid_base,
+                               const uint32_t *__restrict__ pid_prev, const uint64_t *__restrict__ d_pid_base,
                                uint32_t *__restrict__ L_next, uint32_t *__restrict__ pid_next,
                                uint32_t *__restrict__ pat_parent, uint32_t *__restrict__ pat_item,
                                uint32_t *__restrict__ pat_sup) {
@@ -125,11 +137,27 @@ __global__ void k_apriori_keep(const uint32_t *__restrict__ cand, const uint32_t
     if (i >= n || !flag[i]) return;
     const uint64_t p = pos[i];
     for (uint32_t j = 0; j < w; ++j) L_next[p * w + j] = cand[i * w + j];
-    const uint64_t pid = pid_base + p;
+    const uint64_t pid = *d_pid_base + p;
     pid_next[p] = (uint32_t)pid;
     pat_parent[pid] = pid_prev[cand_left[i]];
     pat_item[pid] = cand[i * w + w - 1];
     pat_sup[pid] = sup[i];
+}
+
+// The level's survivors (exclusive scan pos of pass flags): the next level's
+// row count, and the pattern count moved past them.
+__global__ void k_level_close(const uint64_t *__restrict__ pos, const uint32_t *__restrict__ pass, uint64_t n_pairs,
+                              uint64_t *__restrict__ d_n, uint64_t *__restrict__ d_npat) {
+    if (blockIdx.x || threadIdx.x) return;
+    const uint64_t nk = n_pairs ? pos[n_pairs - 1] + pass[n_pairs - 1] : 0;
+    *d_n = nk;
+    *d_npat += nk;
+}
+
+__global__ void k_set_u64x2(uint64_t *__restrict__ a, uint64_t va, uint64_t *__restrict__ b, uint64_t vb) {
+    if (blockIdx.x || threadIdx.x) return;
+    *a = va;
+    *b = vb;
 }
 
 // Level 2 from the pair Gram: rows (f_i, f_j) in (i, j) order with pattern ids.
