@@ -1835,7 +1835,7 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
             CKR(lvl.alloc(&sup, n_pairs));
             CKR(lvl.alloc(&pass, n_pairs));
             CKR(lvl.alloc(&pos, n_pairs));
-            k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, n_ub, k, poff, n_pairs,
+            k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, d_cnt2, k, poff, n_pairs,
                                                                                      cand, left, okf);
             CK(cudaGetLastError());
             k_count_pruned<<<(unsigned)((n_pairs * 32 + 255) / 256), 256, 0, ctx->stream>>>(

@@ -68,11 +68,14 @@ __global__ void k_partners(const uint32_t *__restrict__ flag, const uint64_t *__
 // One thread per join pair t: row a = last row with poff[a] <= t, partner
 // b = a + 1 + t - poff[a].  Writes the candidate and whether every k-subset
 // is frequent (cuApriori.py:488-490).
-__global__ void k_join_pairs(const uint32_t *__restrict__ L, uint64_t n, uint32_t k,
+// The level's rows are L[0, *d_n): the subset searches must not see the
+// rows past them (left over in a buffer sized by an upper bound).
+__global__ void k_join_pairs(const uint32_t *__restrict__ L, const uint64_t *__restrict__ d_n, uint32_t k,
                              const uint64_t *__restrict__ poff, uint64_t n_pairs, uint32_t *__restrict__ cand,
                              uint32_t *__restrict__ cand_left, uint32_t *__restrict__ ok_flag) {
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_pairs) return;
+    const uint64_t n = *d_n;
     uint64_t lo = 0, hi = n;  // upper_bound(poff, t) - 1
     while (lo < hi) {
         const uint64_t mid = (lo + hi) >> 1;
