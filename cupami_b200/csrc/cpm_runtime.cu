@@ -1375,13 +1375,12 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     const uint64_t spin = o.spin_limit ? o.spin_limit : (1ull << 26);
     const size_t prefix_bytes = max_stride * 8;
     const bool smem_prefix = prefix_bytes <= 200 * 1024;
-    // Long tidsets leave room for one CTA per SM: give it 16 or 32 warps so
-    // that enough loads stay in flight; short ones run up to four 8-warp CTAs.
-    // A search with few root units per CTA slot is bound by its chains of
-    // dependent units: 16-warp CTAs finish each unit sooner (planted-100k:
-    // 0.25 ms against 0.32 ms with 8-warp CTAs).
-    unsigned block = max_stride >= 8192 ? 1024 : max_stride >= 2048 ? 512 : 256;
-    if (block == 256 && max_stride >= 1024 && n_units < (uint64_t)ctx->sms * 16) block = 512;
+    // Long tidsets leave room for fewer CTAs per SM: give each 16 or 32 warps
+    // so that enough loads stay in flight; short ones run up to four 8-warp
+    // CTAs.  Measured (deep phase): 1,564-word tidsets (planted-100k) 0.25 ms
+    // with 16-warp CTAs against 0.32 ms with 8-warp ones; 1,024-word tidsets
+    // (dense 65,536 x 128) 1.10 ms with 8-warp CTAs against 1.85 ms.
+    unsigned block = max_stride >= 8192 ? 1024 : max_stride >= 1536 ? 512 : 256;
     int want_ctas = 4;
     if (o.autotune) {
         const auto it = ctx->tune.find(63 - __builtin_clzll(std::max<uint64_t>(1, max_stride)));
