@@ -844,19 +844,22 @@ static int grow(cpm_ctx *ctx, DeepBuffers &b, uint64_t frames_cap, uint64_t memb
 // frame, kept in the persistent region, contributes its positions as new
 // root units, processed next (depth first, so the region stays small).
 static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::vector<DFrame> &top_frames,
-                           const uint32_t *d_uid, const float *d_key, uint64_t n_units, uint64_t P2_total,
+                           const uint32_t *d_uid, const float *d_key, const float *d_unit_key, uint64_t n_units,
+                           uint64_t P2_total,
                            uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix, uint64_t spin,
                            bool keys_in_words, uint32_t lists, const std::vector<unsigned long long> *cont,
                            uint64_t arena_words, uint64_t pat_cap, DeepState &hs, cpm_stats &st);
 
 static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::vector<DFrame> &top_frames,
-                       const uint32_t *d_uid, const float *d_key, uint64_t n_units, uint64_t base_patterns,
+                       const uint32_t *d_uid, const float *d_key, const float *d_unit_key, uint64_t n_units,
+                       uint64_t base_patterns,
                        uint64_t P2_total, uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix,
                        uint64_t spin,
                        uint64_t pat_need, bool with_db, uint64_t arena_limit_words, bool keys_in_words,
                        uint32_t lists, const std::vector<unsigned long long> *cont, DeepState &hs, cpm_stats &st) {
     const bool dbg = getenv("CPM_DEBUG") != nullptr;
-    if (cont) return deep_rounds_run(ctx, ds, b, top_frames, nullptr, nullptr, 0, P2_total, max_stride, grid, block,
+    if (cont) return deep_rounds_run(ctx, ds, b, top_frames, nullptr, nullptr, d_unit_key, 0, P2_total, max_stride,
+                                     grid, block,
                                      smem_prefix, spin, keys_in_words, lists, cont, b.arena_words, b.pat_cap, hs, st);
     // Fixed tables large enough for any round; the arena takes the rest.
     const uint64_t frames_cap = 32ull << 20, members_cap = 256ull << 20, queue_cap = 64ull << 20;
@@ -892,7 +895,8 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
                        ctx->stream));
     hs = DeepState{};
     hs.n_patterns = base_patterns;
-    return deep_rounds_run(ctx, ds, b, top_frames, d_uid, d_key, n_units, P2_total, max_stride, grid, block,
+    return deep_rounds_run(ctx, ds, b, top_frames, d_uid, d_key, d_unit_key, n_units, P2_total, max_stride, grid,
+                           block,
                            smem_prefix, spin, keys_in_words, lists, nullptr, arena_words, pat_cap, hs, st);
 }
 
@@ -901,7 +905,8 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
 // (cont): the root units a first launch deferred, in queue order, with the
 // top level and the patterns found so far (hs.n_patterns) kept in b.
 static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::vector<DFrame> &top_frames,
-                           const uint32_t *d_uid, const float *d_key, uint64_t n_units, uint64_t P2_total,
+                           const uint32_t *d_uid, const float *d_key, const float *d_unit_key, uint64_t n_units,
+                           uint64_t P2_total,
                            uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix, uint64_t spin,
                            bool keys_in_words, uint32_t lists, const std::vector<unsigned long long> *cont,
                            uint64_t arena_words, uint64_t pat_cap, DeepState &hs, cpm_stats &st) {
@@ -954,6 +959,7 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
     P.root_cost = nullptr; P.st = b.st; P.max_stride = max_stride; P.spin_limit = spin; P.cta_time = nullptr;
     P.lists = lists;
     P.root_frames = 0; P.defer_words = 0; P.defer_members = 0; P.defer_frames = 0; P.defer_queue = 0;
+    P.root_key = nullptr; P.top_frames = 0; P.keys_in_words = 0; P.admit_words = 0;
     P.deferred = nullptr; P.deferred_cap = 0;
     const size_t prefix_bytes = max_stride * 8;
     uint64_t rounds = 0, failed = 0, shallow = 0;
@@ -1002,6 +1008,7 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
     // A round that still overflows is discarded and retried with half the
     // units and half the fill level.
     double frac = 0.5;
+    double words_per_key = 0.0;  // largest arena words per admitted key unit seen in a round
     uint64_t deferred_total = 0;
     unsigned long long *d_deferred = nullptr;
     uint64_t deferred_cap = 0;
@@ -1013,6 +1020,15 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
             CKR(ds.alloc(&d_deferred, deferred_cap));
         }
         P.root_frames = (uint32_t)persist_frames;
+        P.root_key = d_unit_key;
+        P.top_frames = (uint32_t)top_frames.size();
+        P.keys_in_words = keys_in_words ? 1u : 0u;
+        // Admission budget in key units: 80% of the free arena over the
+        // arena words a key unit has cost so far (none before a round has run).
+        const uint64_t round_start_arena = persist_arena;
+        P.admit_words = words_per_key > 0
+                            ? (uint64_t)(0.8 * (double)(arena_words - persist_arena) / words_per_key)
+                            : 0ull;
         P.defer_words = persist_arena + std::max<uint64_t>(1, (uint64_t)(frac * (double)(arena_words - persist_arena)));
         P.defer_members = persist_members + (uint64_t)(frac * (double)(b.members_cap - persist_members));
         P.defer_frames = persist_frames + (uint64_t)(frac * (double)(b.frames_cap - persist_frames));
@@ -1048,6 +1064,9 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
             deferred_total += n_def;
             if (limit != ~0ull) limit *= 2;
             frac = std::min(0.5, frac * 1.25);
+            if (hs.admitted)
+                words_per_key = std::max(words_per_key,
+                                         (double)(hs.arena_next - round_start_arena) / (double)hs.admitted);
             continue;
         }
         if (hs.error & DEEP_ERR_SPIN) return set_err(ctx, CPM_ETIMEOUT, "deep-level kernel wait ran out of spins");
@@ -1076,6 +1095,7 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
         if (take > 1) {
             limit = std::max<size_t>(1, take / 2);
             frac = std::max(0.05, frac / 2);
+            words_per_key *= 2;  // the keys under-predicted this round's arena
             continue;
         }
         // One root unit whose subtree does not fit: expand it by one level.
@@ -1513,6 +1533,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         P.defer_queue = n_units + (b.queue_cap - n_units) / 4 * 3;
         P.deferred = d_deferred;
         P.deferred_cap = n_units;
+        P.root_key = nullptr; P.top_frames = 0; P.keys_in_words = 0; P.admit_words = 0;
         CK(cudaEventRecord(ctx->ev[2], ctx->stream));
         if (smem_prefix) k_deep<true><<<grid, block, prefix_bytes, ctx->stream>>>(P);
         else k_deep<false><<<grid, block, 0, ctx->stream>>>(P);
@@ -1584,12 +1605,13 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         st.intersections = hs.intersections;
         st.bytes_alg = hs.bytes_alg;
         st.work_items = hs.work_items;
-        CKR(deep_rounds(ctx, ds, b, frames, nullptr, nullptr, 0, base_patterns, P2_total, max_stride, grid, block,
+        CKR(deep_rounds(ctx, ds, b, frames, nullptr, nullptr, d_key, 0, base_patterns, P2_total, max_stride, grid, block,
                         smem_prefix, spin, 0, with_db, 0, learned, use_lists ? list_div : 0u, &cont, hs, st));
         rounds = continued = true;
         ++st.deep_rounds;  // the first launch
     } else if (rounds) {
-        CKR(deep_rounds(ctx, ds, b, frames, d_uid2, d_key2, n_units, base_patterns, P2_total, max_stride, grid, block,
+        CKR(deep_rounds(ctx, ds, b, frames, d_uid2, d_key2, d_key, n_units, base_patterns, P2_total, max_stride, grid,
+                        block,
                         smem_prefix, spin, pat_cap + base_patterns, with_db, o.arena_bytes ? o.arena_bytes / 8 : 0,
                         learned, use_lists ? list_div : 0u, nullptr, hs, st));
     }
@@ -2656,6 +2678,7 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     P.shallow = 0;
     P.lists = 0;
     P.root_frames = 0; P.defer_words = 0; P.defer_members = 0; P.defer_frames = 0; P.defer_queue = 0;
+    P.root_key = nullptr; P.top_frames = 0; P.keys_in_words = 0; P.admit_words = 0;
     P.deferred = nullptr; P.deferred_cap = 0;
     // Each warp keeps one scratch tidset: leave at least half the arena to children.
     const size_t prefix_bytes = stride * 8;

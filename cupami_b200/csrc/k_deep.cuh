@@ -74,6 +74,7 @@ struct DeepState {
     CPM_LINE(work_items);
     CPM_LINE(survivors);
     CPM_LINE(n_deferred);   // root units handed back to the host (memory-bounded rounds)
+    CPM_LINE(admitted);     // predicted cost of the root units started (memory-bounded rounds)
     unsigned int error;
     unsigned int pad[31];
 };
@@ -100,6 +101,13 @@ struct DeepParams {
     unsigned long long defer_words, defer_members, defer_frames, defer_queue;
     unsigned long long *deferred;
     uint64_t deferred_cap;
+    // Admission by predicted size (rounds only): a root unit of a top-level
+    // frame (below top_frames) costs root_key[unit] (times the frame's stride
+    // when keys count members); a unit whose cost would take the round's sum
+    // past admit_words is handed back, unless it is the round's first.
+    const float *root_key;
+    uint32_t top_frames, keys_in_words;
+    unsigned long long admit_words;
 };
 
 // Child tidset form: a list when it takes at most 1/P.lists of the dense
@@ -260,10 +268,27 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         if (threadIdx.x == 0) {
             s_stop = deep_claim(P, &s_item);
             s_skip = 0;
-            if (!s_stop && P.defer_words && (uint32_t)(s_item >> 32) < P.root_frames &&
-                (ld_acquire_u64(&st->arena_next) >= P.defer_words ||
-                 ld_acquire_u64(&st->n_members) >= P.defer_members || ld_acquire_u64(&st->n_frames) >= P.defer_frames ||
-                 ld_acquire_u64(&st->q_tail) >= P.defer_queue)) {
+            bool hand_back = false;
+            if (!s_stop && P.defer_words && (uint32_t)(s_item >> 32) < P.root_frames) {
+                hand_back = ld_acquire_u64(&st->arena_next) >= P.defer_words ||
+                            ld_acquire_u64(&st->n_members) >= P.defer_members ||
+                            ld_acquire_u64(&st->n_frames) >= P.defer_frames ||
+                            ld_acquire_u64(&st->q_tail) >= P.defer_queue;
+                const uint32_t fid = (uint32_t)(s_item >> 32);
+                if (!hand_back && P.root_key && fid < P.top_frames) {
+                    const DFrame *f = P.frames + fid;
+                    const uint32_t unit = __ldcg(&f->root) + (uint32_t)s_item;
+                    const double k = (double)__ldg(P.root_key + unit);
+                    const unsigned long long w =
+                        1ull + (unsigned long long)(P.keys_in_words ? k : k * (double)__ldcg(&f->stride));
+                    const unsigned long long before = atomicAdd(&st->admitted, w);
+                    if (P.admit_words && before > 0 && before + w > P.admit_words) {
+                        atomicAdd(&st->admitted, 0ull - w);
+                        hand_back = true;
+                    }
+                }
+            }
+            if (hand_back) {
                 // The round's arena is filling up: leave this root unit to the next round.
                 const unsigned long long di = atomicAdd(&st->n_deferred, 1ull);
                 if (di < P.deferred_cap) P.deferred[di] = s_item;
