@@ -990,9 +990,16 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
         const float round_ms = (float)elapsed_ms(ctx, 2, 3);
         deep_ms += round_ms;
         if (dbg)
-            fprintf(stderr, "cpm: round %llu: %zu units, %.3f ms, %.3g bytes, %.0f GB/s, deferred %llu, error 0x%x\n",
+            fprintf(stderr, "cpm: round %llu: %zu units, %.3f ms, %.3g bytes, %.0f GB/s, deferred %llu, error 0x%x, "
+                    "admitted %llu of %llu, arena %llu (hand back at %llu), members %llu (%llu), frames %llu (%llu), "
+                    "queue %llu (%llu)\n",
                     (unsigned long long)rounds, n_take, round_ms, (double)hs.bytes_alg,
-                    round_ms > 0 ? hs.bytes_alg / (round_ms * 1e6) : 0.0, (unsigned long long)hs.n_deferred, hs.error);
+                    round_ms > 0 ? hs.bytes_alg / (round_ms * 1e6) : 0.0, (unsigned long long)hs.n_deferred, hs.error,
+                    (unsigned long long)hs.admitted, (unsigned long long)P.admit_words,
+                    (unsigned long long)hs.arena_next, (unsigned long long)P.defer_words,
+                    (unsigned long long)hs.n_members, (unsigned long long)P.defer_members,
+                    (unsigned long long)hs.n_frames, (unsigned long long)P.defer_frames,
+                    (unsigned long long)hs.q_tail, (unsigned long long)P.defer_queue);
         st.kernel_launches++;
         if (!hs.error) {  // a discarded round's work is not counted (its time is)
             st.intersections += hs.intersections;
@@ -1008,7 +1015,7 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
     // A round that still overflows is discarded and retried with half the
     // units and half the fill level.
     double frac = 0.5;
-    double words_per_key = 0.0;  // largest arena words per admitted key unit seen in a round
+    double words_per_key = 0.0;  // arena words per admitted key unit (0: not known yet)
     uint64_t deferred_total = 0;
     unsigned long long *d_deferred = nullptr;
     uint64_t deferred_cap = 0;
@@ -1062,10 +1069,12 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
                 kept.pop_back();
             }
             deferred_total += n_def;
-            if (limit != ~0ull) limit *= 2;
+            if (limit != ~0ull) limit = limit >= (1ull << 40) ? ~0ull : limit * 2;  // saturating
             frac = std::min(0.5, frac * 1.25);
+            // Arena words per admitted key unit: follow a round that used
+            // more at once, decay slowly after rounds that used less.
             if (hs.admitted)
-                words_per_key = std::max(words_per_key,
+                words_per_key = std::max(0.7 * words_per_key,
                                          (double)(hs.arena_next - round_start_arena) / (double)hs.admitted);
             continue;
         }
