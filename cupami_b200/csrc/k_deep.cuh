@@ -189,27 +189,20 @@ __device__ __forceinline__ uint32_t sibling_count(unsigned long long sraw, uint3
         // List sibling: test its ids against the prefix bitmap.
         const uint32_t *L = reinterpret_cast<const uint32_t *>(sraw & ~1ull);
         const uint32_t n = __ldcg(L);
-        const uint4 *T = reinterpret_cast<const uint4 *>(L + 4);
-        const uint32_t nv = (n + 3) / 4, nfull = n / 4;
-        const uint32_t lo = (uint32_t)((uint64_t)nv * part / parts), hi = (uint32_t)((uint64_t)nv * (part + 1) / parts);
-        const uint32_t hi_full = min(hi, nfull);
+        // Lanes take consecutive ids (32 per warp load, sixteen loads in
+        // flight per lane), so the bit tests of one instruction fall in
+        // nearby, mostly distinct shared-memory banks.
+        const uint32_t *I = L + 4;
+        const uint32_t lo = (uint32_t)((uint64_t)n * part / parts), hi = (uint32_t)((uint64_t)n * (part + 1) / parts);
         uint32_t w = lo + lane;
-        for (; w + 224 < hi_full; w += 256) {  // eight complete groups of four ids
-            uint4 t[8];
+        for (; w + 480 < hi; w += 512) {
+            uint32_t t[16];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) t[u] = __ldcg(T + w + 32 * u);
+            for (int u = 0; u < 16; ++u) t[u] = __ldcg(I + w + 32 * u);
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
-                s += bit_of(s_p32, t[u].x) + bit_of(s_p32, t[u].y) + bit_of(s_p32, t[u].z) + bit_of(s_p32, t[u].w);
+            for (int u = 0; u < 16; ++u) s += bit_of(s_p32, t[u]);
         }
-        for (; w < hi; w += 32) {
-            const uint4 t = __ldcg(T + w);
-            const uint32_t i0 = 4 * w;
-            s += bit_of(s_p32, t.x);
-            if (i0 + 1 < n) s += bit_of(s_p32, t.y);
-            if (i0 + 2 < n) s += bit_of(s_p32, t.z);
-            if (i0 + 3 < n) s += bit_of(s_p32, t.w);
-        }
+        for (; w < hi; w += 32) s += bit_of(s_p32, __ldcg(I + w));
         *bytes = 8ull * list_words(n);
         return s;
     }
