@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     __shared__ uint64_t s_w64[32];
     __shared__ uint64_t s_off[1024];     // child offsets of one chunk of survivors
     __shared__ unsigned long long s_bytes;
+    __shared__ uint32_t s_nsurv;         // survivors counted in pass 1
     __shared__ uint32_t s_part[32];      // per-sibling sums when siblings are split over warps
     uint32_t *const s_p32 = reinterpret_cast<uint32_t *>(s_prefix);
 
@@ -335,6 +336,8 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         if (threadIdx.x == 0) {
             s_bytes = prefix_bytes;
             s_surv = 0;
+            s_nsurv = 0;
+            s_grant = 0;
             const unsigned long long mb = atomicAdd(&st->n_members, (unsigned long long)cnt);
             if (mb + cnt > P.members_cap) deep_fail(st, DEEP_ERR_MEMBERS);
             s_mem_base = mb;
@@ -366,6 +369,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 P.mem_item[m_out] = sib_item;
                 P.mem_bits[m_out] = reinterpret_cast<const uint64_t *>(sraw);
             }
+            if (pid32 != NO_PATTERN) atomicAdd(&s_nsurv, 1u);
         };
         // Fewer siblings than warps: split every sibling into equal slices
         // (at least 4 KB of bitset each) so that every warp has work.
@@ -404,6 +408,21 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             }
         }
         __syncthreads();
+        if (s_nsurv < 2) {
+            // No child frame (the common case): nothing to compact, write or
+            // publish, so the unit ends here without further barriers.
+            if (threadIdx.x == 0) {
+                c_inter += cnt;
+                c_bytes += s_bytes;
+                c_units += 1;
+                c_surv += s_nsurv;
+                if (P.root_cost) atomicAdd(P.root_cost + root, (unsigned long long)cnt);
+                if (P.cta_time) c_busy += global_ns() - t_unit;
+                __threadfence();
+                atomicAdd(&st->pending, ~0ull);  // pending -= 1
+            }
+            continue;
+        }
         // Survivors move to the front of the block in member order, so every
         // child frame keeps its members sorted by column (the pattern tree is
         // then a prefix tree: a pattern's parent is itself minus its last item).
