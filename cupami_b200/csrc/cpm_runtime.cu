@@ -1722,6 +1722,18 @@ struct U32ToU64 {
 static int scan_u32(cpm_ctx *ctx, DevScope &ds, const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *total) {
     if (total) *total = 0;
     if (!n) return CPM_OK;
+    if (n <= 32768) {
+        // Small scans (most Apriori levels): one single-block launch instead
+        // of CUB's two.
+        uint64_t *d_tot = nullptr;
+        CKR(ds.alloc(&d_tot, 1));
+        k_scan_u32<<<1, 1024, 0, ctx->stream>>>(in, n, out, d_tot);
+        CK(cudaGetLastError());
+        if (!total) return CPM_OK;
+        CK(cudaMemcpyAsync(total, d_tot, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        return CPM_OK;
+    }
     thrust::transform_iterator<U32ToU64, const uint32_t *, uint64_t> it(in, U32ToU64());
     size_t bytes = 0;
     CK(cub::DeviceScan::ExclusiveSum(nullptr, bytes, it, out, (int64_t)n, ctx->stream));
