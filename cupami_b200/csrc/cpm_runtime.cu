@@ -1719,14 +1719,14 @@ struct U32ToU64 {
 
 // Exclusive sum of n counts into out; with total, also its sum (one
 // device-to-host copy and a sync), without it nothing leaves the device.
-static int scan_u32(cpm_ctx *ctx, DevScope &ds, const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *total) {
+static int scan_u32(cpm_ctx *ctx, DevScope &ds, const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *total,
+                    uint64_t *d_tot = nullptr) {
     if (total) *total = 0;
     if (!n) return CPM_OK;
     if (n <= 32768) {
         // Small scans (most Apriori levels): one single-block launch instead
         // of CUB's two.
-        uint64_t *d_tot = nullptr;
-        CKR(ds.alloc(&d_tot, 1));
+        if (!d_tot) CKR(ds.alloc(&d_tot, 1));
         k_scan_u32<<<1, 1024, 0, ctx->stream>>>(in, n, out, d_tot);
         CK(cudaGetLastError());
         if (!total) return CPM_OK;
@@ -1777,6 +1777,34 @@ static int patterns_reserve(cpm_ctx *ctx, PatternArrays &pa, uint64_t used, uint
     pa = nw;
     return CPM_OK;
 }
+
+// Grow-only device buffers reused from one Apriori level to the next (one
+// slot per array; freed when the mine ends): levels are small and many, and
+// allocating every array per level cost more host time than their kernels.
+struct LevelScratch {
+    cpm_ctx *ctx;
+    std::vector<std::pair<void *, size_t>> bufs;  // (pointer, bytes)
+    explicit LevelScratch(cpm_ctx *c) : ctx(c) {}
+    ~LevelScratch() {
+        for (auto &b : bufs)
+            if (b.first) cudaFreeAsync(b.first, ctx->stream);
+    }
+    template <class T>
+    int get(size_t slot, T **p, size_t count) {
+        if (bufs.size() <= slot) bufs.resize(slot + 1, {nullptr, 0});
+        const size_t bytes = std::max<size_t>(1, count) * sizeof(T);
+        if (bufs[slot].second < bytes) {
+            if (bufs[slot].first) cudaFreeAsync(bufs[slot].first, ctx->stream);
+            bufs[slot] = {nullptr, 0};
+            const size_t n = (bytes + bytes / 2) / sizeof(T) + 1;
+            T *q = nullptr;
+            CKR(dalloc(ctx, &q, n));
+            bufs[slot] = {q, n * sizeof(T)};
+        }
+        *p = static_cast<T *>(bufs[slot].first);
+        return CPM_OK;
+    }
+};
 
 static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o, cpm_result *res) {
     cpm_stats &st = res->stats;
@@ -1837,6 +1865,9 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
         CK(cudaGetLastError());
         uint64_t n_ub = P2, pat_ub = n_pat;
         uint32_t k = 2;
+        LevelScratch scratch(ctx);
+        uint64_t *d_tot = nullptr;
+        CKR(ds.alloc(&d_tot, 1));
         while (n_ub >= 2) {
             if (k + 1 > 64) {
                 dfree(ctx, L);
@@ -1844,19 +1875,19 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
                 return set_err(ctx, CPM_EINVAL, "patterns longer than 64 items are not supported");
             }
             const uint32_t w = k + 1;
-            DevScope lvl(ctx);
+            DevScope lvl(ctx);  // large-scan temporaries only
             // Prefix groups and join partners of every row.
             uint32_t *gflag = nullptr, *partners = nullptr;
             uint64_t *gid = nullptr, *gfirst = nullptr, *poff = nullptr;
-            CKR(lvl.alloc(&gflag, n_ub));
-            CKR(lvl.alloc(&gid, n_ub));
-            CKR(lvl.alloc(&partners, n_ub));
-            CKR(lvl.alloc(&poff, n_ub));
-            CKR(lvl.alloc(&gfirst, n_ub + 1));
+            CKR(scratch.get(0, &gflag, n_ub));
+            CKR(scratch.get(1, &gid, n_ub));
+            CKR(scratch.get(2, &partners, n_ub));
+            CKR(scratch.get(3, &poff, n_ub));
+            CKR(scratch.get(4, &gfirst, n_ub + 1));
             const unsigned nb = (unsigned)((n_ub + 255) / 256);
             k_group_start<<<nb, 256, 0, ctx->stream>>>(L, n_ub, d_cnt2, k, gflag);
             CK(cudaGetLastError());
-            CKR(scan_u32(ctx, lvl, gflag, gid, n_ub, nullptr));
+            CKR(scan_u32(ctx, lvl, gflag, gid, n_ub, nullptr, d_tot));
             k_group_first<<<nb, 256, 0, ctx->stream>>>(gflag, gid, d_cnt2, gfirst);
             CK(cudaGetLastError());
             k_partners<<<nb, 256, 0, ctx->stream>>>(gflag, gid, gfirst, n_ub, d_cnt2, partners);
@@ -1864,26 +1895,26 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
             uint64_t counts[2] = {0, 0};
             CK(cudaMemcpyAsync(counts, d_cnt2, 16, cudaMemcpyDeviceToHost, ctx->stream));
             uint64_t n_pairs = 0;
-            CKR(scan_u32(ctx, lvl, partners, poff, n_ub, &n_pairs));  // synchronises: counts are in
+            CKR(scan_u32(ctx, lvl, partners, poff, n_ub, &n_pairs, d_tot));  // synchronises: counts are in
             n_pat = counts[1];
             st.kernel_launches += 7;
             if (!n_pairs) break;
             // Join, prune, count, keep.
             uint32_t *cand = nullptr, *left = nullptr, *okf = nullptr, *sup = nullptr, *pass = nullptr;
             uint64_t *pos = nullptr;
-            CKR(lvl.alloc(&cand, n_pairs * w));
-            CKR(lvl.alloc(&left, n_pairs));
-            CKR(lvl.alloc(&okf, n_pairs));
-            CKR(lvl.alloc(&sup, n_pairs));
-            CKR(lvl.alloc(&pass, n_pairs));
-            CKR(lvl.alloc(&pos, n_pairs));
+            CKR(scratch.get(5, &cand, n_pairs * w));
+            CKR(scratch.get(6, &left, n_pairs));
+            CKR(scratch.get(7, &okf, n_pairs));
+            CKR(scratch.get(8, &sup, n_pairs));
+            CKR(scratch.get(9, &pass, n_pairs));
+            CKR(scratch.get(10, &pos, n_pairs));
             k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, d_cnt2, k, poff, n_pairs,
                                                                                      cand, left, okf);
             CK(cudaGetLastError());
             k_count_pruned<<<(unsigned)((n_pairs * 32 + 255) / 256), 256, 0, ctx->stream>>>(
                 db->d_bits, db->stride, cand, okf, n_pairs, w, ms, sup, pass);
             CK(cudaGetLastError());
-            CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, nullptr));
+            CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, nullptr, d_tot));
             st.kernel_launches += 4;
             st.intersections += n_pairs * (w - 1);
             st.bytes_alg += n_pairs * w * db->stride * 8;
