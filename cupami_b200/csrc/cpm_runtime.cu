@@ -1723,9 +1723,9 @@ static int scan_u32(cpm_ctx *ctx, DevScope &ds, const uint32_t *in, uint64_t *ou
                     uint64_t *d_tot = nullptr) {
     if (total) *total = 0;
     if (!n) return CPM_OK;
-    if (n <= 32768) {
-        // Small scans (most Apriori levels): one single-block launch instead
-        // of CUB's two.
+    if (n <= 4096) {
+        // Small scans (most Apriori levels): one single-block launch of at
+        // most four passes instead of CUB's two launches.
         if (!d_tot) CKR(ds.alloc(&d_tot, 1));
         k_scan_u32<<<1, 1024, 0, ctx->stream>>>(in, n, out, d_tot);
         CK(cudaGetLastError());
