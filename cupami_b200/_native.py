@@ -32,6 +32,7 @@ CPM_APRIORI = 1
 CPM_ORDER_ECLAT = 0
 CPM_ORDER_APRIORI = 1
 CPM_ORDER_NONE = 2
+CPM_ORDER_DEPTH_FIRST = 3
 CPM_SCHED_PLAIN = 0
 CPM_SCHED_LEARNED = 1
 
@@ -112,6 +113,12 @@ _SIGNATURES = {
     "cpm_costmodel_gradient": (ctypes.c_int, [_P, _P, _P, _P, _U64, _P, _P]),
     "cpm_costmodel_set": (ctypes.c_int, [_P, _P]),
     "cpm_result_trace": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(_U64)]),
+    "cpm_tdb_from_csr": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, _P, ctypes.c_int64,
+                                        ctypes.POINTER(_P)]),
+    "cpm_mine_periodic": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.POINTER(_P)]),
+    "cpm_result_copy_periodic": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P, _P]),
+    "cpm_periodic_counts": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, _P, _U64, ctypes.c_int64,
+                                           _P, _P]),
     "cpm_mine_eclat_noalloc": (ctypes.c_int, [_P, _P, _U64, ctypes.c_uint32, _U64, ctypes.c_int64,
                                               _P, _P, _P, _U64, ctypes.POINTER(_U64)]),
 }
@@ -263,6 +270,30 @@ class Database:
             dbs.append(db)
         return dbs
 
+    @classmethod
+    def from_temporal(cls, ctx, offsets, cols, n_items, timestamps, end):
+        """Temporal tidsets: every row kept (empty ones too), rows sorted by timestamp."""
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        cols = np.ascontiguousarray(cols, dtype=np.uint32)
+        timestamps = np.ascontiguousarray(timestamps, dtype=np.int64)
+        handle = _P()
+        with ctx.lock:
+            ctx.check(library().cpm_tdb_from_csr(ctx.handle, _ptr(offsets), offsets.size - 1, _ptr(cols),
+                                                 cols.size, int(n_items), _ptr(timestamps), int(end),
+                                                 ctypes.byref(handle)))
+        return cls(ctx, handle)
+
+    def mine_periodic(self, min_sup, max_per, algorithm, order):
+        """Periodic-frequent itemsets of a temporal database (Result with ``periods``)."""
+        res = _P()
+        with self.ctx.lock:
+            self.ctx.check(library().cpm_mine_periodic(self.ctx.handle, self.handle, int(min_sup), int(max_per),
+                                                       int(algorithm), ctypes.byref(res)))
+        try:
+            return Result.collect(res, order, periodic=True)
+        finally:
+            library().cpm_result_free(res)
+
     def mine(self, min_sup, algorithm, opts=None, order=None):
         if opts is None:
             opts = Opts()
@@ -353,9 +384,10 @@ class Result:
         self.supports = supports
         self.stats = stats
         self.trace = None  # (features, log1p(subtree intersections)) per root unit, when traced
+        self.periods = None  # int64 periodicity per pattern (periodic results)
 
     @classmethod
-    def collect(cls, handle, order):
+    def collect(cls, handle, order, periodic=False):
         lib = library()
         n, slots = _U64(), _U64()
         if lib.cpm_result_size(handle, ctypes.byref(n), ctypes.byref(slots)) != CPM_OK:
@@ -363,13 +395,20 @@ class Result:
         offsets = np.zeros(n.value + 1, dtype=np.uint64)
         items = np.zeros(max(1, slots.value), dtype=np.uint32)
         supports = np.zeros(max(1, n.value), dtype=np.uint64)
-        code = lib.cpm_result_copy(handle, int(order), offsets.ctypes.data, items.ctypes.data,
-                                   supports.ctypes.data)
+        periods = np.zeros(max(1, n.value), dtype=np.int64) if periodic else None
+        if periodic:
+            code = lib.cpm_result_copy_periodic(handle, int(order), offsets.ctypes.data, items.ctypes.data,
+                                                supports.ctypes.data, periods.ctypes.data)
+        else:
+            code = lib.cpm_result_copy(handle, int(order), offsets.ctypes.data, items.ctypes.data,
+                                       supports.ctypes.data)
         if code != CPM_OK:
             raise NativeError(code, "result copy")
         st = Stats()
         lib.cpm_result_stats(handle, ctypes.byref(st))
         out = cls(offsets, items[:slots.value], supports[:n.value], st.as_dict())
+        if periodic:
+            out.periods = periods[:n.value]
         nt = _U64()
         lib.cpm_result_trace(handle, None, None, ctypes.byref(nt))
         if nt.value:

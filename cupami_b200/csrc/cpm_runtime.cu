@@ -12,7 +12,7 @@
 #include "k_gram_tc.cuh"
 #include "k_deep.cuh"
 #include "k_apriori.cuh"
-#include "k_batch.cuh"
+#include "k_periodic.cuh"
 #include "k_costmodel.cuh"
 #include "k_units.cuh"
 #include <cub/device/device_radix_sort.cuh>
@@ -76,12 +76,17 @@ struct cpm_db {
     uint64_t *d_bits = nullptr;
     uint32_t *d_support = nullptr;
     std::vector<uint32_t> labels;  // raw ids in column order (cpm_db_from_ids)
+    // Temporal databases (cpm_tdb_from_csr): every row kept, with its timestamp.
+    long long *d_ts = nullptr;
+    long long end = 0;
+    bool temporal = false;
     // Deep-level buffer sizes that the last mine() of this database needed.
     uint64_t hint_frames = 0, hint_members = 0, hint_queue = 0, hint_patterns = 0, hint_arena = 0;
 };
 
 struct cpm_result {
     std::vector<uint32_t> parent, item, support;
+    std::vector<int64_t> period;  // periodic-frequent results only (cpm_mine_periodic)
     cpm_stats stats{};
     int algo = CPM_ECLAT;
     // Per root unit, when traced: cost-model features and log1p(subtree intersections)
@@ -395,6 +400,57 @@ extern "C" int cpm_db_from_csr(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n
     return CPM_OK;
 }
 
+// Temporal database (cupami/periodicFrequentPattern/_temporal.py:109-147):
+// rows in timestamp order and every row kept -- an empty basket keeps its
+// timestamp and counts in the support denominator -- with the timestamps on
+// the device beside the tidsets.  The periodic miner prunes on the timestamps
+// being sorted, so they must not decrease; end closes the last gap.
+extern "C" int cpm_tdb_from_csr(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows, const uint32_t *cols,
+                                uint64_t nnz, uint32_t n_items, const int64_t *timestamps, int64_t end,
+                                cpm_db **out) {
+    if (!ctx || !out || (!offsets && n_rows) || (!cols && nnz) || (!timestamps && n_rows)) return CPM_EINVAL;
+    *out = nullptr;
+    CK(cudaSetDevice(ctx->device));
+    if (!n_rows && nnz) return set_err(ctx, CPM_EINVAL, "nnz must be 0 when there are no rows");
+    if (n_rows) {
+        if (offsets[0] != 0 || offsets[n_rows] != nnz)
+            return set_err(ctx, CPM_EINVAL, "offsets must start at 0 and end at nnz");
+        for (uint64_t r = 0; r < n_rows; ++r) {
+            if (offsets[r + 1] < offsets[r]) return set_err(ctx, CPM_EINVAL, "offsets must be nondecreasing");
+            if (r && timestamps[r] < timestamps[r - 1])
+                return set_err(ctx, CPM_EINVAL, "timestamps must be nondecreasing (rows sorted by timestamp)");
+        }
+        if (end < timestamps[n_rows - 1]) return set_err(ctx, CPM_EINVAL, "end must be at least the last timestamp");
+    }
+    for (uint64_t k = 0; k < nnz; ++k)
+        if (cols[k] >= n_items) return set_err(ctx, CPM_EINVAL, "column %u out of range (n_items %u)", cols[k], n_items);
+    cpm_db *db = new cpm_db();
+    db->ctx = ctx;
+    db->n_tx = n_rows;
+    db->n_items = n_items;
+    db->temporal = true;
+    db->end = end;
+    int r = db_alloc_bits(ctx, db);
+    if (r == CPM_OK) r = dalloc(ctx, &db->d_ts, n_rows);
+    DevScope tmp(ctx);
+    uint64_t *d_off = nullptr;
+    uint32_t *d_ids = nullptr;
+    if (r == CPM_OK) r = tmp.alloc(&d_off, n_rows + 1);
+    if (r == CPM_OK) r = tmp.alloc(&d_ids, nnz);
+    if (r == CPM_OK && n_rows)
+        r = stage_upload(ctx, {{d_off, {offsets, (n_rows + 1) * 8}}, {d_ids, {cols, nnz * 4}},
+                               {db->d_ts, {timestamps, n_rows * 8}}});
+    if (r == CPM_OK) r = db_pack(ctx, db, d_off, d_ids, nullptr);
+    if (r == CPM_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+        r = set_err(ctx, CPM_ECUDA, "pack failed: %s", cudaGetErrorString(cudaGetLastError()));
+    if (r != CPM_OK) {
+        cpm_db_free(db);
+        return r;
+    }
+    *out = db;
+    return CPM_OK;
+}
+
 // Decimal-string order of integer labels: "1" < "10" < "100" < "11" < "2".
 static inline uint64_t decimal_key(uint32_t v) {
     char d[10];
@@ -669,6 +725,7 @@ extern "C" void cpm_db_free(cpm_db *db) {
     cudaSetDevice(ctx->device);
     dfree(ctx, db->d_bits);
     dfree(ctx, db->d_support);
+    dfree(ctx, db->d_ts);
     cudaStreamSynchronize(ctx->stream);
     delete db;
 }
@@ -1964,6 +2021,198 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
     return CPM_OK;
 }
 
+// Periodic-frequent itemsets (cuPFEclat.mine, cupami/periodicFrequentPattern/cuPFEclat.py:146-175;
+// cuPFApriori.mine, cuPFApriori.py:141-157): an itemset is kept when its
+// support is positive and at least min_sup and its periodicity is at most
+// max_per (_temporal.py:166-171).  Adding an item only removes rows, so the
+// support falls and gaps merge: the kept itemsets are closed under taking
+// subsets, and one level-wise search finds them for both miners.  Level 1
+// evaluates every item; each later level joins two kept itemsets that share
+// all but their last item, drops a candidate with a subset that was not kept
+// (k_join_pairs) and evaluates the rest (k_periodic, pruning early).  The
+// miners differ only in insertion order, which cpm_result_copy rebuilds
+// (CPM_ORDER_DEPTH_FIRST for cuPFEclat, CPM_ORDER_APRIORI for cuPFApriori).
+static int mine_periodic(cpm_ctx *ctx, cpm_db *db, long long ms, long long max_per, cpm_result *res) {
+    cpm_stats &st = res->stats;
+    DevScope ds(ctx);
+    CK(cudaEventRecord(ctx->ev[0], ctx->stream));
+    const long long need = std::max<long long>(ms, 1);
+    const auto *bits = reinterpret_cast<const unsigned long long *>(db->d_bits);
+    const uint32_t n_items = db->n_items;
+    auto warp_grid = [](uint64_t n) { return (unsigned)((n + 7) / 8); };  // 8 warps of 256 threads
+    PatternArrays pa;
+    long long *pat_per = nullptr;
+    uint64_t per_cap = 0;
+    uint32_t *L = nullptr, *pid = nullptr;
+    struct Free {
+        cpm_ctx *c; PatternArrays *p; long long **per; uint32_t **L, **pid;
+        ~Free() {
+            dfree(c, p->parent); dfree(c, p->item); dfree(c, p->sup);
+            dfree(c, *per); dfree(c, *L); dfree(c, *pid);
+        }
+    } free_all{ctx, &pa, &pat_per, &L, &pid};
+    // Pattern records and their periods grow together.
+    auto reserve = [&](uint64_t used, uint64_t want) -> int {
+        CKR(patterns_reserve(ctx, pa, used, want));
+        if (per_cap < pa.cap) {
+            long long *nw = nullptr;
+            CKR(dalloc(ctx, &nw, pa.cap));
+            if (used) CK(cudaMemcpyAsync(nw, pat_per, used * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+            dfree(ctx, pat_per);
+            pat_per = nw;
+            per_cap = pa.cap;
+        }
+        return CPM_OK;
+    };
+    uint64_t *d_cnt2 = nullptr, *d_tot = nullptr;  // (rows of the level, patterns so far); scan total
+    CKR(ds.alloc(&d_cnt2, 2));
+    CKR(ds.alloc(&d_tot, 1));
+    k_set_u64x2<<<1, 1, 0, ctx->stream>>>(d_cnt2, 0, d_cnt2 + 1, 0);
+    CK(cudaGetLastError());
+    st.kernel_launches++;
+    CKR(reserve(0, std::max<uint64_t>(1024, db->hint_patterns)));
+    uint64_t n_ub = 0, pat_ub = 0;
+    if (n_items) {
+        uint32_t *cand = nullptr, *pass = nullptr;
+        unsigned long long *sup = nullptr;
+        long long *per = nullptr;
+        uint64_t *pos = nullptr;
+        CKR(ds.alloc(&cand, n_items));
+        CKR(ds.alloc(&pass, n_items));
+        CKR(ds.alloc(&sup, n_items));
+        CKR(ds.alloc(&per, n_items));
+        CKR(ds.alloc(&pos, n_items));
+        k_iota_u32<<<(n_items + 255) / 256, 256, 0, ctx->stream>>>(cand, n_items);
+        CK(cudaGetLastError());
+        k_periodic<unsigned long long, true><<<warp_grid(n_items), 256, 0, ctx->stream>>>(
+            bits, db->stride, cand, nullptr, n_items, 1, db->d_ts, db->n_tx, db->end, need, max_per, sup, per, pass);
+        CK(cudaGetLastError());
+        uint64_t F1 = 0;
+        CKR(scan_u32(ctx, ds, pass, pos, n_items, &F1, d_tot));
+        st.n_frequent_items = F1;
+        CKR(reserve(0, F1 * 4 + db->hint_patterns));
+        CKR(dalloc(ctx, &L, F1));
+        CKR(dalloc(ctx, &pid, F1));
+        k_periodic_keep<<<(n_items + 255) / 256, 256, 0, ctx->stream>>>(
+            cand, nullptr, sup, per, pass, pos, n_items, 1, nullptr, d_cnt2 + 1, L, pid, pa.parent, pa.item, pa.sup,
+            pat_per);
+        CK(cudaGetLastError());
+        k_level_close<<<1, 1, 0, ctx->stream>>>(pos, pass, n_items, d_cnt2, d_cnt2 + 1);
+        CK(cudaGetLastError());
+        st.kernel_launches += 5;
+        st.intersections += n_items;
+        n_ub = pat_ub = F1;
+    }
+    LevelScratch scratch(ctx);
+    uint32_t k = 1;
+    while (n_ub >= 2) {
+        if (k + 1 > 64) return set_err(ctx, CPM_EINVAL, "patterns longer than 64 items are not supported");
+        const uint32_t w = k + 1;
+        DevScope lvl(ctx);  // large-scan temporaries only
+        uint32_t *gflag = nullptr, *partners = nullptr;
+        uint64_t *gid = nullptr, *gfirst = nullptr, *poff = nullptr;
+        CKR(scratch.get(0, &gflag, n_ub));
+        CKR(scratch.get(1, &gid, n_ub));
+        CKR(scratch.get(2, &partners, n_ub));
+        CKR(scratch.get(3, &poff, n_ub));
+        CKR(scratch.get(4, &gfirst, n_ub + 1));
+        const unsigned nb = (unsigned)((n_ub + 255) / 256);
+        k_group_start<<<nb, 256, 0, ctx->stream>>>(L, n_ub, d_cnt2, k, gflag);
+        CK(cudaGetLastError());
+        CKR(scan_u32(ctx, lvl, gflag, gid, n_ub, nullptr, d_tot));
+        k_group_first<<<nb, 256, 0, ctx->stream>>>(gflag, gid, d_cnt2, gfirst);
+        CK(cudaGetLastError());
+        k_partners<<<nb, 256, 0, ctx->stream>>>(gflag, gid, gfirst, n_ub, d_cnt2, partners);
+        CK(cudaGetLastError());
+        uint64_t counts[2] = {0, 0};
+        CK(cudaMemcpyAsync(counts, d_cnt2, 16, cudaMemcpyDeviceToHost, ctx->stream));
+        uint64_t n_pairs = 0;
+        CKR(scan_u32(ctx, lvl, partners, poff, n_ub, &n_pairs, d_tot));  // synchronises: counts are in
+        const uint64_t n_pat = counts[1];
+        st.kernel_launches += 7;
+        if (!n_pairs) break;
+        uint32_t *cand = nullptr, *left = nullptr, *okf = nullptr, *pass = nullptr;
+        unsigned long long *sup = nullptr;
+        long long *per = nullptr;
+        uint64_t *pos = nullptr;
+        CKR(scratch.get(5, &cand, n_pairs * w));
+        CKR(scratch.get(6, &left, n_pairs));
+        CKR(scratch.get(7, &okf, n_pairs));
+        CKR(scratch.get(8, &sup, n_pairs));
+        CKR(scratch.get(9, &pass, n_pairs));
+        CKR(scratch.get(10, &pos, n_pairs));
+        CKR(scratch.get(11, &per, n_pairs));
+        k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, d_cnt2, k, poff, n_pairs, cand,
+                                                                                 left, okf);
+        CK(cudaGetLastError());
+        k_periodic<unsigned long long, true><<<warp_grid(n_pairs), 256, 0, ctx->stream>>>(
+            bits, db->stride, cand, okf, n_pairs, w, db->d_ts, db->n_tx, db->end, need, max_per, sup, per, pass);
+        CK(cudaGetLastError());
+        CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, nullptr, d_tot));
+        st.kernel_launches += 4;
+        st.intersections += n_pairs * (w - 1);
+        uint32_t *L2 = nullptr, *pid2 = nullptr;
+        CKR(reserve(n_pat, pat_ub + n_pairs));
+        CKR(dalloc(ctx, &L2, n_pairs * w));
+        CKR(dalloc(ctx, &pid2, n_pairs));
+        k_periodic_keep<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(
+            cand, left, sup, per, pass, pos, n_pairs, w, pid, d_cnt2 + 1, L2, pid2, pa.parent, pa.item, pa.sup,
+            pat_per);
+        CK(cudaGetLastError());
+        k_level_close<<<1, 1, 0, ctx->stream>>>(pos, pass, n_pairs, d_cnt2, d_cnt2 + 1);
+        CK(cudaGetLastError());
+        st.kernel_launches += 2;
+        dfree(ctx, L);
+        dfree(ctx, pid);
+        L = L2;
+        pid = pid2;
+        pat_ub += n_pairs;
+        n_ub = n_pairs;
+        k = w;
+    }
+    uint64_t n_pat = 0;
+    CK(cudaMemcpyAsync(&n_pat, d_cnt2 + 1, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaEventRecord(ctx->ev[3], ctx->stream));
+    res->parent.resize(n_pat);
+    res->item.resize(n_pat);
+    res->support.resize(n_pat);
+    res->period.resize(n_pat);
+    if (n_pat) {
+        CK(cudaMemcpyAsync(res->parent.data(), pa.parent, n_pat * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(res->item.data(), pa.item, n_pat * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(res->support.data(), pa.sup, n_pat * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(res->period.data(), pat_per, n_pat * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    db->hint_patterns = std::max<uint64_t>(db->hint_patterns, n_pat + n_pat / 4);
+    st.n_patterns = n_pat;
+    st.ms_total = st.ms_deep = elapsed_ms(ctx, 0, 3);
+    return CPM_OK;
+}
+
+extern "C" int cpm_mine_periodic(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, int64_t max_per, int algo,
+                                 cpm_result **out) {
+    if (!ctx || !db || !out || db->ctx != ctx) return CPM_EINVAL;
+    *out = nullptr;
+    if (!db->temporal) return set_err(ctx, CPM_EINVAL, "periodic mining needs a temporal database (cpm_tdb_from_csr)");
+    if (algo != CPM_ECLAT && algo != CPM_APRIORI) return set_err(ctx, CPM_EINVAL, "unknown algorithm %d", algo);
+    CK(cudaSetDevice(ctx->device));
+    // Supports are 32-bit counts; thresholds beyond every count pass nothing.
+    const long long ms = (long long)std::min<int64_t>(min_sup, (int64_t)1 << 40);
+    cpm_result *res = new cpm_result();
+    res->algo = algo;
+    const int r = mine_periodic(ctx, db, ms, (long long)max_per, res);
+    if (r != CPM_OK) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaGetLastError();
+        delete res;
+        return r;
+    }
+    *out = res;
+    return CPM_OK;
+}
+
 extern "C" int cpm_mine(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, int algo, const cpm_opts *opts,
                         cpm_result **out) {
     if (!ctx || !db || !out || db->ctx != ctx) return CPM_EINVAL;
@@ -2120,12 +2369,15 @@ extern "C" int cpm_result_tree(const cpm_result *res, int64_t *parent, uint32_t 
 
 // Patterns of a result in the requested order.  A pattern is its parent's
 // items plus its own.  The device builds a prefix tree (every pattern extends
-// its parent by a larger item), so both insertion orders are traversals of
+// its parent by a larger item), so the insertion orders are traversals of
 // that tree; any other tree is ordered by comparing item lists.
-extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offsets, uint32_t *items,
-                               uint64_t *supports) {
+static int result_copy(const cpm_result *res, int order, uint64_t *offsets, uint32_t *items, uint64_t *supports,
+                       int64_t *periods) {
     if (!res || !offsets || !supports) return CPM_EINVAL;
-    if (order != CPM_ORDER_ECLAT && order != CPM_ORDER_APRIORI && order != CPM_ORDER_NONE) return CPM_EINVAL;
+    if (order != CPM_ORDER_ECLAT && order != CPM_ORDER_APRIORI && order != CPM_ORDER_NONE &&
+        order != CPM_ORDER_DEPTH_FIRST)
+        return CPM_EINVAL;
+    if (periods && res->period.size() != res->parent.size()) return CPM_EINVAL;
     const uint64_t n = res->parent.size();
     const uint32_t *par = res->parent.data(), *itm = res->item.data();
     const bool dbg = getenv("CPM_DEBUG") != nullptr;
@@ -2193,13 +2445,19 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
                 level.swap(next);
             }
         } else {
-            // singletons, pairs, then for every pair: its children, then each
-            // child's subtree in the same way (cuEclat.py:211-245)
+            // Eclat: singletons, pairs, then for every pair: its children, then
+            // each child's subtree in the same way (cuEclat.py:211-245).
+            // Depth first: singletons, then for every singleton: its children,
+            // then each child's subtree (cuPFEclat.py:160-173).
             for (uint64_t r : roots) idx[w++] = r;
             std::vector<uint64_t> pairs;
-            for (uint64_t r : roots)
-                for (uint64_t c = coff[r]; c < coff[r + 1]; ++c) pairs.push_back(kids[c]);
-            for (uint64_t q : pairs) idx[w++] = q;
+            if (order == CPM_ORDER_DEPTH_FIRST) {
+                pairs = roots;
+            } else {
+                for (uint64_t r : roots)
+                    for (uint64_t c = coff[r]; c < coff[r + 1]; ++c) pairs.push_back(kids[c]);
+                for (uint64_t q : pairs) idx[w++] = q;
+            }
             std::vector<std::pair<uint64_t, uint64_t>> stack;  // (node, next child to descend)
             for (uint64_t q : pairs) {
                 for (uint64_t c = coff[q]; c < coff[q + 1]; ++c) idx[w++] = kids[c];
@@ -2236,13 +2494,15 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
                 if (depth[a] != depth[b]) return depth[a] < depth[b];
                 return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
             });
-        } else if (order == CPM_ORDER_ECLAT) {
+        } else if (order == CPM_ORDER_ECLAT || order == CPM_ORDER_DEPTH_FIRST) {
             // cuEclat inserts singletons, then pairs, then every deeper pattern in
-            // the order of its class search: key (x1..x_{k-1}, -1, x_k).
+            // the order of its class search: key (x1..x_{k-1}, -1, x_k).  The
+            // depth-first order uses that key from the pairs on.
+            const uint32_t deep = order == CPM_ORDER_ECLAT ? 3 : 2;
             std::sort(idx, idx + n, [&](uint64_t a, uint64_t b) {
-                const uint32_t ga = std::min<uint32_t>(depth[a], 3), gb = std::min<uint32_t>(depth[b], 3);
+                const uint32_t ga = std::min<uint32_t>(depth[a], deep), gb = std::min<uint32_t>(depth[b], deep);
                 if (ga != gb) return ga < gb;
-                if (ga < 3) return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
+                if (ga < deep) return std::lexicographical_compare(pat(a), pat(a) + depth[a], pat(b), pat(b) + depth[b]);
                 const uint32_t *x = pat(a), *y = pat(b);
                 const int64_t la = depth[a] + 1, lb = depth[b] + 1;
                 for (int64_t i = 0; i < std::min(la, lb); ++i) {
@@ -2262,6 +2522,7 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
     for (int64_t r = 0; r < (int64_t)n; ++r) {
         const uint64_t k = idx[r];
         supports[r] = res->support[k];
+        if (periods) periods[r] = res->period[k];
         if (!items) continue;
         uint32_t *a = items + offsets[r];
         if (!flat.empty()) {
@@ -2274,6 +2535,17 @@ extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offse
     }
     lap("items");
     return CPM_OK;
+}
+
+extern "C" int cpm_result_copy(const cpm_result *res, int order, uint64_t *offsets, uint32_t *items,
+                               uint64_t *supports) {
+    return result_copy(res, order, offsets, items, supports, nullptr);
+}
+
+extern "C" int cpm_result_copy_periodic(const cpm_result *res, int order, uint64_t *offsets, uint32_t *items,
+                                        uint64_t *supports, int64_t *periods) {
+    if (!periods) return CPM_EINVAL;
+    return result_copy(res, order, offsets, items, supports, periods);
 }
 
 extern "C" int cpm_results_copy(cpm_result *const *res, uint32_t n, int order, uint64_t *sizes,
@@ -2351,6 +2623,28 @@ extern "C" int cpm_count_supports(cpm_ctx *ctx, const uint32_t *d_bitsets, uint6
     if (!n_candidates) return CPM_OK;
     k_ref_count<<<(unsigned)((n_candidates * 32 + 255) / 256), 256, 0, ctx->stream>>>(
         d_bitsets, words32, d_candidates, n_candidates, width, reinterpret_cast<unsigned long long *>(d_supports));
+    CK(cudaGetLastError());
+    return CPM_OK;
+}
+
+// periodic_counts of cupami/periodicFrequentPattern/_temporal.py:26-53, called
+// by TemporalInput._evaluate (:156-165): exact supports and periodicities of
+// every candidate (k_periodic without early stopping).
+extern "C" int cpm_periodic_counts(cpm_ctx *ctx, const uint32_t *d_bitsets, uint64_t words32,
+                                   const uint32_t *d_candidates, uint64_t n_candidates, uint32_t width,
+                                   const int64_t *d_timestamps, uint64_t n_transactions, int64_t end,
+                                   uint64_t *d_supports, int64_t *d_periods) {
+    if (!ctx || (n_candidates && (!d_candidates || !d_supports || !d_periods || !width))) return CPM_EINVAL;
+    if (n_candidates && n_transactions && (!d_bitsets || !d_timestamps)) return CPM_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    if (!n_candidates) return CPM_OK;
+    // Rows past the bitsets' words hold no bits (the reference kernel scans
+    // words32 words and skips rows >= n_transactions).
+    const uint64_t rows = std::min<uint64_t>(n_transactions, words32 * 32);
+    k_periodic<uint32_t, false><<<(unsigned)((n_candidates + 7) / 8), 256, 0, ctx->stream>>>(
+        d_bitsets, words32, d_candidates, nullptr, n_candidates, width, reinterpret_cast<const long long *>(d_timestamps),
+        rows, (long long)end, 0, 0, reinterpret_cast<unsigned long long *>(d_supports),
+        reinterpret_cast<long long *>(d_periods), nullptr);
     CK(cudaGetLastError());
     return CPM_OK;
 }

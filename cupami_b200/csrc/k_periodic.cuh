@@ -1,0 +1,167 @@
+// Periodic-frequent support counting (cupami/periodicFrequentPattern/_temporal.py:26-53).
+//
+// For an itemset X held by the rows r_1 < ... < r_s of a temporal database
+// whose rows are sorted by timestamp ts[], the reference kernel returns the
+// support s and the periodicity
+//     max(ts[r_1] - 0, ts[r_2] - ts[r_1], ..., ts[r_s] - ts[r_{s-1}], end - ts[r_s])
+// (end when s = 0), scanning the set bits of the AND of X's rows in order with
+// one thread per candidate (_temporal.py:26-53, launch :156-165).
+//
+// Here one warp handles a candidate: the lanes read 32 consecutive words of
+// every row of the candidate per step (coalesced), each lane reduces its word
+// to a segment summary (count, first and last timestamp, largest inner gap),
+// and the warp joins the 32 summaries in row order with shuffles.  The join
+//     (a, b) -> {a.cnt + b.cnt, a.first, b.last, max(a.gap, b.gap, b.first - a.last)}
+// (an empty side yields the other) is associative, so the tree gives exactly
+// the sequential scan's maximum.  With kPrune (the miner), a candidate stops as
+// soon as it cannot pass: too few rows left for the support, or a gap that is
+// already too long -- rows are sorted by timestamp, so the next set row's gap
+// is at least ts[first unscanned row] - last timestamp seen.
+#pragma once
+#include "common.cuh"
+
+namespace cpm {
+
+struct PSeg {
+    unsigned long long cnt;
+    long long first, last, gap;
+};
+
+__device__ __forceinline__ PSeg pseg_join(const PSeg &a, const PSeg &b) {
+    if (!a.cnt) return b;
+    if (!b.cnt) return a;
+    PSeg r;
+    r.cnt = a.cnt + b.cnt;
+    r.first = a.first;
+    r.last = b.last;
+    r.gap = max(max(a.gap, b.gap), b.first - a.last);
+    return r;
+}
+
+// Lane 0 receives the join of the 32 lanes' segments in lane order.
+__device__ __forceinline__ PSeg pseg_warp_join(PSeg s, unsigned lane) {
+#pragma unroll
+    for (unsigned o = 1; o < 32; o <<= 1) {
+        PSeg t;
+        t.cnt = __shfl_down_sync(CPM_FULL, s.cnt, o);
+        t.first = __shfl_down_sync(CPM_FULL, s.first, o);
+        t.last = __shfl_down_sync(CPM_FULL, s.last, o);
+        t.gap = __shfl_down_sync(CPM_FULL, s.gap, o);
+        if (lane + o < 32) s = pseg_join(s, t);
+    }
+    return s;
+}
+
+__device__ __forceinline__ unsigned word_popc(uint32_t x) { return __popc(x); }
+__device__ __forceinline__ unsigned word_popc(unsigned long long x) { return __popcll(x); }
+__device__ __forceinline__ unsigned word_low(uint32_t x) { return __ffs(x) - 1; }
+__device__ __forceinline__ unsigned word_low(unsigned long long x) { return __ffsll(x) - 1; }
+
+// One warp per candidate c: the AND of the width rows cand[c * width ..] of
+// `bits` (Word: uint32_t or unsigned long long; rows of `stride` words; bit b
+// of word v is row v * bits(Word) + b), restricted to rows < n_tx.  Writes support[c] and period[c]; with kPrune also
+// pass[c] = ok_flag[c] && support >= need && period <= max_per, and a candidate
+// that stops early keeps partial support/period values (only passing ones are
+// exact).  Without kPrune every candidate is exact and pass/ok_flag may be null.
+template <class Word, bool kPrune>
+__global__ void __launch_bounds__(256)
+k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__restrict__ cand,
+           const uint32_t *__restrict__ ok_flag, uint64_t n, uint32_t width, const long long *__restrict__ ts,
+           uint64_t n_tx, long long end, long long need, long long max_per, unsigned long long *__restrict__ support,
+           long long *__restrict__ period, uint32_t *__restrict__ pass) {
+    constexpr unsigned B = sizeof(Word) * 8;
+    const uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (c >= n) return;  // whole warps: c is the same on every lane
+    if (kPrune && ok_flag && !ok_flag[c]) {
+        if (!lane) {
+            support[c] = 0;
+            period[c] = end;
+            pass[c] = 0;
+        }
+        return;
+    }
+    const uint32_t *cc = cand + c * width;
+    const uint64_t words = (n_tx + B - 1) / B;
+    PSeg run{0, 0, 0, 0};
+    bool stopped = false;
+    for (uint64_t base = 0; base < words; base += 32) {
+        const uint64_t v = base + lane;
+        Word x = 0;
+        if (v < words) {
+            x = ~Word(0);
+            for (uint32_t j = 0; j < width; ++j) x &= __ldg(bits + (uint64_t)cc[j] * stride + v);
+            const uint64_t lo = v * B;
+            if (n_tx - lo < B) x &= (Word(1) << (unsigned)(n_tx - lo)) - Word(1);
+        }
+        if (__any_sync(CPM_FULL, x != 0)) {
+            PSeg s{0, 0, 0, 0};
+            if (x) {
+                const uint64_t row0 = v * B;
+                Word y = x;
+                s.cnt = word_popc(x);
+                s.first = __ldg(ts + row0 + word_low(y));
+                s.last = s.first;
+                y &= y - Word(1);
+                while (y) {
+                    const long long t = __ldg(ts + row0 + word_low(y));
+                    s.gap = max(s.gap, t - s.last);
+                    s.last = t;
+                    y &= y - Word(1);
+                }
+            }
+            s = pseg_warp_join(s, lane);
+            if (!lane) run = pseg_join(run, s);
+        }
+        if (kPrune) {
+            int stop = 0;
+            if (!lane) {
+                const uint64_t scanned = (base + 32) * (uint64_t)B;
+                const uint64_t r_end = scanned < n_tx ? scanned : n_tx;
+                const long long next = r_end < n_tx ? __ldg(ts + r_end) : end;
+                const long long bound = run.cnt ? max(max(run.first, run.gap), next - run.last) : next;
+                stop = (long long)(run.cnt + (n_tx - r_end)) < need || bound > max_per;
+            }
+            if (__shfl_sync(CPM_FULL, stop, 0)) {
+                stopped = true;
+                break;
+            }
+        }
+    }
+    if (!lane) {
+        const long long per = run.cnt ? max(max(run.first, run.gap), end - run.last) : end;
+        support[c] = run.cnt;
+        period[c] = per;
+        if (kPrune) pass[c] = !stopped && (long long)run.cnt >= need && per <= max_per ? 1u : 0u;
+    }
+}
+
+__global__ void k_iota_u32(uint32_t *__restrict__ out, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (uint32_t)i;
+}
+
+// Passing candidates, in candidate order, become the next level's rows and
+// pattern records (pattern pid = *d_pid_base + rank among the passing ones).
+// Level 1 has no previous level: pid_prev is null and the parent is none.
+__global__ void k_periodic_keep(const uint32_t *__restrict__ cand, const uint32_t *__restrict__ cand_left,
+                                const unsigned long long *__restrict__ sup, const long long *__restrict__ per,
+                                const uint32_t *__restrict__ pass, const uint64_t *__restrict__ pos, uint64_t n,
+                                uint32_t w, const uint32_t *__restrict__ pid_prev,
+                                const uint64_t *__restrict__ d_pid_base, uint32_t *__restrict__ L_next,
+                                uint32_t *__restrict__ pid_next, uint32_t *__restrict__ pat_parent,
+                                uint32_t *__restrict__ pat_item, uint32_t *__restrict__ pat_sup,
+                                long long *__restrict__ pat_per) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !pass[i]) return;
+    const uint64_t p = pos[i];
+    for (uint32_t j = 0; j < w; ++j) L_next[p * w + j] = cand[i * w + j];
+    const uint64_t pid = *d_pid_base + p;
+    pid_next[p] = (uint32_t)pid;
+    pat_parent[pid] = pid_prev ? pid_prev[cand_left[i]] : 0xffffffffu;
+    pat_item[pid] = cand[i * w + w - 1];
+    pat_sup[pid] = (uint32_t)sup[i];
+    pat_per[pid] = per[i];
+}
+
+}  // namespace cpm

@@ -14,6 +14,12 @@
  *   cpm_mine(algo = CPM_APRIORI)
  *       replaces cuApriori.mine + _generateCandidates + _countCandidateSupports
  *       (cupami/frequentPattern/cuApriori.py:473-535)
+ *   cpm_tdb_from_csr + cpm_mine_periodic
+ *       replace TemporalInput._prepare + cuPFEclat.mine / cuPFApriori.mine
+ *       (cupami/periodicFrequentPattern/_temporal.py:150-171,
+ *        cuPFEclat.py:146-175, cuPFApriori.py:141-157)
+ *   cpm_periodic_counts
+ *       replaces the periodic_counts kernel (_temporal.py:26-53, :156-165)
  *   cpm_build_bitsets / cpm_count_supports / cpm_intersect_extensions
  *       replace the three kernel wrappers of cupami/frequentPattern/_bitsets.py:91-125
  *       one for one (same 32-bit word layout, device pointers in, device
@@ -60,6 +66,9 @@ extern "C" {
 #define CPM_ORDER_ECLAT    0  /* insertion order of cuEclat.mine (cuEclat.py:168-245) */
 #define CPM_ORDER_APRIORI  1  /* insertion order of cuApriori.mine: by length, then tuple */
 #define CPM_ORDER_NONE     2  /* device emission order (fastest) */
+#define CPM_ORDER_DEPTH_FIRST 3  /* insertion order of cuPFEclat.mine: singletons, then for each
+                                    pattern in depth-first order its extensions
+                                    (cupami/periodicFrequentPattern/cuPFEclat.py:150-173) */
 
 /* Deep-level scheduler. */
 #define CPM_SCHED_PLAIN    0  /* frames admitted largest first by member count */
@@ -228,6 +237,34 @@ int cpm_intersect_extensions(cpm_ctx *ctx, const uint32_t *d_prefix,
                              uint64_t n_extensions, uint32_t *d_out, uint64_t *d_supports);
 /* Waits for the context's stream. */
 int cpm_synchronize(cpm_ctx *ctx);
+
+/* ---- periodic-frequent patterns (cupami/periodicFrequentPattern) -----------
+ * A temporal database holds one row per transaction in timestamp order, empty
+ * baskets included (they keep their timestamp and count in the support
+ * denominator, _temporal.py:109-136).  The periodicity of an itemset held by
+ * rows r_1 < ... < r_s is max(ts[r_1] - 0, ts[r_2] - ts[r_1], ...,
+ * ts[r_s] - ts[r_{s-1}], end - ts[r_s]), or end when s = 0 (_temporal.py:26-53). */
+
+/* CSR of item columns, every row kept; timestamps[r] for row r, nondecreasing;
+ * end >= the last timestamp.  Every column must be < n_items. */
+int cpm_tdb_from_csr(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows, const uint32_t *cols,
+                     uint64_t nnz, uint32_t n_items, const int64_t *timestamps, int64_t end, cpm_db **out);
+/* Itemsets with support >= min_sup, support > 0 and periodicity <= max_per
+ * (_temporal.py:166-171).  algo CPM_ECLAT (cuPFEclat) or CPM_APRIORI
+ * (cuPFApriori): the same itemsets; copy them with cpm_result_copy_periodic in
+ * CPM_ORDER_DEPTH_FIRST or CPM_ORDER_APRIORI for the reference's insertion order. */
+int cpm_mine_periodic(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, int64_t max_per, int algo,
+                      cpm_result **out);
+/* cpm_result_copy plus the periodicity of every pattern (periodic results only). */
+int cpm_result_copy_periodic(const cpm_result *res, int order, uint64_t *offsets, uint32_t *items,
+                             uint64_t *supports, int64_t *periods);
+/* The reference kernel periodic_counts: for every candidate (width columns of
+ * the 32-bit bitsets of cpm_build_bitsets), its support and periodicity over
+ * rows < n_transactions with d_timestamps[row] (_temporal.py:26-53). */
+int cpm_periodic_counts(cpm_ctx *ctx, const uint32_t *d_bitsets, uint64_t words32,
+                        const uint32_t *d_candidates, uint64_t n_candidates, uint32_t width,
+                        const int64_t *d_timestamps, uint64_t n_transactions, int64_t end,
+                        uint64_t *d_supports, int64_t *d_periods);
 
 /* ---- Eclat without device allocation ---------------------------------------
  * No counterpart in the reference: cuPAMI allocates through CuPy's pool on

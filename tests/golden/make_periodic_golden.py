@@ -1,0 +1,124 @@
+"""Regenerate ``periodic_patterns.json`` from the reference periodic miners.
+
+Run in a checkout that has the cuPAMI sources (default ``/root/reference``;
+override with ``CUPAMI_REFERENCE``).  ``cuPFEclat.mine`` and
+``cuPFApriori.mine`` (cupami/periodicFrequentPattern/cuPFEclat.py:146-175,
+cuPFApriori.py:141-157) and everything they call in ``TemporalInput`` run
+unchanged; only the CUDA plumbing is replaced:
+
+* ``cuApriori._getCudaModule`` returns the NumPy namespace of
+  ``make_golden.py`` (plus ``empty``);
+* ``_bitsets.build_bitsets`` is the NumPy statement of ``make_golden.py``;
+* ``_temporal._kernel`` returns a launcher that computes the
+  ``periodic_counts`` kernel (_temporal.py:26-53) with ``oracle.periodic``.
+
+Each case records its rows, thresholds and both miners' ``getPatterns()`` as
+ordered lists, so the checks compare insertion order as well as content.
+Nothing at test time reads the reference checkout.
+"""
+
+from __future__ import annotations
+
+import json
+import random
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE))
+sys.path.insert(0, str(HERE.parents[1]))
+
+from make_golden import REF, load_reference, numpy_cuda_namespace  # noqa: E402
+
+from oracle import periodic  # noqa: E402
+
+
+def numpy_launcher(device):
+    def launch(grid, block, args):
+        bits, words, idx, width, count, ts, n, end, supports, periods = args
+        assert bits.shape[1] == int(words) and idx.shape == (int(count), int(width))
+        out = periodic.periodic_counts(bits, idx.astype(np.int64).tolist(), np.asarray(ts), int(n), int(end))
+        supports[:] = [s for s, _ in out]
+        periods[:] = [p for _, p in out]
+    return launch
+
+
+def load():
+    cupami = load_reference()
+    import importlib
+
+    temporal = importlib.import_module("cupami.periodicFrequentPattern._temporal")
+    apriori_mod = importlib.import_module("cupami.frequentPattern.cuApriori")
+    ns = numpy_cuda_namespace()
+    ns.empty = np.empty
+    apriori_mod.cuApriori._getCudaModule = staticmethod(lambda: ns)
+    temporal._kernel = numpy_launcher
+    return cupami
+
+
+def run(cupami, rows, min_sup, max_per, end=None):
+    out = {"minSup": min_sup, "maxPer": max_per, "endTime": end}
+    for name in ("cuPFEclat", "cuPFApriori"):
+        miner = getattr(cupami, name)(rows, min_sup, max_per, endTime=end)
+        miner.mine()
+        out[name] = [[k, int(s), int(p)] for k, (s, p) in miner.getPatterns().items()]
+    return out
+
+
+def cases(cupami):
+    out = []
+
+    def add(name, rows, settings):
+        out.append({"name": name, "rows": rows,
+                    "results": [run(cupami, rows, *s) for s in settings]})
+
+    # tests/test_periodic_miners.py: the paper example (9 patterns, a-b = (4, 3)).
+    baskets = ["ab", "acdi", "cefj", "abfgh", "bcd", "def", "abi", "cde", "abef", "acg"]
+    add("paper-example", [[i + 1, *b] for i, b in enumerate(baskets)], [(3, 3)])
+    # Randomized rows with empty baskets, shuffled (rows are re-sorted by timestamp).
+    for seed in range(4):
+        rng = random.Random(seed)
+        rows = [[i * 3, *rng.sample(range(6), rng.randint(0, 6))] for i in range(1, 19)]
+        rng.shuffle(rows)
+        add(f"random-seed{seed}", rows, [(1, 54), (3, 15), (5, 9)])
+    # Boundaries: duplicates, empty baskets, explicit end, empty input, equal
+    # timestamps, timestamps past 2**53.
+    add("boundaries-0", [[9, "a"], [0, "a", "a", "0"], [4], [9, "a", "b"], [15]], [(1, 10)])
+    add("boundaries-1", [[2, "x"], [3, "x"]], [(1, 5, 20)])
+    add("boundaries-2", [], [(1, 0)])
+    add("boundaries-3", [[0, "x"], [0, "y"]], [(1, 0)])
+    add("boundaries-4", [[2**53 + 1, "x"], [2**53 + 3, "x"]], [(1, 2**53 + 1)])
+    # One path across a 64-row word boundary.
+    add("word-boundaries", [[i, "a", "b", *(["c"] if i % 2 else [])] for i in range(1, 66)], [(1, 4)])
+    # Fractional thresholds: minSup 0.4 of 5 rows, maxPer 0.4 of the timeline.
+    add("fractional", [[2, "a"], [4, "a"], [6, "b"], [8, "a"], [10, "a"]], [(0.4, 0.4)])
+    # The reference's temporal generator (50 rows, 5 items, repeats and gaps).
+    from cupami import TemporalDatabase
+    g = TemporalDatabase(50, 5, avg_length=2.5, seed=42, repeatAllowed=True, missingAllowed=True)
+    g.create()
+    add("generator-50x5", [list(r) for r in g.getTransactions()], [(3, 20)])
+    # Deeper seeded cases: dense baskets over 14-16 items, increasing timestamps
+    # with repeats, several 64-row words.
+    for seed, n_rows, n_items in ((0, 600, 14), (1, 1500, 16), (2, 4000, 12)):
+        rng = np.random.default_rng(200 + seed)
+        p = rng.uniform(0.35, 0.95, n_items)
+        ts = np.cumsum(rng.integers(0, 4, n_rows))
+        rows = [[int(t), *[f"i{j}" for j in np.nonzero(rng.random(n_items) < p)[0]]] for t in ts]
+        end = int(ts[-1])
+        add(f"dense-seed{seed}", rows, [(0.3, max(8, end // 40)), (0.5, end // 10)])
+    return out
+
+
+def main():
+    cupami = load()
+    fixtures = {"generator": "tests/golden/make_periodic_golden.py", "reference": str(REF.name),
+                "cases": cases(cupami)}
+    (HERE / "periodic_patterns.json").write_text(json.dumps(fixtures, separators=(",", ":")))
+    n = sum(len(r[m]) for c in fixtures["cases"] for r in c["results"] for m in ("cuPFEclat", "cuPFApriori"))
+    print(f"wrote {len(fixtures['cases'])} cases, {n} patterns")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,283 @@
+"""Periodic-frequent miners (cuPFEclat / cuPFApriori) and the periodic_counts kernel.
+
+CPU part: the oracle (oracle/periodic.py) against the reference miners' own
+outputs (golden/periodic_patterns.json, made by golden/make_periodic_golden.py)
+and against a brute force; the depth-first and level orders built from
+shuffled pattern trees by the C ABI; the temporal input rules.
+GPU part: the drop-in miners and cpm_periodic_counts against the same
+fixtures and the oracle -- supports and periodicities exact, order included.
+"""
+import json
+import struct
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+GOLDEN = Path(__file__).parent / "golden" / "periodic_patterns.json"
+
+
+@pytest.fixture(scope="module")
+def fixtures():
+    return json.loads(GOLDEN.read_text())
+
+
+def _runs(fixtures):
+    for case in fixtures["cases"]:
+        for run in case["results"]:
+            yield case, run
+
+
+# ---- CPU: the oracle against the reference's own outputs ---------------------
+
+def test_oracle_reproduces_reference_miners(fixtures):
+    from oracle import periodic
+
+    checked = 0
+    for case, run in _runs(fixtures):
+        for name, algo in (("cuPFEclat", "eclat"), ("cuPFApriori", "apriori")):
+            got = periodic.mine(case["rows"], run["minSup"], run["maxPer"], algo, run["endTime"])
+            assert [[k, s, p] for k, (s, p) in got.items()] == run[name], (case["name"], name)
+            checked += 1
+    assert checked == 2 * sum(len(c["results"]) for c in fixtures["cases"])
+
+
+def test_paper_example_known_answer(fixtures):
+    run = fixtures["cases"][0]["results"][0]
+    assert len(run["cuPFApriori"]) == 9
+    assert ["a\tb", 4, 3] in run["cuPFApriori"]
+
+
+def test_oracle_matches_brute_force(fixtures):
+    from oracle import periodic
+
+    for case, run in _runs(fixtures):
+        labels = {str(x).strip() for r in case["rows"] for x in r[1:]}
+        if len(labels) > 12:
+            continue
+        want = periodic.brute_force(case["rows"], run["minSup"], run["maxPer"], run["endTime"])
+        got = periodic.mine(case["rows"], run["minSup"], run["maxPer"], "apriori", run["endTime"])
+        assert got == want, case["name"]
+
+
+def _tree(patterns, rng, prefix_tree):
+    """Pattern tree of (sorted column tuple, support, period) in a random emission order."""
+    order = sorted(range(len(patterns)), key=lambda i: (len(patterns[i][0]), rng.random()))
+    by_set, parent, item, support, period = {}, [], [], [], []
+    for new_id, i in enumerate(order):
+        items, sup, per = patterns[i]
+        if len(items) == 1:
+            parent.append(-1)
+            item.append(items[0])
+        else:
+            drop = len(items) - 1 if prefix_tree else int(rng.integers(len(items)))
+            parent.append(by_set[frozenset(items[:drop] + items[drop + 1:])])
+            item.append(items[drop])
+        support.append(sup)
+        period.append(per)
+        by_set[frozenset(items)] = new_id
+    return parent, item, support, period
+
+
+@pytest.mark.parametrize("prefix_tree", [False, True])
+@pytest.mark.parametrize("name,order", [("cuPFEclat", 3), ("cuPFApriori", 1)])
+def test_insertion_order_from_shuffled_trees(fixtures, name, order, prefix_tree):
+    from cupami_b200._native import Result
+
+    rng = np.random.default_rng(1)
+    checked = 0
+    for case, run in _runs(fixtures):
+        pats = [(k.split("\t"), s, p) for k, s, p in run[name]]
+        if not pats:
+            continue
+        labels = sorted({x for p, _, _ in pats for x in p})
+        col = {x: i for i, x in enumerate(labels)}
+        patterns = [(tuple(sorted(col[x] for x in p)), s, per) for p, s, per in pats]
+        parent, item, support, _ = _tree(patterns, rng, prefix_tree)
+        res = Result.from_tree(parent, item, support, order)
+        o = res.offsets.tolist()
+        got = [["\t".join(labels[c] for c in res.items[o[k]:o[k + 1]].tolist()), int(res.supports[k])]
+               for k in range(len(res))]
+        assert got == [[k, s] for k, s, _ in run[name]], (case["name"], name)
+        checked += 1
+    assert checked >= 12
+
+
+# ---- CPU: temporal input rules -------------------------------------------------
+
+def test_temporal_rows_sorting_empties_and_thresholds():
+    import cupami_b200
+
+    m = cupami_b200.cuPFEclat([[9, "a"], [0, " a", "a ", "0"], [4], ["", " "], [9, "a", "b"], [15]], 0.5, 0.5)
+    assert m._timestamps == [0, 4, 9, 9, 15]
+    assert m._Database == [("a", "0"), (), ("a",), ("a", "b"), ()]
+    assert m._transactionCount == 5 and m._minSup == 3
+    assert m._endTimestamp == 15 and m._maxPer == 7.5 and m._periodLimit() == 7
+    m = cupami_b200.cuPFApriori([[2, "x"], [3, "x"]], 1, 5, endTime=20)
+    assert m._endTimestamp == 20 and m._maxPer == 5
+    big = cupami_b200.cuPFApriori([[1, "x"]], 1, 1e30)
+    assert big._periodLimit() == np.iinfo(np.int64).max
+
+
+@pytest.mark.parametrize("cls_name", ["cuPFEclat", "cuPFApriori"])
+def test_invalid_temporal_inputs(tmp_path, cls_name):
+    import cupami_b200
+
+    cls = getattr(cupami_b200, cls_name)
+    for rows in ([[-1, "a"]], [[1.2, "a"]], [["bad", "a"]], [[2**63, "a"]]):
+        with pytest.raises(ValueError):
+            cls(rows, 1, 2)
+    for support, period in [(0, 1), (1, -1), (1, float("nan")), (float("inf"), 1), (True, 1), (1, True)]:
+        with pytest.raises((ValueError, OverflowError)):
+            cls([[1, "a"]], support, period)
+    with pytest.raises(ValueError):
+        cls([[5, "a"]], 1, 2, endTime=3)
+    path = tmp_path / "transactional.bin"
+    path.write_bytes(b"CUPAMI01" + bytes(24))
+    with pytest.raises(ValueError, match="temporal BIN"):
+        cls(path, 1, 2)
+
+
+def test_temporal_text_bin_and_parquet_inputs(tmp_path):
+    import pyarrow as pa
+    import pyarrow.parquet as pq
+
+    import cupami_b200
+
+    tab = tmp_path / "tab.txt"
+    tab.write_text("1\ta\tb\n3\ta\n5\tb\n")
+    assert cupami_b200.cuPFApriori(tab, 1, 5)._timestamps == [1, 3, 5]
+    space = tmp_path / "space.txt"
+    space.write_text("4 x y\n\n2 y\n")
+    m = cupami_b200.cuPFApriori(space, 1, 5)
+    assert m._timestamps == [2, 4] and m._Database == [("y",), ("x", "y")]
+    rows = [[3, 7, 7, 1], [1], [2, 4294967295]]
+    offsets, flat = [0], []
+    for r in rows:
+        flat.extend(r[1:])
+        offsets.append(len(flat))
+    path = tmp_path / "t.bin"
+    path.write_bytes(struct.pack("<8sQQQ", b"CUPAMIT1", len(rows), len(flat), 4294967295)
+                     + struct.pack(f"<{len(rows)}q", *[r[0] for r in rows])
+                     + struct.pack(f"<{len(offsets)}Q", *offsets) + struct.pack(f"<{len(flat)}I", *flat))
+    m = cupami_b200.cuPFEclat(path, 1, 3)
+    assert m._timestamps == [1, 2, 3]
+    assert m._Database == [(), ("4294967295",), ("7", "1")]
+    path.write_bytes(path.read_bytes()[:-4])
+    with pytest.raises(ValueError, match="size"):
+        cupami_b200.cuPFEclat(path, 1, 3)
+    table = pa.table({"timestamp": pa.array([r[0] for r in rows], pa.int64()),
+                      "items": pa.array([r[1:] for r in rows], pa.list_(pa.uint32()))})
+    pq.write_table(table, tmp_path / "t.parquet")
+    m = cupami_b200.cuPFEclat(tmp_path / "t.parquet", 1, 3)
+    assert m._timestamps == [1, 2, 3] and m._Database == [(), ("4294967295",), ("7", "1")]
+
+
+# ---- GPU: the drop-in miners against the reference's outputs ------------------
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["cuPFEclat", "cuPFApriori"])
+def test_gpu_miners_match_reference(fixtures, name):
+    import cupami_b200
+
+    cls = getattr(cupami_b200, name)
+    for case, run in _runs(fixtures):
+        miner = cls(case["rows"], run["minSup"], run["maxPer"], endTime=run["endTime"])
+        miner.mine()
+        got = [[k, s, p] for k, (s, p) in miner.getPatterns().items()]
+        assert got == run[name], (case["name"], run["minSup"], run["maxPer"])
+        miner.mine()  # mining again gives the same answer
+        assert [[k, s, p] for k, (s, p) in miner.getPatterns().items()] == run[name]
+
+
+@pytest.mark.gpu
+def test_gpu_output_apis(tmp_path, fixtures):
+    import cupami_b200
+
+    case = fixtures["cases"][0]
+    miner = cupami_b200.cuPFApriori(case["rows"], 3, 3)
+    miner.mine()
+    df = miner.getPatternsAsDataFrame()
+    assert list(df.columns) == ["Patterns", "Support", "Periodicity"] and len(df) == 9
+    out = tmp_path / "patterns.txt"
+    miner.save(out)
+    lines = out.read_text().splitlines()
+    assert "a\tb : 4 : 3" in lines and lines == sorted(lines, key=lambda x: tuple(x.split(" : ")[0].split("\t")))
+    assert miner.getRuntime() >= 0 and miner.getInputBackend()["backend"] == "cpu"
+    assert miner.getKernelStats()["n_patterns"] == 9
+
+
+def _random_temporal(seed, n_rows, n_items, density=(0.2, 0.9), max_step=5):
+    rng = np.random.default_rng(seed)
+    p = rng.uniform(*density, n_items)
+    ts = np.cumsum(rng.integers(0, max_step, n_rows))
+    return [[int(t), *[f"v{j}" for j in np.nonzero(rng.random(n_items) < p)[0]]] for t in ts]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed,n_rows,n_items", [(5, 20000, 14), (6, 70001, 10), (7, 3000, 40)])
+def test_gpu_miners_match_oracle_on_larger_inputs(seed, n_rows, n_items):
+    """Many 64-row words, ragged last word, deep levels; both miners, order included."""
+    import cupami_b200
+    from oracle import periodic
+
+    rows = _random_temporal(seed, n_rows, n_items, density=(0.3, 0.95) if n_items <= 20 else (0.05, 0.6))
+    end = rows[-1][0]
+    for min_sup, max_per in ((0.25, max(6, end // 400)), (0.1, end // 50)):
+        labels, bits, timestamps, end_ts = periodic.prepare(rows)
+        count, limit = periodic.thresholds(min_sup, max_per, len(timestamps), end_ts)
+        want_a = periodic.pf_apriori(labels, bits, timestamps, end_ts, count, limit)
+        for name, want in (("cuPFApriori", want_a), ("cuPFEclat", None)):
+            miner = getattr(cupami_b200, name)(rows, min_sup, max_per)
+            miner.mine()
+            got = [(k, s, p) for k, (s, p) in miner.getPatterns().items()]
+            if want is None:
+                want = periodic.pf_eclat(labels, bits, timestamps, end_ts, count, limit)
+            assert got == [("\t".join(p), s, per) for p, s, per in want], (name, min_sup, max_per)
+
+
+@pytest.mark.gpu
+def test_gpu_periodic_counts_kernel_exact():
+    """cpm_periodic_counts (the reference kernel's drop-in) on random candidates:
+    supports and periodicities equal the oracle's for every candidate, passing or not."""
+    import torch
+
+    from cupami_b200.frequentPattern import _bitsets
+    from cupami_b200.periodicFrequentPattern import _temporal
+    from oracle import periodic
+
+    rng = np.random.default_rng(11)
+    for n_rows, n_items, base in ((1, 3, 0), (31, 5, 7), (32, 5, 0), (33, 6, 2**40), (1000, 12, 0), (4097, 9, 2**53)):
+        rows = _random_temporal(int(rng.integers(1 << 30)), n_rows, n_items, density=(0.05, 0.95))
+        for r in rows:
+            r[0] += base
+        labels, bits, timestamps, end = periodic.prepare(rows, end_time=rows[-1][0] + 3)
+        d_bits = torch.from_numpy(bits.view(np.int32).copy()).cuda()
+        d_ts = torch.from_numpy(timestamps.copy()).cuda()
+        for width in (1, 2, 3, len(labels)):
+            cands = [sorted(rng.choice(len(labels), size=min(width, len(labels)), replace=False).tolist())
+                     for _ in range(50)]
+            got = _temporal.periodic_counts(d_bits, cands, d_ts, len(timestamps), end)
+            assert got == periodic.periodic_counts(bits, cands, timestamps, len(timestamps), end), (n_rows, width)
+        # fewer transactions than bitset rows: rows past n are skipped
+        cut = max(0, len(timestamps) - 5)
+        cands = [[c] for c in range(len(labels))]
+        assert (_temporal.periodic_counts(d_bits, cands, d_ts, cut, end)
+                == periodic.periodic_counts(bits, cands, timestamps, cut, end))
+    assert _bitsets is not None
+
+
+@pytest.mark.gpu
+def test_gpu_empty_and_degenerate_inputs():
+    import cupami_b200
+
+    for cls in (cupami_b200.cuPFEclat, cupami_b200.cuPFApriori):
+        m = cls([], 1, 0)
+        m.mine()
+        assert m.getPatterns() == {}
+        m = cls([[3], [5]], 1, 10)  # only empty baskets: no items
+        m.mine()
+        assert m.getPatterns() == {}
+        m = cls([[0, "x"], [0, "y"]], 1, 0)
+        m.mine()
+        assert m.getPatterns() == {"x": (1, 0), "y": (1, 0)}
