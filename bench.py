@@ -51,7 +51,12 @@ WORKLOADS = {
     "sparse-zipf-250k": ("sparse_zipf_250k", 0.001, ("eclat",)),
     # 512 independent databases mined in one pass (cuEclat.mineBatch)
     "batched-zipf-512": ("batched_zipf", 0.01, ("eclat-batch",)),
+    # temporal database (100,000 rows, 200 items) mined by cuPFEclat and cuPFApriori
+    "temporal-100k": ("temporal_planted", 0.005, ("pf-eclat", "pf-apriori")),
 }
+
+# Periodicity limits (timestamp units) of the temporal workloads.
+MAX_PER = {"temporal-100k": 2500}
 
 
 # Published mine() seconds of the reference on a workload (cuEclat + cuApriori
@@ -298,6 +303,224 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def periodic_workload(name, rank):
+    """(csr, timestamps, transactions as label tuples, minSup, maxPer, seed) of a temporal workload."""
+    from cupami_b200 import datasets
+
+    gen, minsup, _ = WORKLOADS[name]
+    seed = rank_seed(name, rank)
+    csr, ts = getattr(datasets, gen)(seed=seed)
+    o, it = csr.offsets.tolist(), [str(v) for v in csr.items.tolist()]
+    baskets = [tuple(it[o[i]:o[i + 1]]) for i in range(len(o) - 1)]
+    return csr, ts, baskets, minsup, MAX_PER[name], seed
+
+
+def periodic_cpu_seconds(baskets, ts, minsup, maxper):
+    """The reference's periodic miners restated on one core (oracle.periodic), one full step."""
+    from oracle import periodic
+
+    t0 = time.perf_counter()
+    rows = [[int(t), *b] for t, b in zip(ts.tolist(), baskets)]
+    labels, bits, timestamps, end = periodic.prepare(rows)
+    count, limit = periodic.thresholds(minsup, maxper, len(timestamps), end)
+    for fn in (periodic.pf_eclat, periodic.pf_apriori):
+        fn(labels, bits, timestamps, end, count, limit)
+    return time.perf_counter() - t0
+
+
+def run_periodic_reference(args, world, rank, local):
+    if rank != 0:
+        return
+    csr, ts, baskets, minsup, maxper, seed = periodic_workload(args.workload, 0)
+    times = [periodic_cpu_seconds(baskets, ts, minsup, maxper) for _ in range(args.warmup + args.steps)]
+    v = statistics.mean(times[args.warmup:])
+    line = {
+        "impl": "reference", "metric": "mine() seconds per step (pf-eclat+pf-apriori)",
+        "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "i64", "data": "synthetic",
+        "config": {"workload": args.workload, "seed": seed, "minSup": minsup, "maxPer": maxper},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "port",
+                         "sample": "whole step (NumPy restatement of the reference periodic miners)"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_periodic(args, world, rank, local):
+    """cuPFEclat + cuPFApriori on a temporal database: device time with resident
+    tidsets, the drop-in API from host rows, the periodic_counts kernel against
+    the roofline, and the reference's kernels and host path beside them."""
+    import torch
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    import cupami_b200
+    from cupami_b200 import _native
+    from cupami_b200.frequentPattern import _bitsets
+    from cupami_b200.periodicFrequentPattern import _temporal
+
+    csr, ts, baskets, minsup, maxper, seed = periodic_workload(args.workload, rank)
+    n = len(baskets)
+    end = int(ts[-1])
+    labels = sorted({x for b in baskets for x in b})
+    index = {label: i for i, label in enumerate(labels)}
+    cols = np.fromiter((index[x] for b in baskets for x in b), dtype=np.uint32, count=csr.nnz)
+    ctx = _native.context(local)
+    db = _native.Database.from_temporal(ctx, csr.offsets, cols, len(labels), ts, end)
+    ms_count = cupami_b200.cuApriori._getSupportCount(minsup, n)
+    codes = [("pf-eclat", _native.CPM_ECLAT, _native.CPM_ORDER_DEPTH_FIRST),
+             ("pf-apriori", _native.CPM_APRIORI, _native.CPM_ORDER_APRIORI)]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+
+    def device_step():
+        return [(a, db.mine_periodic(ms_count, maxper, code, order)) for a, code, order in codes]
+
+    for _ in range(args.warmup):
+        device_step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    sampler = ClockSampler(local)
+    step_ms, launches, last = [], 0, None
+    for _ in range(args.steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        last = device_step()
+        step_ms.append(sum(r.stats["ms_total"] for _, r in last))
+        launches += sum(int(r.stats["kernel_launches"]) for _, r in last)
+    clocks = sampler.stop()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+
+    def api_step():
+        t, d2h = 0.0, 0
+        for cls in (cupami_b200.cuPFEclat, cupami_b200.cuPFApriori):
+            m = cls([[int(t_), *b] for t_, b in zip(ts.tolist(), baskets)], minsup, maxper)
+            m.mine()
+            t += m.getMiningTime()
+            d2h += 20 * len(m._result)  # parent, item, support (4 bytes each) and periodicity (8) per pattern
+        return t, d2h
+
+    for _ in range(args.warmup):
+        api_step()
+    e2e, d2h = [], 0
+    for _ in range(args.steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        t, d2h = api_step()
+        e2e.append(t)
+    value = statistics.mean(step_ms) / 1e3
+    e2e_v = statistics.mean(e2e)
+    if pg:
+        value, e2e_v = max_over_ranks([value, e2e_v], "cuda")
+        pg.destroy_process_group()
+    # The counting kernel alone (k_periodic through cpm_periodic_counts, no early
+    # stop) on every pair of the kept items, timed with CUDA events on the
+    # library's stream.  Algorithmic bytes per candidate: its two rows of 32-bit
+    # words, a timestamp per set row, the two column ids and the two results.
+    rows_idx = torch.from_numpy(np.repeat(np.arange(n, dtype=np.int64),
+                                          np.diff(csr.offsets.astype(np.int64))).copy()).cuda()
+    bits32 = _bitsets.build_bitsets(None, rows_idx, torch.from_numpy(cols.view(np.int32).copy()).cuda(), n,
+                                    len(labels))
+    d_ts = torch.from_numpy(ts.copy()).cuda()
+    apriori = dict(last)["pf-apriori"]  # by length: the kept single items come first
+    singles = int(np.count_nonzero(np.diff(apriori.offsets.astype(np.int64)) == 1))
+    kept = sorted(int(c) for c in apriori.items[:singles])
+    pairs = np.array([(a, b) for i, a in enumerate(kept) for b in kept[i + 1:]], dtype=np.uint32).reshape(-1, 2)
+    d_pairs = torch.from_numpy(pairs.view(np.int32).copy()).cuda()
+    sup = torch.zeros(len(pairs), dtype=torch.int64, device="cuda")
+    per = torch.zeros(len(pairs), dtype=torch.int64, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    lib = _native.library()
+
+    def launch():
+        ctx.check(lib.cpm_periodic_counts(ctx.handle, bits32.data_ptr(), bits32.shape[1], d_pairs.data_ptr(),
+                                          len(pairs), 2, d_ts.data_ptr(), n, end, sup.data_ptr(), per.data_ptr()))
+
+    for _ in range(3):
+        launch()
+    ctx.check(lib.cpm_synchronize(ctx.handle))
+    kms = []
+    for _ in range(args.steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launch()
+        e1.record(stream)
+        e1.synchronize()
+        kms.append(e0.elapsed_time(e1))
+    k_ms = statistics.mean(kms)
+    alg_bytes = len(pairs) * (2 * bits32.shape[1] * 4 + 8 + 16) + 8 * int(sup.sum().item())
+    achieved = alg_bytes / (k_ms * 1e-3) / 1e9
+    hbm, _, src = peaks()
+    roof = {"kernel": "k_periodic (cpm_periodic_counts, every pair of the kept items)", "bound": "hbm",
+            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+            "peak_source": src, "ms_per_launch": k_ms, "alg_bytes_per_launch": alg_bytes, "candidates": len(pairs),
+            "alg_bytes": "per candidate: 2 rows x words32 x 4 + 8 per set row (timestamps) + 24 (ids, results); "
+                         "the bitsets (items x rows / 8 bytes) stay in L2 between candidates"}
+    if rank != 0:
+        return
+    ours = {a: [("\t".join(labels[c] for c in r.items[int(r.offsets[k]):int(r.offsets[k + 1])].tolist()),
+                 int(r.supports[k]), int(r.periods[k])) for k in range(len(r))] for a, r in last}
+    ref_leg = None
+    if not args.no_ref_gpu:
+        from oracle import ref_gpu
+
+        if ref_gpu.available():
+            k = ref_gpu.RefKernels(local)
+            limit = min(int(np.floor(maxper)), np.iinfo(np.int64).max)
+            got = {}
+            for warm in (True, False):
+                t0 = time.perf_counter()
+                for a in ("pf-eclat", "pf-apriori"):
+                    found = ref_gpu.periodic_mine(baskets, ts.tolist(), end, ms_count, limit,
+                                                  "eclat" if a == "pf-eclat" else "apriori", k)
+                    got[a] = [("\t".join(p), s_, p_) for p, s_, p_ in found]
+                spent = time.perf_counter() - t0
+                if warm:
+                    first = spent
+            ref_leg = {"value": spent, "unit": "s", "first_call_s": first, "sample": "whole step, warm",
+                       "identical_output": got == ours,
+                       "kind": "reference periodic_counts and build_bitsets (cupami sources, nvcc sm_100a) "
+                               "+ reference driver loops; torch tensors in place of CuPy arrays"}
+        else:
+            ref_leg = {"unavailable": "oracle/_ref/libref_bitsets.so not built"}
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = {"value": periodic_cpu_seconds(baskets, ts, minsup, maxper), "unit": "s", "cores": 1,
+               "kind": "port", "sample": "whole step (NumPy restatement of the reference periodic miners)"}
+    line = {
+        "metric": "mine() seconds per step (pf-eclat+pf-apriori)",
+        "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "i64", "data": "synthetic",
+        "config": {"workload": args.workload, "seed": seed, "minSup": minsup, "maxPer": maxper,
+                   "transactions": n, "items": len(labels), "l2": "256 MB buffer rewritten before every timed step",
+                   "parallelism": f"replicas{world}" if world > 1 else "single"},
+        "e2e": {"value": e2e_v, "unit": "s", "h2d_bytes_per_step": 2 * (csr.offsets.nbytes + csr.nnz * 4 + ts.nbytes),
+                "d2h_bytes_per_step": d2h},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "reference_gpu": ref_leg,
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "patterns": [len(r) for _, r in last],
+        "kernel_stats": [r.stats for _, r in last],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -316,6 +539,8 @@ def main():
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup()
+    if args.workload in MAX_PER:
+        return (run_periodic_reference if args.impl == "reference" else run_periodic)(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, world, rank)
 

@@ -107,6 +107,7 @@ _SIGNATURES = {
     "cpm_count_supports": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, _P]),
     "cpm_intersect_extensions": (ctypes.c_int, [_P, _P, _P, _U64, _U64, _P, _P]),
     "cpm_synchronize": (ctypes.c_int, [_P]),
+    "cpm_stream": (ctypes.c_void_p, [_P]),
     "cpm_costmodel_params": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
     "cpm_costmodel_train": (ctypes.c_int, [_P, _P, _P, _U64, ctypes.c_uint32, ctypes.c_float, _U64, _P, _P]),
     "cpm_costmodel_predict": (ctypes.c_int, [_P, _P, _P, _U64, _P]),
@@ -171,6 +172,10 @@ class Context:
         if code != CPM_OK:
             msg = library().cpm_last_error(self.handle)
             raise NativeError(code, msg.decode() if msg else "")
+
+    def stream(self):
+        """The library's CUDA stream on this context, as an integer handle."""
+        return int(library().cpm_stream(self.handle) or 0)
 
     def close(self):
         if self.handle:

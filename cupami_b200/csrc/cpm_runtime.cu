@@ -235,6 +235,8 @@ extern "C" void cpm_shutdown(cpm_ctx *ctx) {
 
 extern "C" const char *cpm_last_error(const cpm_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
 
+extern "C" void *cpm_stream(const cpm_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
 extern "C" int cpm_synchronize(cpm_ctx *ctx) {
     if (!ctx) return CPM_EINVAL;
     CK(cudaStreamSynchronize(ctx->stream));

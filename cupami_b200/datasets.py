@@ -27,7 +27,7 @@ import numpy as np
 __all__ = [
     "TransactionCSR", "uniform_poisson", "planted_zipf", "dense_fixed_length",
     "dense_bernoulli", "sparse_zipf", "batched_zipf", "reference_uniform_baskets",
-    "workload",
+    "temporal_planted", "workload",
 ]
 
 
@@ -302,6 +302,41 @@ _WORKLOADS = {
     "dense-bernoulli-64k": (dense_bernoulli, 0.6),
     "sparse-zipf-1m": (sparse_zipf, 0.001),
 }
+
+
+def temporal_planted(n=100_000, n_items=200, mean=6, n_patterns=40, pattern_mean=3, planted=0.35,
+                     empty=0.02, s=1.1, seed=23):
+    """A temporal database: ``(csr, timestamps)`` with one row per transaction.
+
+    Timestamps are a running sum of gaps drawn uniformly from {0, 1, 2, 3}
+    (equal timestamps occur).  A pool of ``n_patterns`` patterns (lengths
+    max(1, Poisson(pattern_mean)), Zipf(s) items) is drawn first; each row
+    holds one pattern from the pool with probability ``planted`` and is filled
+    with Zipf(s) noise to a Poisson(mean) length; a fraction ``empty`` of the
+    rows are empty baskets, which temporal databases keep.
+    """
+    rng = np.random.default_rng(seed)
+    zipf = _zipf_sampler(n_items, s)
+    plen = np.clip(rng.poisson(pattern_mean, n_patterns), 1, n_items)
+    p_off, p_items = _sample_distinct(rng, zipf, plen)
+    width = int(plen.max())
+    pool = np.full((n_patterns + 1, width), -1, dtype=np.int64)  # last row: no pattern
+    for i in range(n_patterns):
+        seg = p_items[p_off[i]:p_off[i + 1]]
+        pool[i, :seg.size] = seg
+    choice = np.where(rng.random(n) < planted, rng.integers(0, n_patterns, n), n_patterns)
+    lengths = np.clip(rng.poisson(mean, n), 1, n_items)
+    offsets, items = _sample_distinct(rng, zipf, lengths, prefix=pool[choice])
+    lengths = np.diff(offsets.astype(np.int64))
+    keep = rng.random(n) >= empty
+    starts = offsets[:-1].astype(np.int64)
+    mask = np.repeat(keep, lengths)
+    new_len = np.where(keep, lengths, 0).astype(np.uint64)
+    new_off = np.zeros(n + 1, dtype=np.uint64)
+    np.cumsum(new_len, out=new_off[1:])
+    del starts
+    timestamps = np.cumsum(rng.integers(0, 4, n)).astype(np.int64)
+    return TransactionCSR(new_off, items[mask], n_items), timestamps
 
 
 def workload(name: str):

@@ -237,6 +237,9 @@ int cpm_intersect_extensions(cpm_ctx *ctx, const uint32_t *d_prefix,
                              uint64_t n_extensions, uint32_t *d_out, uint64_t *d_supports);
 /* Waits for the context's stream. */
 int cpm_synchronize(cpm_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t), so that callers can order their
+ * own work or timing events with the library's launches. */
+void *cpm_stream(const cpm_ctx *ctx);
 
 /* ---- periodic-frequent patterns (cupami/periodicFrequentPattern) -----------
  * A temporal database holds one row per transaction in timestamp order, empty

@@ -1,12 +1,13 @@
 """Build recipe for oracle/_ref/libref_bitsets.so -- TEST INFRASTRUCTURE ONLY.
 
-The reference compiles its three bitset kernels at run time from a CUDA source
-string (``_SOURCE`` in cupami/frequentPattern/_bitsets.py:19-78, NVRTC, cached
-per device).  This recipe compiles the same string ahead of time for sm_100a:
-it reads the string out of the reference file with ``ast`` (the module is not
-imported or executed), writes it to a temporary file under ``oracle/_ref/``
-(deleted after the compile) and builds ``oracle/ref_launch.cu`` (host
-launchers written here) around it with nvcc.
+The reference compiles its kernels at run time from CUDA source strings
+(``_SOURCE`` in cupami/frequentPattern/_bitsets.py:19-78 -- the three bitset
+kernels -- and in cupami/periodicFrequentPattern/_temporal.py:26-53 --
+``periodic_counts``; NVRTC, cached per device).  This recipe compiles the same
+strings ahead of time for sm_100a: it reads them out of the reference files
+with ``ast`` (the modules are not imported or executed), writes them to a
+temporary file under ``oracle/_ref/`` (deleted after the compile) and builds
+``oracle/ref_launch.cu`` (host launchers written here) around it with nvcc.
 Outputs go to ``oracle/_ref/`` only; that folder is git-ignored and ships with
 the built library.  Without the reference sources (as on a machine that only
 has the prebuilt files) it does nothing.
@@ -29,21 +30,31 @@ DEFAULT_ROOT = Path("/root/reference")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 
+SOURCES = (("frequentPattern", "_bitsets.py"), ("periodicFrequentPattern", "_temporal.py"))
+
+
 def reference_source(root: Path) -> str:
-    src = (root / "cupami" / "frequentPattern" / "_bitsets.py").read_text()
-    for node in ast.parse(src).body:
-        if isinstance(node, ast.Assign) and any(getattr(t, "id", None) == "_SOURCE" for t in node.targets):
-            return ast.literal_eval(node.value)
-    raise RuntimeError("_SOURCE not found in the reference's _bitsets.py")
+    """The kernel source strings of the reference files in SOURCES, one after the other."""
+    out = []
+    for package, name in SOURCES:
+        src = (root / "cupami" / package / name).read_text()
+        for node in ast.parse(src).body:
+            if isinstance(node, ast.Assign) and any(getattr(t, "id", None) == "_SOURCE" for t in node.targets):
+                out.append(ast.literal_eval(node.value))
+                break
+        else:
+            raise RuntimeError(f"_SOURCE not found in the reference's {name}")
+    return "\n".join(out)
 
 
 def build(root: Path = DEFAULT_ROOT, force: bool = False) -> Path | None:
     """Compile the reference kernels; returns the library path (None without the sources)."""
-    ref_file = root / "cupami" / "frequentPattern" / "_bitsets.py"
-    if not ref_file.exists():
+    ref_files = [root / "cupami" / package / name for package, name in SOURCES]
+    if not all(f.exists() for f in ref_files):
         return LIB if LIB.exists() else None
     shim = HERE / "ref_launch.cu"
-    if not force and LIB.exists() and LIB.stat().st_mtime >= max(shim.stat().st_mtime, ref_file.stat().st_mtime):
+    newest = max([shim.stat().st_mtime, Path(__file__).stat().st_mtime] + [f.stat().st_mtime for f in ref_files])
+    if not force and LIB.exists() and LIB.stat().st_mtime >= newest:
         return LIB
     OUT.mkdir(exist_ok=True)
     cu = OUT / ("ref_bitsets.%d.cu" % os.getpid())  # build intermediate, removed below

@@ -90,14 +90,24 @@ def _accept(support, period, min_sup, max_per):
     return support >= min_sup and support > 0 and period <= max_per
 
 
-def pf_eclat(labels, bits, timestamps, end, min_sup, max_per, batch=4096):
-    """cuPFEclat.mine: ``[(pattern tuple, support, periodicity)]`` in insertion order."""
+def _counter(bits, timestamps, end, counts):
+    """Candidate column lists -> [(support, periodicity)]: the NumPy kernel, or
+    ``counts`` (another implementation of the same kernel, e.g. the reference's
+    CUDA kernel) when given."""
+    if counts is not None:
+        return counts
     n = len(timestamps)
+    return lambda cands: periodic_counts(bits, cands, timestamps, n, end)
+
+
+def pf_eclat(labels, bits, timestamps, end, min_sup, max_per, batch=4096, counts=None):
+    """cuPFEclat.mine: ``[(pattern tuple, support, periodicity)]`` in insertion order."""
     index = {label: i for i, label in enumerate(labels)}
     found = []
+    count = _counter(bits, timestamps, end, counts)
 
     def evaluate(patterns):
-        return periodic_counts(bits, [[index[x] for x in p] for p in patterns], timestamps, n, end)
+        return count([[index[x] for x in p] for p in patterns])
 
     singles = [(label,) for label in labels]
     frequent = []
@@ -146,18 +156,17 @@ def _generate(level):
     return sorted(out)
 
 
-def pf_apriori(labels, bits, timestamps, end, min_sup, max_per, batch=4096):
+def pf_apriori(labels, bits, timestamps, end, min_sup, max_per, batch=4096, counts=None):
     """cuPFApriori.mine: ``[(pattern tuple, support, periodicity)]`` level by level."""
-    n = len(timestamps)
     index = {label: i for i, label in enumerate(labels)}
     found = []
+    count = _counter(bits, timestamps, end, counts)
     candidates = [(label,) for label in labels]
     while candidates:
         level = []
         for start in range(0, len(candidates), batch):
             chunk = candidates[start:start + batch]
-            counts = periodic_counts(bits, [[index[x] for x in p] for p in chunk], timestamps, n, end)
-            for pattern, (s, p) in zip(chunk, counts):
+            for pattern, (s, p) in zip(chunk, count([[index[x] for x in p] for p in chunk])):
                 if _accept(s, p, min_sup, max_per):
                     found.append((pattern, s, p))
                     level.append(pattern)

@@ -14,6 +14,9 @@ the reference has them:
   singletons, pair batches       cupami/frequentPattern/cuEclat.py:168-203
   class search                   cupami/frequentPattern/cuEclat.py:211-245
   Apriori levels                 cupami/frequentPattern/cuApriori.py:473-535
+  periodic miners                cupami/periodicFrequentPattern/_temporal.py:150-171,
+                                 cuPFEclat.py:146-175, cuPFApriori.py:141-157
+                                 (drivers restated in ``oracle.periodic``)
 
 Used by the benchmark's reference-GPU leg and by a parity test; the product
 never imports it.
@@ -45,7 +48,9 @@ def _load():
         lib.ref_build_bitsets.argtypes = [u64, p, p, u64, p, p]
         lib.ref_count_supports.argtypes = [p, u64, p, u32, u64, p, p]
         lib.ref_intersect_extensions.argtypes = [p, p, u64, u64, p, p, p]
-        for f in (lib.ref_build_bitsets, lib.ref_count_supports, lib.ref_intersect_extensions):
+        lib.ref_periodic_counts.argtypes = [p, u64, p, u32, u32, p, u64, ctypes.c_int64, p, p, p]
+        for f in (lib.ref_build_bitsets, lib.ref_count_supports, lib.ref_intersect_extensions,
+                  lib.ref_periodic_counts):
             f.restype = ctypes.c_int
         _lib = lib
     return _lib
@@ -162,3 +167,46 @@ def mine(off, ids, minsup_count, algorithm="eclat", kernels=None, out=None):
         minsup_count = support_count(minsup_count, n_tx)
     fn = numpy_port.eclat if algorithm == "eclat" else numpy_port.apriori
     return fn(labels, rows, cols, n_tx, minsup_count, k, out)
+
+
+def periodic_mine(transactions, timestamps, end, min_sup, max_per, algorithm="eclat", kernels=None):
+    """The reference's periodic miners on this GPU: ``[(pattern, support, periodicity)]``.
+
+    ``transactions`` are the cleaned baskets in timestamp order (empty ones
+    included) and ``timestamps`` their timestamps; ``min_sup`` and ``max_per``
+    are resolved thresholds.  As ``TemporalInput._prepare`` does
+    (_temporal.py:150-157): (row, column) pairs built on the host
+    (cuApriori.py:396-404), tidsets by the reference's build_bitsets, the
+    timestamps uploaded; then the restated driver loop launches the reference's
+    periodic_counts on every candidate batch with one upload of the candidates
+    and one download of the results per batch, as ``_evaluate`` does (:159-165)."""
+    import torch
+
+    from . import periodic
+
+    k = kernels or RefKernels()
+    labels = sorted({item for row in transactions for item in row})
+    index = {label: i for i, label in enumerate(labels)}
+    rows, cols = [], []
+    for r, basket in enumerate(transactions):
+        rows.extend([r] * len(basket))
+        cols.extend(index[item] for item in basket)
+    d_rows = torch.tensor(rows, dtype=torch.int64).to(k.device)
+    d_cols = torch.tensor(cols, dtype=torch.int32).to(k.device)
+    n = len(transactions)
+    bits = k.pack(d_rows, d_cols, n, len(labels))
+    d_ts = torch.tensor(list(timestamps), dtype=torch.int64).to(k.device)
+
+    def counts(cands):
+        k._time_left()
+        idx = torch.tensor(cands, dtype=torch.int64).to(torch.int32).to(k.device)
+        m = idx.shape[0]
+        sup = torch.empty(m, dtype=torch.int64, device=k.device)
+        per = torch.empty(m, dtype=torch.int64, device=k.device)
+        k._check(k.lib.ref_periodic_counts(bits.data_ptr(), bits.shape[1], idx.data_ptr(), idx.shape[1], m,
+                                           d_ts.data_ptr() if n else None, n, int(end), sup.data_ptr(),
+                                           per.data_ptr(), k._stream()), "periodic_counts")
+        return list(zip(sup.cpu().tolist(), per.cpu().tolist()))
+
+    fn = periodic.pf_eclat if algorithm == "eclat" else periodic.pf_apriori
+    return fn(labels, None, None, end, min_sup, max_per, counts=counts)

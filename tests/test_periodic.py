@@ -252,6 +252,8 @@ def test_gpu_periodic_counts_kernel_exact():
         for r in rows:
             r[0] += base
         labels, bits, timestamps, end = periodic.prepare(rows, end_time=rows[-1][0] + 3)
+        if not labels:
+            continue
         d_bits = torch.from_numpy(bits.view(np.int32).copy()).cuda()
         d_ts = torch.from_numpy(timestamps.copy()).cuda()
         for width in (1, 2, 3, len(labels)):
@@ -281,3 +283,33 @@ def test_gpu_empty_and_degenerate_inputs():
         m = cls([[0, "x"], [0, "y"]], 1, 0)
         m.mine()
         assert m.getPatterns() == {"x": (1, 0), "y": (1, 0)}
+
+
+@pytest.mark.gpu
+def test_gpu_reference_kernel_agrees_with_fixtures(fixtures):
+    """The reference's own periodic_counts (compiled from its source into
+    oracle/_ref) under the restated drivers gives the fixtures' answers: the
+    kernel statement used to make the fixtures is the reference kernel's."""
+    from oracle import periodic, ref_gpu
+
+    if not ref_gpu.available():
+        pytest.skip("oracle/_ref/libref_bitsets.so is not built")
+    kernels = ref_gpu.RefKernels(0)
+    for case, run in _runs(fixtures):
+        rows = case["rows"]
+        labels, bits, timestamps, end = periodic.prepare(rows, run["endTime"])
+        count, limit = periodic.thresholds(run["minSup"], run["maxPer"], len(timestamps), end)
+        limit = min(int(np.floor(limit)), np.iinfo(np.int64).max)
+        records = sorted(((int(str(r[0]).strip()), r) for r in rows if any(str(v).strip() for v in r)),
+                         key=lambda x: x[0])
+        baskets = []
+        for _, r in records:
+            items = []
+            for v in r[1:]:
+                label = str(v).strip()
+                if label and label not in items:
+                    items.append(label)
+            baskets.append(tuple(items))
+        for name, algo in (("cuPFEclat", "eclat"), ("cuPFApriori", "apriori")):
+            found = ref_gpu.periodic_mine(baskets, timestamps.tolist(), end, count, limit, algo, kernels)
+            assert [["\t".join(p), s, per] for p, s, per in found] == run[name], (case["name"], name)
