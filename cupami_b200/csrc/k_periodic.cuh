@@ -7,10 +7,11 @@
 // (end when s = 0), scanning the set bits of the AND of X's rows in order with
 // one thread per candidate (_temporal.py:26-53, launch :156-165).
 //
-// Here one warp handles a candidate: the lanes read 32 consecutive words of
-// every row of the candidate per step (coalesced), each lane reduces its word
-// to a segment summary (count, first and last timestamp, largest inner gap),
-// and the warp joins the 32 summaries in row order with shuffles.  The join
+// Here one warp handles a candidate: per step the lanes read 32 * 4
+// consecutive words of every row of the candidate (4 consecutive words a
+// lane), each lane reduces its words to a segment summary (count, first and
+// last timestamp, largest inner gap), and the warp joins the 32 summaries in
+// row order with shuffles.  The join
 //     (a, b) -> {a.cnt + b.cnt, a.first, b.last, max(a.gap, b.gap, b.first - a.last)}
 // (an empty side yields the other) is associative, so the tree gives exactly
 // the sequential scan's maximum.  With kPrune (the miner), a candidate stops as
@@ -70,6 +71,10 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
            uint64_t n_tx, long long end, long long need, long long max_per, unsigned long long *__restrict__ support,
            long long *__restrict__ period, uint32_t *__restrict__ pass) {
     constexpr unsigned B = sizeof(Word) * 8;
+    // Each lane takes PL consecutive words per step (independent loads in
+    // flight, and one shuffle tree per 32 * PL words).
+    constexpr unsigned PL = 4;
+    constexpr uint64_t TILE = 32 * PL;
     const uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     if (c >= n) return;  // whole warps: c is the same on every lane
@@ -85,29 +90,36 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
     const uint64_t words = (n_tx + B - 1) / B;
     PSeg run{0, 0, 0, 0};
     bool stopped = false;
-    for (uint64_t base = 0; base < words; base += 32) {
-        const uint64_t v = base + lane;
-        Word x = 0;
-        if (v < words) {
-            x = ~Word(0);
-            for (uint32_t j = 0; j < width; ++j) x &= __ldg(bits + (uint64_t)cc[j] * stride + v);
-            const uint64_t lo = v * B;
-            if (n_tx - lo < B) x &= (Word(1) << (unsigned)(n_tx - lo)) - Word(1);
+    for (uint64_t base = 0; base < words; base += TILE) {
+        const uint64_t v0 = base + (uint64_t)lane * PL;
+        Word x[PL];
+#pragma unroll
+        for (unsigned q = 0; q < PL; ++q) x[q] = v0 + q < words ? ~Word(0) : Word(0);
+        for (uint32_t j = 0; j < width; ++j) {
+            const Word *row = bits + (uint64_t)cc[j] * stride;
+#pragma unroll
+            for (unsigned q = 0; q < PL; ++q)
+                if (v0 + q < words) x[q] &= __ldg(row + v0 + q);
         }
-        if (__any_sync(CPM_FULL, x != 0)) {
+        Word any = 0;
+#pragma unroll
+        for (unsigned q = 0; q < PL; ++q) {
+            const uint64_t lo = (v0 + q) * B;
+            if (v0 + q < words && n_tx - lo < B) x[q] &= (Word(1) << (unsigned)(n_tx - lo)) - Word(1);
+            any |= x[q];
+        }
+        if (__any_sync(CPM_FULL, any != 0)) {
+            // This lane's rows in order: one timestamp load per set row.
             PSeg s{0, 0, 0, 0};
-            if (x) {
-                const uint64_t row0 = v * B;
-                Word y = x;
-                s.cnt = word_popc(x);
-                s.first = __ldg(ts + row0 + word_low(y));
-                s.last = s.first;
-                y &= y - Word(1);
-                while (y) {
+#pragma unroll
+            for (unsigned q = 0; q < PL; ++q) {
+                const uint64_t row0 = (v0 + q) * B;
+                for (Word y = x[q]; y; y &= y - Word(1)) {
                     const long long t = __ldg(ts + row0 + word_low(y));
-                    s.gap = max(s.gap, t - s.last);
+                    if (s.cnt) s.gap = max(s.gap, t - s.last);
+                    else s.first = t;
                     s.last = t;
-                    y &= y - Word(1);
+                    ++s.cnt;
                 }
             }
             s = pseg_warp_join(s, lane);
@@ -116,7 +128,7 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
         if (kPrune) {
             int stop = 0;
             if (!lane) {
-                const uint64_t scanned = (base + 32) * (uint64_t)B;
+                const uint64_t scanned = (base + TILE) * (uint64_t)B;
                 const uint64_t r_end = scanned < n_tx ? scanned : n_tx;
                 const long long next = r_end < n_tx ? __ldg(ts + r_end) : end;
                 const long long bound = run.cnt ? max(max(run.first, run.gap), next - run.last) : next;
