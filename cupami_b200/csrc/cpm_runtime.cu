@@ -406,7 +406,8 @@ extern "C" int cpm_db_from_csr(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n
 // rows in timestamp order and every row kept -- an empty basket keeps its
 // timestamp and counts in the support denominator -- with the timestamps on
 // the device beside the tidsets.  The periodic miner prunes on the timestamps
-// being sorted, so they must not decrease; end closes the last gap.
+// being sorted and nonnegative (as the reference requires, _temporal.py:89-99);
+// end closes the last gap.
 extern "C" int cpm_tdb_from_csr(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows, const uint32_t *cols,
                                 uint64_t nnz, uint32_t n_items, const int64_t *timestamps, int64_t end,
                                 cpm_db **out) {
@@ -422,6 +423,7 @@ extern "C" int cpm_tdb_from_csr(cpm_ctx *ctx, const uint64_t *offsets, uint64_t 
             if (r && timestamps[r] < timestamps[r - 1])
                 return set_err(ctx, CPM_EINVAL, "timestamps must be nondecreasing (rows sorted by timestamp)");
         }
+        if (timestamps[0] < 0) return set_err(ctx, CPM_EINVAL, "timestamps must be nonnegative");
         if (end < timestamps[n_rows - 1]) return set_err(ctx, CPM_EINVAL, "end must be at least the last timestamp");
     }
     for (uint64_t k = 0; k < nnz; ++k)
@@ -2034,6 +2036,36 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
 // (k_join_pairs) and evaluates the rest (k_periodic, pruning early).  The
 // miners differ only in insertion order, which cpm_result_copy rebuilds
 // (CPM_ORDER_DEPTH_FIRST for cuPFEclat, CPM_ORDER_APRIORI for cuPFApriori).
+// Warps per candidate for k_periodic: enough for about 32 resident warps per
+// SM when a level has few candidates, at most one per step of a row.
+static uint32_t periodic_parts(const cpm_ctx *ctx, uint64_t n, uint64_t words) {
+    const uint64_t tiles = (words + PERIODIC_TILE - 1) / PERIODIC_TILE;
+    const uint64_t target = (uint64_t)ctx->sms * 32;
+    if (!n || n >= target || tiles <= 1) return 1;
+    return (uint32_t)std::min<uint64_t>(std::min<uint64_t>((target + n - 1) / n, tiles), 1024);
+}
+
+// k_periodic over n candidates, split `parts` ways (seg: n * parts summaries),
+// plus k_periodic_join when split.
+template <class Word, bool kPrune>
+static int periodic_launch(cpm_ctx *ctx, uint32_t parts, PSeg *seg, const Word *bits, uint64_t stride,
+                           const uint32_t *cand, const uint32_t *okf, uint64_t n, uint32_t width, const long long *ts,
+                           uint64_t n_tx, long long end, long long need, long long max_per, unsigned long long *sup,
+                           long long *per, uint32_t *pass, uint64_t &launches) {
+    const uint64_t warps = n * parts;
+    k_periodic<Word, kPrune><<<(unsigned)((warps + 7) / 8), 256, 0, ctx->stream>>>(
+        bits, stride, cand, okf, n, width, ts, n_tx, end, need, max_per, parts, seg, sup, per, pass);
+    CK(cudaGetLastError());
+    launches++;
+    if (parts > 1) {
+        k_periodic_join<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(seg, parts, okf, n, end, need, max_per,
+                                                                              sup, per, pass);
+        CK(cudaGetLastError());
+        launches++;
+    }
+    return CPM_OK;
+}
+
 static int mine_periodic(cpm_ctx *ctx, cpm_db *db, long long ms, long long max_per, cpm_result *res) {
     cpm_stats &st = res->stats;
     DevScope ds(ctx);
@@ -2041,7 +2073,7 @@ static int mine_periodic(cpm_ctx *ctx, cpm_db *db, long long ms, long long max_p
     const long long need = std::max<long long>(ms, 1);
     const auto *bits = reinterpret_cast<const unsigned long long *>(db->d_bits);
     const uint32_t n_items = db->n_items;
-    auto warp_grid = [](uint64_t n) { return (unsigned)((n + 7) / 8); };  // 8 warps of 256 threads
+    const uint64_t words = (db->n_tx + 63) / 64;
     PatternArrays pa;
     long long *pat_per = nullptr;
     uint64_t per_cap = 0;
@@ -2086,9 +2118,12 @@ static int mine_periodic(cpm_ctx *ctx, cpm_db *db, long long ms, long long max_p
         CKR(ds.alloc(&pos, n_items));
         k_iota_u32<<<(n_items + 255) / 256, 256, 0, ctx->stream>>>(cand, n_items);
         CK(cudaGetLastError());
-        k_periodic<unsigned long long, true><<<warp_grid(n_items), 256, 0, ctx->stream>>>(
-            bits, db->stride, cand, nullptr, n_items, 1, db->d_ts, db->n_tx, db->end, need, max_per, sup, per, pass);
-        CK(cudaGetLastError());
+        const uint32_t parts = periodic_parts(ctx, n_items, words);
+        PSeg *seg = nullptr;
+        if (parts > 1) CKR(ds.alloc(&seg, (uint64_t)n_items * parts));
+        CKR((periodic_launch<unsigned long long, true>(ctx, parts, seg, bits, db->stride, cand, nullptr, n_items, 1,
+                                                        db->d_ts, db->n_tx, db->end, need, max_per, sup, per, pass,
+                                                        st.kernel_launches)));
         uint64_t F1 = 0;
         CKR(scan_u32(ctx, ds, pass, pos, n_items, &F1, d_tot));
         st.n_frequent_items = F1;
@@ -2101,7 +2136,7 @@ static int mine_periodic(cpm_ctx *ctx, cpm_db *db, long long ms, long long max_p
         CK(cudaGetLastError());
         k_level_close<<<1, 1, 0, ctx->stream>>>(pos, pass, n_items, d_cnt2, d_cnt2 + 1);
         CK(cudaGetLastError());
-        st.kernel_launches += 5;
+        st.kernel_launches += 4;
         st.intersections += n_items;
         n_ub = pat_ub = F1;
     }
@@ -2147,11 +2182,14 @@ static int mine_periodic(cpm_ctx *ctx, cpm_db *db, long long ms, long long max_p
         k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, d_cnt2, k, poff, n_pairs, cand,
                                                                                  left, okf);
         CK(cudaGetLastError());
-        k_periodic<unsigned long long, true><<<warp_grid(n_pairs), 256, 0, ctx->stream>>>(
-            bits, db->stride, cand, okf, n_pairs, w, db->d_ts, db->n_tx, db->end, need, max_per, sup, per, pass);
-        CK(cudaGetLastError());
+        const uint32_t parts = periodic_parts(ctx, n_pairs, words);
+        PSeg *seg = nullptr;
+        if (parts > 1) CKR(scratch.get(12, &seg, n_pairs * parts));
+        CKR((periodic_launch<unsigned long long, true>(ctx, parts, seg, bits, db->stride, cand, okf, n_pairs, w,
+                                                        db->d_ts, db->n_tx, db->end, need, max_per, sup, per, pass,
+                                                        st.kernel_launches)));
         CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, nullptr, d_tot));
-        st.kernel_launches += 4;
+        st.kernel_launches += 3;
         st.intersections += n_pairs * (w - 1);
         uint32_t *L2 = nullptr, *pid2 = nullptr;
         CKR(reserve(n_pat, pat_ub + n_pairs));
@@ -2643,12 +2681,15 @@ extern "C" int cpm_periodic_counts(cpm_ctx *ctx, const uint32_t *d_bitsets, uint
     // Rows past the bitsets' words hold no bits (the reference kernel scans
     // words32 words and skips rows >= n_transactions).
     const uint64_t rows = std::min<uint64_t>(n_transactions, words32 * 32);
-    k_periodic<uint32_t, false><<<(unsigned)((n_candidates + 7) / 8), 256, 0, ctx->stream>>>(
-        d_bitsets, words32, d_candidates, nullptr, n_candidates, width, reinterpret_cast<const long long *>(d_timestamps),
-        rows, (long long)end, 0, 0, reinterpret_cast<unsigned long long *>(d_supports),
-        reinterpret_cast<long long *>(d_periods), nullptr);
-    CK(cudaGetLastError());
-    return CPM_OK;
+    const uint32_t parts = periodic_parts(ctx, n_candidates, (rows + 31) / 32);
+    DevScope ds(ctx);
+    PSeg *seg = nullptr;
+    if (parts > 1) CKR(ds.alloc(&seg, n_candidates * parts));
+    uint64_t launches = 0;
+    return periodic_launch<uint32_t, false>(ctx, parts, seg, d_bitsets, words32, d_candidates, nullptr, n_candidates,
+                                            width, reinterpret_cast<const long long *>(d_timestamps), rows,
+                                            (long long)end, 0, 0, reinterpret_cast<unsigned long long *>(d_supports),
+                                            reinterpret_cast<long long *>(d_periods), nullptr, launches);
 }
 
 extern "C" int cpm_intersect_extensions(cpm_ctx *ctx, const uint32_t *d_prefix, const uint32_t *d_extensions,

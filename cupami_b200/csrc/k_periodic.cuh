@@ -14,10 +14,13 @@
 // row order with shuffles.  The join
 //     (a, b) -> {a.cnt + b.cnt, a.first, b.last, max(a.gap, b.gap, b.first - a.last)}
 // (an empty side yields the other) is associative, so the tree gives exactly
-// the sequential scan's maximum.  With kPrune (the miner), a candidate stops as
-// soon as it cannot pass: too few rows left for the support, or a gap that is
-// already too long -- rows are sorted by timestamp, so the next set row's gap
-// is at least ts[first unscanned row] - last timestamp seen.
+// the sequential scan's maximum -- also across warps: when a level has too
+// few candidates to fill the GPU, each candidate's rows are split over several
+// warps whose summaries k_periodic_join joins in order.  With kPrune (the
+// miner), a candidate stops as soon as it cannot pass: too few rows left for
+// the support, or a gap that is already too long -- rows are sorted by
+// timestamp, so the next set row's gap is at least ts[first unscanned row] -
+// last timestamp seen.
 #pragma once
 #include "common.cuh"
 
@@ -58,39 +61,54 @@ __device__ __forceinline__ unsigned word_popc(unsigned long long x) { return __p
 __device__ __forceinline__ unsigned word_low(uint32_t x) { return __ffs(x) - 1; }
 __device__ __forceinline__ unsigned word_low(unsigned long long x) { return __ffsll(x) - 1; }
 
-// One warp per candidate c: the AND of the width rows cand[c * width ..] of
-// `bits` (Word: uint32_t or unsigned long long; rows of `stride` words; bit b
-// of word v is row v * bits(Word) + b), restricted to rows < n_tx.  Writes support[c] and period[c]; with kPrune also
-// pass[c] = ok_flag[c] && support >= need && period <= max_per, and a candidate
-// that stops early keeps partial support/period values (only passing ones are
-// exact).  Without kPrune every candidate is exact and pass/ok_flag may be null.
+// Rows per step of one warp: 32 lanes x PERIODIC_PL consecutive words each.
+constexpr unsigned PERIODIC_PL = 4;
+constexpr uint64_t PERIODIC_TILE = 32 * PERIODIC_PL;  // words per step
+
+// `parts` warps per candidate c (warp g: candidate g / parts, part g % parts),
+// each over an equal share of the steps: the AND of the width rows
+// cand[c * width ..] of `bits` (Word: uint32_t or unsigned long long; rows of
+// `stride` words; bit b of word v is row v * bits(Word) + b), restricted to
+// rows < n_tx.  With parts = 1 the warp writes support[c] and period[c] (and,
+// with kPrune, pass[c] = ok_flag[c] && support >= need && period <= max_per);
+// with parts > 1 each warp writes its segment summary to seg[c * parts + part]
+// and k_periodic_join finishes.  With kPrune a warp stops as soon as its rows
+// prove the candidate fails: a gap already above max_per (a stretch without
+// set rows from row a to row b gives a gap of at least ts[b] - ts[a - 1];
+// timestamps are nonnegative and sorted), or, with one part, too few rows left
+// for the support.  A stopped part reports gap = LLONG_MAX; only passing
+// candidates have exact values.  Without kPrune every candidate is exact.
 template <class Word, bool kPrune>
 __global__ void __launch_bounds__(256)
 k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__restrict__ cand,
            const uint32_t *__restrict__ ok_flag, uint64_t n, uint32_t width, const long long *__restrict__ ts,
-           uint64_t n_tx, long long end, long long need, long long max_per, unsigned long long *__restrict__ support,
-           long long *__restrict__ period, uint32_t *__restrict__ pass) {
+           uint64_t n_tx, long long end, long long need, long long max_per, uint32_t parts, PSeg *__restrict__ seg,
+           unsigned long long *__restrict__ support, long long *__restrict__ period, uint32_t *__restrict__ pass) {
     constexpr unsigned B = sizeof(Word) * 8;
-    // Each lane takes PL consecutive words per step (independent loads in
-    // flight, and one shuffle tree per 32 * PL words).
-    constexpr unsigned PL = 4;
-    constexpr uint64_t TILE = 32 * PL;
-    const uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    constexpr unsigned PL = PERIODIC_PL;
+    constexpr uint64_t TILE = PERIODIC_TILE;
+    const uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
+    const uint64_t c = g / parts;
+    const uint32_t part = (uint32_t)(g % parts);
     if (c >= n) return;  // whole warps: c is the same on every lane
-    if (kPrune && ok_flag && !ok_flag[c]) {
-        if (!lane) {
+    if (ok_flag && !ok_flag[c]) {
+        if (parts == 1 && !lane) {
             support[c] = 0;
             period[c] = end;
-            pass[c] = 0;
+            if (pass) pass[c] = 0;
         }
         return;
     }
     const uint32_t *cc = cand + c * width;
     const uint64_t words = (n_tx + B - 1) / B;
+    const uint64_t tiles = (words + TILE - 1) / TILE;
+    const uint64_t t0 = tiles * part / parts, t1 = tiles * (part + 1) / parts;
+    const uint64_t row_lo = t0 * TILE * B;  // first row of this part (< n_tx when t0 < tiles)
+    const long long before = row_lo ? __ldg(ts + row_lo - 1) : 0;
     PSeg run{0, 0, 0, 0};
     bool stopped = false;
-    for (uint64_t base = 0; base < words; base += TILE) {
+    for (uint64_t base = t0 * TILE; base < t1 * TILE; base += TILE) {
         const uint64_t v0 = base + (uint64_t)lane * PL;
         Word x[PL];
 #pragma unroll
@@ -131,8 +149,9 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
                 const uint64_t scanned = (base + TILE) * (uint64_t)B;
                 const uint64_t r_end = scanned < n_tx ? scanned : n_tx;
                 const long long next = r_end < n_tx ? __ldg(ts + r_end) : end;
-                const long long bound = run.cnt ? max(max(run.first, run.gap), next - run.last) : next;
-                stop = (long long)(run.cnt + (n_tx - r_end)) < need || bound > max_per;
+                const long long bound =
+                    run.cnt ? max(max(run.first - before, run.gap), next - run.last) : next - before;
+                stop = bound > max_per || (parts == 1 && (long long)(run.cnt + (n_tx - r_end)) < need);
             }
             if (__shfl_sync(CPM_FULL, stop, 0)) {
                 stopped = true;
@@ -140,12 +159,41 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
             }
         }
     }
-    if (!lane) {
+    if (lane) return;
+    if (parts == 1) {
         const long long per = run.cnt ? max(max(run.first, run.gap), end - run.last) : end;
         support[c] = run.cnt;
         period[c] = per;
         if (kPrune) pass[c] = !stopped && (long long)run.cnt >= need && per <= max_per ? 1u : 0u;
+    } else {
+        if (stopped) {
+            run.cnt = run.cnt ? run.cnt : 1;
+            run.gap = 0x7fffffffffffffffll;
+        }
+        seg[c * parts + part] = run;
     }
+}
+
+// One thread per candidate: joins its parts' summaries in row order and
+// writes what k_periodic writes with one part.
+__global__ void k_periodic_join(const PSeg *__restrict__ seg, uint32_t parts, const uint32_t *__restrict__ ok_flag,
+                                uint64_t n, long long end, long long need, long long max_per,
+                                unsigned long long *__restrict__ support, long long *__restrict__ period,
+                                uint32_t *__restrict__ pass) {
+    const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    if (ok_flag && !ok_flag[c]) {
+        support[c] = 0;
+        period[c] = end;
+        if (pass) pass[c] = 0;
+        return;
+    }
+    PSeg run{0, 0, 0, 0};
+    for (uint32_t p = 0; p < parts; ++p) run = pseg_join(run, seg[c * parts + p]);
+    const long long per = run.cnt ? max(max(run.first, run.gap), end - run.last) : end;
+    support[c] = run.cnt;
+    period[c] = per;
+    if (pass) pass[c] = (long long)run.cnt >= need && per <= max_per ? 1u : 0u;
 }
 
 __global__ void k_iota_u32(uint32_t *__restrict__ out, uint64_t n) {

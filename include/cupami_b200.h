@@ -248,8 +248,8 @@ void *cpm_stream(const cpm_ctx *ctx);
  * rows r_1 < ... < r_s is max(ts[r_1] - 0, ts[r_2] - ts[r_1], ...,
  * ts[r_s] - ts[r_{s-1}], end - ts[r_s]), or end when s = 0 (_temporal.py:26-53). */
 
-/* CSR of item columns, every row kept; timestamps[r] for row r, nondecreasing;
- * end >= the last timestamp.  Every column must be < n_items. */
+/* CSR of item columns, every row kept; timestamps[r] for row r, nonnegative and
+ * nondecreasing; end >= the last timestamp.  Every column must be < n_items. */
 int cpm_tdb_from_csr(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows, const uint32_t *cols,
                      uint64_t nnz, uint32_t n_items, const int64_t *timestamps, int64_t end, cpm_db **out);
 /* Itemsets with support >= min_sup, support > 0 and periodicity <= max_per

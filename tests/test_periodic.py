@@ -247,7 +247,8 @@ def test_gpu_periodic_counts_kernel_exact():
     from oracle import periodic
 
     rng = np.random.default_rng(11)
-    for n_rows, n_items, base in ((1, 3, 0), (31, 5, 7), (32, 5, 0), (33, 6, 2**40), (1000, 12, 0), (4097, 9, 2**53)):
+    for n_rows, n_items, base in ((1, 3, 0), (31, 5, 7), (32, 5, 0), (33, 6, 2**40), (1000, 12, 0), (4097, 9, 2**53),
+                                  (100000, 6, 0)):
         rows = _random_temporal(int(rng.integers(1 << 30)), n_rows, n_items, density=(0.05, 0.95))
         for r in rows:
             r[0] += base
