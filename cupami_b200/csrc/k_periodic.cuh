@@ -7,20 +7,18 @@
 // (end when s = 0), scanning the set bits of the AND of X's rows in order with
 // one thread per candidate (_temporal.py:26-53, launch :156-165).
 //
-// Here one warp handles a candidate: per step the lanes read 32 * 4
-// consecutive words of every row of the candidate (4 consecutive words a
-// lane), each lane reduces its words to a segment summary (count, first and
-// last timestamp, largest inner gap), and the warp joins the 32 summaries in
-// row order with shuffles.  The join
+// Here one warp handles a candidate: each lane walks a contiguous share of
+// the candidate's words (4 loads in flight per row) and reduces its rows to a
+// segment summary (count, first and last timestamp, largest inner gap); the
+// warp joins the 32 summaries once, in row order, with shuffles.  The join
 //     (a, b) -> {a.cnt + b.cnt, a.first, b.last, max(a.gap, b.gap, b.first - a.last)}
 // (an empty side yields the other) is associative, so the tree gives exactly
 // the sequential scan's maximum -- also across warps: when a level has too
 // few candidates to fill the GPU, each candidate's rows are split over several
 // warps whose summaries k_periodic_join joins in order.  With kPrune (the
-// miner), a candidate stops as soon as it cannot pass: too few rows left for
-// the support, or a gap that is already too long -- rows are sorted by
-// timestamp, so the next set row's gap is at least ts[first unscanned row] -
-// last timestamp seen.
+// miner), a candidate stops as soon as a gap is already too long -- rows are
+// sorted by timestamp, so the next set row's gap is at least
+// ts[first unscanned row] - last timestamp seen.
 #pragma once
 #include "common.cuh"
 
@@ -61,23 +59,26 @@ __device__ __forceinline__ unsigned word_popc(unsigned long long x) { return __p
 __device__ __forceinline__ unsigned word_low(uint32_t x) { return __ffs(x) - 1; }
 __device__ __forceinline__ unsigned word_low(unsigned long long x) { return __ffsll(x) - 1; }
 
-// Rows per step of one warp: 32 lanes x PERIODIC_PL consecutive words each.
+// Words a lane loads per step (independent loads in flight), and the fewest
+// words a part of a split candidate takes (PERIODIC_PL per lane).
 constexpr unsigned PERIODIC_PL = 4;
-constexpr uint64_t PERIODIC_TILE = 32 * PERIODIC_PL;  // words per step
+constexpr uint64_t PERIODIC_TILE = 32 * PERIODIC_PL;
 
 // `parts` warps per candidate c (warp g: candidate g / parts, part g % parts),
-// each over an equal share of the steps: the AND of the width rows
-// cand[c * width ..] of `bits` (Word: uint32_t or unsigned long long; rows of
-// `stride` words; bit b of word v is row v * bits(Word) + b), restricted to
-// rows < n_tx.  With parts = 1 the warp writes support[c] and period[c] (and,
-// with kPrune, pass[c] = ok_flag[c] && support >= need && period <= max_per);
-// with parts > 1 each warp writes its segment summary to seg[c * parts + part]
-// and k_periodic_join finishes.  With kPrune a warp stops as soon as its rows
-// prove the candidate fails: a gap already above max_per (a stretch without
-// set rows from row a to row b gives a gap of at least ts[b] - ts[a - 1];
-// timestamps are nonnegative and sorted), or, with one part, too few rows left
-// for the support.  A stopped part reports gap = LLONG_MAX; only passing
-// candidates have exact values.  Without kPrune every candidate is exact.
+// each over an equal share of the words, and each lane of a warp over a
+// contiguous share of its part: the AND of the width rows cand[c * width ..]
+// of `bits` (Word: uint32_t or unsigned long long; rows of `stride` words;
+// bit b of word v is row v * bits(Word) + b), restricted to rows < n_tx.  A
+// lane summarises its rows as it goes; the warp joins the 32 summaries once,
+// in lane (= row) order.  With parts = 1 the warp writes support[c] and
+// period[c] (and, with kPrune, pass[c] = ok_flag[c] && support >= need &&
+// period <= max_per); with parts > 1 each warp writes its summary to
+// seg[c * parts + part] and k_periodic_join finishes.  With kPrune a warp
+// stops as soon as one lane's rows prove the candidate fails: a gap already
+// above max_per (a stretch without set rows from row a to row b gives a gap
+// of at least ts[b] - ts[a - 1]; timestamps are nonnegative and sorted).  A
+// stopped candidate has pass = 0, a stopped part reports gap = LLONG_MAX; only
+// passing candidates have exact values.  Without kPrune every candidate is exact.
 template <class Word, bool kPrune>
 __global__ void __launch_bounds__(256)
 k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__restrict__ cand,
@@ -86,7 +87,6 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
            unsigned long long *__restrict__ support, long long *__restrict__ period, uint32_t *__restrict__ pass) {
     constexpr unsigned B = sizeof(Word) * 8;
     constexpr unsigned PL = PERIODIC_PL;
-    constexpr uint64_t TILE = PERIODIC_TILE;
     const uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     const uint64_t c = g / parts;
@@ -102,75 +102,65 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
     }
     const uint32_t *cc = cand + c * width;
     const uint64_t words = (n_tx + B - 1) / B;
-    const uint64_t tiles = (words + TILE - 1) / TILE;
-    const uint64_t t0 = tiles * part / parts, t1 = tiles * (part + 1) / parts;
-    const uint64_t row_lo = t0 * TILE * B;  // first row of this part (< n_tx when t0 < tiles)
-    const long long before = row_lo ? __ldg(ts + row_lo - 1) : 0;
-    PSeg run{0, 0, 0, 0};
+    const uint64_t w0 = words * part / parts, w1 = words * (part + 1) / parts;  // this part
+    const uint64_t per_lane = (w1 - w0 + 31) / 32;
+    const uint64_t lo_raw = w0 + lane * per_lane;
+    const uint64_t lo = lo_raw < w1 ? lo_raw : w1;
+    const uint64_t hi = lo + per_lane < w1 ? lo + per_lane : w1;  // this lane: words [lo, hi)
+    const long long before = kPrune && lo < hi && lo ? __ldg(ts + lo * B - 1) : 0;
+    PSeg s{0, 0, 0, 0};
     bool stopped = false;
-    for (uint64_t base = t0 * TILE; base < t1 * TILE; base += TILE) {
-        const uint64_t v0 = base + (uint64_t)lane * PL;
+    for (uint64_t i = 0; i < per_lane; i += PL) {  // the same trip count on every lane
+        const uint64_t v0 = lo + i;
         Word x[PL];
 #pragma unroll
-        for (unsigned q = 0; q < PL; ++q) x[q] = v0 + q < words ? ~Word(0) : Word(0);
+        for (unsigned q = 0; q < PL; ++q) x[q] = v0 + q < hi ? ~Word(0) : Word(0);
         for (uint32_t j = 0; j < width; ++j) {
             const Word *row = bits + (uint64_t)cc[j] * stride;
 #pragma unroll
             for (unsigned q = 0; q < PL; ++q)
-                if (v0 + q < words) x[q] &= __ldg(row + v0 + q);
+                if (v0 + q < hi) x[q] &= __ldg(row + v0 + q);
         }
-        Word any = 0;
 #pragma unroll
         for (unsigned q = 0; q < PL; ++q) {
-            const uint64_t lo = (v0 + q) * B;
-            if (v0 + q < words && n_tx - lo < B) x[q] &= (Word(1) << (unsigned)(n_tx - lo)) - Word(1);
-            any |= x[q];
-        }
-        if (__any_sync(CPM_FULL, any != 0)) {
-            // This lane's rows in order: one timestamp load per set row.
-            PSeg s{0, 0, 0, 0};
-#pragma unroll
-            for (unsigned q = 0; q < PL; ++q) {
-                const uint64_t row0 = (v0 + q) * B;
-                for (Word y = x[q]; y; y &= y - Word(1)) {
-                    const long long t = __ldg(ts + row0 + word_low(y));
-                    if (s.cnt) s.gap = max(s.gap, t - s.last);
-                    else s.first = t;
-                    s.last = t;
-                    ++s.cnt;
-                }
+            const uint64_t row0 = (v0 + q) * B;
+            if (v0 + q < hi && n_tx - row0 < B) x[q] &= (Word(1) << (unsigned)(n_tx - row0)) - Word(1);
+            for (Word y = x[q]; y; y &= y - Word(1)) {  // one timestamp load per set row
+                const long long t = __ldg(ts + row0 + word_low(y));
+                if (s.cnt) s.gap = max(s.gap, t - s.last);
+                else s.first = t;
+                s.last = t;
+                ++s.cnt;
             }
-            s = pseg_warp_join(s, lane);
-            if (!lane) run = pseg_join(run, s);
         }
         if (kPrune) {
-            int stop = 0;
-            if (!lane) {
-                const uint64_t scanned = (base + TILE) * (uint64_t)B;
-                const uint64_t r_end = scanned < n_tx ? scanned : n_tx;
+            bool bad = false;
+            if (lo < hi) {
+                const uint64_t done = v0 + PL < hi ? v0 + PL : hi;
+                const uint64_t r_end = done * B < n_tx ? done * B : n_tx;
                 const long long next = r_end < n_tx ? __ldg(ts + r_end) : end;
-                const long long bound =
-                    run.cnt ? max(max(run.first - before, run.gap), next - run.last) : next - before;
-                stop = bound > max_per || (parts == 1 && (long long)(run.cnt + (n_tx - r_end)) < need);
+                const long long bound = s.cnt ? max(max(s.first - before, s.gap), next - s.last) : next - before;
+                bad = bound > max_per;
             }
-            if (__shfl_sync(CPM_FULL, stop, 0)) {
+            if (__any_sync(CPM_FULL, bad)) {
                 stopped = true;
                 break;
             }
         }
     }
+    s = pseg_warp_join(s, lane);
     if (lane) return;
     if (parts == 1) {
-        const long long per = run.cnt ? max(max(run.first, run.gap), end - run.last) : end;
-        support[c] = run.cnt;
+        const long long per = s.cnt ? max(max(s.first, s.gap), end - s.last) : end;
+        support[c] = s.cnt;
         period[c] = per;
-        if (kPrune) pass[c] = !stopped && (long long)run.cnt >= need && per <= max_per ? 1u : 0u;
+        if (kPrune) pass[c] = !stopped && (long long)s.cnt >= need && per <= max_per ? 1u : 0u;
     } else {
         if (stopped) {
-            run.cnt = run.cnt ? run.cnt : 1;
-            run.gap = 0x7fffffffffffffffll;
+            s.cnt = s.cnt ? s.cnt : 1;
+            s.gap = 0x7fffffffffffffffll;
         }
-        seg[c * parts + part] = run;
+        seg[c * parts + part] = s;
     }
 }
 

@@ -246,13 +246,13 @@ class cuApriori:
             db = _native.Database.from_ids(ctx, offsets, ids)
             labels = [str(v) for v in db.labels.tolist()]
             return db, labels
-        labels = sorted({item for row in self._Database for item in row})
-        index = {label: i for i, label in enumerate(labels)}
+        flat = list(chain.from_iterable(self._Database))
+        labels = sorted(set(flat))
+        index = dict(zip(labels, range(len(labels))))
         offsets = np.zeros(len(self._Database) + 1, dtype=np.uint64)
-        np.cumsum(np.fromiter((len(r) for r in self._Database), dtype=np.uint64,
-                              count=len(self._Database)), out=offsets[1:])
-        cols = np.fromiter((index[item] for row in self._Database for item in row),
-                           dtype=np.uint32, count=int(offsets[-1]))
+        np.cumsum(np.fromiter(map(len, self._Database), dtype=np.uint64, count=len(self._Database)),
+                  out=offsets[1:])
+        cols = np.fromiter(map(index.__getitem__, flat), dtype=np.uint32, count=len(flat))
         return _native.Database.from_columns(ctx, offsets, cols, len(labels)), labels
 
     def _options(self):

@@ -33,6 +33,7 @@ import math
 import numbers
 import struct
 import time
+from itertools import chain
 from pathlib import Path
 from urllib.parse import urlparse
 from urllib.request import urlopen
@@ -218,13 +219,13 @@ class TemporalInput(cuApriori):
 
     def _deviceDatabase(self, ctx):
         """Temporal tidsets (every row, empty ones too) and the sorted labels."""
-        labels = sorted({item for row in self._Database for item in row})
-        index = {label: i for i, label in enumerate(labels)}
+        flat = list(chain.from_iterable(self._Database))
+        labels = sorted(set(flat))
+        index = dict(zip(labels, range(len(labels))))
         n = len(self._Database)
         offsets = np.zeros(n + 1, dtype=np.uint64)
-        np.cumsum(np.fromiter((len(r) for r in self._Database), dtype=np.uint64, count=n), out=offsets[1:])
-        cols = np.fromiter((index[item] for row in self._Database for item in row), dtype=np.uint32,
-                           count=int(offsets[-1]))
+        np.cumsum(np.fromiter(map(len, self._Database), dtype=np.uint64, count=n), out=offsets[1:])
+        cols = np.fromiter(map(index.__getitem__, flat), dtype=np.uint32, count=len(flat))
         timestamps = np.asarray(self._timestamps, dtype=np.int64)
         return _native.Database.from_temporal(ctx, offsets, cols, len(labels), timestamps,
                                               self._endTimestamp), labels
