@@ -7,18 +7,20 @@
 // (end when s = 0), scanning the set bits of the AND of X's rows in order with
 // one thread per candidate (_temporal.py:26-53, launch :156-165).
 //
-// Here one warp handles a candidate: each lane walks a contiguous share of
-// the candidate's words (4 loads in flight per row) and reduces its rows to a
-// segment summary (count, first and last timestamp, largest inner gap); the
-// warp joins the 32 summaries once, in row order, with shuffles.  The join
-//     (a, b) -> {a.cnt + b.cnt, a.first, b.last, max(a.gap, b.gap, b.first - a.last)}
-// (an empty side yields the other) is associative, so the tree gives exactly
-// the sequential scan's maximum -- also across warps: when a level has too
+// Here one warp handles a candidate: per step its lanes load 32 * 4
+// consecutive words of each of the candidate's rows (coalesced), each lane
+// scans the set rows of its 4 words in order, and the gaps that cross lane and
+// step boundaries come from a ballot and one shuffle per step; only the
+// largest gap needs a warp reduction, once at the end.  When a level has too
 // few candidates to fill the GPU, each candidate's rows are split over several
-// warps whose summaries k_periodic_join joins in order.  With kPrune (the
-// miner), a candidate stops as soon as a gap is already too long -- rows are
-// sorted by timestamp, so the next set row's gap is at least
-// ts[first unscanned row] - last timestamp seen.
+// warps, each summarising its rows as (count, first and last timestamp,
+// largest inner gap), and k_periodic_join joins the summaries in row order
+// with the associative join
+//     (a, b) -> {a.cnt + b.cnt, a.first, b.last, max(a.gap, b.gap, b.first - a.last)}
+// (an empty side yields the other).  With kPrune (the miner), a candidate
+// stops as soon as a gap is already too long -- rows are sorted by timestamp,
+// so the next set row's gap is at least ts[first unscanned row] - last
+// timestamp seen.
 #pragma once
 #include "common.cuh"
 
@@ -40,45 +42,37 @@ __device__ __forceinline__ PSeg pseg_join(const PSeg &a, const PSeg &b) {
     return r;
 }
 
-// Lane 0 receives the join of the 32 lanes' segments in lane order.
-__device__ __forceinline__ PSeg pseg_warp_join(PSeg s, unsigned lane) {
-#pragma unroll
-    for (unsigned o = 1; o < 32; o <<= 1) {
-        PSeg t;
-        t.cnt = __shfl_down_sync(CPM_FULL, s.cnt, o);
-        t.first = __shfl_down_sync(CPM_FULL, s.first, o);
-        t.last = __shfl_down_sync(CPM_FULL, s.last, o);
-        t.gap = __shfl_down_sync(CPM_FULL, s.gap, o);
-        if (lane + o < 32) s = pseg_join(s, t);
-    }
-    return s;
-}
-
 __device__ __forceinline__ unsigned word_popc(uint32_t x) { return __popc(x); }
 __device__ __forceinline__ unsigned word_popc(unsigned long long x) { return __popcll(x); }
 __device__ __forceinline__ unsigned word_low(uint32_t x) { return __ffs(x) - 1; }
 __device__ __forceinline__ unsigned word_low(unsigned long long x) { return __ffsll(x) - 1; }
 
-// Words a lane loads per step (independent loads in flight), and the fewest
-// words a part of a split candidate takes (PERIODIC_PL per lane).
+// Words a lane loads per step (independent loads in flight); a step of a
+// warp covers PERIODIC_TILE consecutive words.
 constexpr unsigned PERIODIC_PL = 4;
 constexpr uint64_t PERIODIC_TILE = 32 * PERIODIC_PL;
 
 // `parts` warps per candidate c (warp g: candidate g / parts, part g % parts),
-// each over an equal share of the words, and each lane of a warp over a
-// contiguous share of its part: the AND of the width rows cand[c * width ..]
-// of `bits` (Word: uint32_t or unsigned long long; rows of `stride` words;
-// bit b of word v is row v * bits(Word) + b), restricted to rows < n_tx.  A
-// lane summarises its rows as it goes; the warp joins the 32 summaries once,
-// in lane (= row) order.  With parts = 1 the warp writes support[c] and
-// period[c] (and, with kPrune, pass[c] = ok_flag[c] && support >= need &&
-// period <= max_per); with parts > 1 each warp writes its summary to
-// seg[c * parts + part] and k_periodic_join finishes.  With kPrune a warp
-// stops as soon as one lane's rows prove the candidate fails: a gap already
-// above max_per (a stretch without set rows from row a to row b gives a gap
-// of at least ts[b] - ts[a - 1]; timestamps are nonnegative and sorted).  A
-// stopped candidate has pass = 0, a stopped part reports gap = LLONG_MAX; only
-// passing candidates have exact values.  Without kPrune every candidate is exact.
+// each over an equal share of the steps: the AND of the width rows
+// cand[c * width ..] of `bits` (Word: uint32_t or unsigned long long; rows of
+// `stride` words; bit b of word v is row v * bits(Word) + b), restricted to
+// rows < n_tx.  Per step lane l takes the PERIODIC_PL words at
+// base + PERIODIC_PL * l (coalesced) and scans their set rows in order.  The
+// warp needs no ordered reduction per step: every lane keeps the running
+// count, first and last timestamp of the rows scanned so far (identical on all
+// lanes) and its own running maximum of the gaps it has seen -- inside its
+// words, and from the previous set row (the last set row of the nearest lower
+// lane with one, found by a ballot and one shuffle, or of an earlier step) to
+// its first -- and the maxima are reduced once at the end.
+// With parts = 1 the warp writes support[c] and period[c] (and, with kPrune,
+// pass[c] = ok_flag[c] && support >= need && period <= max_per); with
+// parts > 1 each warp writes its summary to seg[c * parts + part] and
+// k_periodic_join finishes.  With kPrune a warp stops as soon as its rows
+// prove the candidate fails: a gap already above max_per (a stretch without
+// set rows from row a to row b gives a gap of at least ts[b] - ts[a - 1];
+// timestamps are nonnegative and sorted).  A stopped candidate has pass = 0,
+// a stopped part reports gap = LLONG_MAX; only passing candidates have exact
+// values.  Without kPrune every candidate is exact.
 template <class Word, bool kPrune>
 __global__ void __launch_bounds__(256)
 k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__restrict__ cand,
@@ -87,6 +81,7 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
            unsigned long long *__restrict__ support, long long *__restrict__ period, uint32_t *__restrict__ pass) {
     constexpr unsigned B = sizeof(Word) * 8;
     constexpr unsigned PL = PERIODIC_PL;
+    constexpr uint64_t TILE = PERIODIC_TILE;
     const uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     const uint64_t c = g / parts;
@@ -102,45 +97,61 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
     }
     const uint32_t *cc = cand + c * width;
     const uint64_t words = (n_tx + B - 1) / B;
-    const uint64_t w0 = words * part / parts, w1 = words * (part + 1) / parts;  // this part
-    const uint64_t per_lane = (w1 - w0 + 31) / 32;
-    const uint64_t lo_raw = w0 + lane * per_lane;
-    const uint64_t lo = lo_raw < w1 ? lo_raw : w1;
-    const uint64_t hi = lo + per_lane < w1 ? lo + per_lane : w1;  // this lane: words [lo, hi)
-    const long long before = kPrune && lo < hi && lo ? __ldg(ts + lo * B - 1) : 0;
-    PSeg s{0, 0, 0, 0};
+    const uint64_t tiles = (words + TILE - 1) / TILE;
+    const uint64_t t0 = tiles * part / parts, t1 = tiles * (part + 1) / parts;
+    const uint64_t row_lo = t0 * TILE * B;  // first row of this part (< n_tx when t0 < tiles)
+    const long long before = row_lo ? __ldg(ts + row_lo - 1) : 0;
+    unsigned long long run_cnt = 0;  // rows scanned so far: the same on every lane
+    long long run_first = 0, run_last = 0;
+    long long gmax = 0;              // this lane's largest gap seen
     bool stopped = false;
-    for (uint64_t i = 0; i < per_lane; i += PL) {  // the same trip count on every lane
-        const uint64_t v0 = lo + i;
+    for (uint64_t base = t0 * TILE; base < t1 * TILE; base += TILE) {
+        const uint64_t v0 = base + (uint64_t)lane * PL;
         Word x[PL];
 #pragma unroll
-        for (unsigned q = 0; q < PL; ++q) x[q] = v0 + q < hi ? ~Word(0) : Word(0);
+        for (unsigned q = 0; q < PL; ++q) x[q] = v0 + q < words ? ~Word(0) : Word(0);
         for (uint32_t j = 0; j < width; ++j) {
             const Word *row = bits + (uint64_t)cc[j] * stride;
 #pragma unroll
             for (unsigned q = 0; q < PL; ++q)
-                if (v0 + q < hi) x[q] &= __ldg(row + v0 + q);
+                if (v0 + q < words) x[q] &= __ldg(row + v0 + q);
         }
+        unsigned lc = 0;  // this lane's set rows in this step
+        long long lf = 0, ll = 0;
 #pragma unroll
         for (unsigned q = 0; q < PL; ++q) {
             const uint64_t row0 = (v0 + q) * B;
-            if (v0 + q < hi && n_tx - row0 < B) x[q] &= (Word(1) << (unsigned)(n_tx - row0)) - Word(1);
+            if (v0 + q < words && n_tx - row0 < B) x[q] &= (Word(1) << (unsigned)(n_tx - row0)) - Word(1);
             for (Word y = x[q]; y; y &= y - Word(1)) {  // one timestamp load per set row
                 const long long t = __ldg(ts + row0 + word_low(y));
-                if (s.cnt) s.gap = max(s.gap, t - s.last);
-                else s.first = t;
-                s.last = t;
-                ++s.cnt;
+                if (lc) gmax = max(gmax, t - ll);
+                else lf = t;
+                ll = t;
+                ++lc;
             }
         }
+        const unsigned mask = __ballot_sync(CPM_FULL, lc != 0);
+        if (mask) {
+            const unsigned below = mask & ((1u << lane) - 1u);
+            const int src = below ? 31 - __clz(below) : (int)lane;
+            const long long prev = __shfl_sync(CPM_FULL, ll, src);  // last set row of the nearest lower lane
+            if (lc) {
+                if (below) gmax = max(gmax, lf - prev);
+                else if (run_cnt) gmax = max(gmax, lf - run_last);
+            }
+            const long long step_first = __shfl_sync(CPM_FULL, lf, __ffs(mask) - 1);
+            run_last = __shfl_sync(CPM_FULL, ll, 31 - __clz(mask));
+            if (!run_cnt) run_first = step_first;
+            run_cnt += __reduce_add_sync(CPM_FULL, lc);
+        }
         if (kPrune) {
-            bool bad = false;
-            if (lo < hi) {
-                const uint64_t done = v0 + PL < hi ? v0 + PL : hi;
-                const uint64_t r_end = done * B < n_tx ? done * B : n_tx;
+            bool bad = gmax > max_per;
+            if (!lane) {
+                const uint64_t scanned = (base + TILE) * (uint64_t)B;
+                const uint64_t r_end = scanned < n_tx ? scanned : n_tx;
                 const long long next = r_end < n_tx ? __ldg(ts + r_end) : end;
-                const long long bound = s.cnt ? max(max(s.first - before, s.gap), next - s.last) : next - before;
-                bad = bound > max_per;
+                const long long bound = run_cnt ? max(run_first - before, next - run_last) : next - before;
+                bad = bad || bound > max_per;
             }
             if (__any_sync(CPM_FULL, bad)) {
                 stopped = true;
@@ -148,19 +159,21 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
             }
         }
     }
-    s = pseg_warp_join(s, lane);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) gmax = max(gmax, __shfl_xor_sync(CPM_FULL, gmax, o));
     if (lane) return;
     if (parts == 1) {
-        const long long per = s.cnt ? max(max(s.first, s.gap), end - s.last) : end;
-        support[c] = s.cnt;
+        const long long per = run_cnt ? max(max(run_first, gmax), end - run_last) : end;
+        support[c] = run_cnt;
         period[c] = per;
-        if (kPrune) pass[c] = !stopped && (long long)s.cnt >= need && per <= max_per ? 1u : 0u;
+        if (kPrune) pass[c] = !stopped && (long long)run_cnt >= need && per <= max_per ? 1u : 0u;
     } else {
+        PSeg out{run_cnt, run_first, run_last, gmax};
         if (stopped) {
-            s.cnt = s.cnt ? s.cnt : 1;
-            s.gap = 0x7fffffffffffffffll;
+            out.cnt = out.cnt ? out.cnt : 1;
+            out.gap = 0x7fffffffffffffffll;
         }
-        seg[c * parts + part] = s;
+        seg[c * parts + part] = out;
     }
 }
 
