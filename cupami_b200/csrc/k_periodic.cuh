@@ -7,9 +7,9 @@
 // (end when s = 0), scanning the set bits of the AND of X's rows in order with
 // one thread per candidate (_temporal.py:26-53, launch :156-165).
 //
-// Here one warp handles a candidate: per step its lanes load 32 * 4
-// consecutive words of each of the candidate's rows (coalesced), each lane
-// scans the set rows of its 4 words in order, and the gaps that cross lane and
+// Here one warp handles a candidate: per step its lanes load 2 KB of
+// consecutive words of each of the candidate's rows (coalesced, 64 bytes a
+// lane), each lane scans the set rows of its words in order, and the gaps that cross lane and
 // step boundaries come from a ballot and one shuffle per step; only the
 // largest gap needs a warp reduction, once at the end.  When a level has too
 // few candidates to fill the GPU, each candidate's rows are split over several
@@ -47,17 +47,18 @@ __device__ __forceinline__ unsigned word_popc(unsigned long long x) { return __p
 __device__ __forceinline__ unsigned word_low(uint32_t x) { return __ffs(x) - 1; }
 __device__ __forceinline__ unsigned word_low(unsigned long long x) { return __ffsll(x) - 1; }
 
-// Words a lane loads per step (independent loads in flight); a step of a
-// warp covers PERIODIC_TILE consecutive words.
-constexpr unsigned PERIODIC_PL = 4;
-constexpr uint64_t PERIODIC_TILE = 32 * PERIODIC_PL;
+// Bytes of each row a lane loads per step (independent loads in flight): a
+// step of a warp covers periodic_tile<Word>() consecutive words.
+constexpr unsigned PERIODIC_LANE_BYTES = 64;
+template <class Word>
+__host__ __device__ constexpr uint64_t periodic_tile() { return 32 * (PERIODIC_LANE_BYTES / sizeof(Word)); }
 
 // `parts` warps per candidate c (warp g: candidate g / parts, part g % parts),
 // each over an equal share of the steps: the AND of the width rows
 // cand[c * width ..] of `bits` (Word: uint32_t or unsigned long long; rows of
 // `stride` words; bit b of word v is row v * bits(Word) + b), restricted to
-// rows < n_tx.  Per step lane l takes the PERIODIC_PL words at
-// base + PERIODIC_PL * l (coalesced) and scans their set rows in order.  The
+// rows < n_tx.  Per step lane l takes the PL = 64 / sizeof(Word) words at
+// base + PL * l (coalesced) and scans their set rows in order.  The
 // warp needs no ordered reduction per step: every lane keeps the running
 // count, first and last timestamp of the rows scanned so far (identical on all
 // lanes) and its own running maximum of the gaps it has seen -- inside its
@@ -74,14 +75,14 @@ constexpr uint64_t PERIODIC_TILE = 32 * PERIODIC_PL;
 // a stopped part reports gap = LLONG_MAX; only passing candidates have exact
 // values.  Without kPrune every candidate is exact.
 template <class Word, bool kPrune>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
 k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__restrict__ cand,
            const uint32_t *__restrict__ ok_flag, uint64_t n, uint32_t width, const long long *__restrict__ ts,
            uint64_t n_tx, long long end, long long need, long long max_per, uint32_t parts, PSeg *__restrict__ seg,
            unsigned long long *__restrict__ support, long long *__restrict__ period, uint32_t *__restrict__ pass) {
     constexpr unsigned B = sizeof(Word) * 8;
-    constexpr unsigned PL = PERIODIC_PL;
-    constexpr uint64_t TILE = PERIODIC_TILE;
+    constexpr unsigned PL = PERIODIC_LANE_BYTES / sizeof(Word);
+    constexpr uint64_t TILE = periodic_tile<Word>();
     const uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     const uint64_t c = g / parts;
