@@ -430,8 +430,9 @@ def run_periodic(args, world, rank, local):
     # words, a timestamp per set row, the two column ids and the two results.
     rows_idx = torch.from_numpy(np.repeat(np.arange(n, dtype=np.int64),
                                           np.diff(csr.offsets.astype(np.int64))).copy()).cuda()
-    bits32 = _bitsets.build_bitsets(None, rows_idx, torch.from_numpy(cols.view(np.int32).copy()).cuda(), n,
-                                    len(labels))
+    # rows padded to a multiple of 4 words (16-byte aligned rows); the kernel scans the first n rows
+    bits32 = _bitsets.build_bitsets(None, rows_idx, torch.from_numpy(cols.view(np.int32).copy()).cuda(),
+                                    (n + 127) // 128 * 128, len(labels))
     d_ts = torch.from_numpy(ts.copy()).cuda()
     apriori = dict(last)["pf-apriori"]  # by length: the kept single items come first
     singles = int(np.count_nonzero(np.diff(apriori.offsets.astype(np.int64)) == 1))
@@ -461,7 +462,7 @@ def run_periodic(args, world, rank, local):
         e1.synchronize()
         kms.append(e0.elapsed_time(e1))
     k_ms = statistics.mean(kms)
-    alg_bytes = len(pairs) * (2 * bits32.shape[1] * 4 + 8 + 16) + 8 * int(sup.sum().item())
+    alg_bytes = len(pairs) * (2 * ((n + 31) // 32) * 4 + 8 + 16) + 8 * int(sup.sum().item())
     achieved = alg_bytes / (k_ms * 1e-3) / 1e9
     hbm, _, src = peaks()
     roof = {"kernel": "k_periodic (cpm_periodic_counts, every pair of the kept items)", "bound": "hbm",

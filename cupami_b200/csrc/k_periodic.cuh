@@ -8,8 +8,9 @@
 // one thread per candidate (_temporal.py:26-53, launch :156-165).
 //
 // Here one warp handles a candidate: per step its lanes load 2 KB of
-// consecutive words of each of the candidate's rows (coalesced, 64 bytes a
-// lane), each lane scans the set rows of its words in order, and the gaps that cross lane and
+// consecutive words of each of the candidate's rows (four coalesced 512-byte
+// spans, 16 bytes a lane each), each lane scans the set rows of its words in
+// order, and the gaps that cross lane and
 // step boundaries come from a ballot and one shuffle per step; only the
 // largest gap needs a warp reduction, once at the end.  When a level has too
 // few candidates to fill the GPU, each candidate's rows are split over several
@@ -47,24 +48,36 @@ __device__ __forceinline__ unsigned word_popc(unsigned long long x) { return __p
 __device__ __forceinline__ unsigned word_low(uint32_t x) { return __ffs(x) - 1; }
 __device__ __forceinline__ unsigned word_low(unsigned long long x) { return __ffsll(x) - 1; }
 
-// Bytes of each row a lane loads per step (independent loads in flight): a
-// step of a warp covers periodic_tile<Word>() consecutive words.
-constexpr unsigned PERIODIC_LANE_BYTES = 64;
+// A step of a warp: PERIODIC_SUB sub-steps, each 16 bytes of every row per
+// lane (512 contiguous bytes per warp: one 16-byte load per lane where the
+// row is 16-byte aligned), all loaded before any is scanned.
+constexpr unsigned PERIODIC_SUB = 4;
 template <class Word>
-__host__ __device__ constexpr uint64_t periodic_tile() { return 32 * (PERIODIC_LANE_BYTES / sizeof(Word)); }
+__host__ __device__ constexpr unsigned periodic_pl() { return 16 / sizeof(Word); }
+template <class Word>
+__host__ __device__ constexpr uint64_t periodic_tile() { return 32ull * PERIODIC_SUB * periodic_pl<Word>(); }
+
+__device__ __forceinline__ void unpack16(const uint4 &u, uint32_t (&w)[4]) {
+    w[0] = u.x; w[1] = u.y; w[2] = u.z; w[3] = u.w;
+}
+__device__ __forceinline__ void unpack16(const uint4 &u, unsigned long long (&w)[2]) {
+    w[0] = (unsigned long long)u.x | ((unsigned long long)u.y << 32);
+    w[1] = (unsigned long long)u.z | ((unsigned long long)u.w << 32);
+}
 
 // `parts` warps per candidate c (warp g: candidate g / parts, part g % parts),
 // each over an equal share of the steps: the AND of the width rows
 // cand[c * width ..] of `bits` (Word: uint32_t or unsigned long long; rows of
 // `stride` words; bit b of word v is row v * bits(Word) + b), restricted to
-// rows < n_tx.  Per step lane l takes the PL = 64 / sizeof(Word) words at
-// base + PL * l (coalesced) and scans their set rows in order.  The
-// warp needs no ordered reduction per step: every lane keeps the running
-// count, first and last timestamp of the rows scanned so far (identical on all
-// lanes) and its own running maximum of the gaps it has seen -- inside its
-// words, and from the previous set row (the last set row of the nearest lower
-// lane with one, found by a ballot and one shuffle, or of an earlier step) to
-// its first -- and the maxima are reduced once at the end.
+// rows < n_tx.  In sub-step k of a step at word `base`, lane l takes the
+// PL = 16 / sizeof(Word) words at base + 32 * PL * k + PL * l and scans their
+// set rows in order.  The warp needs no ordered reduction per sub-step: every
+// lane keeps the running count, first and last timestamp of the rows scanned
+// so far (identical on all lanes) and its own running maximum of the gaps it
+// has seen -- inside its words, and from the previous set row (the last set
+// row of the nearest lower lane with one, found by a ballot and one shuffle,
+// or of an earlier sub-step) to its first -- and the maxima are reduced once
+// at the end.
 // With parts = 1 the warp writes support[c] and period[c] (and, with kPrune,
 // pass[c] = ok_flag[c] && support >= need && period <= max_per); with
 // parts > 1 each warp writes its summary to seg[c * parts + part] and
@@ -81,7 +94,8 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
            uint64_t n_tx, long long end, long long need, long long max_per, uint32_t parts, PSeg *__restrict__ seg,
            unsigned long long *__restrict__ support, long long *__restrict__ period, uint32_t *__restrict__ pass) {
     constexpr unsigned B = sizeof(Word) * 8;
-    constexpr unsigned PL = PERIODIC_LANE_BYTES / sizeof(Word);
+    constexpr unsigned PL = periodic_pl<Word>();
+    constexpr unsigned SUB = PERIODIC_SUB;
     constexpr uint64_t TILE = periodic_tile<Word>();
     const uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
@@ -107,43 +121,60 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
     long long gmax = 0;              // this lane's largest gap seen
     bool stopped = false;
     for (uint64_t base = t0 * TILE; base < t1 * TILE; base += TILE) {
-        const uint64_t v0 = base + (uint64_t)lane * PL;
-        Word x[PL];
+        Word x[SUB][PL];
 #pragma unroll
-        for (unsigned q = 0; q < PL; ++q) x[q] = v0 + q < words ? ~Word(0) : Word(0);
+        for (unsigned k = 0; k < SUB; ++k)
+#pragma unroll
+            for (unsigned q = 0; q < PL; ++q) x[k][q] = base + (32 * k + lane) * PL + q < words ? ~Word(0) : Word(0);
         for (uint32_t j = 0; j < width; ++j) {
             const Word *row = bits + (uint64_t)cc[j] * stride;
+            const bool aligned = (reinterpret_cast<uintptr_t>(row) & 15) == 0;
 #pragma unroll
-            for (unsigned q = 0; q < PL; ++q)
-                if (v0 + q < words) x[q] &= __ldg(row + v0 + q);
-        }
-        unsigned lc = 0;  // this lane's set rows in this step
-        long long lf = 0, ll = 0;
+            for (unsigned k = 0; k < SUB; ++k) {
+                const uint64_t v0 = base + (32 * k + lane) * PL;
+                if (aligned && v0 + PL <= words) {
+                    Word w[PL];
+                    unpack16(__ldg(reinterpret_cast<const uint4 *>(row + v0)), w);
 #pragma unroll
-        for (unsigned q = 0; q < PL; ++q) {
-            const uint64_t row0 = (v0 + q) * B;
-            if (v0 + q < words && n_tx - row0 < B) x[q] &= (Word(1) << (unsigned)(n_tx - row0)) - Word(1);
-            for (Word y = x[q]; y; y &= y - Word(1)) {  // one timestamp load per set row
-                const long long t = __ldg(ts + row0 + word_low(y));
-                if (lc) gmax = max(gmax, t - ll);
-                else lf = t;
-                ll = t;
-                ++lc;
+                    for (unsigned q = 0; q < PL; ++q) x[k][q] &= w[q];
+                } else {
+#pragma unroll
+                    for (unsigned q = 0; q < PL; ++q)
+                        if (v0 + q < words) x[k][q] &= __ldg(row + v0 + q);
+                }
             }
         }
-        const unsigned mask = __ballot_sync(CPM_FULL, lc != 0);
-        if (mask) {
-            const unsigned below = mask & ((1u << lane) - 1u);
-            const int src = below ? 31 - __clz(below) : (int)lane;
-            const long long prev = __shfl_sync(CPM_FULL, ll, src);  // last set row of the nearest lower lane
-            if (lc) {
-                if (below) gmax = max(gmax, lf - prev);
-                else if (run_cnt) gmax = max(gmax, lf - run_last);
+#pragma unroll
+        for (unsigned k = 0; k < SUB; ++k) {
+            const uint64_t v0 = base + (32 * k + lane) * PL;
+            unsigned lc = 0;  // this lane's set rows in this sub-step
+            long long lf = 0, ll = 0;
+#pragma unroll
+            for (unsigned q = 0; q < PL; ++q) {
+                const uint64_t row0 = (v0 + q) * B;
+                if (v0 + q < words && n_tx - row0 < B) x[k][q] &= (Word(1) << (unsigned)(n_tx - row0)) - Word(1);
+                for (Word y = x[k][q]; y; y &= y - Word(1)) {  // one timestamp load per set row
+                    const long long t = __ldg(ts + row0 + word_low(y));
+                    if (lc) gmax = max(gmax, t - ll);
+                    else lf = t;
+                    ll = t;
+                    ++lc;
+                }
             }
-            const long long step_first = __shfl_sync(CPM_FULL, lf, __ffs(mask) - 1);
-            run_last = __shfl_sync(CPM_FULL, ll, 31 - __clz(mask));
-            if (!run_cnt) run_first = step_first;
-            run_cnt += __reduce_add_sync(CPM_FULL, lc);
+            const unsigned mask = __ballot_sync(CPM_FULL, lc != 0);
+            if (mask) {
+                const unsigned below = mask & ((1u << lane) - 1u);
+                const int src = below ? 31 - __clz(below) : (int)lane;
+                const long long prev = __shfl_sync(CPM_FULL, ll, src);  // last set row of the nearest lower lane
+                if (lc) {
+                    if (below) gmax = max(gmax, lf - prev);
+                    else if (run_cnt) gmax = max(gmax, lf - run_last);
+                }
+                const long long sub_first = __shfl_sync(CPM_FULL, lf, __ffs(mask) - 1);
+                run_last = __shfl_sync(CPM_FULL, ll, 31 - __clz(mask));
+                if (!run_cnt) run_first = sub_first;
+                run_cnt += __reduce_add_sync(CPM_FULL, lc);
+            }
         }
         if (kPrune) {
             bool bad = gmax > max_per;
