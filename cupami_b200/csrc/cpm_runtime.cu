@@ -2038,9 +2038,8 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
 // (CPM_ORDER_DEPTH_FIRST for cuPFEclat, CPM_ORDER_APRIORI for cuPFApriori).
 // Warps per candidate for k_periodic: enough for about 32 resident warps per
 // SM when a level has few candidates, at most one per step of a row.
-template <class Word>
 static uint32_t periodic_parts(const cpm_ctx *ctx, uint64_t n, uint64_t words) {
-    const uint64_t tiles = (words + periodic_tile<Word>() - 1) / periodic_tile<Word>();
+    const uint64_t tiles = (words + PERIODIC_TILE - 1) / PERIODIC_TILE;
     const uint64_t target = (uint64_t)ctx->sms * 32;
     if (!n || n >= target || tiles <= 1) return 1;
     return (uint32_t)std::min<uint64_t>(std::min<uint64_t>((target + n - 1) / n, tiles), 1024);
@@ -2119,7 +2118,7 @@ static int mine_periodic(cpm_ctx *ctx, cpm_db *db, long long ms, long long max_p
         CKR(ds.alloc(&pos, n_items));
         k_iota_u32<<<(n_items + 255) / 256, 256, 0, ctx->stream>>>(cand, n_items);
         CK(cudaGetLastError());
-        const uint32_t parts = periodic_parts<unsigned long long>(ctx, n_items, words);
+        const uint32_t parts = periodic_parts(ctx, n_items, words);
         PSeg *seg = nullptr;
         if (parts > 1) CKR(ds.alloc(&seg, (uint64_t)n_items * parts));
         CKR((periodic_launch<unsigned long long, true>(ctx, parts, seg, bits, db->stride, cand, nullptr, n_items, 1,
@@ -2183,7 +2182,7 @@ static int mine_periodic(cpm_ctx *ctx, cpm_db *db, long long ms, long long max_p
         k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, d_cnt2, k, poff, n_pairs, cand,
                                                                                  left, okf);
         CK(cudaGetLastError());
-        const uint32_t parts = periodic_parts<unsigned long long>(ctx, n_pairs, words);
+        const uint32_t parts = periodic_parts(ctx, n_pairs, words);
         PSeg *seg = nullptr;
         if (parts > 1) CKR(scratch.get(12, &seg, n_pairs * parts));
         CKR((periodic_launch<unsigned long long, true>(ctx, parts, seg, bits, db->stride, cand, okf, n_pairs, w,
@@ -2682,7 +2681,7 @@ extern "C" int cpm_periodic_counts(cpm_ctx *ctx, const uint32_t *d_bitsets, uint
     // Rows past the bitsets' words hold no bits (the reference kernel scans
     // words32 words and skips rows >= n_transactions).
     const uint64_t rows = std::min<uint64_t>(n_transactions, words32 * 32);
-    const uint32_t parts = periodic_parts<uint32_t>(ctx, n_candidates, (rows + 31) / 32);
+    const uint32_t parts = periodic_parts(ctx, n_candidates, (rows + 31) / 32);
     DevScope ds(ctx);
     PSeg *seg = nullptr;
     if (parts > 1) CKR(ds.alloc(&seg, n_candidates * parts));

@@ -7,10 +7,9 @@
 // (end when s = 0), scanning the set bits of the AND of X's rows in order with
 // one thread per candidate (_temporal.py:26-53, launch :156-165).
 //
-// Here one warp handles a candidate: per step its lanes load 2 KB of
-// consecutive words of each of the candidate's rows (four coalesced 512-byte
-// spans, 16 bytes a lane each), each lane scans the set rows of its words in
-// order, and the gaps that cross lane and
+// Here one warp handles a candidate: per step its lanes load 32 * 4
+// consecutive words of each of the candidate's rows (coalesced), each lane
+// scans the set rows of its 4 words in order, and the gaps that cross lane and
 // step boundaries come from a ballot and one shuffle per step; only the
 // largest gap needs a warp reduction, once at the end.  When a level has too
 // few candidates to fill the GPU, each candidate's rows are split over several
@@ -48,36 +47,23 @@ __device__ __forceinline__ unsigned word_popc(unsigned long long x) { return __p
 __device__ __forceinline__ unsigned word_low(uint32_t x) { return __ffs(x) - 1; }
 __device__ __forceinline__ unsigned word_low(unsigned long long x) { return __ffsll(x) - 1; }
 
-// A step of a warp: PERIODIC_SUB sub-steps, each 16 bytes of every row per
-// lane (512 contiguous bytes per warp: one 16-byte load per lane where the
-// row is 16-byte aligned), all loaded before any is scanned.
-constexpr unsigned PERIODIC_SUB = 4;
-template <class Word>
-__host__ __device__ constexpr unsigned periodic_pl() { return 16 / sizeof(Word); }
-template <class Word>
-__host__ __device__ constexpr uint64_t periodic_tile() { return 32ull * PERIODIC_SUB * periodic_pl<Word>(); }
-
-__device__ __forceinline__ void unpack16(const uint4 &u, uint32_t (&w)[4]) {
-    w[0] = u.x; w[1] = u.y; w[2] = u.z; w[3] = u.w;
-}
-__device__ __forceinline__ void unpack16(const uint4 &u, unsigned long long (&w)[2]) {
-    w[0] = (unsigned long long)u.x | ((unsigned long long)u.y << 32);
-    w[1] = (unsigned long long)u.z | ((unsigned long long)u.w << 32);
-}
+// Words a lane loads per step (independent loads in flight); a step of a
+// warp covers PERIODIC_TILE consecutive words.
+constexpr unsigned PERIODIC_PL = 4;
+constexpr uint64_t PERIODIC_TILE = 32 * PERIODIC_PL;
 
 // `parts` warps per candidate c (warp g: candidate g / parts, part g % parts),
 // each over an equal share of the steps: the AND of the width rows
 // cand[c * width ..] of `bits` (Word: uint32_t or unsigned long long; rows of
 // `stride` words; bit b of word v is row v * bits(Word) + b), restricted to
-// rows < n_tx.  In sub-step k of a step at word `base`, lane l takes the
-// PL = 16 / sizeof(Word) words at base + 32 * PL * k + PL * l and scans their
-// set rows in order.  The warp needs no ordered reduction per sub-step: every
-// lane keeps the running count, first and last timestamp of the rows scanned
-// so far (identical on all lanes) and its own running maximum of the gaps it
-// has seen -- inside its words, and from the previous set row (the last set
-// row of the nearest lower lane with one, found by a ballot and one shuffle,
-// or of an earlier sub-step) to its first -- and the maxima are reduced once
-// at the end.
+// rows < n_tx.  Per step lane l takes the PERIODIC_PL words at
+// base + PERIODIC_PL * l (coalesced) and scans their set rows in order.  The
+// warp needs no ordered reduction per step: every lane keeps the running
+// count, first and last timestamp of the rows scanned so far (identical on all
+// lanes) and its own running maximum of the gaps it has seen -- inside its
+// words, and from the previous set row (the last set row of the nearest lower
+// lane with one, found by a ballot and one shuffle, or of an earlier step) to
+// its first -- and the maxima are reduced once at the end.
 // With parts = 1 the warp writes support[c] and period[c] (and, with kPrune,
 // pass[c] = ok_flag[c] && support >= need && period <= max_per); with
 // parts > 1 each warp writes its summary to seg[c * parts + part] and
@@ -88,15 +74,14 @@ __device__ __forceinline__ void unpack16(const uint4 &u, unsigned long long (&w)
 // a stopped part reports gap = LLONG_MAX; only passing candidates have exact
 // values.  Without kPrune every candidate is exact.
 template <class Word, bool kPrune>
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256)
 k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__restrict__ cand,
            const uint32_t *__restrict__ ok_flag, uint64_t n, uint32_t width, const long long *__restrict__ ts,
            uint64_t n_tx, long long end, long long need, long long max_per, uint32_t parts, PSeg *__restrict__ seg,
            unsigned long long *__restrict__ support, long long *__restrict__ period, uint32_t *__restrict__ pass) {
     constexpr unsigned B = sizeof(Word) * 8;
-    constexpr unsigned PL = periodic_pl<Word>();
-    constexpr unsigned SUB = PERIODIC_SUB;
-    constexpr uint64_t TILE = periodic_tile<Word>();
+    constexpr unsigned PL = PERIODIC_PL;
+    constexpr uint64_t TILE = PERIODIC_TILE;
     const uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     const uint64_t c = g / parts;
@@ -121,60 +106,43 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
     long long gmax = 0;              // this lane's largest gap seen
     bool stopped = false;
     for (uint64_t base = t0 * TILE; base < t1 * TILE; base += TILE) {
-        Word x[SUB][PL];
+        const uint64_t v0 = base + (uint64_t)lane * PL;
+        Word x[PL];
 #pragma unroll
-        for (unsigned k = 0; k < SUB; ++k)
-#pragma unroll
-            for (unsigned q = 0; q < PL; ++q) x[k][q] = base + (32 * k + lane) * PL + q < words ? ~Word(0) : Word(0);
+        for (unsigned q = 0; q < PL; ++q) x[q] = v0 + q < words ? ~Word(0) : Word(0);
         for (uint32_t j = 0; j < width; ++j) {
             const Word *row = bits + (uint64_t)cc[j] * stride;
-            const bool aligned = (reinterpret_cast<uintptr_t>(row) & 15) == 0;
 #pragma unroll
-            for (unsigned k = 0; k < SUB; ++k) {
-                const uint64_t v0 = base + (32 * k + lane) * PL;
-                if (aligned && v0 + PL <= words) {
-                    Word w[PL];
-                    unpack16(__ldg(reinterpret_cast<const uint4 *>(row + v0)), w);
+            for (unsigned q = 0; q < PL; ++q)
+                if (v0 + q < words) x[q] &= __ldg(row + v0 + q);
+        }
+        unsigned lc = 0;  // this lane's set rows in this step
+        long long lf = 0, ll = 0;
 #pragma unroll
-                    for (unsigned q = 0; q < PL; ++q) x[k][q] &= w[q];
-                } else {
-#pragma unroll
-                    for (unsigned q = 0; q < PL; ++q)
-                        if (v0 + q < words) x[k][q] &= __ldg(row + v0 + q);
-                }
+        for (unsigned q = 0; q < PL; ++q) {
+            const uint64_t row0 = (v0 + q) * B;
+            if (v0 + q < words && n_tx - row0 < B) x[q] &= (Word(1) << (unsigned)(n_tx - row0)) - Word(1);
+            for (Word y = x[q]; y; y &= y - Word(1)) {  // one timestamp load per set row
+                const long long t = __ldg(ts + row0 + word_low(y));
+                if (lc) gmax = max(gmax, t - ll);
+                else lf = t;
+                ll = t;
+                ++lc;
             }
         }
-#pragma unroll
-        for (unsigned k = 0; k < SUB; ++k) {
-            const uint64_t v0 = base + (32 * k + lane) * PL;
-            unsigned lc = 0;  // this lane's set rows in this sub-step
-            long long lf = 0, ll = 0;
-#pragma unroll
-            for (unsigned q = 0; q < PL; ++q) {
-                const uint64_t row0 = (v0 + q) * B;
-                if (v0 + q < words && n_tx - row0 < B) x[k][q] &= (Word(1) << (unsigned)(n_tx - row0)) - Word(1);
-                for (Word y = x[k][q]; y; y &= y - Word(1)) {  // one timestamp load per set row
-                    const long long t = __ldg(ts + row0 + word_low(y));
-                    if (lc) gmax = max(gmax, t - ll);
-                    else lf = t;
-                    ll = t;
-                    ++lc;
-                }
+        const unsigned mask = __ballot_sync(CPM_FULL, lc != 0);
+        if (mask) {
+            const unsigned below = mask & ((1u << lane) - 1u);
+            const int src = below ? 31 - __clz(below) : (int)lane;
+            const long long prev = __shfl_sync(CPM_FULL, ll, src);  // last set row of the nearest lower lane
+            if (lc) {
+                if (below) gmax = max(gmax, lf - prev);
+                else if (run_cnt) gmax = max(gmax, lf - run_last);
             }
-            const unsigned mask = __ballot_sync(CPM_FULL, lc != 0);
-            if (mask) {
-                const unsigned below = mask & ((1u << lane) - 1u);
-                const int src = below ? 31 - __clz(below) : (int)lane;
-                const long long prev = __shfl_sync(CPM_FULL, ll, src);  // last set row of the nearest lower lane
-                if (lc) {
-                    if (below) gmax = max(gmax, lf - prev);
-                    else if (run_cnt) gmax = max(gmax, lf - run_last);
-                }
-                const long long sub_first = __shfl_sync(CPM_FULL, lf, __ffs(mask) - 1);
-                run_last = __shfl_sync(CPM_FULL, ll, 31 - __clz(mask));
-                if (!run_cnt) run_first = sub_first;
-                run_cnt += __reduce_add_sync(CPM_FULL, lc);
-            }
+            const long long step_first = __shfl_sync(CPM_FULL, lf, __ffs(mask) - 1);
+            run_last = __shfl_sync(CPM_FULL, ll, 31 - __clz(mask));
+            if (!run_cnt) run_first = step_first;
+            run_cnt += __reduce_add_sync(CPM_FULL, lc);
         }
         if (kPrune) {
             bool bad = gmax > max_per;
