@@ -122,12 +122,27 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
         for (unsigned q = 0; q < PL; ++q) {
             const uint64_t row0 = (v0 + q) * B;
             if (v0 + q < words && n_tx - row0 < B) x[q] &= (Word(1) << (unsigned)(n_tx - row0)) - Word(1);
-            for (Word y = x[q]; y; y &= y - Word(1)) {  // one timestamp load per set row
-                const long long t = __ldg(ts + row0 + word_low(y));
-                if (lc) gmax = max(gmax, t - ll);
-                else lf = t;
-                ll = t;
-                ++lc;
+            // One timestamp load per set row, four set rows at a time: the
+            // loads are issued before their gaps are taken, so dense words
+            // do not wait on one load after another.
+            for (Word y = x[q]; y;) {
+                long long t[4];
+                unsigned m = 0;
+#pragma unroll
+                for (unsigned u = 0; u < 4; ++u)
+                    if (y) {
+                        t[u] = __ldg(ts + row0 + word_low(y));
+                        y &= y - Word(1);
+                        m = u + 1;
+                    }
+#pragma unroll
+                for (unsigned u = 0; u < 4; ++u)
+                    if (u < m) {
+                        if (lc) gmax = max(gmax, t[u] - ll);
+                        else lf = t[u];
+                        ll = t[u];
+                        ++lc;
+                    }
             }
         }
         const unsigned mask = __ballot_sync(CPM_FULL, lc != 0);
