@@ -1867,6 +1867,48 @@ struct LevelScratch {
     }
 };
 
+// One level's join, shared by the Apriori and the periodic miners
+// (cuApriori.py:482-490): the prefix groups of the level's rows L[0, d_cnt2[0])
+// of k items, the join partners of every row, then every joined candidate of
+// k + 1 items (scratch slot 5), its left row (slot 6) and whether all of its
+// k-subsets are in the level (slot 7).  One host round trip: n_pairs is the
+// candidate count (0: the search is over) and n_pat the pattern count so far
+// (d_cnt2[1]).  Scratch slots 0-7 are used.
+static int level_join(cpm_ctx *ctx, LevelScratch &scratch, DevScope &lvl, const uint32_t *L, uint64_t n_ub,
+                      const uint64_t *d_cnt2, uint32_t k, uint64_t *d_tot, uint64_t &n_pairs, uint64_t &n_pat,
+                      uint32_t *&cand, uint32_t *&left, uint32_t *&okf, uint64_t &launches) {
+    uint32_t *gflag = nullptr, *partners = nullptr;
+    uint64_t *gid = nullptr, *gfirst = nullptr, *poff = nullptr;
+    CKR(scratch.get(0, &gflag, n_ub));
+    CKR(scratch.get(1, &gid, n_ub));
+    CKR(scratch.get(2, &partners, n_ub));
+    CKR(scratch.get(3, &poff, n_ub));
+    CKR(scratch.get(4, &gfirst, n_ub + 1));
+    const unsigned nb = (unsigned)((n_ub + 255) / 256);
+    k_group_start<<<nb, 256, 0, ctx->stream>>>(L, n_ub, d_cnt2, k, gflag);
+    CK(cudaGetLastError());
+    CKR(scan_u32(ctx, lvl, gflag, gid, n_ub, nullptr, d_tot));
+    k_group_first<<<nb, 256, 0, ctx->stream>>>(gflag, gid, d_cnt2, gfirst);
+    CK(cudaGetLastError());
+    k_partners<<<nb, 256, 0, ctx->stream>>>(gflag, gid, gfirst, n_ub, d_cnt2, partners);
+    CK(cudaGetLastError());
+    uint64_t counts[2] = {0, 0};
+    CK(cudaMemcpyAsync(counts, d_cnt2, 16, cudaMemcpyDeviceToHost, ctx->stream));
+    CKR(scan_u32(ctx, lvl, partners, poff, n_ub, &n_pairs, d_tot));  // synchronises: counts are in
+    n_pat = counts[1];
+    launches += 7;
+    cand = left = okf = nullptr;
+    if (!n_pairs) return CPM_OK;
+    CKR(scratch.get(5, &cand, n_pairs * (k + 1)));
+    CKR(scratch.get(6, &left, n_pairs));
+    CKR(scratch.get(7, &okf, n_pairs));
+    k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, d_cnt2, k, poff, n_pairs, cand, left,
+                                                                             okf);
+    CK(cudaGetLastError());
+    launches++;
+    return CPM_OK;
+}
+
 static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o, cpm_result *res) {
     cpm_stats &st = res->stats;
     DevScope ds(ctx);
@@ -1937,46 +1979,21 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
             }
             const uint32_t w = k + 1;
             DevScope lvl(ctx);  // large-scan temporaries only
-            // Prefix groups and join partners of every row.
-            uint32_t *gflag = nullptr, *partners = nullptr;
-            uint64_t *gid = nullptr, *gfirst = nullptr, *poff = nullptr;
-            CKR(scratch.get(0, &gflag, n_ub));
-            CKR(scratch.get(1, &gid, n_ub));
-            CKR(scratch.get(2, &partners, n_ub));
-            CKR(scratch.get(3, &poff, n_ub));
-            CKR(scratch.get(4, &gfirst, n_ub + 1));
-            const unsigned nb = (unsigned)((n_ub + 255) / 256);
-            k_group_start<<<nb, 256, 0, ctx->stream>>>(L, n_ub, d_cnt2, k, gflag);
-            CK(cudaGetLastError());
-            CKR(scan_u32(ctx, lvl, gflag, gid, n_ub, nullptr, d_tot));
-            k_group_first<<<nb, 256, 0, ctx->stream>>>(gflag, gid, d_cnt2, gfirst);
-            CK(cudaGetLastError());
-            k_partners<<<nb, 256, 0, ctx->stream>>>(gflag, gid, gfirst, n_ub, d_cnt2, partners);
-            CK(cudaGetLastError());
-            uint64_t counts[2] = {0, 0};
-            CK(cudaMemcpyAsync(counts, d_cnt2, 16, cudaMemcpyDeviceToHost, ctx->stream));
+            // Join and prune, then count and keep.
             uint64_t n_pairs = 0;
-            CKR(scan_u32(ctx, lvl, partners, poff, n_ub, &n_pairs, d_tot));  // synchronises: counts are in
-            n_pat = counts[1];
-            st.kernel_launches += 7;
-            if (!n_pairs) break;
-            // Join, prune, count, keep.
             uint32_t *cand = nullptr, *left = nullptr, *okf = nullptr, *sup = nullptr, *pass = nullptr;
             uint64_t *pos = nullptr;
-            CKR(scratch.get(5, &cand, n_pairs * w));
-            CKR(scratch.get(6, &left, n_pairs));
-            CKR(scratch.get(7, &okf, n_pairs));
+            CKR(level_join(ctx, scratch, lvl, L, n_ub, d_cnt2, k, d_tot, n_pairs, n_pat, cand, left, okf,
+                           st.kernel_launches));
+            if (!n_pairs) break;
             CKR(scratch.get(8, &sup, n_pairs));
             CKR(scratch.get(9, &pass, n_pairs));
             CKR(scratch.get(10, &pos, n_pairs));
-            k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, d_cnt2, k, poff, n_pairs,
-                                                                                     cand, left, okf);
-            CK(cudaGetLastError());
             k_count_pruned<<<(unsigned)((n_pairs * 32 + 255) / 256), 256, 0, ctx->stream>>>(
                 db->d_bits, db->stride, cand, okf, n_pairs, w, ms, sup, pass);
             CK(cudaGetLastError());
             CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, nullptr, d_tot));
-            st.kernel_launches += 4;
+            st.kernel_launches += 3;
             st.intersections += n_pairs * (w - 1);
             st.bytes_alg += n_pairs * w * db->stride * 8;
             // Survivors: at most n_pairs rows and patterns.
@@ -2146,42 +2163,18 @@ static int mine_periodic(cpm_ctx *ctx, cpm_db *db, long long ms, long long max_p
         if (k + 1 > 64) return set_err(ctx, CPM_EINVAL, "patterns longer than 64 items are not supported");
         const uint32_t w = k + 1;
         DevScope lvl(ctx);  // large-scan temporaries only
-        uint32_t *gflag = nullptr, *partners = nullptr;
-        uint64_t *gid = nullptr, *gfirst = nullptr, *poff = nullptr;
-        CKR(scratch.get(0, &gflag, n_ub));
-        CKR(scratch.get(1, &gid, n_ub));
-        CKR(scratch.get(2, &partners, n_ub));
-        CKR(scratch.get(3, &poff, n_ub));
-        CKR(scratch.get(4, &gfirst, n_ub + 1));
-        const unsigned nb = (unsigned)((n_ub + 255) / 256);
-        k_group_start<<<nb, 256, 0, ctx->stream>>>(L, n_ub, d_cnt2, k, gflag);
-        CK(cudaGetLastError());
-        CKR(scan_u32(ctx, lvl, gflag, gid, n_ub, nullptr, d_tot));
-        k_group_first<<<nb, 256, 0, ctx->stream>>>(gflag, gid, d_cnt2, gfirst);
-        CK(cudaGetLastError());
-        k_partners<<<nb, 256, 0, ctx->stream>>>(gflag, gid, gfirst, n_ub, d_cnt2, partners);
-        CK(cudaGetLastError());
-        uint64_t counts[2] = {0, 0};
-        CK(cudaMemcpyAsync(counts, d_cnt2, 16, cudaMemcpyDeviceToHost, ctx->stream));
-        uint64_t n_pairs = 0;
-        CKR(scan_u32(ctx, lvl, partners, poff, n_ub, &n_pairs, d_tot));  // synchronises: counts are in
-        const uint64_t n_pat = counts[1];
-        st.kernel_launches += 7;
-        if (!n_pairs) break;
+        uint64_t n_pairs = 0, n_pat = 0;
         uint32_t *cand = nullptr, *left = nullptr, *okf = nullptr, *pass = nullptr;
         unsigned long long *sup = nullptr;
         long long *per = nullptr;
         uint64_t *pos = nullptr;
-        CKR(scratch.get(5, &cand, n_pairs * w));
-        CKR(scratch.get(6, &left, n_pairs));
-        CKR(scratch.get(7, &okf, n_pairs));
+        CKR(level_join(ctx, scratch, lvl, L, n_ub, d_cnt2, k, d_tot, n_pairs, n_pat, cand, left, okf,
+                       st.kernel_launches));
+        if (!n_pairs) break;
         CKR(scratch.get(8, &sup, n_pairs));
         CKR(scratch.get(9, &pass, n_pairs));
         CKR(scratch.get(10, &pos, n_pairs));
         CKR(scratch.get(11, &per, n_pairs));
-        k_join_pairs<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(L, d_cnt2, k, poff, n_pairs, cand,
-                                                                                 left, okf);
-        CK(cudaGetLastError());
         const uint32_t parts = periodic_parts(ctx, n_pairs, words);
         PSeg *seg = nullptr;
         if (parts > 1) CKR(scratch.get(12, &seg, n_pairs * parts));
@@ -2189,7 +2182,7 @@ static int mine_periodic(cpm_ctx *ctx, cpm_db *db, long long ms, long long max_p
                                                         db->d_ts, db->n_tx, db->end, need, max_per, sup, per, pass,
                                                         st.kernel_launches)));
         CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, nullptr, d_tot));
-        st.kernel_launches += 3;
+        st.kernel_launches += 2;
         st.intersections += n_pairs * (w - 1);
         uint32_t *L2 = nullptr, *pid2 = nullptr;
         CKR(reserve(n_pat, pat_ub + n_pairs));
