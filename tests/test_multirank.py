@@ -27,7 +27,7 @@ def _rank_main(rank, world, port, out):
     try:
         import bench
 
-        seed = bench.rank_seed("planted-100k", rank)
+        seed = (bench.rank_seed("planted-100k", rank), bench.rank_seed("temporal-100k", rank))
         # rank 1 is slower on the first value, rank 0 on the second
         got = bench.max_over_ranks([1.0 + rank, 5.0 - rank], "cpu")
         out.put((rank, seed, got))
@@ -49,6 +49,6 @@ def test_replicas_take_distinct_seeds_and_max_timings():
         p.join(timeout=60)
         assert p.exitcode == 0
     seeds = [s for _, s, _ in results]
-    assert seeds == [7, 8]
+    assert seeds == [(7, 23), (8, 24)]
     for _, _, got in results:
         assert got == [2.0, 5.0]

@@ -173,6 +173,39 @@ def test_temporal_text_bin_and_parquet_inputs(tmp_path):
     assert m._timestamps == [1, 2, 3] and m._Database == [(), ("4294967295",), ("7", "1")]
 
 
+def test_temporal_workload_generator():
+    """The benchmark's temporal database: seeded, one row per transaction, empty
+    baskets kept, timestamps sorted with repeats, planted patterns periodic."""
+    from cupami_b200 import datasets
+
+    csr, ts = datasets.temporal_planted(n=20_000, seed=5)
+    again, ts2 = datasets.temporal_planted(n=20_000, seed=5)
+    assert np.array_equal(csr.offsets, again.offsets) and np.array_equal(csr.items, again.items)
+    assert np.array_equal(ts, ts2) and ts.dtype == np.int64
+    lengths = np.diff(csr.offsets.astype(np.int64))
+    assert csr.n_transactions == 20_000 == ts.size
+    assert 0.01 < np.mean(lengths == 0) < 0.03  # empty baskets kept
+    assert np.all(np.diff(ts) >= 0) and np.any(np.diff(ts) == 0) and ts[0] >= 0
+    for r in range(0, 20_000, 997):  # baskets are sets of ids in [1, 200]
+        basket = csr.items[csr.offsets[r]:csr.offsets[r + 1]]
+        assert np.unique(basket).size == basket.size and (basket.size == 0 or basket.min() >= 1)
+    assert csr.items.max() <= 200
+
+
+def test_temporal_workload_mines_deep_patterns_on_the_oracle():
+    """At the benchmark's thresholds a quarter-size database still yields periodic
+    patterns several items long (the workload exercises the level loop)."""
+    from cupami_b200 import datasets
+    from oracle import periodic
+
+    csr, ts = datasets.temporal_planted(n=25_000, seed=23)
+    o, it = csr.offsets.tolist(), csr.items.tolist()
+    rows = [[int(t), *it[o[i]:o[i + 1]]] for i, t in enumerate(ts.tolist())]
+    got = periodic.mine(rows, 0.005, 2500 // 4, "apriori")
+    lengths = [len(k.split("\t")) for k in got]
+    assert len(got) > 100 and max(lengths) >= 4
+
+
 # ---- GPU: the drop-in miners against the reference's outputs ------------------
 
 @pytest.mark.gpu
