@@ -42,8 +42,6 @@ __device__ __forceinline__ PSeg pseg_join(const PSeg &a, const PSeg &b) {
     return r;
 }
 
-__device__ __forceinline__ unsigned word_popc(uint32_t x) { return __popc(x); }
-__device__ __forceinline__ unsigned word_popc(unsigned long long x) { return __popcll(x); }
 __device__ __forceinline__ unsigned word_low(uint32_t x) { return __ffs(x) - 1; }
 __device__ __forceinline__ unsigned word_low(unsigned long long x) { return __ffsll(x) - 1; }
 
