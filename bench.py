@@ -402,10 +402,12 @@ def run_periodic(args, world, rank, local):
     if pg:
         pg.barrier()
 
+    from cupami_b200.datasets import TemporalCSR
+
     def api_step():
         t, d2h = 0.0, 0
         for cls in (cupami_b200.cuPFEclat, cupami_b200.cuPFApriori):
-            m = cls([[int(t_), *b] for t_, b in zip(ts.tolist(), baskets)], minsup, maxper)
+            m = cls(TemporalCSR(csr.offsets, csr.items, ts), minsup, maxper)
             m.mine()
             t += m.getMiningTime()
             d2h += 20 * len(m._result)  # parent, item, support (4 bytes each) and periodicity (8) per pattern

@@ -25,7 +25,7 @@ from dataclasses import dataclass
 import numpy as np
 
 __all__ = [
-    "TransactionCSR", "uniform_poisson", "planted_zipf", "dense_fixed_length",
+    "TransactionCSR", "TemporalCSR", "uniform_poisson", "planted_zipf", "dense_fixed_length",
     "dense_bernoulli", "sparse_zipf", "batched_zipf", "reference_uniform_baskets",
     "temporal_planted", "workload",
 ]
@@ -63,6 +63,29 @@ class TransactionCSR:
         if universe is None:
             universe = int(flat.max()) if flat.size else 1
         return cls(offsets, flat, max(1, int(universe)))
+
+
+@dataclass
+class TemporalCSR:
+    """A temporal database in compressed-row form: row r holds the item ids
+    ``items[offsets[r]:offsets[r + 1]]`` (empty rows allowed) at ``timestamps[r]``."""
+
+    offsets: np.ndarray     # uint64[N + 1]
+    items: np.ndarray       # uint32[nnz]
+    timestamps: np.ndarray  # int64[N], nonnegative
+
+    @property
+    def n_transactions(self) -> int:
+        return int(self.offsets.size - 1)
+
+    @property
+    def nnz(self) -> int:
+        return int(self.items.size)
+
+    def rows(self):
+        """Rows ``[timestamp, *item ids]`` as Python lists (small databases only)."""
+        o, it = self.offsets.tolist(), self.items.tolist()
+        return [[t, *it[o[i]:o[i + 1]]] for i, t in enumerate(self.timestamps.tolist())]
 
 
 def _zipf_cdf(n_items: int, s: float) -> np.ndarray:

@@ -19,6 +19,11 @@ Input rules (reference ``:67-147``):
 * ``minSup`` as in ``cuApriori``; ``maxPer`` floats in (0, 1] are fractions of
   the timeline end, anything else is in timestamp units (``:85``).
 
+Integer inputs given as a :class:`~cupami_b200.datasets.TemporalCSR` take a
+numeric path: the arrays are checked and sorted by timestamp as they are, and
+the ids are mapped to columns in the order of their decimal strings -- the
+labels and columns the string path builds, without Python rows.
+
 An itemset is kept when its support is positive and reaches ``minSup`` and its
 periodicity -- the largest gap between consecutive timestamps of the rows
 holding it, counting the gap from 0 to the first and from the last to the end
@@ -41,6 +46,7 @@ from urllib.request import urlopen
 import numpy as np
 
 from .. import _native
+from ..datasets import TemporalCSR
 from ..frequentPattern.cuApriori import _PatternDict, cuApriori
 
 __all__ = ["TemporalInput", "periodic_counts", "read_binary", "read_parquet"]
@@ -150,6 +156,7 @@ class TemporalInput(cuApriori):
     def __init__(self, iFile, minSup, maxPer, sep=None, *, endTime=None):
         loading_start = time.perf_counter()
         self._timestamps = []
+        self._tcsr = None  # (offsets, ids, timestamps) of a TemporalCSR input, rows sorted by timestamp
         self.endTime = endTime
         self.maxPer = maxPer
         super().__init__(iFile, minSup, sep, use_gds=False, use_gpu_io=False)
@@ -174,6 +181,8 @@ class TemporalInput(cuApriori):
         return timestamp
 
     def _readTransactions(self, source):
+        if isinstance(source, TemporalCSR):
+            return self._useTemporalCsr(source)
         if isinstance(source, (str, Path)):
             suffix = Path(str(source)).suffix.lower()
             is_url = urlparse(str(source)).scheme in ("http", "https")
@@ -197,6 +206,42 @@ class TemporalInput(cuApriori):
             rows = source
         return self._cleanTemporalRows(rows)
 
+    def _setTimeline(self, last):
+        self._endTimestamp = last if self.endTime is None else self._timestamp(self.endTime)
+        if self._endTimestamp < last:
+            raise ValueError("endTime must be at least the last timestamp")
+
+    def _useTemporalCsr(self, source):
+        """Integer arrays: every row a transaction (empty ones too), sorted by timestamp (stable)."""
+        offsets = np.ascontiguousarray(source.offsets, dtype=np.uint64)
+        ids = np.ascontiguousarray(source.items, dtype=np.uint32)
+        ts = np.asarray(source.timestamps)
+        n = offsets.size - 1
+        if n < 0 or ts.shape != (n,):
+            raise ValueError("TemporalCSR needs one timestamp per row")
+        if not np.issubdtype(ts.dtype, np.integer) or (ts.size and (ts.min() < 0 or ts.max() > _INT64_MAX)):
+            raise ValueError("timestamps must be nonnegative int64 integers")
+        ts = ts.astype(np.int64)
+        if offsets[0] != 0 or offsets[-1] != ids.size or np.any(offsets[1:] < offsets[:-1]):
+            raise ValueError("Invalid TemporalCSR offsets")
+        if np.any(ts[1:] < ts[:-1]):
+            order = np.argsort(ts, kind="stable")
+            lengths = np.diff(offsets.astype(np.int64))[order]
+            starts = offsets[:-1].astype(np.int64)[order]
+            new_offsets = np.zeros(n + 1, dtype=np.int64)
+            np.cumsum(lengths, out=new_offsets[1:])
+            gather = np.repeat(starts - new_offsets[:-1], lengths) + np.arange(int(new_offsets[-1]), dtype=np.int64)
+            ids = ids[gather]
+            offsets = new_offsets.astype(np.uint64)
+            ts = ts[order]
+        self._tcsr = (offsets, ids, ts)
+        self._transactionCount = n
+        self._timestamps = ts.tolist()
+        self._setTimeline(int(ts[-1]) if n else 0)
+        self._inputBackend = {"backend": "numpy-cuda",
+                              "reason": "Integer temporal arrays sent to the GPU; no Python transactions"}
+        return None
+
     def _cleanTemporalRows(self, rows):
         records = []
         for row in rows:
@@ -206,10 +251,7 @@ class TemporalInput(cuApriori):
             records.append((self._timestamp(row[0]), self._cleanTransaction(row[1:])))
         records.sort(key=lambda record: record[0])
         self._timestamps = [record[0] for record in records]
-        last = self._timestamps[-1] if records else 0
-        self._endTimestamp = last if self.endTime is None else self._timestamp(self.endTime)
-        if self._endTimestamp < last:
-            raise ValueError("endTime must be at least the last timestamp")
+        self._setTimeline(self._timestamps[-1] if records else 0)
         self._inputBackend = {"backend": "cpu", "reason": "Temporal reader; mining uses CUDA"}
         return [record[1] for record in records]
 
@@ -217,8 +259,17 @@ class TemporalInput(cuApriori):
         """The largest periodicity that passes, as an int64 (periods are integers)."""
         return min(math.floor(self._maxPer), int(_INT64_MAX))
 
-    def _deviceDatabase(self, ctx):
-        """Temporal tidsets (every row, empty ones too) and the sorted labels."""
+    def _temporalColumns(self):
+        """(offsets, columns, n_items, timestamps, labels) of the tidsets to build."""
+        if self._tcsr is not None:
+            offsets, ids, ts = self._tcsr
+            uniq = np.unique(ids)
+            names = [str(v) for v in uniq.tolist()]
+            order = sorted(range(len(names)), key=names.__getitem__)  # decimal-string order of the ids
+            rank = np.empty(len(names), dtype=np.uint32)
+            rank[order] = np.arange(len(names), dtype=np.uint32)
+            cols = rank[np.searchsorted(uniq, ids)] if ids.size else np.zeros(0, dtype=np.uint32)
+            return offsets, cols, len(names), ts, [names[i] for i in order]
         flat = list(chain.from_iterable(self._Database))
         labels = sorted(set(flat))
         index = dict(zip(labels, range(len(labels))))
@@ -226,9 +277,12 @@ class TemporalInput(cuApriori):
         offsets = np.zeros(n + 1, dtype=np.uint64)
         np.cumsum(np.fromiter(map(len, self._Database), dtype=np.uint64, count=n), out=offsets[1:])
         cols = np.fromiter(map(index.__getitem__, flat), dtype=np.uint32, count=len(flat))
-        timestamps = np.asarray(self._timestamps, dtype=np.int64)
-        return _native.Database.from_temporal(ctx, offsets, cols, len(labels), timestamps,
-                                              self._endTimestamp), labels
+        return offsets, cols, len(labels), np.asarray(self._timestamps, dtype=np.int64), labels
+
+    def _deviceDatabase(self, ctx):
+        """Temporal tidsets (every row, empty ones too) and the sorted labels."""
+        offsets, cols, n_items, timestamps, labels = self._temporalColumns()
+        return _native.Database.from_temporal(ctx, offsets, cols, n_items, timestamps, self._endTimestamp), labels
 
     def autotune(self):
         raise NotImplementedError("the periodic miners have no launch shapes to tune")

@@ -173,6 +173,61 @@ def test_temporal_text_bin_and_parquet_inputs(tmp_path):
     assert m._timestamps == [1, 2, 3] and m._Database == [(), ("4294967295",), ("7", "1")]
 
 
+def _row_pairs(offsets, cols):
+    o = np.asarray(offsets, dtype=np.int64)
+    return [sorted(set(cols[o[r]:o[r + 1]].tolist())) for r in range(o.size - 1)]
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_temporal_csr_input_builds_the_string_paths_tidsets(seed):
+    """A TemporalCSR (integer ids, unsorted timestamps, repeated ids in a row,
+    empty rows) gives the same labels, rows, timestamps and thresholds as the
+    same data given as rows -- the arrays handed to cpm_tdb_from_csr agree."""
+    import cupami_b200
+    from cupami_b200.datasets import TemporalCSR
+
+    rng = np.random.default_rng(seed)
+    n = 500
+    lengths = rng.integers(0, 6, n)
+    offsets = np.zeros(n + 1, dtype=np.uint64)
+    np.cumsum(lengths, out=offsets[1:])
+    ids = rng.choice(np.array([1, 2, 3, 10, 11, 20, 100, 4294967295], dtype=np.uint32), int(offsets[-1]))
+    ts = rng.integers(0, 300, n).astype(np.int64)
+    tcsr = TemporalCSR(offsets, ids, ts)
+    for cls in (cupami_b200.cuPFEclat, cupami_b200.cuPFApriori):
+        a = cls(tcsr, 0.05, 0.2)
+        b = cls(tcsr.rows(), 0.05, 0.2)
+        assert a._Database is None and a.getInputBackend()["backend"] == "numpy-cuda"
+        assert (a._transactionCount, a._minSup, a._endTimestamp, a._maxPer) == \
+            (b._transactionCount, b._minSup, b._endTimestamp, b._maxPer)
+        assert a._timestamps == b._timestamps
+        oa, ca, na, tsa, la = a._temporalColumns()
+        ob, cb, nb, tsb, lb = b._temporalColumns()
+        assert la == lb and na == nb and np.array_equal(tsa, tsb)
+        assert _row_pairs(oa, ca) == _row_pairs(ob, cb)
+
+
+def test_temporal_csr_input_checks():
+    import cupami_b200
+    from cupami_b200.datasets import TemporalCSR
+
+    off = np.array([0, 1, 2], dtype=np.uint64)
+    ids = np.array([1, 2], dtype=np.uint32)
+    with pytest.raises(ValueError):
+        cupami_b200.cuPFEclat(TemporalCSR(off, ids, np.array([1, -1])), 1, 2)
+    with pytest.raises(ValueError):
+        cupami_b200.cuPFEclat(TemporalCSR(off, ids, np.array([1])), 1, 2)
+    with pytest.raises(ValueError):
+        cupami_b200.cuPFEclat(TemporalCSR(np.array([0, 2, 1], dtype=np.uint64), ids, np.array([1, 2])), 1, 2)
+    with pytest.raises(ValueError):
+        cupami_b200.cuPFEclat(TemporalCSR(off, ids, np.array([1.5, 2.0])), 1, 2)
+    with pytest.raises(ValueError):
+        cupami_b200.cuPFEclat(TemporalCSR(off, ids, np.array([5, 1])), 1, 2, endTime=3)
+    m = cupami_b200.cuPFApriori(TemporalCSR(np.zeros(1, np.uint64), np.zeros(0, np.uint32),
+                                            np.zeros(0, np.int64)), 1, 0)
+    assert m._transactionCount == 0 and m._temporalColumns()[2] == 0
+
+
 def test_temporal_workload_generator():
     """The benchmark's temporal database: seeded, one row per transaction, empty
     baskets kept, timestamps sorted with repeats, planted patterns periodic."""
@@ -221,6 +276,23 @@ def test_gpu_miners_match_reference(fixtures, name):
         assert got == run[name], (case["name"], run["minSup"], run["maxPer"])
         miner.mine()  # mining again gives the same answer
         assert [[k, s, p] for k, (s, p) in miner.getPatterns().items()] == run[name]
+
+
+@pytest.mark.gpu
+def test_gpu_temporal_csr_input_matches_rows():
+    import cupami_b200
+    from cupami_b200 import datasets
+
+    csr, ts = datasets.temporal_planted(n=30_000, seed=9)
+    tcsr = datasets.TemporalCSR(csr.offsets, csr.items, ts[::-1].copy())  # unsorted rows
+    rows = tcsr.rows()
+    for cls in (cupami_b200.cuPFEclat, cupami_b200.cuPFApriori):
+        a = cls(tcsr, 0.005, 900)
+        a.mine()
+        b = cls(rows, 0.005, 900)
+        b.mine()
+        assert list(a.getPatterns().items()) == list(b.getPatterns().items())
+        assert len(a.getPatterns()) > 50
 
 
 @pytest.mark.gpu
