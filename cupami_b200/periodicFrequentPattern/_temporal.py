@@ -263,12 +263,26 @@ class TemporalInput(cuApriori):
         """(offsets, columns, n_items, timestamps, labels) of the tidsets to build."""
         if self._tcsr is not None:
             offsets, ids, ts = self._tcsr
-            uniq = np.unique(ids)
+            top = int(ids.max()) if ids.size else 0
+            small = top < (1 << 24)  # a dense table over the id range
+            if small:
+                present = np.zeros(top + 1, dtype=bool)
+                present[ids] = True
+                uniq = np.flatnonzero(present)
+            else:
+                uniq = np.unique(ids)
             names = [str(v) for v in uniq.tolist()]
             order = sorted(range(len(names)), key=names.__getitem__)  # decimal-string order of the ids
             rank = np.empty(len(names), dtype=np.uint32)
             rank[order] = np.arange(len(names), dtype=np.uint32)
-            cols = rank[np.searchsorted(uniq, ids)] if ids.size else np.zeros(0, dtype=np.uint32)
+            if not ids.size:
+                cols = np.zeros(0, dtype=np.uint32)
+            elif small:
+                table = np.zeros(top + 1, dtype=np.uint32)
+                table[uniq] = rank
+                cols = table[ids]
+            else:
+                cols = rank[np.searchsorted(uniq, ids)]
             return offsets, cols, len(names), ts, [names[i] for i in order]
         flat = list(chain.from_iterable(self._Database))
         labels = sorted(set(flat))

@@ -178,8 +178,8 @@ def _row_pairs(offsets, cols):
     return [sorted(set(cols[o[r]:o[r + 1]].tolist())) for r in range(o.size - 1)]
 
 
-@pytest.mark.parametrize("seed", [0, 1, 2])
-def test_temporal_csr_input_builds_the_string_paths_tidsets(seed):
+@pytest.mark.parametrize("seed,large_ids", [(0, True), (1, True), (2, False), (3, False)])
+def test_temporal_csr_input_builds_the_string_paths_tidsets(seed, large_ids):
     """A TemporalCSR (integer ids, unsorted timestamps, repeated ids in a row,
     empty rows) gives the same labels, rows, timestamps and thresholds as the
     same data given as rows -- the arrays handed to cpm_tdb_from_csr agree."""
@@ -191,7 +191,8 @@ def test_temporal_csr_input_builds_the_string_paths_tidsets(seed):
     lengths = rng.integers(0, 6, n)
     offsets = np.zeros(n + 1, dtype=np.uint64)
     np.cumsum(lengths, out=offsets[1:])
-    ids = rng.choice(np.array([1, 2, 3, 10, 11, 20, 100, 4294967295], dtype=np.uint32), int(offsets[-1]))
+    pool = [1, 2, 3, 10, 11, 20, 100, 4294967295] if large_ids else [0, 1, 2, 3, 10, 11, 20, 100, 1000, 99]
+    ids = rng.choice(np.array(pool, dtype=np.uint32), int(offsets[-1]))
     ts = rng.integers(0, 300, n).astype(np.int64)
     tcsr = TemporalCSR(offsets, ids, ts)
     for cls in (cupami_b200.cuPFEclat, cupami_b200.cuPFApriori):
