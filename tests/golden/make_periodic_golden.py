@@ -111,10 +111,53 @@ def cases(cupami):
     return out
 
 
+def input_cases(cupami):
+    """The reference constructor's view of input files: timestamps, baskets,
+    counts and resolved thresholds (TemporalInput.__init__ and readers,
+    _temporal.py:56-147; formats of cupami/extras/_temporal_io.py)."""
+    import base64
+    import tempfile
+
+    from cupami.extras import _temporal_io
+
+    texts = {
+        "comma.csv": "3,a,b\n1,b\n2,a,a, c \n",
+        "tab.txt": "1\ta\tb\n3\ta\n5\tb\n",
+        "space.txt": "4 x y\n\n2 y\n 6 x\n",
+        "bom-blank.csv": "\ufeff5,p\n\n,\n7,q,p\n7\n",
+        "semicolon.txt": "2;a;b\n1;b\n",
+    }
+    out = []
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        files = {}
+        for name, text in texts.items():
+            (d / name).write_text(text, encoding="utf-8")
+            files[name] = {"text": text}
+        rows = [[3, 7, 7, 1], [1], [2, 4294967295], [2, 5]]
+        _temporal_io.write_binary(d / "t.bin", rows, 4294967295)
+        files["t.bin"] = {"base64": base64.b64encode((d / "t.bin").read_bytes()).decode()}
+        _temporal_io.write_parquet(d / "t.parquet", rows, 4294967295)
+        files["t.parquet"] = {"base64": base64.b64encode((d / "t.parquet").read_bytes()).decode()}
+        settings = {"comma.csv": [(1, 2, None, None), (0.5, 0.5, None, None)],
+                    "tab.txt": [(1, 5, None, None)], "space.txt": [(2, 3, None, 10)],
+                    "bom-blank.csv": [(1, 4, None, None)], "semicolon.txt": [(1, 2, ";", None)],
+                    "t.bin": [(0.25, 1.0, None, None)], "t.parquet": [(2, 2, None, 5)]}
+        for name, runs in settings.items():
+            for min_sup, max_per, sep, end in runs:
+                miner = cupami.cuPFApriori(d / name, min_sup, max_per, sep, endTime=end)
+                out.append({"file": name, "minSup": min_sup, "maxPer": max_per, "sep": sep, "endTime": end,
+                            "timestamps": list(miner._timestamps),
+                            "baskets": [list(b) for b in miner._Database],
+                            "transactions": int(miner._transactionCount), "resolvedMinSup": int(miner._minSup),
+                            "resolvedMaxPer": miner._maxPer, "end": int(miner._endTimestamp)})
+    return {"files": files, "runs": out}
+
+
 def main():
     cupami = load()
     fixtures = {"generator": "tests/golden/make_periodic_golden.py", "reference": str(REF.name),
-                "cases": cases(cupami)}
+                "cases": cases(cupami), "inputs": input_cases(cupami)}
     (HERE / "periodic_patterns.json").write_text(json.dumps(fixtures, separators=(",", ":")))
     n = sum(len(r[m]) for c in fixtures["cases"] for r in c["results"] for m in ("cuPFEclat", "cuPFApriori"))
     print(f"wrote {len(fixtures['cases'])} cases, {n} patterns")

@@ -105,6 +105,32 @@ def test_insertion_order_from_shuffled_trees(fixtures, name, order, prefix_tree)
 
 # ---- CPU: temporal input rules -------------------------------------------------
 
+@pytest.mark.parametrize("cls_name", ["cuPFEclat", "cuPFApriori"])
+def test_input_files_read_as_the_reference_reads_them(tmp_path, fixtures, cls_name):
+    """Temporal CSV/TSV/whitespace text (BOM, blank lines and values, explicit
+    separator), CUPAMIT1 BIN and Parquet files: timestamps, baskets, row count
+    and resolved thresholds equal the reference constructor's."""
+    import base64
+
+    import cupami_b200
+
+    inputs = fixtures["inputs"]
+    for name, content in inputs["files"].items():
+        path = tmp_path / name
+        if "text" in content:
+            path.write_bytes(content["text"].encode("utf-8"))
+        else:
+            path.write_bytes(base64.b64decode(content["base64"]))
+    cls = getattr(cupami_b200, cls_name)
+    for run in inputs["runs"]:
+        m = cls(tmp_path / run["file"], run["minSup"], run["maxPer"], run["sep"], endTime=run["endTime"])
+        got = {"timestamps": m._timestamps, "baskets": [list(b) for b in m._Database],
+               "transactions": m._transactionCount, "resolvedMinSup": m._minSup,
+               "resolvedMaxPer": m._maxPer, "end": m._endTimestamp}
+        assert got == {k: run[k] for k in got}, run["file"]
+    assert len(inputs["runs"]) >= 8
+
+
 def test_temporal_rows_sorting_empties_and_thresholds():
     import cupami_b200
 
