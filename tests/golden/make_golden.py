@@ -154,10 +154,57 @@ def quickstart(cupami):
     return {"name": "quickstart-10000x50-seed42", "data": "quickstart_10000x50.npz", "results": res}
 
 
+def input_cases(cupami):
+    """The reference constructor's view of input files (cuApriori.__init__ and its
+    readers, cupami/frequentPattern/cuApriori.py:173-456, with use_gpu_io=False
+    and use_gds=False): baskets, transaction count and resolved threshold."""
+    import base64
+    import struct
+    import tempfile
+
+    texts = {
+        "comma.csv": "a,b\n b ,a,a\n\n10,2\n",
+        "tab.tsv": "x\ty\n\ny\n",
+        "semicolon.txt": "1;2\n2;3;;\n",
+        "bom.csv": "\ufeffa,b\nb\n",
+        "spaces.csv": " , ,\nq, r \n",
+    }
+    out = []
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        files = {}
+        for name, text in texts.items():
+            (d / name).write_bytes(text.encode("utf-8"))
+            files[name] = {"text": text}
+        rows = [[1, 1, 2], [], [0, 2], [4294967295, 2]]
+        flat, offsets = [], [0]
+        for r in rows:
+            flat.extend(r)
+            offsets.append(len(flat))
+        blob = (struct.pack("<8sQQQ", b"CUPAMI01", len(rows), len(flat), 4294967295)
+                + struct.pack(f"<{len(offsets)}Q", *offsets) + struct.pack(f"<{len(flat)}I", *flat))
+        (d / "t.bin").write_bytes(blob)
+        files["t.bin"] = {"base64": base64.b64encode(blob).decode()}
+        import pyarrow as pa
+        import pyarrow.parquet as pq
+        pq.write_table(pa.table({"items": pa.array(rows, pa.list_(pa.uint32()))}), d / "t.parquet")
+        files["t.parquet"] = {"base64": base64.b64encode((d / "t.parquet").read_bytes()).decode()}
+        settings = {"comma.csv": [(1, None), (0.5, None)], "tab.tsv": [(1, None)], "semicolon.txt": [(1, ";")],
+                    "bom.csv": [(1, None)], "spaces.csv": [(1, None)], "t.bin": [(0.5, None)],
+                    "t.parquet": [(2, None)]}
+        for name, runs in settings.items():
+            for min_sup, sep in runs:
+                miner = cupami.cuApriori(d / name, min_sup, sep, use_gds=False, use_gpu_io=False)
+                out.append({"file": name, "minSup": min_sup, "sep": sep,
+                            "baskets": [list(b) for b in miner._Database],
+                            "transactions": int(miner._transactionCount), "resolvedMinSup": int(miner._minSup)})
+    return {"files": files, "runs": out}
+
+
 def main():
     cupami = load_reference()
     fixtures = {"generator": "tests/golden/make_golden.py", "reference": "cuPAMI 2026.11.02",
-                "cases": cases(cupami), "quickstart": quickstart(cupami)}
+                "cases": cases(cupami), "quickstart": quickstart(cupami), "inputs": input_cases(cupami)}
     (HERE / "reference_patterns.json").write_text(json.dumps(fixtures, separators=(",", ":")))
     n = sum(len(r["patterns"]) for c in fixtures["cases"] for rs in c["results"].values() for r in rs)
     print(f"wrote {len(fixtures['cases'])} cases, {n} patterns, quickstart "

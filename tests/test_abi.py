@@ -180,3 +180,30 @@ def test_text_url_and_timing(tmp_path):
     m = cupami_b200.cuApriori(csv_path, 1)
     assert m.getInputBackend()["backend"] == "cpu"
     assert m._Database == [("apple,pear", "banana"), ("banana",)]
+
+
+@pytest.mark.parametrize("cls_name", ["cuEclat", "cuApriori"])
+def test_input_files_read_as_the_reference_reads_them(tmp_path, golden, cls_name):
+    """CSV/TSV text (detected or explicit separator, blank lines and values, a
+    byte-order mark kept as the reference keeps it), CUPAMI01 BIN and Parquet:
+    baskets, transaction count and resolved threshold equal the reference
+    constructor's; the numeric BIN/Parquet path agrees on the counts."""
+    import base64
+
+    import cupami_b200
+
+    inputs = golden["inputs"]
+    for name, content in inputs["files"].items():
+        data = content["text"].encode("utf-8") if "text" in content else base64.b64decode(content["base64"])
+        (tmp_path / name).write_bytes(data)
+    cls = getattr(cupami_b200, cls_name)
+    for run in inputs["runs"]:
+        path = tmp_path / run["file"]
+        m = cls(path, run["minSup"], run["sep"], use_gds=False, use_gpu_io=False)
+        got = {"baskets": [list(b) for b in m._Database], "transactions": m._transactionCount,
+               "resolvedMinSup": m._minSup}
+        assert got == {k: run[k] for k in got}, run["file"]
+        if path.suffix in (".bin", ".parquet"):
+            fast = cls(path, run["minSup"], run["sep"])
+            assert (fast._transactionCount, fast._minSup) == (run["transactions"], run["resolvedMinSup"])
+    assert len(inputs["runs"]) >= 8
