@@ -26,3 +26,30 @@ def oracle_lib():
 
     oracle.build()
     return oracle
+
+
+def _inject_result(miner, patterns, order):
+    """Give a miner the result `patterns` ([[tab-joined labels, support], ...] in
+    insertion order, prefixes first) without a GPU: a host pattern tree ordered
+    by the C ABI, as mine() would leave it."""
+    from cupami_b200._native import Result
+
+    labels = sorted({x for key, *_ in patterns for x in key.split("\t")})
+    col = {x: i for i, x in enumerate(labels)}
+    ids = {}
+    parent, item, support = [], [], []
+    for k, (key, sup, *_) in enumerate(patterns):
+        items = [col[x] for x in key.split("\t")]
+        parent.append(ids[tuple(items[:-1])] if len(items) > 1 else -1)
+        item.append(items[-1])
+        support.append(sup)
+        ids[tuple(items)] = k
+    miner._result = Result.from_tree(parent, item, support, order)
+    miner._labels = labels
+    miner._patterns = None
+    return miner
+
+
+@pytest.fixture(scope="session")
+def inject():
+    return _inject_result

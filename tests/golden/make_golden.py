@@ -201,10 +201,34 @@ def input_cases(cupami):
     return {"files": files, "runs": out}
 
 
+def output_cases(cupami):
+    """The reference's save() text and getPatternsAsDataFrame() rows
+    (cuApriori.py:537-560) for a few cases, both miners."""
+    import tempfile
+
+    out = []
+    for name, rows, min_sup in (("labels", [[" a", "a ", "b,c"], ["b,c", 10, "10"], ["a", 9, "b,c"], [2, 10]], 1),
+                                ("deep", [["a", "b", "c", "d"]] * 3 + [["a", "c"], ["b", "d"]], 2)):
+        for algo in ("cuEclat", "cuApriori"):
+            miner = getattr(cupami, algo)(rows, min_sup, use_gpu_io=False, use_gds=False)
+            miner.mine()
+            with tempfile.TemporaryDirectory() as d:
+                path = Path(d) / "out.txt"
+                miner.save(path)
+                text = path.read_text(encoding="utf-8")
+            df = miner.getPatternsAsDataFrame()
+            out.append({"name": name, "algorithm": algo, "minSup": min_sup, "rows": [list(map(str, r)) for r in rows],
+                        "patterns": [[k, int(v)] for k, v in miner.getPatterns().items()],
+                        "save": text, "columns": list(df.columns),
+                        "frame": [[str(a), int(b)] for a, b in df.values.tolist()]})
+    return out
+
+
 def main():
     cupami = load_reference()
     fixtures = {"generator": "tests/golden/make_golden.py", "reference": "cuPAMI 2026.11.02",
-                "cases": cases(cupami), "quickstart": quickstart(cupami), "inputs": input_cases(cupami)}
+                "cases": cases(cupami), "quickstart": quickstart(cupami), "inputs": input_cases(cupami),
+                "outputs": output_cases(cupami)}
     (HERE / "reference_patterns.json").write_text(json.dumps(fixtures, separators=(",", ":")))
     n = sum(len(r["patterns"]) for c in fixtures["cases"] for rs in c["results"].values() for r in rs)
     print(f"wrote {len(fixtures['cases'])} cases, {n} patterns, quickstart "

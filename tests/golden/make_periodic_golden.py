@@ -154,10 +154,34 @@ def input_cases(cupami):
     return {"files": files, "runs": out}
 
 
+def output_cases(cupami):
+    """The reference's save() text and getPatternsAsDataFrame() rows
+    (_temporal.py:173-181) for the paper example, both miners."""
+    import tempfile
+
+    baskets = ["ab", "acdi", "cefj", "abfgh", "bcd", "def", "abi", "cde", "abef", "acg"]
+    rows = [[i + 1, *b] for i, b in enumerate(baskets)]
+    out = []
+    for name in ("cuPFEclat", "cuPFApriori"):
+        miner = getattr(cupami, name)(rows, 3, 3)
+        miner.mine()
+        with tempfile.TemporaryDirectory() as d:
+            path = Path(d) / "out.txt"
+            miner.save(path)
+            text = path.read_text(encoding="utf-8")
+        df = miner.getPatternsAsDataFrame()
+        out.append({"algorithm": name, "rows": rows, "minSup": 3, "maxPer": 3,
+                    "patterns": [[k, int(s), int(p)] for k, (s, p) in miner.getPatterns().items()],
+                    "save": text, "columns": list(df.columns),
+                    "frame": [[str(a), int(b), int(c)] for a, b, c in df.values.tolist()]})
+    return out
+
+
 def main():
     cupami = load()
     fixtures = {"generator": "tests/golden/make_periodic_golden.py", "reference": str(REF.name),
-                "cases": cases(cupami), "inputs": input_cases(cupami)}
+                "cases": cases(cupami), "inputs": input_cases(cupami),
+                "outputs": output_cases(cupami)}
     (HERE / "periodic_patterns.json").write_text(json.dumps(fixtures, separators=(",", ":")))
     n = sum(len(r[m]) for c in fixtures["cases"] for r in c["results"] for m in ("cuPFEclat", "cuPFApriori"))
     print(f"wrote {len(fixtures['cases'])} cases, {n} patterns")

@@ -207,3 +207,22 @@ def test_input_files_read_as_the_reference_reads_them(tmp_path, golden, cls_name
             fast = cls(path, run["minSup"], run["sep"])
             assert (fast._transactionCount, fast._minSup) == (run["transactions"], run["resolvedMinSup"])
     assert len(inputs["runs"]) >= 8
+
+
+@pytest.mark.parametrize("index", range(4))
+def test_save_and_dataframe_match_the_reference(tmp_path, golden, inject, index):
+    """save() text and getPatternsAsDataFrame() rows, byte for byte the
+    reference's, from the reference's patterns (cuApriori.py:537-560)."""
+    import cupami_b200
+    from cupami_b200 import _native
+
+    case = golden["outputs"][index]
+    cls = getattr(cupami_b200, case["algorithm"])
+    order = _native.CPM_ORDER_ECLAT if case["algorithm"] == "cuEclat" else _native.CPM_ORDER_APRIORI
+    m = inject(cls(case["rows"], case["minSup"]), case["patterns"], order)
+    assert [[k, v] for k, v in m.getPatterns().items()] == case["patterns"]
+    m.save(tmp_path / "out.txt")
+    assert (tmp_path / "out.txt").read_text(encoding="utf-8") == case["save"]
+    df = m.getPatternsAsDataFrame()
+    assert list(df.columns) == case["columns"]
+    assert [[str(a), int(b)] for a, b in df.values.tolist()] == case["frame"]

@@ -131,6 +131,30 @@ def test_input_files_read_as_the_reference_reads_them(tmp_path, fixtures, cls_na
     assert len(inputs["runs"]) >= 8
 
 
+@pytest.mark.parametrize("index", [0, 1])
+def test_save_and_dataframe_match_the_reference(tmp_path, fixtures, inject, index):
+    """save() lines "{pattern} : {support} : {periodicity}" and the DataFrame
+    (Patterns, Support, Periodicity), the reference's own, from its patterns
+    (_temporal.py:173-181); the result is given to the miner on the host."""
+    import cupami_b200
+    from cupami_b200 import _native
+
+    case = fixtures["outputs"][index]
+    cls = getattr(cupami_b200, case["algorithm"])
+    order = _native.CPM_ORDER_DEPTH_FIRST if case["algorithm"] == "cuPFEclat" else _native.CPM_ORDER_APRIORI
+    m = inject(cls(case["rows"], case["minSup"], case["maxPer"]), case["patterns"], order)
+    period = {key: per for key, _, per in case["patterns"]}
+    o = m._result.offsets.tolist()
+    keys = ["\t".join(m._labels[c] for c in m._result.items[o[k]:o[k + 1]].tolist()) for k in range(len(o) - 1)]
+    m._result.periods = np.array([period[k] for k in keys], dtype=np.int64)
+    assert [[k, s, p] for k, (s, p) in m.getPatterns().items()] == case["patterns"]
+    m.save(tmp_path / "out.txt")
+    assert (tmp_path / "out.txt").read_text(encoding="utf-8") == case["save"]
+    df = m.getPatternsAsDataFrame()
+    assert list(df.columns) == case["columns"]
+    assert [[str(a), int(b), int(c)] for a, b, c in df.values.tolist()] == case["frame"]
+
+
 def test_temporal_rows_sorting_empties_and_thresholds():
     import cupami_b200
 
