@@ -155,6 +155,45 @@ def test_save_and_dataframe_match_the_reference(tmp_path, fixtures, inject, inde
     assert [[str(a), int(b), int(c)] for a, b, c in df.values.tolist()] == case["frame"]
 
 
+# tests/test_miner_examples.py:52-72 of the reference: a manual known answer.
+MANUAL_ROWS = [[1, 1, 2], [1, 2, 3], [3, 1, 3], [5, 1, 2, 3], [8]]
+MANUAL_EXPECTED = {"1": (3, 3), "2": (3, 4), "3": (3, 3), "1\t2": (2, 4), "1\t3": (2, 3), "2\t3": (2, 4)}
+
+
+def _manual_files(directory):
+    csv_path = directory / "manual.csv"
+    csv_path.write_text("".join(",".join(map(str, r)) + "\n" for r in MANUAL_ROWS), encoding="utf-8")
+    offsets, flat = [0], []
+    for r in MANUAL_ROWS:
+        flat.extend(r[1:])
+        offsets.append(len(flat))
+    bin_path = directory / "manual.bin"
+    bin_path.write_bytes(struct.pack("<8sQQQ", b"CUPAMIT1", len(MANUAL_ROWS), len(flat), 3)
+                         + struct.pack(f"<{len(MANUAL_ROWS)}q", *[r[0] for r in MANUAL_ROWS])
+                         + struct.pack(f"<{len(offsets)}Q", *offsets) + struct.pack(f"<{len(flat)}I", *flat))
+    import pyarrow as pa
+    import pyarrow.parquet as pq
+
+    pq_path = directory / "manual.parquet"
+    pq.write_table(pa.table({"timestamp": pa.array([r[0] for r in MANUAL_ROWS], pa.int64()),
+                             "items": pa.array([r[1:] for r in MANUAL_ROWS], pa.list_(pa.uint32()))}), pq_path)
+    return [MANUAL_ROWS, csv_path, bin_path, pq_path]
+
+
+@pytest.mark.parametrize("support", [2, 0.4])
+def test_manual_known_answer_on_the_oracle(tmp_path, support):
+    import cupami_b200
+    from oracle import periodic
+
+    for algo in ("eclat", "apriori"):
+        assert periodic.mine(MANUAL_ROWS, support, 4, algo) == MANUAL_EXPECTED
+    ref = cupami_b200.cuPFEclat(MANUAL_ROWS, support, 4)
+    for source in _manual_files(tmp_path)[1:]:  # every format reads as the rows do
+        m = cupami_b200.cuPFEclat(source, support, 4)
+        assert (m._timestamps, m._Database, m._minSup, m._endTimestamp) == \
+            (ref._timestamps, ref._Database, ref._minSup, ref._endTimestamp), source
+
+
 def test_temporal_rows_sorting_empties_and_thresholds():
     import cupami_b200
 
@@ -327,6 +366,19 @@ def test_gpu_miners_match_reference(fixtures, name):
         assert got == run[name], (case["name"], run["minSup"], run["maxPer"])
         miner.mine()  # mining again gives the same answer
         assert [[k, s, p] for k, (s, p) in miner.getPatterns().items()] == run[name]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["cuPFEclat", "cuPFApriori"])
+def test_gpu_manual_known_answer_all_formats(tmp_path, name):
+    import cupami_b200
+
+    cls = getattr(cupami_b200, name)
+    for source in _manual_files(tmp_path):
+        for support in (2, 0.4):
+            m = cls(source, support, maxPer=4)
+            m.mine()
+            assert m.getPatterns() == MANUAL_EXPECTED, (source, support)
 
 
 @pytest.mark.gpu
