@@ -226,3 +226,26 @@ def test_save_and_dataframe_match_the_reference(tmp_path, golden, inject, index)
     df = m.getPatternsAsDataFrame()
     assert list(df.columns) == case["columns"]
     assert [[str(a), int(b)] for a, b in df.values.tolist()] == case["frame"]
+
+
+@pytest.mark.parametrize("cls_name", ["cuEclat", "cuApriori"])
+def test_timing_labels_exclude_idle_time(cls_name):
+    """Loading time covers the constructor only, mining time mine() only
+    (the reference's tests/test_miner_examples.py:18-28)."""
+    from unittest.mock import patch
+
+    import importlib
+
+    import cupami_b200
+
+    mod = importlib.import_module("cupami_b200.frequentPattern.cuApriori")
+    cls = getattr(cupami_b200, cls_name)
+    with patch.object(cls, "_readTransactions", return_value=[("a",)]), \
+            patch.object(mod.time, "perf_counter", side_effect=[10, 12.5]):
+        miner = cls([], 1, use_gpu_io=False, use_gds=False)
+    assert miner.getLoadingTime() == 2.5
+    assert miner.getMiningTime() == 0
+    assert miner.getTotalRuntime() == 2.5
+    miner._startTime, miner._endTime = 100, 104
+    assert miner.getMiningTime() == 4 and miner.getRuntime() == 4
+    assert miner.getTotalRuntime() == 6.5
