@@ -118,6 +118,7 @@ _SIGNATURES = {
                                         ctypes.POINTER(_P)]),
     "cpm_mine_periodic": (ctypes.c_int, [_P, _P, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.POINTER(_P)]),
     "cpm_result_copy_periodic": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P, _P]),
+    "cpm_result_from_tree_periodic": (ctypes.c_int, [_P, _P, _P, _P, _U64, ctypes.POINTER(_P)]),
     "cpm_periodic_counts": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, _P, _U64, ctypes.c_int64,
                                            _P, _P]),
     "cpm_mine_eclat_noalloc": (ctypes.c_int, [_P, _P, _U64, ctypes.c_uint32, _U64, ctypes.c_int64,
@@ -436,17 +437,22 @@ class Result:
                 for k, s in enumerate(self.supports.tolist())}
 
     @classmethod
-    def from_tree(cls, parent, item, support, order):
-        """Order a host pattern tree (no device work)."""
+    def from_tree(cls, parent, item, support, order, period=None):
+        """Order a host pattern tree (no device work); with ``period`` a periodic result."""
         parent = np.ascontiguousarray(parent, dtype=np.int64)
         item = np.ascontiguousarray(item, dtype=np.uint32)
         support = np.ascontiguousarray(support, dtype=np.uint64)
         handle = _P()
-        code = library().cpm_result_from_tree(_ptr(parent), _ptr(item), _ptr(support), parent.size,
-                                              ctypes.byref(handle))
+        if period is None:
+            code = library().cpm_result_from_tree(_ptr(parent), _ptr(item), _ptr(support), parent.size,
+                                                  ctypes.byref(handle))
+        else:
+            period = np.ascontiguousarray(period, dtype=np.int64)
+            code = library().cpm_result_from_tree_periodic(_ptr(parent), _ptr(item), _ptr(support), _ptr(period),
+                                                           parent.size, ctypes.byref(handle))
         if code != CPM_OK:
             raise NativeError(code, "invalid pattern tree")
         try:
-            return cls.collect(handle, order)
+            return cls.collect(handle, order, periodic=period is not None)
         finally:
             library().cpm_result_free(handle)

@@ -2622,6 +2622,15 @@ extern "C" int cpm_result_from_tree(const int64_t *parent, const uint32_t *item,
     return CPM_OK;
 }
 
+extern "C" int cpm_result_from_tree_periodic(const int64_t *parent, const uint32_t *item, const uint64_t *support,
+                                             const int64_t *period, uint64_t n, cpm_result **out) {
+    if (!out || (n && !period)) return CPM_EINVAL;
+    const int r = cpm_result_from_tree(parent, item, support, n, out);
+    if (r != CPM_OK) return r;
+    (*out)->period.assign(period, period + n);
+    return CPM_OK;
+}
+
 extern "C" int cpm_result_stats(const cpm_result *res, cpm_stats *stats) {
     if (!res || !stats) return CPM_EINVAL;
     *stats = res->stats;

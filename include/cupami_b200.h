@@ -258,6 +258,9 @@ int cpm_tdb_from_csr(cpm_ctx *ctx, const uint64_t *offsets, uint64_t n_rows, con
  * CPM_ORDER_DEPTH_FIRST or CPM_ORDER_APRIORI for the reference's insertion order. */
 int cpm_mine_periodic(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, int64_t max_per, int algo,
                       cpm_result **out);
+/* cpm_result_from_tree for periodic results: period[k] is pattern k's periodicity. */
+int cpm_result_from_tree_periodic(const int64_t *parent, const uint32_t *item, const uint64_t *support,
+                                  const int64_t *period, uint64_t n, cpm_result **out);
 /* cpm_result_copy plus the periodicity of every pattern (periodic results only). */
 int cpm_result_copy_periodic(const cpm_result *res, int order, uint64_t *offsets, uint32_t *items,
                              uint64_t *supports, int64_t *periods);

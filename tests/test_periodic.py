@@ -93,12 +93,12 @@ def test_insertion_order_from_shuffled_trees(fixtures, name, order, prefix_tree)
         labels = sorted({x for p, _, _ in pats for x in p})
         col = {x: i for i, x in enumerate(labels)}
         patterns = [(tuple(sorted(col[x] for x in p)), s, per) for p, s, per in pats]
-        parent, item, support, _ = _tree(patterns, rng, prefix_tree)
-        res = Result.from_tree(parent, item, support, order)
+        parent, item, support, period = _tree(patterns, rng, prefix_tree)
+        res = Result.from_tree(parent, item, support, order, period=period)
         o = res.offsets.tolist()
-        got = [["\t".join(labels[c] for c in res.items[o[k]:o[k + 1]].tolist()), int(res.supports[k])]
-               for k in range(len(res))]
-        assert got == [[k, s] for k, s, _ in run[name]], (case["name"], name)
+        got = [["\t".join(labels[c] for c in res.items[o[k]:o[k + 1]].tolist()), int(res.supports[k]),
+                int(res.periods[k])] for k in range(len(res))]
+        assert got == run[name], (case["name"], name)
         checked += 1
     assert checked >= 12
 
@@ -143,10 +143,6 @@ def test_save_and_dataframe_match_the_reference(tmp_path, fixtures, inject, inde
     cls = getattr(cupami_b200, case["algorithm"])
     order = _native.CPM_ORDER_DEPTH_FIRST if case["algorithm"] == "cuPFEclat" else _native.CPM_ORDER_APRIORI
     m = inject(cls(case["rows"], case["minSup"], case["maxPer"]), case["patterns"], order)
-    period = {key: per for key, _, per in case["patterns"]}
-    o = m._result.offsets.tolist()
-    keys = ["\t".join(m._labels[c] for c in m._result.items[o[k]:o[k + 1]].tolist()) for k in range(len(o) - 1)]
-    m._result.periods = np.array([period[k] for k in keys], dtype=np.int64)
     assert [[k, s, p] for k, (s, p) in m.getPatterns().items()] == case["patterns"]
     m.save(tmp_path / "out.txt")
     assert (tmp_path / "out.txt").read_text(encoding="utf-8") == case["save"]
