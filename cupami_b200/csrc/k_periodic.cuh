@@ -3,9 +3,11 @@
 // For an itemset X held by the rows r_1 < ... < r_s of a temporal database
 // whose rows are sorted by timestamp ts[], the reference kernel returns the
 // support s and the periodicity
-//     max(ts[r_1] - 0, ts[r_2] - ts[r_1], ..., ts[r_s] - ts[r_{s-1}], end - ts[r_s])
-// (end when s = 0), scanning the set bits of the AND of X's rows in order with
-// one thread per candidate (_temporal.py:26-53, launch :156-165).
+//     max(0, ts[r_1] - 0, ts[r_2] - ts[r_1], ..., ts[r_s] - ts[r_{s-1}], end - ts[r_s])
+// (max(0, end) when s = 0; the 0 is the reference scan's starting value and
+// only matters for unsorted or negative inputs), scanning the set bits of the
+// AND of X's rows in order with one thread per candidate (_temporal.py:26-53,
+// launch :156-165).
 //
 // Here one warp handles a candidate: per step its lanes load 32 * 4
 // consecutive words of each of the candidate's rows (coalesced), each lane
@@ -176,7 +178,7 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
     for (int o = 16; o; o >>= 1) gmax = max(gmax, __shfl_xor_sync(CPM_FULL, gmax, o));
     if (lane) return;
     if (parts == 1) {
-        const long long per = run_cnt ? max(max(run_first, gmax), end - run_last) : end;
+        const long long per = run_cnt ? max(max(run_first, gmax), end - run_last) : max(0ll, end);
         support[c] = run_cnt;
         period[c] = per;
         if (kPrune) pass[c] = !stopped && (long long)run_cnt >= need && per <= max_per ? 1u : 0u;
@@ -206,7 +208,7 @@ __global__ void k_periodic_join(const PSeg *__restrict__ seg, uint32_t parts, co
     }
     PSeg run{0, 0, 0, 0};
     for (uint32_t p = 0; p < parts; ++p) run = pseg_join(run, seg[c * parts + p]);
-    const long long per = run.cnt ? max(max(run.first, run.gap), end - run.last) : end;
+    const long long per = run.cnt ? max(max(run.first, run.gap), end - run.last) : max(0ll, end);
     support[c] = run.cnt;
     period[c] = per;
     if (pass) pass[c] = (long long)run.cnt >= need && per <= max_per ? 1u : 0u;

@@ -61,8 +61,8 @@ def prepare(rows, end_time=None):
 def periodic_counts(bits, candidates, timestamps, n, end):
     """``[(support, periodicity)]`` per candidate (column lists): the kernel
     of _temporal.py:26-53 -- AND the rows, then scan the set rows < n in order,
-    the periodicity being the largest of ts[first] - 0, the gaps between
-    consecutive set rows and end - ts[last] (end when no row is set)."""
+    the periodicity being the largest of 0, ts[first] - 0, the gaps between
+    consecutive set rows and end - ts[last] (max(0, end) when no row is set)."""
     out = []
     if not len(candidates):
         return out
@@ -73,16 +73,17 @@ def periodic_counts(bits, candidates, timestamps, n, end):
             acc &= bits[c]
         rows = np.flatnonzero(np.unpackbits(acc.view(np.uint8), bitorder="little"))
         rows = rows[rows < n]
+        # the scan starts from a periodicity of 0 (_temporal.py:38)
         if rows.size == 0:
-            out.append((0, int(end)))
+            out.append((0, max(0, int(end))))
             continue
         ts = timestamps[rows]
-        if int(end) < 2**62:  # no int64 overflow in the differences
+        if abs(int(end)) < 2**62 and np.all(np.abs(ts) < 2**62):  # no int64 overflow in the differences
             gaps = np.diff(np.concatenate(([0], ts, [end])).astype(np.int64))
-            out.append((int(rows.size), int(gaps.max())))
+            out.append((int(rows.size), max(0, int(gaps.max()))))
         else:  # exact Python integers
             points = [0, *ts.tolist(), int(end)]
-            out.append((int(rows.size), max(b - a for a, b in zip(points, points[1:]))))
+            out.append((int(rows.size), max(0, *(b - a for a, b in zip(points, points[1:])))))
     return out
 
 
