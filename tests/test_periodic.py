@@ -475,6 +475,30 @@ def test_gpu_periodic_counts_kernel_exact():
 
 
 @pytest.mark.gpu
+def test_gpu_periodic_counts_kernel_any_timestamps():
+    """The drop-in kernel is exact on any timestamps, as the reference kernel's
+    scan is: unsorted and negative timestamps, negative, zero and positive ends
+    (the periodicity then starts from 0, _temporal.py:38-53)."""
+    import torch
+
+    from cupami_b200.periodicFrequentPattern import _temporal
+    from oracle import periodic
+
+    rng = np.random.default_rng(21)
+    for n_rows, n_items in ((700, 3), (3000, 5), (40000, 4)):
+        rows = [[0, *[f"v{j}" for j in range(n_items) if rng.random() < 0.4]] for _ in range(n_rows)]
+        labels, bits, _, _ = periodic.prepare(rows)
+        ts = rng.integers(-100, 100, n_rows).astype(np.int64)
+        d_bits = torch.from_numpy(bits.view(np.int32).copy()).cuda()
+        d_ts = torch.from_numpy(ts.copy()).cuda()
+        cands = [[c] for c in range(len(labels))] + [
+            sorted(rng.choice(len(labels), 2, replace=False).tolist()) for _ in range(20)]
+        for end in (-7, 0, 150):
+            assert (_temporal.periodic_counts(d_bits, cands, d_ts, n_rows, end)
+                    == periodic.periodic_counts(bits, cands, ts, n_rows, end)), (n_rows, end)
+
+
+@pytest.mark.gpu
 def test_gpu_empty_and_degenerate_inputs():
     import cupami_b200
 
