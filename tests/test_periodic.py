@@ -491,11 +491,12 @@ def test_gpu_periodic_counts_kernel_any_timestamps():
         ts = rng.integers(-100, 100, n_rows).astype(np.int64)
         d_bits = torch.from_numpy(bits.view(np.int32).copy()).cuda()
         d_ts = torch.from_numpy(ts.copy()).cuda()
-        cands = [[c] for c in range(len(labels))] + [
-            sorted(rng.choice(len(labels), 2, replace=False).tolist()) for _ in range(20)]
+        singles = [[c] for c in range(len(labels))]
+        pairs = [sorted(rng.choice(len(labels), 2, replace=False).tolist()) for _ in range(20)]
         for end in (-7, 0, 150):
-            assert (_temporal.periodic_counts(d_bits, cands, d_ts, n_rows, end)
-                    == periodic.periodic_counts(bits, cands, ts, n_rows, end)), (n_rows, end)
+            for cands in (singles, pairs):  # one candidate width per call, as the reference launches
+                assert (_temporal.periodic_counts(d_bits, cands, d_ts, n_rows, end)
+                        == periodic.periodic_counts(bits, cands, ts, n_rows, end)), (n_rows, end, len(cands[0]))
 
 
 @pytest.mark.gpu
