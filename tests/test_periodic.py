@@ -543,3 +543,40 @@ def test_gpu_reference_kernel_agrees_with_fixtures(fixtures):
         for name, algo in (("cuPFEclat", "eclat"), ("cuPFApriori", "apriori")):
             found = ref_gpu.periodic_mine(baskets, timestamps.tolist(), end, count, limit, algo, kernels)
             assert [["\t".join(p), s, per] for p, s, per in found] == run[name], (case["name"], name)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_depth_first_and_level_orders_on_random_families(seed):
+    """For random downward-closed families of itemsets, the C ABI's
+    CPM_ORDER_DEPTH_FIRST / CPM_ORDER_APRIORI rebuild, from trees in a random
+    emission order, the insertion orders of the restated cuPFEclat /
+    cuPFApriori drivers run with 'is in the family' as their acceptance test."""
+    from itertools import combinations
+
+    from cupami_b200._native import Result
+    from oracle import periodic
+
+    rng = np.random.default_rng(seed)
+    n_items = int(rng.integers(4, 9))
+    labels = [f"L{i}" for i in range(n_items)]
+    # a random family closed under subsets: keep each itemset whose subsets are all kept, with probability p
+    family = set()
+    for width in range(1, n_items + 1):
+        for combo in combinations(range(n_items), width):
+            if all(sub in family for sub in combinations(combo, width - 1) if sub) and rng.random() < 0.7:
+                family.add(combo)
+    index = {label: i for i, label in enumerate(labels)}
+
+    def counts(cands):  # support 1 and periodicity 0 inside the family, support 0 outside
+        return [(1, 0) if tuple(sorted(c)) in family else (0, 0) for c in cands]
+
+    for order, driver in ((3, periodic.pf_eclat), (1, periodic.pf_apriori)):
+        want = [p for p, _, _ in driver(labels, None, None, 0, 1, 0, counts=counts)]
+        assert {tuple(index[x] for x in p) for p in want} == family
+        pats = [(tuple(index[x] for x in p), 1, 0) for p in want]
+        for prefix_tree in (False, True):
+            parent, item, support, period = _tree(pats, rng, prefix_tree)
+            res = Result.from_tree(parent, item, support, order, period=period)
+            o = res.offsets.tolist()
+            got = [tuple(labels[c] for c in res.items[o[k]:o[k + 1]].tolist()) for k in range(len(res))]
+            assert got == want, (seed, order, prefix_tree)
