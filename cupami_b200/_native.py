@@ -122,7 +122,7 @@ _SIGNATURES = {
     "cpm_periodic_counts": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, _P, _U64, ctypes.c_int64,
                                            _P, _P]),
     "cpm_mine_eclat_noalloc": (ctypes.c_int, [_P, _P, _U64, ctypes.c_uint32, _U64, ctypes.c_int64,
-                                              _P, _P, _P, _U64, ctypes.POINTER(_U64)]),
+                                              ctypes.POINTER(Opts), _P, _P, _P, _U64, ctypes.POINTER(_U64)]),
 }
 
 _lib = None

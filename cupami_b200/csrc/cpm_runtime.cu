@@ -2917,13 +2917,14 @@ struct NoallocCarve {
 };
 
 extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint64_t stride, uint32_t n_items,
-                                      uint64_t n_transactions, int64_t min_sup, uint32_t *d_parent,
-                                      uint32_t *d_item, uint32_t *d_support, uint64_t capacity,
-                                      uint64_t *n_patterns) {
+                                      uint64_t n_transactions, int64_t min_sup, const cpm_opts *opts,
+                                      uint32_t *d_parent, uint32_t *d_item, uint32_t *d_support,
+                                      uint64_t capacity, uint64_t *n_patterns) {
     if (!ctx || !n_patterns) return CPM_EINVAL;
     *n_patterns = 0;
     if ((n_items && !d_bits) || (capacity && (!d_parent || !d_item || !d_support)))
         return set_err(ctx, CPM_EINVAL, "null input or output pointer");
+    if (n_items == 0) return CPM_OK;  // an empty database has no patterns, as with cpm_mine
     if (stride < 2 || (stride & 1) || (reinterpret_cast<uintptr_t>(d_bits) & 15))
         return set_err(ctx, CPM_EINVAL, "tidset rows need an even stride and a 16-byte aligned base");
     if (n_transactions > stride * 64) return set_err(ctx, CPM_EINVAL, "stride too small for the transactions");
@@ -3064,7 +3065,8 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     P.queue = d_queue; P.queue_cap = queue_cap;
     P.arena = d_arena; P.arena_words = arena_slots * stride;
     P.pat_parent = d_parent; P.pat_item = d_item; P.pat_sup = d_support; P.pat_db = nullptr; P.pat_cap = capacity;
-    P.root_cost = d_root_cost; P.st = d_st; P.max_stride = stride; P.spin_limit = 1ull << 26;
+    P.root_cost = d_root_cost; P.st = d_st; P.max_stride = stride;
+    P.spin_limit = opts && opts->spin_limit ? opts->spin_limit : (1ull << 26);
     P.cta_time = nullptr;
     P.shallow = 0;
     P.lists = 0;
@@ -3076,7 +3078,8 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     const bool smem_prefix = prefix_bytes <= 200 * 1024;
     int per_sm = 1;
     if (smem_prefix) {
-        CK(cudaFuncSetAttribute(k_deep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)prefix_bytes));
+        // cpm_init already allows k_deep<true> 200 KB of dynamic shared memory;
+        // the attribute is process-wide, so it is not touched here.
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_deep<true>, 256, prefix_bytes));
     } else {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_deep<false>, 256, 0));
@@ -3088,7 +3091,9 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(&hs, d_st, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    if (hs.error & DEEP_ERR_SPIN) return set_err(ctx, CPM_ETIMEOUT, "deep-level kernel wait ran out of spins");
+    if (hs.error & DEEP_ERR_SPIN)
+        return set_err(ctx, CPM_ETIMEOUT, "deep-level kernel wait ran out of spins (limit %llu)",
+                       (unsigned long long)P.spin_limit);
     if (hs.error & DEEP_ERR_PATTERNS)
         return set_err(ctx, CPM_EOVERFLOW, "output capacity %llu is below the number of patterns",
                        (unsigned long long)capacity);

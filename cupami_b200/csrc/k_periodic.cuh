@@ -90,7 +90,7 @@ k_periodic(const Word *__restrict__ bits, uint64_t stride, const uint32_t *__res
     if (ok_flag && !ok_flag[c]) {
         if (parts == 1 && !lane) {
             support[c] = 0;
-            period[c] = end;
+            period[c] = max(0ll, end);
             if (pass) pass[c] = 0;
         }
         return;
@@ -202,7 +202,7 @@ __global__ void k_periodic_join(const PSeg *__restrict__ seg, uint32_t parts, co
     if (c >= n) return;
     if (ok_flag && !ok_flag[c]) {
         support[c] = 0;
-        period[c] = end;
+        period[c] = max(0ll, end);
         if (pass) pass[c] = 0;
         return;
     }

@@ -78,22 +78,18 @@ class cuApriori:
     _TIDSETS = 0
 
     def __init__(self, iFile, minSup, sep=None, use_gds="auto", use_gpu_io="auto"):
-        loading_start = time.perf_counter()
-        if use_gds not in ("auto", True, False):
-            raise ValueError('use_gds must be "auto", True, or False')
-        if use_gpu_io not in ("auto", True, False):
-            raise ValueError('use_gpu_io must be "auto", True, or False')
-        self.iFile = iFile
-        self.minSup = minSup
-        self.sep = sep
-        self.use_gds = use_gds
-        self.use_gpu_io = use_gpu_io
-        self._csr = None
+        t0 = time.perf_counter()
+        # The two switches accept the same three values as the reference, with its messages.
+        for flag, value in (("use_gds", use_gds), ("use_gpu_io", use_gpu_io)):
+            if value not in ("auto", True, False):
+                raise ValueError(f'{flag} must be "auto", True, or False')
+        self.iFile, self.minSup, self.sep = iFile, minSup, sep
+        self.use_gds, self.use_gpu_io = use_gds, use_gpu_io
+        self._csr = None               # (offsets, ids) when the input is numeric
         self._inputBackend = {"backend": "cpu", "reason": "Text or Parquet input"}
-        if use_gds is True and (not isinstance(iFile, (str, Path))
-                                or Path(iFile).suffix.lower() != ".bin"
-                                or urlparse(str(iFile)).scheme in ("http", "https")):
+        if use_gds is True and not self._isLocalBin(iFile):
             raise ValueError("Required GDS input currently supports local BIN files only")
+        # Numeric inputs set _csr and the transaction count and return None.
         self._Database = self._readTransactions(iFile)
         if self._Database is not None:
             self._transactionCount = len(self._Database)
@@ -101,9 +97,13 @@ class cuApriori:
         self._patterns = None          # cached dict built from the arrays
         self._result = None            # _native.Result of the latest mine()
         self._labels = []
-        self._startTime = 0.0
-        self._endTime = 0.0
-        self._loadingTime = time.perf_counter() - loading_start
+        self._startTime = self._endTime = 0.0
+        self._loadingTime = time.perf_counter() - t0
+
+    @staticmethod
+    def _isLocalBin(source):
+        return (isinstance(source, (str, Path)) and Path(source).suffix.lower() == ".bin"
+                and urlparse(str(source)).scheme not in ("http", "https"))
 
     # ---- input -----------------------------------------------------------
 
@@ -199,29 +199,21 @@ class cuApriori:
                             "arrow-cuda", "Parquet list arrays sent to the GPU; no Python transactions")
 
     def _readDelimitedFile(self, inputStream):
-        firstLine = inputStream.readline()
-        delimiter = self.sep
-        if delimiter is None:
-            delimiter = "\t" if "\t" in firstLine else ","
-        rows = csv.reader(chain((firstLine,), inputStream), delimiter=delimiter)
-        return self._cleanTransactions(rows)
+        """Rows of delimited text; with no ``sep`` the first line decides between
+        a tab (when it holds one) and a comma, as the reference does."""
+        head = inputStream.readline()
+        sep = self.sep if self.sep is not None else ("\t" if "\t" in head else ",")
+        return self._cleanTransactions(csv.reader(chain((head,), inputStream), delimiter=sep))
 
     def _cleanTransactions(self, rows):
-        transactions = []
-        for row in rows:
-            transaction = self._cleanTransaction(row)
-            if transaction:
-                transactions.append(transaction)
-        return transactions
+        """Cleaned baskets, empty ones left out."""
+        return [basket for basket in map(self._cleanTransaction, rows) if basket]
 
     @staticmethod
     def _cleanTransaction(transaction):
-        seen = {}
-        for value in transaction:
-            label = str(value).strip()
-            if label:
-                seen.setdefault(label, None)
-        return tuple(seen)
+        """Stripped, non-empty labels in first-seen order, each once."""
+        labels = (str(value).strip() for value in transaction)
+        return tuple(dict.fromkeys(label for label in labels if label))
 
     @staticmethod
     def _getSupportCount(minSup, transactionCount):
@@ -335,55 +327,66 @@ class cuApriori:
         return dict(self._result.stats) if self._result is not None else {}
 
     def getPatterns(self):
-        return {"\t".join(pattern): support for pattern, support in self._finalPatterns.items()}
+        """{tab-joined pattern: support} in the reference's insertion order."""
+        return dict(zip(map("\t".join, self._finalPatterns), self._finalPatterns.values()))
 
     def getPatternsAsDataFrame(self):
+        """The patterns of getPatterns() as a DataFrame with columns Patterns and Support."""
         import pandas as pd
 
-        rows = [("\t".join(pattern), support) for pattern, support in self._finalPatterns.items()]
-        return pd.DataFrame(rows, columns=["Patterns", "Support"])
+        found = self.getPatterns()
+        return pd.DataFrame({"Patterns": list(found), "Support": list(found.values())},
+                            columns=["Patterns", "Support"])
 
     def save(self, outputFile):
+        """One ``"<tab-joined pattern> : <support>"`` line per pattern, in sorted tuple order."""
+        lines = ("\t".join(p) + f" : {v}\n" for p, v in sorted(self._finalPatterns.items()))
         with Path(outputFile).open("w", encoding="utf-8") as file:
-            for pattern, support in sorted(self._finalPatterns.items()):
-                file.write(f"{chr(9).join(pattern)} : {support}\n")
+            file.writelines(lines)
 
     def getRuntime(self):
-        """Mining time in seconds, excluding constructor input loading."""
+        """Seconds the latest mine() took: upload, packing, mining and copy-back;
+        the constructor's reading of the input is not in it."""
         return self._endTime - self._startTime
 
     def getLoadingTime(self):
-        """Constructor input parsing/loading time."""
+        """Seconds the constructor spent reading and cleaning the input."""
         return self._loadingTime
 
     def getMiningTime(self):
-        """Time of the latest mine() call, including device packing."""
+        """Same as getRuntime()."""
         return self.getRuntime()
 
     def getTotalRuntime(self):
+        """Reading plus the latest mine()."""
         return self.getLoadingTime() + self.getMiningTime()
 
-    def getMemoryRSS(self):
+    @staticmethod
+    def _memory(kind):
+        """Resident ("rss") or unique ("uss") bytes of this process; 0 without psutil."""
         try:
             import psutil
         except ImportError:
             return 0
-        return int(psutil.Process().memory_info().rss)
+        proc = psutil.Process()
+        info = proc.memory_info() if kind == "rss" else proc.memory_full_info()
+        return int(getattr(info, kind))
+
+    def getMemoryRSS(self):
+        return self._memory("rss")
 
     def getMemoryUSS(self):
-        try:
-            import psutil
-        except ImportError:
-            return 0
-        return int(psutil.Process().memory_full_info().uss)
+        return self._memory("uss")
 
     def printResults(self):
-        print("Total number of Frequent Patterns:", len(self._finalPatterns))
-        print("Total Memory in USS:", self.getMemoryUSS())
-        print("Total Memory in RSS:", self.getMemoryRSS())
-        print("Loading time (seconds):", self.getLoadingTime())
-        print("Mining time (seconds):", self.getMiningTime())
-        print("Total time (seconds):", self.getTotalRuntime())
+        report = (("Total number of Frequent Patterns:", len(self._finalPatterns)),
+                  ("Total Memory in USS:", self.getMemoryUSS()),
+                  ("Total Memory in RSS:", self.getMemoryRSS()),
+                  ("Loading time (seconds):", self.getLoadingTime()),
+                  ("Mining time (seconds):", self.getMiningTime()),
+                  ("Total time (seconds):", self.getTotalRuntime()))
+        for caption, value in report:
+            print(caption, value)
 
 
 Apriori = cuApriori

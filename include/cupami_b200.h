@@ -292,14 +292,18 @@ int cpm_periodic_counts(cpm_ctx *ctx, const uint32_t *d_bitsets, uint64_t words3
  * the process exits.  Inputs needing more (a pair matrix or child tidsets that
  * do not fit) are rejected with CPM_EINVAL or CPM_EOVERFLOW and a message in
  * cpm_last_error.  The first call on each device looks up the array's device
- * address, so make that first call before any stream capture.  All calls share
- * the array, so calls that overlap on the GPU (two contexts, two threads) race
- * and must be serialised by the caller. */
+ * address, so make that first call before any stream capture; the address is
+ * kept for the life of the process and does not survive cudaDeviceReset (do
+ * not reset a device between calls).  All calls share the array, so calls that
+ * overlap on the GPU (two contexts, two threads) race and must be serialised
+ * by the caller.  `opts` may be null; only its spin_limit is read (the bounded
+ * wait of the deep-level work queue, CPM_ETIMEOUT when it runs out).  With
+ * n_items == 0 the call returns CPM_OK and no patterns. */
 #define CPM_NOALLOC_SCRATCH_BYTES (64ull << 20)
 int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint64_t stride, uint32_t n_items,
-                           uint64_t n_transactions, int64_t min_sup, uint32_t *d_parent,
-                           uint32_t *d_item, uint32_t *d_support, uint64_t capacity,
-                           uint64_t *n_patterns);
+                           uint64_t n_transactions, int64_t min_sup, const cpm_opts *opts,
+                           uint32_t *d_parent, uint32_t *d_item, uint32_t *d_support,
+                           uint64_t capacity, uint64_t *n_patterns);
 
 #ifdef __cplusplus
 }

@@ -12,6 +12,9 @@ Outputs go to ``oracle/_ref/`` only; that folder is git-ignored and ships with
 the built library.  Without the reference sources (as on a machine that only
 has the prebuilt files) it does nothing.
 
+The cuPAMI checkout is the argument, else ``$CUPAMI_REFERENCE``, else a
+directory named ``reference`` beside this repository's own directory.
+
     python oracle/build_ref.py [path/to/cupami]
 """
 
@@ -26,7 +29,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
 LIB = OUT / "libref_bitsets.so"
-DEFAULT_ROOT = Path("/root/reference")
+DEFAULT_ROOT = Path(os.environ.get("CUPAMI_REFERENCE", HERE.parent.parent / "reference"))
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 

@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures from the reference miners themselves.
 
-Run in a checkout that has the cuPAMI sources (default ``/root/reference``;
-override with ``CUPAMI_REFERENCE``).  The reference drivers ``cuEclat.mine``
+Run where the cuPAMI sources can be read: ``$CUPAMI_REFERENCE``, else a
+directory named ``reference`` beside this repository's own directory.  The reference drivers ``cuEclat.mine``
 and ``cuApriori.mine`` run unchanged; only their CUDA plumbing is replaced:
 
 * ``cuApriori._getCudaModule`` returns a NumPy namespace with the CuPy calls
@@ -26,7 +26,7 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("CUPAMI_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("CUPAMI_REFERENCE", HERE.parents[2] / "reference"))
 
 
 def numpy_cuda_namespace():

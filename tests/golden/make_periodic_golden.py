@@ -1,7 +1,7 @@
 """Regenerate ``periodic_patterns.json`` from the reference periodic miners.
 
-Run in a checkout that has the cuPAMI sources (default ``/root/reference``;
-override with ``CUPAMI_REFERENCE``).  ``cuPFEclat.mine`` and
+Run where the cuPAMI sources can be read: ``$CUPAMI_REFERENCE``, else a
+directory named ``reference`` beside this repository's own directory.  ``cuPFEclat.mine`` and
 ``cuPFApriori.mine`` (cupami/periodicFrequentPattern/cuPFEclat.py:146-175,
 cuPFApriori.py:141-157) and everything they call in ``TemporalInput`` run
 unchanged; only the CUDA plumbing is replaced:
