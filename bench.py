@@ -1,9 +1,11 @@
 """Benchmark: mine() seconds and bitset-AND GB/s on the B200 engine.
 
-Default workload: the planted-pattern database (100,000 transactions over
-1,000 items, 2,000 planted Zipf(1.1) patterns + Zipf(1.1) noise, mean length
-10, seed 7) mined at minSup 0.005 by cuEclat and cuApriori; one step mines it
-with both.  ``--workload`` selects another synthetic database.
+Default workload: the large sparse database (1,000,000 transactions over
+20,000 items, Poisson(40) lengths, Zipf(1.0) items, seed 3) mined by cuEclat
+at minSup 0.001 (6,280,597 patterns); one step mines it once.  The
+planted-pattern database (100,000 x 1,000, cuEclat + cuApriori) and the 512
+batched databases are measured after it and reported under ``others``.
+``--workload`` selects another synthetic database as the headline.
 
 * ``value``: seconds per step with the transaction tidsets already resident in
   HBM (cpm_mine on a loaded database), timed with CUDA events on the library's
@@ -14,7 +16,10 @@ with both.  ``--workload`` selects another synthetic database.
   of the patterns (the reference's own ``getMiningTime()`` definition).
 * ``roofline``: the dominant kernel of the step against MEASURED_PEAKS.json.
 * ``cpu_baseline``: the reference's host path (NumPy in place of CuPy,
-  ``oracle.numpy_port``) on one core, one full step.
+  ``oracle.numpy_port``) on one core: one full step where that takes seconds;
+  on the 1M x 20k workload (hours on one core) an estimate from timed samples
+  of every operation the reference's driver runs, times the exact number of
+  times it runs them (``estimate_reference_cpu``).
 
 ``--impl reference`` times that host path alone on this box's cores.
 Multi-GPU runs (torchrun) give every rank its own database of the same shape
@@ -105,6 +110,19 @@ def dist_setup():
     return world, rank, local
 
 
+# Exact counts of the reference driver's operations on a workload's answer
+# (frames, positions, intersections, copied rows), from the oracle's summary.
+SEARCH_COUNTS = {"sparse-zipf-1m": ROOT / "tests" / "golden" / "sparse_zipf_1m_summary.json"}
+
+
+def search_counts(workload):
+    p = SEARCH_COUNTS.get(workload)
+    if p is None or not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    return (d["reference_search"], d["patterns"]) if "reference_search" in d else None
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -154,14 +172,15 @@ class ClockSampler:
 
 
 def deep_traffic(workload, tidsets, arena_mb):
-    """DRAM bytes of one k_deep launch of this workload, from a committed ncu capture (None if none)."""
+    """The committed ncu record of one k_deep launch of this workload (DRAM
+    bytes per launch, L2 throughput), or None if there is none."""
     p = ROOT / "profiles" / "k_deep_traffic.json"
     if not p.exists() or arena_mb:
         return None
     d = json.loads(p.read_text()).get(workload)
     if not d or d.get("tidsets", 0) != tidsets:
         return None
-    return d["dram_bytes_per_launch"]
+    return d
 
 
 def flush_l2(buf):
@@ -219,6 +238,113 @@ def cpu_step_seconds(csr, minsup, algos, budget_s=30.0):
         _port_step(csr, minsup, algos)
         times.append(time.perf_counter() - t0)
     return statistics.median(times), f"whole step, median of {len(times)}"
+
+
+class ReferenceCpuModel:
+    """Seconds the reference's Eclat driver takes on one core with NumPy kernels
+    (``oracle.numpy_port``), for a database too large to mine that way in a
+    benchmark: the label mapping, packing and singleton counts run in full;
+    every other operation of the driver (cuEclat.py:168-245) is timed on
+    samples of the real tidsets and multiplied by how often the driver runs it
+    on this database (``counts``: pair candidates, top-level class members,
+    positions, intersected rows, copied child rows, patterns).
+
+    The model is per operation, not per pattern: ``count_supports`` of a pair
+    (two gathered rows, AND, popcount), ``intersect_extensions`` per call and per
+    row, ``take`` per copied row, the top-level vertical gather per member, and
+    one dict insertion per pattern.  NumPy's costs here do not depend on the
+    bits' values, only on the row width, which is the same for every tidset
+    (the reference keeps every tidset as a full-width bitset)."""
+
+    def __init__(self, csr, counts, patterns):
+        from oracle import numpy_port
+
+        self.np = numpy_port
+        self.counts, self.patterns = counts, patterns
+        t0 = time.perf_counter()
+        labels, rows, cols, n_tx = numpy_port.device_pairs_from_csr(csr.offsets, csr.items)
+        self.bits = numpy_port.pack(rows, cols, n_tx, len(labels))
+        sup = numpy_port.supports_of(self.bits, [[i] for i in range(len(labels))])
+        self.fixed_s = time.perf_counter() - t0
+        self.n_tx = n_tx
+        self.frequent = np.array([i for i, v in enumerate(sup) if v >= 1], dtype=np.int64)
+
+    @staticmethod
+    def _slope(fn, sizes, reps=2):
+        """(per-call, per-unit) seconds from the best of ``reps`` timings at each size (least squares)."""
+        xs, ys = [], []
+        for n in sizes:
+            best = min(fn(n) for _ in range(reps))
+            xs.append(n)
+            ys.append(best)
+        b, a = np.polyfit(np.asarray(xs, float), np.asarray(ys, float), 1)
+        return max(a, 0.0), max(b, 0.0)
+
+    def sample(self, seed):
+        """One estimate (seconds) from a fresh sample; returns (seconds, detail)."""
+        rng = np.random.default_rng(seed)
+        k, bits, fr = self.np, self.bits, self.frequent
+        pick = lambda n: fr[rng.integers(0, fr.size, n)]
+
+        def t_pairs(n):
+            batch = np.stack([pick(n), pick(n)], axis=1).tolist()
+            t0 = time.perf_counter()
+            k.supports_of(bits, batch)
+            return time.perf_counter() - t0
+
+        def t_vertical(n):
+            members, left = pick(n), int(pick(1)[0])
+            t0 = time.perf_counter()
+            k.NUMPY.vertical(bits, members, left)
+            return time.perf_counter() - t0
+
+        rows = bits[pick(513)]
+
+        def t_frame(m):
+            # The driver's own search loop over one frame of m members whose
+            # children all fail: m - 1 positions, m(m - 1)/2 intersected rows.
+            t0 = time.perf_counter()
+            k._search({}, ("p",), [str(i) for i in range(m)], rows[:m], self.n_tx + 1)
+            return time.perf_counter() - t0
+
+        child = rows[1:]
+
+        def t_take(n):
+            keep = sorted(rng.choice(child.shape[0], n, replace=False).tolist())
+            t0 = time.perf_counter()
+            k.NUMPY.take(child, keep)
+            return time.perf_counter() - t0
+
+        names = [str(i) for i in range(1024)]
+        big = {(names[i & 1023], names[i >> 10], "x"): i for i in range(1 << 20)}  # a dict of realistic size
+
+        def t_dict(n):
+            head = ("a", "b")
+            t0 = time.perf_counter()
+            for i in range(n):
+                big[head + (names[i & 1023], names[(i >> 10) & 1023])] = int(i)
+            return time.perf_counter() - t0
+
+        c = self.counts
+        # Pair batches large enough that the gathered rows (two per pair) leave
+        # the caches, as the driver's 65,536-pair batches do: up to 1 GB each.
+        width = bits.shape[1] * 4
+        top = int(min(c["pair_candidates"], max(256, (1 << 30) // width)))
+        _, pair = self._slope(t_pairs, sorted({max(1, top // 4), max(1, top // 2), top}))
+        _, vert = self._slope(t_vertical, (64, 128, 256))
+        ms = (2, 4, 16, 64)
+        tf = [min(t_frame(m) for _ in range(2)) for m in ms]
+        (call, row), *_ = np.linalg.lstsq(np.array([[m - 1, m * (m - 1) / 2] for m in ms], float),
+                                          np.array(tf), rcond=None)
+        call, row = max(float(call), 0.0), max(float(row), 0.0)
+        _, take = self._slope(t_take, (8, 64, 256))
+        _, ins = self._slope(t_dict, (20_000, 100_000))
+        positions = c["top_positions"] + c["deep_positions"]
+        intersections = c["top_intersections"] + c["deep_intersections"]
+        parts = {"fixed": self.fixed_s, "pairs": pair * c["pair_candidates"], "vertical": vert * c["top_members"],
+                 "intersect_calls": call * positions, "intersect_rows": row * intersections,
+                 "take": take * c["copied_children"], "dict": ins * self.patterns}
+        return sum(parts.values()), parts
 
 
 def reference_gpu_seconds(csr, minsup, algos, ours, device, budget_s=60.0):
@@ -284,9 +410,20 @@ def run_reference(args, world, rank):
         return
     csr, minsup, algos, seed = make_workload(args.workload, 0)
     budget = 20.0 if isinstance(csr, list) else 60.0
-    times, sample = [], ""
+    times, sample, estimated = [], "", False
+    counts = search_counts(args.workload)
+    model = ReferenceCpuModel(csr, *counts) if counts and algos == ("eclat",) else None
     for i in range(args.warmup + args.steps):
-        v, sample = cpu_step_seconds(csr, minsup, algos, budget_s=budget if isinstance(csr, list) else 0.0)
+        if model is not None:
+            v, parts = model.sample(seed=i)
+            sample = ("estimate: label mapping, packing and singletons run in full (%.1f s); pair counts, "
+                      "vertical gathers, intersect calls and rows, child copies and dict inserts timed on "
+                      "samples of the real tidsets and scaled by the driver's exact operation counts on this "
+                      "database; last step's parts (s): %s" % (model.fixed_s, json.dumps(
+                          {key: round(val, 1) for key, val in parts.items()})))
+            estimated = True
+        else:
+            v, sample = cpu_step_seconds(csr, minsup, algos, budget_s=budget if isinstance(csr, list) else 0.0)
         if i >= args.warmup:
             times.append(v)
     v = statistics.mean(times)
@@ -296,7 +433,7 @@ def run_reference(args, world, rank):
         "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "u64", "data": "synthetic",
         "config": {"workload": args.workload, "seed": seed, "minSup": minsup, "algorithms": list(algos)},
-        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "port",
+        "cpu_baseline": {"value": v, "unit": "s", "cores": 1, "kind": "port", "estimated": estimated,
                          "sample": f"{sample} (NumPy restatement of the reference host path)"},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -524,17 +661,172 @@ def run_periodic(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def device_options(sched, args):
+    from cupami_b200 import _native
+
+    o = _native.Opts()
+    _native.library().cpm_default_opts(o)
+    o.scheduler = _native.CPM_SCHED_LEARNED if sched == "learned" else _native.CPM_SCHED_PLAIN
+    o.arena_bytes = args.arena_mb << 20
+    o.tidsets = args.tidsets
+    return o
+
+
+def deep_bound(traffic, alg_bytes):
+    """What serves the deep kernel's bytes: DRAM when ncu saw at least half of
+    the algorithmic bytes there, else the L2 (the working set stays on chip)."""
+    if traffic is None or not alg_bytes:
+        return "unmeasured"
+    return "hbm" if traffic >= 0.5 * alg_bytes else "l2"
+
+
+class Workload:
+    """One synthetic database (or batch of databases) loaded on the device,
+    with the device step, the public-API step and their timings."""
+
+    def __init__(self, name, rank, local, args):
+        import cupami_b200
+        from cupami_b200 import _native
+
+        self.name, self.args, self.local = name, args, local
+        self.csr, self.minsup, self.algos, self.seed = make_workload(name, rank)
+        self.batched = isinstance(self.csr, list)
+        self.csrs = self.csr if self.batched else [self.csr]
+        self.n_tx = n_transactions(self.csr)
+        # The first public-API mine() of the process: library load, context,
+        # module loading and allocator warm-up, then the step itself.
+        self.first_call_s, _ = self.api_step(args.scheduler, materialise=False)
+        self.ctx = _native.context(local)
+        self.dbs = [_native.Database.from_ids(self.ctx, c.offsets, c.items) for c in self.csrs]
+        self.ms_counts = [cupami_b200.cuApriori._getSupportCount(self.minsup, n_transactions(c)) for c in self.csrs]
+
+    def close(self):
+        for db in self.dbs:
+            db.close()
+        self.dbs = []
+
+    def device_step(self, sched):
+        """[(algorithm, stats, results)] of one step with resident tidsets."""
+        from cupami_b200 import _native
+
+        codes = {"eclat": (_native.CPM_ECLAT, _native.CPM_ORDER_ECLAT),
+                 "apriori": (_native.CPM_APRIORI, _native.CPM_ORDER_APRIORI)}
+        out = []
+        for a in self.algos:
+            if a == "eclat-batch":
+                res = _native.mine_batch(self.ctx, self.dbs, self.ms_counts, device_options(sched, self.args))
+                out.append((a, res[0].stats, res))
+            else:
+                code, order = codes[a]
+                res = self.dbs[0].mine(self.ms_counts[0], code, device_options(sched, self.args), order)
+                out.append((a, res.stats, [res]))
+        return out
+
+    def api_step(self, sched, materialise):
+        """(seconds, d2h bytes) of one step through the public Python API from
+        host arrays; with ``materialise`` the seconds also cover building the
+        pattern dict of every miner (what the reference's mine() builds)."""
+        import cupami_b200
+
+        t, d2h = 0.0, 0
+        for a in self.algos:
+            if a == "eclat-batch":
+                t0 = time.perf_counter()
+                miners = cupami_b200.cuEclat.mineBatch(self.csrs, self.minsup)
+                if materialise:
+                    for m in miners:
+                        m.getPatterns()
+                t += time.perf_counter() - t0
+                for m in miners:
+                    off, it, sup, _ = m.getPatternArrays()
+                    d2h += it.nbytes + sup.nbytes // 2 * 3
+            else:
+                m = (cupami_b200.cuEclat if a == "eclat" else cupami_b200.cuApriori)(self.csr, self.minsup)
+                m.scheduler = sched
+                m.mine()
+                t += m.getMiningTime()
+                if materialise:
+                    t0 = time.perf_counter()
+                    m.getPatterns()
+                    t += time.perf_counter() - t0
+                off, it, sup, _ = m.getPatternArrays()
+                d2h += it.nbytes + sup.nbytes // 2 * 3
+        return t, d2h
+
+    def h2d_bytes(self):
+        return sum(int(c.offsets.nbytes + c.items.nbytes) for c in self.csrs) * len(self.algos)
+
+
+def timed_device(w, sched, steps, warmup, flush, barrier):
+    for _ in range(warmup):
+        w.device_step(sched)
+    barrier()
+    ms, kst, launches, last = [], [], 0, None
+    for _ in range(steps):
+        flush_l2(flush)
+        torch_sync()
+        out = w.device_step(sched)
+        ms.append(sum(st["ms_total"] for _, st, _ in out))
+        kst.append(out)
+        launches += sum(int(st["kernel_launches"]) for _, st, _ in out)
+        last = out
+    barrier()
+    return ms, kst, launches, last
+
+
+def timed_api(w, sched, steps, warmup, flush, barrier, materialise=False):
+    for _ in range(warmup):
+        w.api_step(sched, materialise)
+    barrier()
+    e2e, d2h = [], 0
+    for _ in range(steps):
+        flush_l2(flush)
+        torch_sync()
+        t, d2h = w.api_step(sched, materialise)
+        e2e.append(t)
+    barrier()
+    return e2e, d2h
+
+
+def torch_sync():
+    import torch
+
+    torch.cuda.synchronize()
+
+
+def other_workload(name, args, local, flush, steps=5, warmup=3):
+    """value and e2e of a secondary workload (single rank), same definitions as the headline."""
+    w = Workload(name, 0, local, args)
+    try:
+        ms, kst, launches, last = timed_device(w, args.scheduler, steps, warmup, flush, torch_sync)
+        e2e, _ = timed_api(w, args.scheduler, steps, 1, flush, torch_sync)
+        deep_ms = statistics.mean(sum(st["ms_deep"] for a, st, _ in out if a != "apriori") for out in kst)
+        deep_bytes = statistics.mean(sum(st["bytes_alg"] for a, st, _ in out if a != "apriori") for out in kst)
+        return {"value": statistics.mean(ms) / 1e3, "unit": "s", "e2e": statistics.mean(e2e),
+                "first_call_s": w.first_call_s, "steps": steps, "seed": w.seed, "minSup": w.minsup,
+                "algorithms": list(w.algos), "databases": len(w.csrs), "transactions": w.n_tx,
+                "patterns": [int(st["n_patterns"]) for _, st, _ in last],
+                "deep_ms": deep_ms, "deep_alg_gbs": deep_bytes / (deep_ms * 1e-3) / 1e9 if deep_ms else None,
+                "apriori_ms": statistics.mean(sum(st["ms_total"] for a, st, _ in out if a == "apriori")
+                                              for out in kst) if "apriori" in w.algos else None}
+    finally:
+        w.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="planted-100k", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="sparse-zipf-1m", choices=sorted(WORKLOADS))
     ap.add_argument("--scheduler", default="plain", choices=["plain", "learned"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-ab", action="store_true", help="skip the learned-vs-plain scheduler comparison")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference-GPU-path leg")
+    ap.add_argument("--no-others", action="store_true", help="skip the secondary workloads")
+    ap.add_argument("--others", default="planted-100k,batched-zipf-512",
+                    help="secondary workloads measured after the headline (comma separated)")
     ap.add_argument("--arena-mb", type=int, default=0,
                     help="deep-level arena size (memory-bounded rounds past it); 0 = automatic")
     ap.add_argument("--tidsets", type=int, default=0, choices=[0, 1, 2],
@@ -546,7 +838,10 @@ def main():
         return (run_periodic_reference if args.impl == "reference" else run_periodic)(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    run_ours(args, world, rank, local)
 
+
+def run_ours(args, world, rank, local):
     import torch
 
     torch.cuda.set_device(local)
@@ -556,75 +851,28 @@ def main():
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
         pg = dist
-    import cupami_b200
     from cupami_b200 import _native, costmodel
 
-    csr, minsup, algos, seed = make_workload(args.workload, rank)
-    batched = isinstance(csr, list)
-    csrs = csr if batched else [csr]
-    n_tx = n_transactions(csr)
-    ctx = _native.context(local)
-    have_model = costmodel.ensure_default(ctx)
-    dbs = [_native.Database.from_ids(ctx, c.offsets, c.items) for c in csrs]
-    ms_counts = [cupami_b200.cuApriori._getSupportCount(minsup, n_transactions(c)) for c in csrs]
-
-    def options(sched):
-        o = _native.Opts()
-        _native.library().cpm_default_opts(o)
-        o.scheduler = _native.CPM_SCHED_LEARNED if sched == "learned" else _native.CPM_SCHED_PLAIN
-        o.arena_bytes = args.arena_mb << 20
-        o.tidsets = args.tidsets
-        return o
-
-    algo_code = {"eclat": (_native.CPM_ECLAT, _native.CPM_ORDER_ECLAT),
-                 "apriori": (_native.CPM_APRIORI, _native.CPM_ORDER_APRIORI)}
+    w = Workload(args.workload, rank, local, args)
+    have_model = costmodel.ensure_default(w.ctx)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
-
-    def device_step(sched):
-        """[(algorithm, stats, results)] of one step with resident tidsets."""
-        out = []
-        for a in algos:
-            if a == "eclat-batch":
-                res = _native.mine_batch(ctx, dbs, ms_counts, options(sched))
-                out.append((a, res[0].stats, res))
-            else:
-                code, order = algo_code[a]
-                res = dbs[0].mine(ms_counts[0], code, options(sched), order)
-                out.append((a, res.stats, [res]))
-        return out
 
     def barrier():
         torch.cuda.synchronize()
         if pg:
             pg.barrier()
 
-    def timed(sched, steps):
-        for _ in range(args.warmup):
-            device_step(sched)
-        barrier()
-        ms, kst, launches, last = [], [], 0, None
-        for _ in range(steps):
-            flush_l2(flush)
-            torch.cuda.synchronize()
-            out = device_step(sched)
-            ms.append(sum(st["ms_total"] for _, st, _ in out))
-            kst.append(out)
-            launches += sum(int(st["kernel_launches"]) for _, st, _ in out)
-            last = out
-        barrier()
-        return ms, kst, launches, last
-
     sampler = ClockSampler(local)
-    step_ms, per_kernel, launches, last = timed(args.scheduler, args.steps)
+    step_ms, per_kernel, launches, last = timed_device(w, args.scheduler, args.steps, args.warmup, flush, barrier)
     clocks = sampler.stop()
     # Scheduler A/B on the same resident data (Eclat deep phase only).
     ab = None
-    if not args.no_ab and have_model and any(a != "apriori" for a in algos):
+    if not args.no_ab and have_model and any(a != "apriori" for a in w.algos):
         other = "learned" if args.scheduler == "plain" else "plain"
-        o_ms, o_kst, _, o_last = timed(other, args.steps)
+        o_ms, o_kst, _, o_last = timed_device(w, other, args.steps, args.warmup, flush, barrier)
         deep = lambda kst: statistics.mean(sum(st["ms_deep"] for a, st, _ in out if a != "apriori") for out in kst)
         same = all(np.array_equal(r1.supports, r2.supports) and np.array_equal(r1.items, r2.items)
                    for (_, _, a1), (_, _, a2) in zip(last, o_last) for r1, r2 in zip(a1, a2))
@@ -634,39 +882,15 @@ def main():
               "speedup_step": times["plain"][0] / times["learned"][0],
               "speedup_deep": times["plain"][1] / times["learned"][1] if times["learned"][1] else None,
               "identical_output": bool(same)}
-    # e2e through the public API from host arrays.
-    def api_step():
-        t, d2h = 0.0, 0
-        for a in algos:
-            if a == "eclat-batch":
-                miners = cupami_b200.cuEclat.mineBatch(csrs, minsup)
-                t += miners[0].getMiningTime()
-                for m in miners:
-                    off, it, sup, _ = m.getPatternArrays()
-                    d2h += it.nbytes + sup.nbytes // 2 * 3
-            else:
-                m = (cupami_b200.cuEclat if a == "eclat" else cupami_b200.cuApriori)(csr, minsup)
-                m.scheduler = args.scheduler
-                m.mine()
-                t += m.getMiningTime()
-                off, it, sup, _ = m.getPatternArrays()
-                d2h += it.nbytes + sup.nbytes // 2 * 3
-        return t, d2h
-
-    for _ in range(args.warmup):
-        api_step()
-    barrier()
-    e2e, d2h = [], 0
-    for _ in range(args.steps):
-        flush_l2(flush)
-        torch.cuda.synchronize()
-        t, d2h = api_step()
-        e2e.append(t)
-    barrier()
+    # e2e through the public API from host arrays: arrays only (the headline),
+    # then with the pattern dict built as the reference's mine() does.
+    e2e, d2h = timed_api(w, args.scheduler, args.steps, args.warmup, flush, barrier)
+    e2e_dict, _ = timed_api(w, args.scheduler, max(1, min(3, args.steps)), 0, flush, barrier, materialise=True)
     value = statistics.mean(step_ms) / 1e3
     e2e_v = statistics.mean(e2e)
+    e2e_dict_v = statistics.mean(e2e_dict)
     if pg:
-        value, e2e_v = max_over_ranks([value, e2e_v], "cuda")
+        value, e2e_v, e2e_dict_v = max_over_ranks([value, e2e_v, e2e_dict_v], "cuda")
         # The last collective: rank 0's baselines below run on its own, so no
         # rank waits on a barrier while they do.
         pg.destroy_process_group()
@@ -679,13 +903,19 @@ def main():
         deep_ms = statistics.mean(sum(s["ms_deep"] for s in st) for st in eclat_stats)
         deep_bytes = statistics.mean(sum(s["bytes_alg"] for s in st) for st in eclat_stats)
         achieved = deep_bytes / (deep_ms * 1e-3) / 1e9 if deep_ms else 0.0
-        traffic = deep_traffic(args.workload, args.tidsets, args.arena_mb)
-        roof = {"kernel": "k_deep (deep-level AND+popcount, persistent)", "bound": "hbm", "achieved": achieved,
-                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_source": src,
-                "traffic_source": "profiles/k_deep_traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                  "of one launch)" if traffic is not None else None,
+        tr = deep_traffic(args.workload, args.tidsets, args.arena_mb)
+        traffic = tr["dram_bytes_per_launch"] if tr else None
+        roof = {"kernel": "k_deep (deep-level AND+popcount, persistent)", "bound": deep_bound(traffic, deep_bytes),
+                "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                "peak_source": src, "frac_of": "HBM copy bandwidth (" + src + "); algorithmic bytes / kernel time",
+                "frac_of_8tbs_spec": achieved / 8000.0,
+                "dram_share_of_alg_bytes": traffic / deep_bytes if traffic and deep_bytes else None,
+                "l2_throughput_pct": tr.get("l2_throughput_pct") if tr else None,
+                "traffic_source": ("profiles/k_deep_traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                   "of one launch): " + tr["profile"]) if tr else None,
                 "ms_per_launch": deep_ms, "alg_bytes_per_launch": deep_bytes,
-                "alg_bytes": "sum over units of 8*W*(1 + siblings + children written)"}
+                "alg_bytes": "sum over units of the prefix, every sibling and every child written, each at its "
+                             "own form's size (bitset 8*W, list 16 + 4*ids)"}
     pair_ms = statistics.mean(sum(st["ms_pairs"] for _, st, _ in out) for out in per_kernel)
     pair_ops = statistics.mean(sum(st["pair_ops"] for _, st, _ in out) for out in per_kernel)
     int8_peak = int8_peak_tops()
@@ -696,30 +926,51 @@ def main():
             "frac": gram_tops / int8_peak if int8_peak else None,
             "ops": "2*128*256*K per issued tile (full tiles of the upper triangle)"}
     if rank != 0:
+        w.close()
         return
     ref_gpu_leg = None
     if not args.no_ref_gpu:
         ours = [[r.patterns(db.labels) for r in res] for db, res in
-                zip(dbs, zip(*[res for _, _, res in last]))]
-        ref_gpu_leg = reference_gpu_seconds(csr, minsup, algos, ours, local)
+                zip(w.dbs, zip(*[res for _, _, res in last]))]
+        ref_gpu_leg = reference_gpu_seconds(w.csr, w.minsup, w.algos, ours, local)
+        del ours
+    last_stats = [st for _, st, _ in last]
+    w.close()
     cpu = None
     if not args.no_cpu_baseline:
-        v, sample = cpu_step_seconds(csr, minsup, algos)
-        cpu = {"value": v, "unit": "s", "cores": 1, "kind": "port",
-               "sample": f"{sample} (NumPy restatement of the reference host path)"}
-    h2d = sum(int(c.offsets.nbytes + c.items.nbytes) for c in csrs) * len(algos)
-    last_stats = [st for _, st, _ in last]
+        counts = search_counts(args.workload)
+        if counts and w.algos == ("eclat",):
+            model = ReferenceCpuModel(w.csr, *counts)
+            v, parts = model.sample(seed=0)
+            cpu = {"value": v, "unit": "s", "cores": 1, "kind": "port", "estimated": True,
+                   "sample": "estimate of the NumPy restatement of the reference host path: label mapping, "
+                             "packing and singletons run in full; every other driver operation timed on samples "
+                             "of the real tidsets and scaled by its exact count on this database",
+                   "parts_s": {k: round(x, 2) for k, x in parts.items()}}
+        else:
+            v, sample = cpu_step_seconds(w.csr, w.minsup, w.algos)
+            cpu = {"value": v, "unit": "s", "cores": 1, "kind": "port", "estimated": False,
+                   "sample": f"{sample} (NumPy restatement of the reference host path)"}
+    others = None
+    if not args.no_others and world == 1:
+        others = {}
+        for name in [x for x in args.others.split(",") if x and x != args.workload]:
+            others[name] = other_workload(name, args, local, flush)
     line = {
-        "metric": "mine() seconds per step (" + "+".join(algos) + ")",
+        "metric": "mine() seconds per step (" + "+".join(w.algos) + ")",
         "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": value / PUBLISHED[args.workload] if args.workload in PUBLISHED else None,
         "dtype": "u64", "data": "synthetic",
-        "config": {"workload": args.workload, "seed": seed, "minSup": minsup, "algorithms": list(algos),
-                   "databases": len(csrs), "transactions": n_tx, "scheduler": args.scheduler,
+        "config": {"workload": args.workload, "seed": w.seed, "minSup": w.minsup, "algorithms": list(w.algos),
+                   "databases": len(w.csrs), "transactions": w.n_tx, "scheduler": args.scheduler,
                    "l2": "256 MB buffer rewritten before every timed step",
                    "parallelism": f"replicas{world}" if world > 1 else "single"},
-        "e2e": {"value": e2e_v, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "e2e": {"value": e2e_v, "unit": "s", "h2d_bytes_per_step": w.h2d_bytes(), "d2h_bytes_per_step": d2h,
+                "with_pattern_dict_s": e2e_dict_v, "first_call_s": w.first_call_s,
+                "api": "cuEclat/cuApriori(TransactionCSR, minSup).mine() + getPatternArrays(); "
+                       "with_pattern_dict_s adds getPatterns() (the dict the reference's mine() builds); "
+                       "first_call_s is the process's first mine(), library and context set-up included"},
         "roofline": roof,
         "pair_gram": gram,
         "cpu_baseline": cpu,
@@ -729,6 +980,7 @@ def main():
         "clocks": clocks,
         "patterns": [int(st["n_patterns"]) for st in last_stats],
         "kernel_stats": last_stats,
+        "others": others,
     }
     print(json.dumps(line), flush=True)
 

@@ -1018,6 +1018,7 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
     P.pat_parent = b.pat_parent; P.pat_item = b.pat_item; P.pat_sup = b.pat_sup; P.pat_db = b.pat_db;
     P.pat_cap = b.pat_cap;
     P.root_cost = nullptr; P.st = b.st; P.max_stride = max_stride; P.spin_limit = spin; P.cta_time = nullptr;
+    P.unit_log = nullptr; P.unit_log_cap = 0;
     P.lists = lists;
     P.root_frames = 0; P.defer_words = 0; P.defer_members = 0; P.defer_frames = 0; P.defer_queue = 0;
     P.root_key = nullptr; P.top_frames = 0; P.keys_in_words = 0; P.admit_words = 0;
@@ -1592,6 +1593,15 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
             CK(cudaMemsetAsync(d_ct, 0, 16ull * grid, ctx->stream));
         }
         P.cta_time = d_ct;
+        // CPM_UNIT_LOG=<file>: write one record per deep-level unit (k_deep.cuh) there.
+        const char *log_path = getenv("CPM_UNIT_LOG");
+        P.unit_log = nullptr;
+        P.unit_log_cap = 0;
+        if (log_path) {
+            P.unit_log_cap = 8ull << 20;
+            CKR(ds.alloc(&P.unit_log, 1 + P.unit_log_cap * UNIT_LOG_WORDS));
+            CK(cudaMemsetAsync(P.unit_log, 0, 8, ctx->stream));
+        }
         P.shallow = 0;
         P.lists = use_lists ? list_div : 0u;
         // Root units claimed once the arena is three-quarters full are handed
@@ -1612,6 +1622,17 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         st.kernel_launches++;
         CK(cudaMemcpyAsync(&hs, b.st, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        if (P.unit_log) {
+            unsigned long long n_log = 0;
+            CK(cudaMemcpy(&n_log, P.unit_log, 8, cudaMemcpyDeviceToHost));
+            n_log = std::min<unsigned long long>(n_log, P.unit_log_cap);
+            std::vector<unsigned long long> rec(n_log * UNIT_LOG_WORDS);
+            CK(cudaMemcpy(rec.data(), P.unit_log + 1, rec.size() * 8, cudaMemcpyDeviceToHost));
+            if (FILE *f = fopen(log_path, "wb")) {
+                fwrite(rec.data(), 8, rec.size(), f);
+                fclose(f);
+            }
+        }
         if (timing) {
             std::vector<unsigned long long> ct(2ull * grid);
             CK(cudaMemcpy(ct.data(), d_ct, 16ull * grid, cudaMemcpyDeviceToHost));
@@ -1909,6 +1930,9 @@ static int level_join(cpm_ctx *ctx, LevelScratch &scratch, DevScope &lvl, const 
     return CPM_OK;
 }
 
+// Largest prefix k_count_grouped stages in shared memory.
+constexpr size_t APRIORI_GROUP_SMEM = 160 * 1024;
+
 static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &o, cpm_result *res) {
     cpm_stats &st = res->stats;
     DevScope ds(ctx);
@@ -1971,6 +1995,21 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
         LevelScratch scratch(ctx);
         uint64_t *d_tot = nullptr;
         CKR(ds.alloc(&d_tot, 1));
+        // Candidates sharing a left row share its prefix AND (k_count_grouped)
+        // when that prefix fits in shared memory; else every candidate ANDs
+        // all of its rows (k_count_pruned).
+        const size_t pre_bytes = db->stride * 8;
+        const bool grouped = pre_bytes <= APRIORI_GROUP_SMEM;
+        unsigned long long *d_bytes = nullptr;
+        CKR(ds.alloc(&d_bytes, 1));
+        CK(cudaMemsetAsync(d_bytes, 0, 8, ctx->stream));
+        int group_ctas = 1;
+        if (grouped) {
+            CK(cudaFuncSetAttribute(k_count_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)APRIORI_GROUP_SMEM));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&group_ctas, k_count_grouped, 256, pre_bytes));
+            group_ctas = std::max(1, group_ctas);
+        }
         while (n_ub >= 2) {
             if (k + 1 > 64) {
                 dfree(ctx, L);
@@ -1989,13 +2028,23 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
             CKR(scratch.get(8, &sup, n_pairs));
             CKR(scratch.get(9, &pass, n_pairs));
             CKR(scratch.get(10, &pos, n_pairs));
-            k_count_pruned<<<(unsigned)((n_pairs * 32 + 255) / 256), 256, 0, ctx->stream>>>(
-                db->d_bits, db->stride, cand, okf, n_pairs, w, ms, sup, pass);
+            if (grouped) {
+                uint64_t *poff = nullptr;
+                uint32_t *partners = nullptr;
+                CKR(scratch.get(2, &partners, n_ub));  // written by level_join
+                CKR(scratch.get(3, &poff, n_ub));
+                const uint64_t grid = std::min<uint64_t>(n_ub, (uint64_t)ctx->sms * group_ctas);
+                k_count_grouped<<<(unsigned)grid, 256, pre_bytes, ctx->stream>>>(
+                    db->d_bits, db->stride, L, d_cnt2, k, poff, partners, cand, okf, ms, sup, pass, d_bytes);
+            } else {
+                k_count_pruned<<<(unsigned)((n_pairs * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+                    db->d_bits, db->stride, cand, okf, n_pairs, w, ms, sup, pass);
+                st.bytes_alg += n_pairs * w * db->stride * 8;
+            }
             CK(cudaGetLastError());
             CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, nullptr, d_tot));
             st.kernel_launches += 3;
             st.intersections += n_pairs * (w - 1);
-            st.bytes_alg += n_pairs * w * db->stride * 8;
             // Survivors: at most n_pairs rows and patterns.
             uint32_t *L2 = nullptr, *pid2 = nullptr;
             CKR(patterns_reserve(ctx, pa, n_pat, pat_ub + n_pairs));
@@ -2016,9 +2065,12 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
             k = w;
         }
         uint64_t final_pat = 0;
+        unsigned long long grouped_bytes = 0;
         CK(cudaMemcpyAsync(&final_pat, d_cnt2 + 1, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(&grouped_bytes, d_bytes, 8, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
         n_pat = final_pat;
+        st.bytes_alg += grouped_bytes;
         dfree(ctx, L);
         dfree(ctx, pid);
     }
@@ -3068,6 +3120,7 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     P.root_cost = d_root_cost; P.st = d_st; P.max_stride = stride;
     P.spin_limit = opts && opts->spin_limit ? opts->spin_limit : (1ull << 26);
     P.cta_time = nullptr;
+    P.unit_log = nullptr; P.unit_log_cap = 0;
     P.shallow = 0;
     P.lists = 0;
     P.root_frames = 0; P.defer_words = 0; P.defer_members = 0; P.defer_frames = 0; P.defer_queue = 0;

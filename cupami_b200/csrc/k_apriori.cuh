@@ -128,6 +128,73 @@ __global__ void k_count_pruned(const uint64_t *__restrict__ bits, uint64_t strid
     }
 }
 
+// The same supports as k_count_pruned, with the prefix shared.  The
+// candidates joined on left row a of the level (t in [poff[a], poff[a] +
+// partners[a]), cand rows L[a] + one last item) share the k items of L[a], so
+// their complete intersection is (AND of the k rows of L[a]) AND (the last
+// item's row).  One CTA takes one left row at a time (grid stride): it stages
+// the prefix AND in shared memory once (stride words), then each warp streams
+// one candidate's last-item row against it, eight 16-byte loads in flight per
+// lane.  A group of p candidates reads k + p rows instead of (k + 1) p.
+// *bytes_alg gains the rows read.  Rows at or past *d_n have no partners.
+__global__ void __launch_bounds__(256) k_count_grouped(const uint64_t *__restrict__ bits, uint64_t stride,
+                                                       const uint32_t *__restrict__ L, const uint64_t *__restrict__ d_n,
+                                                       uint32_t k, const uint64_t *__restrict__ poff,
+                                                       const uint32_t *__restrict__ partners,
+                                                       const uint32_t *__restrict__ cand,
+                                                       const uint32_t *__restrict__ ok_flag, long long minsup,
+                                                       uint32_t *__restrict__ support, uint32_t *__restrict__ pass,
+                                                       unsigned long long *__restrict__ bytes_alg) {
+    extern __shared__ ulonglong2 s_pre[];
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint64_t n = *d_n, n2 = stride / 2;
+    const uint32_t w = k + 1;
+    unsigned long long rows_read = 0;
+    for (uint64_t a = blockIdx.x; a < n; a += gridDim.x) {
+        const uint32_t p = partners[a];
+        if (!p) continue;  // the same for every thread of the CTA
+        const uint32_t *ra = L + a * k;
+        for (uint64_t v = threadIdx.x; v < n2; v += blockDim.x) {
+            ulonglong2 acc = ld_stream(reinterpret_cast<const ulonglong2 *>(bits + (uint64_t)ra[0] * stride) + v);
+            for (uint32_t j = 1; j < k; ++j)
+                acc = and2(acc, ld_stream(reinterpret_cast<const ulonglong2 *>(bits + (uint64_t)ra[j] * stride) + v));
+            s_pre[v] = acc;
+        }
+        __syncthreads();
+        const uint64_t t0 = poff[a];
+        for (uint32_t j = wid; j < p; j += nw) {
+            const uint64_t t = t0 + j;
+            if (!ok_flag[t]) {
+                if (!lane) {
+                    support[t] = 0;
+                    pass[t] = 0;
+                }
+                continue;
+            }
+            const ulonglong2 *row = reinterpret_cast<const ulonglong2 *>(bits + (uint64_t)cand[t * w + k] * stride);
+            uint32_t s = 0;
+            uint64_t v = lane;
+            for (; v + 224 < n2; v += 256) {
+                ulonglong2 x[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) x[u] = ld_stream(row + v + 32 * u);
+#pragma unroll
+                for (int u = 0; u < 8; ++u) s += popc2(and2(x[u], s_pre[v + 32 * u]));
+            }
+            for (; v < n2; v += 32) s += popc2(and2(ld_stream(row + v), s_pre[v]));
+            s = warp_sum_u32(s);
+            if (!lane) {
+                support[t] = s;
+                pass[t] = (long long)s >= minsup ? 1u : 0u;
+                ++rows_read;  // the last item's row
+            }
+        }
+        if (!threadIdx.x) rows_read += k;  // the prefix rows
+        __syncthreads();
+    }
+    if (!lane && rows_read) atomicAdd(bytes_alg, rows_read * 8ull * stride);
+}
+
 // Survivors, in candidate order, become the next level and pattern records.
 __global__ void k_apriori_keep(const uint32_t *__restrict__ cand, const uint32_t *__restrict__ cand_left,
                                const uint32_t *__restrict__ sup, const uint32_t *__restrict__ flag,

@@ -108,7 +108,16 @@ struct DeepParams {
     const float *root_key;
     uint32_t top_frames, keys_in_words;
     unsigned long long admit_words;
+    // Diagnostics (null: off): per unit, UNIT_LOG_WORDS words -- claim,
+    // prefix-staged, pass-1-done and end times (globaltimer ns), CTA,
+    // siblings | survivors << 32, sibling bytes, largest sibling's bytes,
+    // prefix bytes | list prefix << 63 | top-level << 62.
+    // unit_log[0] counts the units logged; records start at unit_log + 1.
+    unsigned long long *unit_log;
+    unsigned long long unit_log_cap;
 };
+
+constexpr int UNIT_LOG_WORDS = 9;
 
 // Child tidset form: a list when it takes at most 1/P.lists of the dense
 // words (P.lists = 0: bitsets only).
@@ -251,7 +260,9 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     __shared__ unsigned long long s_bytes;
     __shared__ uint32_t s_nsurv;         // survivors counted in pass 1
     __shared__ uint32_t s_part[32];      // per-sibling sums when siblings are split over warps
+    __shared__ unsigned long long s_maxb;  // largest sibling's bytes (diagnostics only)
     uint32_t *const s_p32 = reinterpret_cast<uint32_t *>(s_prefix);
+    __shared__ unsigned long long lg[4];   // claim, staged, pass 1 done, prefix word (diagnostics only)
 
     const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     DeepState *st = P.st;
@@ -299,6 +310,10 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             continue;
         }
         if (threadIdx.x == 0 && P.cta_time) t_unit = global_ns();
+        if (threadIdx.x == 0 && P.unit_log) {
+            lg[0] = global_ns();
+            s_maxb = 0;
+        }
         const uint32_t fid = (uint32_t)(s_item >> 32), p = (uint32_t)s_item;
         const DFrame *fp = P.frames + fid;
         const ulonglong2 *mk = reinterpret_cast<const ulonglong2 *>(
@@ -344,6 +359,10 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             s_ok = ld_acquire_u32(&st->error) == 0;
         }
         __syncthreads();
+        if (threadIdx.x == 0 && P.unit_log) {
+            lg[1] = global_ns();
+            lg[3] = prefix_bytes | (SMEM_PREFIX && (praw & 1ull) ? 1ull << 63 : 0ull) | (mk ? 1ull << 62 : 0ull);
+        }
         const bool ok = s_ok != 0;
         const uint32_t parent_pat = __ldcg(P.mem_pat + mem_off + p);
         // ---- pass 1: supports of every later member ----
@@ -384,6 +403,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 s = warp_sum_u32(s);
                 if (lane == 0) {
                     atomicAdd(&s_bytes, (unsigned long long)b);
+                    if (P.unit_log) atomicMax(&s_maxb, (unsigned long long)b);
                     emit(q, s, sib_item, sraw);
                 }
             }
@@ -399,6 +419,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 if (lane == 0) {
                     atomicAdd(&s_part[q], s);
                     if (j == 0) atomicAdd(&s_bytes, (unsigned long long)b);
+                    if (j == 0 && P.unit_log) atomicMax(&s_maxb, (unsigned long long)b);
                 }
             }
             __syncthreads();
@@ -408,10 +429,21 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             }
         }
         __syncthreads();
+        if (threadIdx.x == 0 && P.unit_log) lg[2] = global_ns();
+        // Diagnostics record of this unit (thread 0, at its end).
+        auto log_unit = [&](uint32_t nsurv) {
+            const unsigned long long k = atomicAdd(P.unit_log, 1ull);
+            if (k >= P.unit_log_cap) return;
+            unsigned long long *r = P.unit_log + 1 + k * UNIT_LOG_WORDS;
+            r[0] = lg[0]; r[1] = lg[1]; r[2] = lg[2]; r[3] = global_ns(); r[4] = blockIdx.x;
+            r[5] = (unsigned long long)cnt | ((unsigned long long)nsurv << 32);
+            r[6] = s_bytes - (lg[3] & ((1ull << 62) - 1)); r[7] = s_maxb; r[8] = lg[3];
+        };
         if (s_nsurv < 2) {
             // No child frame (the common case): nothing to compact, write or
             // publish, so the unit ends here without further barriers.
             if (threadIdx.x == 0) {
+                if (P.unit_log) log_unit(s_nsurv);
                 c_inter += cnt;
                 c_bytes += s_bytes;
                 c_units += 1;
@@ -620,6 +652,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         }
         __syncthreads();
         if (threadIdx.x == 0) {
+            if (P.unit_log) log_unit(ns);
             c_inter += cnt;
             c_bytes += s_bytes + (s_grant ? 8ull * child_words : 0ull);
             c_units += 1;
