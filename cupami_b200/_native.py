@@ -58,7 +58,7 @@ class Opts(ctypes.Structure):
         ("arena_bytes", ctypes.c_uint64), ("spin_limit", ctypes.c_uint64),
         ("collect_trace", ctypes.c_int32), ("deep_block", ctypes.c_int32),
         ("deep_ctas_per_sm", ctypes.c_int32), ("autotune", ctypes.c_int32), ("tidsets", ctypes.c_int32),
-        ("list_div", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2),
+        ("list_div", ctypes.c_int32), ("deep_balance", ctypes.c_int32), ("reserved", ctypes.c_int32),
     ]
 
 
@@ -121,6 +121,10 @@ _SIGNATURES = {
     "cpm_result_from_tree_periodic": (ctypes.c_int, [_P, _P, _P, _P, _U64, ctypes.POINTER(_P)]),
     "cpm_periodic_counts": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, _P, _U64, ctypes.c_int64,
                                            _P, _P]),
+    "cpm_parse_int_text": (ctypes.c_int, [_P, _P, _U64, ctypes.c_int32, ctypes.POINTER(_P)]),
+    "cpm_csr_size": (ctypes.c_int, [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
+    "cpm_csr_copy": (ctypes.c_int, [_P, _P, _P]),
+    "cpm_csr_free": (None, [_P]),
     "cpm_mine_eclat_noalloc": (ctypes.c_int, [_P, _P, _U64, ctypes.c_uint32, _U64, ctypes.c_int64,
                                               ctypes.POINTER(Opts), _P, _P, _P, _U64, ctypes.POINTER(_U64)]),
 }
@@ -324,6 +328,26 @@ class Database:
             self.close()
         except Exception:
             pass
+
+
+def parse_int_text(ctx, data: bytes, sep: str):
+    """(offsets uint64[n+1], ids uint32[nnz]) of delimited integer baskets,
+    parsed on the device; raises NativeError (CPM_EINVAL) for any other layout."""
+    lib = library()
+    buf = np.frombuffer(data, dtype=np.uint8)
+    handle = _P()
+    with ctx.lock:
+        ctx.check(lib.cpm_parse_int_text(ctx.handle, buf.ctypes.data if buf.size else None, buf.size,
+                                         ord(sep), ctypes.byref(handle)))
+    try:
+        n, nnz = _U64(), _U64()
+        lib.cpm_csr_size(handle, ctypes.byref(n), ctypes.byref(nnz))
+        offsets = np.zeros(n.value + 1, dtype=np.uint64)
+        ids = np.zeros(max(1, nnz.value), dtype=np.uint32)
+        ctx.check(lib.cpm_csr_copy(handle, offsets.ctypes.data, ids.ctypes.data))
+        return offsets, ids[:nnz.value]
+    finally:
+        lib.cpm_csr_free(handle)
 
 
 def autotune(ctx, db, min_sup, opts=None):

@@ -15,6 +15,7 @@
 #include "k_periodic.cuh"
 #include "k_costmodel.cuh"
 #include "k_units.cuh"
+#include "k_text.cuh"
 #include <cub/device/device_radix_sort.cuh>
 
 #include <cub/device/device_scan.cuh>
@@ -57,6 +58,7 @@ struct cpm_ctx {
     unsigned deep_occ_block = 0;  // block size the occupancies above were taken for
     std::vector<float> model;  // cost-model parameters (empty: none loaded)
     float last_deep_ms = 0.f;  // deep-phase kernel time of the last bounded-round run
+    uint32_t deep_balance = 1;  // k_deep pass 1 of the current mine: 1 siblings split by size, 0 warp each
     int last_deep_block = 0, last_deep_ctas = 0;  // launch shape of the last deep phase
     size_t l2_bytes = 126ull << 20;               // device L2 size (cpm_init)
     void *pinned = nullptr;                       // host staging for uploads (stage_upload)
@@ -213,8 +215,8 @@ extern "C" int cpm_init(int device, cpm_ctx **out) {
     ctx->tc_ok = (major == 10 && minor == 0);
     size_t total = 0;
     cudaMemGetInfo(&ctx->mem_free, &total);
-    // The deep kernel stages prefixes of up to 200 KB in shared memory.
-    cudaFuncSetAttribute(k_deep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    // The deep kernel stages prefixes of up to DEEP_SMEM_PREFIX_MAX bytes in shared memory.
+    cudaFuncSetAttribute(k_deep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DEEP_SMEM_PREFIX_MAX);
     cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
     cudaGetLastError();
     *out = ctx;
@@ -1040,6 +1042,7 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
         s0.arena_next = persist_arena;
         CK(cudaMemcpyAsync(b.st, &s0, sizeof s0, cudaMemcpyHostToDevice, ctx->stream));
         P.shallow = shallow_mode;
+        P.balance = ctx->deep_balance;
         // Queue entries beyond the memset stay stale: bound the round's queue.
         P.queue_cap = std::min<uint64_t>(queue_cap, q.size() * 64 + (1u << 20));
         CK(cudaEventRecord(ctx->ev[2], ctx->stream));
@@ -1233,6 +1236,9 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         t_start = now;
     };
     DevScope ds(ctx);
+    if (o.deep_balance < 0 || o.deep_balance > 2)
+        return set_err(ctx, CPM_EINVAL, "deep_balance must be 0, 1 or 2 (got %d)", o.deep_balance);
+    ctx->deep_balance = o.deep_balance == 1 ? 0u : 1u;
     CK(cudaEventRecord(ctx->ev[0], ctx->stream));
     // ---- singletons ----
     std::vector<DbDesc> h(n_db);
@@ -1273,7 +1279,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     {
         uint64_t biggest = 0;
         for (uint32_t d = 0; d < n_db; ++d) biggest = std::max<uint64_t>(biggest, (uint64_t)F[d] * dbs[d]->stride * 8);
-        use_lists = o.tidsets != 1 && max_stride * 8 <= 200 * 1024 &&
+        use_lists = o.tidsets != 1 && max_stride * 8 <= DEEP_SMEM_PREFIX_MAX &&
                     (o.tidsets == 2 || biggest > (uint64_t)ctx->l2_bytes / 2);
     }
     // A tidset becomes a list when its list takes at most 1/list_div of its
@@ -1282,7 +1288,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     if (o.tidsets == 0 && !o.list_div && o.autotune) {
         const auto it = ctx->tune_lists.find(63 - __builtin_clzll(std::max<uint64_t>(1, max_stride)));
         if (it != ctx->tune_lists.end()) {
-            use_lists = it->second > 0 && max_stride * 8 <= 200 * 1024;
+            use_lists = it->second > 0 && max_stride * 8 <= DEEP_SMEM_PREFIX_MAX;
             if (it->second > 0) list_div = (uint32_t)it->second;
         }
     }
@@ -1465,7 +1471,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
                                                 n_db == 1 ? db0->hint_arena : 0}));
     const uint64_t spin = o.spin_limit ? o.spin_limit : (1ull << 26);
     const size_t prefix_bytes = max_stride * 8;
-    const bool smem_prefix = prefix_bytes <= 200 * 1024;
+    const bool smem_prefix = prefix_bytes <= DEEP_SMEM_PREFIX_MAX;
     // Long tidsets leave room for fewer CTAs per SM: give each 16 or 32 warps
     // so that enough loads stay in flight; short ones run up to four 8-warp
     // CTAs.  Measured (deep phase): 1,564-word tidsets (planted-100k) 0.25 ms
@@ -1603,6 +1609,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
             CK(cudaMemsetAsync(P.unit_log, 0, 8, ctx->stream));
         }
         P.shallow = 0;
+        P.balance = ctx->deep_balance;
         P.lists = use_lists ? list_div : 0u;
         // Root units claimed once the arena is three-quarters full are handed
         // back and finished in memory-bounded rounds after this launch.
@@ -2390,7 +2397,7 @@ extern "C" int cpm_autotune(cpm_ctx *ctx, cpm_db *db, int64_t min_sup, const cpm
     const int bucket = 63 - __builtin_clzll(std::max<uint64_t>(1, db->stride));
     ctx->tune[bucket] = {best_block, best_ctas};
     // Tidset forms at that shape: bitsets only, or lists below 1/1 .. 1/8 of the bitset.
-    if (db->stride * 8 <= 200 * 1024) {
+    if (db->stride * 8 <= DEEP_SMEM_PREFIX_MAX) {
         o.deep_block = best_block;
         o.deep_ctas_per_sm = best_ctas;
         int best_div = -1;
@@ -3122,16 +3129,17 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     P.cta_time = nullptr;
     P.unit_log = nullptr; P.unit_log_cap = 0;
     P.shallow = 0;
+    P.balance = 0;
     P.lists = 0;
     P.root_frames = 0; P.defer_words = 0; P.defer_members = 0; P.defer_frames = 0; P.defer_queue = 0;
     P.root_key = nullptr; P.top_frames = 0; P.keys_in_words = 0; P.admit_words = 0;
     P.deferred = nullptr; P.deferred_cap = 0;
     // Each warp keeps one scratch tidset: leave at least half the arena to children.
     const size_t prefix_bytes = stride * 8;
-    const bool smem_prefix = prefix_bytes <= 200 * 1024;
+    const bool smem_prefix = prefix_bytes <= DEEP_SMEM_PREFIX_MAX;
     int per_sm = 1;
     if (smem_prefix) {
-        // cpm_init already allows k_deep<true> 200 KB of dynamic shared memory;
+        // cpm_init already allows k_deep<true> DEEP_SMEM_PREFIX_MAX bytes of dynamic shared memory;
         // the attribute is process-wide, so it is not touched here.
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_deep<true>, 256, prefix_bytes));
     } else {
@@ -3156,3 +3164,98 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     *n_patterns = hs.n_patterns;
     return CPM_OK;
 }
+
+// ---------------------------------------------------------------------------
+// delimited text of integer baskets, parsed on the device
+// ---------------------------------------------------------------------------
+
+struct cpm_csr {
+    std::vector<uint64_t> offsets;  // n_rows + 1
+    std::vector<uint32_t> ids;
+};
+
+extern "C" int cpm_parse_int_text(cpm_ctx *ctx, const char *text, uint64_t n_bytes, int32_t sep, cpm_csr **out) {
+    if (!ctx || !out) return CPM_EINVAL;
+    *out = nullptr;
+    if (n_bytes && !text) return set_err(ctx, CPM_EINVAL, "null text");
+    if (sep < 1 || sep > 127 || (sep >= '0' && sep <= '9') || sep == '\n')
+        return set_err(ctx, CPM_EINVAL, "the separator must be one ASCII character other than a digit or newline");
+    CK(cudaSetDevice(ctx->device));
+    std::unique_ptr<cpm_csr> csr(new cpm_csr());
+    // Lines: one per newline, plus a last one when the text does not end in a newline.
+    const bool tail = n_bytes && text[n_bytes - 1] != '\n';
+    if (n_bytes == 0) {
+        csr->offsets.assign(1, 0);
+        *out = csr.release();
+        return CPM_OK;
+    }
+    DevScope ds(ctx);
+    unsigned char *d_text = nullptr;
+    uint32_t *d_flag = nullptr;
+    uint64_t *d_pos = nullptr;
+    unsigned int *d_reject = nullptr;
+    CKR(ds.alloc(&d_text, n_bytes));
+    CKR(ds.alloc(&d_flag, n_bytes));
+    CKR(ds.alloc(&d_pos, n_bytes));
+    CKR(ds.alloc(&d_reject, 1));
+    CKR(stage_upload(ctx, {{d_text, {text, n_bytes}}}));
+    CK(cudaMemsetAsync(d_reject, 0, 4, ctx->stream));
+    const unsigned grid = (unsigned)std::min<uint64_t>((n_bytes + 255) / 256, (uint64_t)ctx->sms * 32);
+    k_text_newlines<<<grid, 256, 0, ctx->stream>>>(d_text, n_bytes, d_flag);
+    CK(cudaGetLastError());
+    uint64_t n_nl = 0;
+    CKR(scan_u32(ctx, ds, d_flag, d_pos, n_bytes, &n_nl));
+    const uint64_t n_lines = n_nl + (tail ? 1 : 0);
+    uint64_t *d_nl = nullptr, *d_off = nullptr;
+    uint32_t *d_cnt = nullptr;
+    CKR(ds.alloc(&d_nl, std::max<uint64_t>(1, n_nl)));
+    CKR(ds.alloc(&d_cnt, std::max<uint64_t>(1, n_lines)));
+    CKR(ds.alloc(&d_off, n_lines + 1));
+    k_text_scatter<<<grid, 256, 0, ctx->stream>>>(d_flag, d_pos, n_bytes, d_nl);
+    CK(cudaGetLastError());
+    const unsigned lgrid = (unsigned)((n_lines + 255) / 256);
+    if (n_lines) {
+        k_text_lines<false><<<lgrid, 256, 0, ctx->stream>>>(d_text, n_bytes, d_nl, n_nl, n_lines, (unsigned char)sep,
+                                                            d_cnt, nullptr, nullptr, d_reject);
+        CK(cudaGetLastError());
+    }
+    uint64_t nnz = 0;
+    CKR(scan_u32(ctx, ds, d_cnt, d_off, n_lines, &nnz));
+    unsigned int reject = 0;
+    CK(cudaMemcpyAsync(&reject, d_reject, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (reject)
+        return set_err(ctx, CPM_EINVAL, "the text is not unquoted integer baskets (canonical ids up to 4294967295, "
+                       "one separator between tokens, ASCII only)");
+    uint32_t *d_ids = nullptr;
+    CKR(ds.alloc(&d_ids, std::max<uint64_t>(1, nnz)));
+    if (n_lines && nnz) {
+        k_text_lines<true><<<lgrid, 256, 0, ctx->stream>>>(d_text, n_bytes, d_nl, n_nl, n_lines, (unsigned char)sep,
+                                                           nullptr, d_off, d_ids, d_reject);
+        CK(cudaGetLastError());
+    }
+    csr->offsets.resize(n_lines + 1);
+    csr->ids.resize(nnz);
+    if (n_lines) CK(cudaMemcpyAsync(csr->offsets.data(), d_off, n_lines * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    if (nnz) CK(cudaMemcpyAsync(csr->ids.data(), d_ids, nnz * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    csr->offsets[n_lines] = nnz;
+    *out = csr.release();
+    return CPM_OK;
+}
+
+extern "C" int cpm_csr_size(const cpm_csr *csr, uint64_t *n_rows, uint64_t *nnz) {
+    if (!csr || !n_rows || !nnz) return CPM_EINVAL;
+    *n_rows = csr->offsets.size() - 1;
+    *nnz = csr->ids.size();
+    return CPM_OK;
+}
+
+extern "C" int cpm_csr_copy(const cpm_csr *csr, uint64_t *offsets, uint32_t *ids) {
+    if (!csr || !offsets || (!ids && !csr->ids.empty())) return CPM_EINVAL;
+    memcpy(offsets, csr->offsets.data(), csr->offsets.size() * 8);
+    if (!csr->ids.empty()) memcpy(ids, csr->ids.data(), csr->ids.size() * 4);
+    return CPM_OK;
+}
+
+extern "C" void cpm_csr_free(cpm_csr *csr) { delete csr; }

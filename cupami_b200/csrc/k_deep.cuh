@@ -44,6 +44,10 @@ enum : unsigned {
 // 64-bit words of a list of n transaction ids (16-byte header, 16-byte padding).
 __host__ __device__ __forceinline__ uint64_t list_words(uint64_t n) { return (n + 7) / 4 * 2; }
 
+// Largest prefix bitmap (bytes) staged in shared memory: the kernel's static
+// shared memory (about 30 KB) and this fit in the 227 KB a CTA may use.
+constexpr size_t DEEP_SMEM_PREFIX_MAX = 192 * 1024;
+
 constexpr unsigned long long QUEUE_EMPTY = ~0ull;
 constexpr uint32_t NO_PATTERN = 0xffffffffu;
 
@@ -92,6 +96,7 @@ struct DeepParams {
     unsigned long long spin_limit;
     unsigned long long *cta_time;   // optional [2 * grid]: busy ns, exit time (globaltimer)
     uint32_t shallow;               // 1: child frames are recorded, not queued
+    uint32_t balance;               // pass 1: 0 a warp per sibling; 1 siblings split over warps by size
     uint32_t lists;                 // list-form threshold divisor (0: bitsets only; needs SMEM_PREFIX)
     // Memory-bounded rounds: a unit of a frame below root_frames (a root
     // unit) claimed while the arena, the member table or the frame table has
@@ -185,25 +190,33 @@ __device__ int deep_claim(const DeepParams &P, unsigned long long *item) {
     return 1;
 }
 
-// This lane's share of |prefix & sibling| over part `part` of `parts` equal
-// slices of the sibling (dense words or list ids); *bytes gets the sibling's
-// size in its own form.  Eight 16-byte loads in flight per lane.
+// Work units of a sibling: 16-byte words of a bitset (n2), or ids of a list
+// (its header's count; lists only when the prefix is in shared memory).
 template <bool SMEM_PREFIX>
-__device__ __forceinline__ uint32_t sibling_count(unsigned long long sraw, uint32_t part, uint32_t parts, uint64_t n2,
-                                                  const ulonglong2 *s_prefix, const uint32_t *s_p32,
-                                                  const ulonglong2 *pb, const ulonglong2 *mk, unsigned lane,
-                                                  uint64_t *bytes) {
+__device__ __forceinline__ uint64_t sibling_units(unsigned long long sraw, uint64_t n2) {
+    return (SMEM_PREFIX && (sraw & 1ull)) ? (uint64_t)__ldcg(reinterpret_cast<const uint32_t *>(sraw & ~1ull)) : n2;
+}
+
+// A sibling's size in its own form (the bytes a full pass reads).
+template <bool SMEM_PREFIX>
+__device__ __forceinline__ uint64_t sibling_bytes(unsigned long long sraw, uint64_t units) {
+    return (SMEM_PREFIX && (sraw & 1ull)) ? 8ull * list_words(units) : 16ull * units;
+}
+
+// This lane's share of |prefix & sibling| over work units [lo, hi) of the
+// sibling (dense words or list ids).  Eight 16-byte loads (or sixteen ids) in
+// flight per lane.
+template <bool SMEM_PREFIX>
+__device__ __forceinline__ uint32_t sibling_count_range(unsigned long long sraw, uint64_t lo, uint64_t hi,
+                                                        const ulonglong2 *s_prefix, const uint32_t *s_p32,
+                                                        const ulonglong2 *pb, const ulonglong2 *mk, unsigned lane) {
     uint32_t s = 0;
     if (SMEM_PREFIX && (sraw & 1ull)) {
-        // List sibling: test its ids against the prefix bitmap.
-        const uint32_t *L = reinterpret_cast<const uint32_t *>(sraw & ~1ull);
-        const uint32_t n = __ldcg(L);
-        // Lanes take consecutive ids (32 per warp load, sixteen loads in
-        // flight per lane), so the bit tests of one instruction fall in
-        // nearby, mostly distinct shared-memory banks.
-        const uint32_t *I = L + 4;
-        const uint32_t lo = (uint32_t)((uint64_t)n * part / parts), hi = (uint32_t)((uint64_t)n * (part + 1) / parts);
-        uint32_t w = lo + lane;
+        // List sibling: test its ids against the prefix bitmap.  Lanes take
+        // consecutive ids (32 per warp load), so the bit tests of one
+        // instruction fall in nearby, mostly distinct shared-memory banks.
+        const uint32_t *I = reinterpret_cast<const uint32_t *>(sraw & ~1ull) + 4;
+        uint64_t w = lo + lane;
         for (; w + 480 < hi; w += 512) {
             uint32_t t[16];
 #pragma unroll
@@ -212,11 +225,9 @@ __device__ __forceinline__ uint32_t sibling_count(unsigned long long sraw, uint3
             for (int u = 0; u < 16; ++u) s += bit_of(s_p32, t[u]);
         }
         for (; w < hi; w += 32) s += bit_of(s_p32, __ldcg(I + w));
-        *bytes = 8ull * list_words(n);
         return s;
     }
     const ulonglong2 *sb = reinterpret_cast<const ulonglong2 *>(sraw);
-    const uint64_t lo = n2 * part / parts, hi = n2 * (part + 1) / parts;
     uint64_t v = lo + lane;
     for (; v + 224 < hi; v += 256) {
         ulonglong2 x[8];
@@ -243,8 +254,101 @@ __device__ __forceinline__ uint32_t sibling_count(unsigned long long sraw, uint3
         }
         s += popc2(x);
     }
-    *bytes = 16ull * n2;
     return s;
+}
+
+// This lane's share of |prefix & sibling| over part `part` of `parts` equal
+// slices of the sibling; *bytes gets the sibling's size in its own form.
+template <bool SMEM_PREFIX>
+__device__ __forceinline__ uint32_t sibling_count(unsigned long long sraw, uint32_t part, uint32_t parts, uint64_t n2,
+                                                  const ulonglong2 *s_prefix, const uint32_t *s_p32,
+                                                  const ulonglong2 *pb, const ulonglong2 *mk, unsigned lane,
+                                                  uint64_t *bytes) {
+    const uint64_t units = sibling_units<SMEM_PREFIX>(sraw, n2);
+    *bytes = sibling_bytes<SMEM_PREFIX>(sraw, units);
+    return sibling_count_range<SMEM_PREFIX>(sraw, units * part / parts, units * (part + 1) / parts, s_prefix, s_p32,
+                                            pb, mk, lane);
+}
+
+// Child list piece: the ids of the sibling's transactions that the prefix
+// bitmap holds, over work units [lo, hi) of the sibling (list ids or bitset
+// words), written in ascending order to o32[4 + at ...] (never past sc ids).
+// Returns the position after the last id.  Loads run eight id chunks (or
+// four word chunks) ahead of the ballot compaction.
+__device__ __forceinline__ uint32_t write_list_piece(unsigned long long sraw, uint64_t lo, uint64_t hi,
+                                                     const ulonglong2 *s_prefix, const uint32_t *s_p32,
+                                                     uint32_t *o32, uint32_t at, uint32_t sc, unsigned lane) {
+    const unsigned below = (1u << lane) - 1u;
+    if (sraw & 1ull) {
+        const uint32_t *I = reinterpret_cast<const uint32_t *>(sraw & ~1ull) + 4;
+        for (uint64_t w0 = lo; w0 < hi; w0 += 256) {
+            uint32_t t[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const uint64_t j = w0 + 32 * u + lane;
+                t[u] = j < hi ? __ldcg(I + j) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const bool keep = w0 + 32 * u + lane < hi && bit_of(s_p32, t[u]);
+                const unsigned bal = __ballot_sync(CPM_FULL, keep);
+                const uint32_t pos = at + __popc(bal & below);
+                if (keep && pos < sc) o32[4 + pos] = t[u];
+                at += __popc(bal);
+            }
+        }
+        return at;
+    }
+    const ulonglong2 *sb = reinterpret_cast<const ulonglong2 *>(sraw);
+    for (uint64_t v0 = lo; v0 < hi; v0 += 128) {
+        ulonglong2 x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint64_t v = v0 + 32 * u + lane;
+            x[u] = v < hi ? and2(ld_cg(sb + v), s_prefix[v]) : make_ulonglong2(0ull, 0ull);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint64_t v = v0 + 32 * u + lane;
+            const uint32_t c = popc2(x[u]);
+            uint32_t incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(CPM_FULL, incl, o);
+                if (lane >= (unsigned)o) incl += y;
+            }
+            uint32_t pos = at + incl - c;
+            for (unsigned long long b = x[u].x; b; b &= b - 1, ++pos)
+                if (pos < sc) o32[4 + pos] = (uint32_t)(v * 128 + __ffsll((long long)b) - 1);
+            for (unsigned long long b = x[u].y; b; b &= b - 1, ++pos)
+                if (pos < sc) o32[4 + pos] = (uint32_t)(v * 128 + 64 + __ffsll((long long)b) - 1);
+            at += __shfl_sync(CPM_FULL, incl, 31);
+        }
+    }
+    return at;
+}
+
+// Child bitset piece: words [lo, hi) of prefix & sibling (a bitset), four
+// 16-byte loads in flight per lane.
+template <bool SMEM_PREFIX>
+__device__ __forceinline__ void write_dense_piece(unsigned long long sraw, uint64_t lo, uint64_t hi,
+                                                  const ulonglong2 *s_prefix, const ulonglong2 *pb,
+                                                  const ulonglong2 *mk, ulonglong2 *dst, unsigned lane) {
+    const ulonglong2 *sb = reinterpret_cast<const ulonglong2 *>(sraw);
+    auto with_prefix = [&](ulonglong2 x, uint64_t v) {
+        if (SMEM_PREFIX) return and2(x, s_prefix[v]);
+        x = and2(x, ld_cg(pb + v));
+        return mk ? and2(x, ld_cg(mk + v)) : x;
+    };
+    uint64_t v = lo + lane;
+    for (; v + 96 < hi; v += 128) {
+        ulonglong2 x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = ld_cg(sb + v + 32 * u);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) dst[v + 32 * u] = with_prefix(x[u], v + 32 * u);
+    }
+    for (; v < hi; v += 32) dst[v] = with_prefix(ld_cg(sb + v), v);
 }
 
 template <bool SMEM_PREFIX>
@@ -256,7 +360,11 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     __shared__ unsigned long long s_mem_base, s_arena_base, s_fid, s_qbase;
     __shared__ uint32_t s_wtot[32];
     __shared__ uint64_t s_w64[32];
-    __shared__ uint64_t s_off[1024];     // child offsets of one chunk of survivors
+    __shared__ uint64_t s_off[1025];     // child offsets of one chunk of survivors; pass-1 work offsets
+    __shared__ unsigned long long s_raw[1024];  // pass 1 (balanced): sibling pointers of one chunk
+    __shared__ uint32_t s_cnt[1024];             // pass 1 (balanced): their supports; pass 2: child supports
+    __shared__ uint64_t s_coff[1024];            // pass 2: arena offsets of one chunk's children
+    __shared__ uint32_t s_clast[32];             // pass 2: ids in each warp's last piece of a split child
     __shared__ unsigned long long s_bytes;
     __shared__ uint32_t s_nsurv;         // survivors counted in pass 1
     __shared__ uint32_t s_part[32];      // per-sibling sums when siblings are split over warps
@@ -266,8 +374,16 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
 
     const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     DeepState *st = P.st;
+    if (!SMEM_PREFIX && P.lists) {
+        // List tidsets are tested against a prefix bitmap in shared memory:
+        // without one the host must not ask for them.
+        if (threadIdx.x == 0 && blockIdx.x == 0) deep_fail(st, DEEP_ERR_INTERNAL);
+        return;
+    }
     // Per-CTA statistics (thread 0), added to the global counters at exit.
-    unsigned long long c_inter = 0, c_bytes = 0, c_units = 0, c_surv = 0, c_busy = 0, t_unit = 0;
+    // Kept in shared memory, not registers: only thread 0 touches them.
+    __shared__ unsigned long long c_inter, c_bytes, c_units, c_surv, c_busy, t_unit;
+    if (threadIdx.x == 0) c_inter = c_bytes = c_units = c_surv = c_busy = t_unit = 0;
 
     for (;;) {
         if (threadIdx.x == 0) {
@@ -393,7 +509,54 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         // Fewer siblings than warps: split every sibling into equal slices
         // (at least 4 KB of bitset each) so that every warp has work.
         const uint32_t parts = (cnt && cnt < nw) ? max(1u, min(nw / cnt, (uint32_t)(n2 >> 8))) : 1u;
-        if (parts == 1) {
+        if (P.balance) {
+            // Siblings split over warps by size.  Per chunk of up to blockDim
+            // siblings: every sibling's work (bitset words or list ids) is
+            // laid end to end, each warp takes an equal slice of the total
+            // (crossing sibling boundaries) and adds its partial counts into
+            // s_cnt; then each sibling is emitted.  A unit takes as long as
+            // its bytes, not as long as its largest sibling.
+            for (uint32_t c0 = 0; ok && c0 < cnt; c0 += blockDim.x) {
+                const uint32_t cn = min((uint32_t)blockDim.x, cnt - c0);
+                uint64_t wk = 0;
+                unsigned long long raw = 0;
+                if (threadIdx.x < cn) {
+                    raw = ld_raw_ptr(P.mem_bits + mem_off + p + 1 + c0 + threadIdx.x);
+                    wk = sibling_units<SMEM_PREFIX>(raw, n2);
+                    s_raw[threadIdx.x] = raw;
+                    s_cnt[threadIdx.x] = 0;
+                }
+                uint64_t tot = 0;
+                const uint64_t ex = block_excl_scan_u64(wk, s_w64, &tot);
+                if (threadIdx.x < cn) s_off[threadIdx.x] = ex;
+                if (threadIdx.x == 0) s_off[cn] = tot;
+                __syncthreads();
+                const uint64_t lo = tot * wid / nw, hi = tot * (wid + 1) / nw;
+                if (lo < hi) {
+                    uint32_t a = 0, b = cn;  // first sibling whose work ends past lo
+                    while (a < b) {
+                        const uint32_t mid = (a + b) >> 1;
+                        if (s_off[mid + 1] <= lo) a = mid + 1; else b = mid;
+                    }
+                    for (uint32_t i = a; i < cn && s_off[i] < hi; ++i) {
+                        const uint64_t u0 = max(lo, s_off[i]) - s_off[i], u1 = min(hi, s_off[i + 1]) - s_off[i];
+                        if (u0 >= u1) continue;
+                        uint32_t c = sibling_count_range<SMEM_PREFIX>(s_raw[i], u0, u1, s_prefix, s_p32, pb, mk, lane);
+                        c = warp_sum_u32(c);
+                        if (lane == 0 && c) atomicAdd(&s_cnt[i], c);
+                    }
+                }
+                __syncthreads();
+                if (threadIdx.x < cn) {
+                    const uint64_t b = sibling_bytes<SMEM_PREFIX>(raw, wk);
+                    atomicAdd(&s_bytes, (unsigned long long)b);
+                    if (P.unit_log) atomicMax(&s_maxb, (unsigned long long)b);
+                    emit(c0 + threadIdx.x, s_cnt[threadIdx.x], __ldcg(P.mem_item + mem_off + p + 1 + c0 + threadIdx.x),
+                         raw);
+                }
+                __syncthreads();
+            }
+        } else if (parts == 1) {
             for (uint32_t q = wid; ok && q < cnt; q += nw) {
                 const uint64_t mi = mem_off + p + 1 + q;
                 const unsigned long long sraw = ld_raw_ptr(P.mem_bits + mi);
@@ -519,99 +682,100 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         }
         __syncthreads();
         // ---- pass 2: child tidsets of the survivors (only when they recurse) ----
+        // Per chunk of up to blockDim survivors: their siblings' work (list
+        // ids or bitset words) is laid end to end and each warp takes an
+        // equal slice, crossing child boundaries, so that every warp writes
+        // even when few children survive.  A list child split over warps needs
+        // each piece's first output position: a warp whose slice ends inside
+        // a list child first counts that last piece (s_clast), and a warp that
+        // starts inside one adds up the counts of the warps before it.
         if (s_grant) {
             uint64_t chunk_base = 0;
             for (uint32_t start = 0; start < ns; start += blockDim.x) {
-                // Offsets of this chunk's children within the unit's block.
-                const uint32_t i = start + threadIdx.x;
-                uint64_t sz = 0;
-                if (i < ns) {
-                    if (P.lists) {
-                        const uint32_t sc = __ldcg(P.pat_sup + __ldcg(P.mem_pat + s_mem_base + i));
-                        sz = as_list(P, sc, stride) ? list_words(sc) : stride;
-                    } else {
-                        sz = stride;
+                const uint32_t cn = min((uint32_t)blockDim.x, ns - start);
+                uint64_t sz = 0, wk = 0;
+                if (threadIdx.x < cn) {
+                    const uint64_t m_out = s_mem_base + start + threadIdx.x;
+                    const unsigned long long raw = ld_raw_ptr(P.mem_bits + m_out);
+                    const uint32_t sc = P.lists ? __ldcg(P.pat_sup + __ldcg(P.mem_pat + m_out)) : 0u;
+                    sz = (SMEM_PREFIX && as_list(P, sc, stride)) ? list_words(sc) : stride;
+                    wk = sibling_units<SMEM_PREFIX>(raw, n2);
+                    s_raw[threadIdx.x] = raw;
+                    s_cnt[threadIdx.x] = sc;
+                }
+                uint64_t ctot = 0, wtot = 0;
+                const uint64_t cex = block_excl_scan_u64(sz, s_w64, &ctot);
+                const uint64_t wex = block_excl_scan_u64(wk, s_w64, &wtot);
+                if (threadIdx.x < cn) {
+                    s_coff[threadIdx.x] = chunk_base + cex;
+                    s_off[threadIdx.x] = wex;
+                }
+                if (threadIdx.x == 0) s_off[cn] = wtot;
+                if (threadIdx.x < 32) s_clast[threadIdx.x] = 0;
+                __syncthreads();
+                const uint64_t lo = wtot * wid / nw, hi = wtot * (wid + 1) / nw;
+                uint32_t first = cn;  // first child whose work ends past lo
+                if (lo < hi) {
+                    uint32_t a = 0, b = cn;
+                    while (a < b) {
+                        const uint32_t mid = (a + b) >> 1;
+                        if (s_off[mid + 1] <= lo) a = mid + 1; else b = mid;
+                    }
+                    first = a;
+                    // The child this slice ends in, when it goes on past the slice.
+                    uint32_t z = first;
+                    while (z + 1 < cn && s_off[z + 1] < hi) ++z;
+                    const bool list_child = SMEM_PREFIX && as_list(P, s_cnt[z], stride);
+                    if (list_child && s_off[z + 1] > hi) {
+                        uint32_t c = sibling_count_range<SMEM_PREFIX>(s_raw[z], max(lo, s_off[z]) - s_off[z],
+                                                                      hi - s_off[z], s_prefix, s_p32, pb, mk, lane);
+                        c = warp_sum_u32(c);
+                        if (lane == 0) s_clast[wid] = c;
                     }
                 }
-                uint64_t chunk_total = 0;
-                const uint64_t excl = block_excl_scan_u64(sz, s_w64, &chunk_total);
-                s_off[threadIdx.x] = chunk_base + excl;
                 __syncthreads();
-                const uint32_t stop = min(ns, start + blockDim.x);
-                for (uint32_t idx = start + wid; idx < stop; idx += nw) {
-                    const uint64_t m_out = s_mem_base + idx;
-                    const unsigned long long sraw = ld_raw_ptr(P.mem_bits + m_out);
-                    const ulonglong2 *sb = reinterpret_cast<const ulonglong2 *>(sraw);
-                    uint64_t *out = P.arena + s_arena_base + s_off[idx - start];
-                    const uint32_t sc = P.lists ? __ldcg(P.pat_sup + __ldcg(P.mem_pat + m_out)) : 0u;
-                    unsigned long long tagged;
+                for (uint32_t i = first; i < cn && s_off[i] < hi; ++i) {
+                    const uint64_t u0 = max(lo, s_off[i]) - s_off[i], u1 = min(hi, s_off[i + 1]) - s_off[i];
+                    const uint64_t units = s_off[i + 1] - s_off[i];
+                    uint64_t *out = P.arena + s_arena_base + s_coff[i];
+                    const uint32_t sc = s_cnt[i];
                     if (SMEM_PREFIX && as_list(P, sc, stride)) {
-                        // List child: the ids of the sibling's transactions that the
-                        // prefix holds, in ascending order.
                         uint32_t *o32 = reinterpret_cast<uint32_t *>(out);
-                        uint32_t written = 0;
-                        if (sraw & 1ull) {
-                            const uint32_t *L = reinterpret_cast<const uint32_t *>(sraw & ~1ull);
-                            const uint32_t n = __ldcg(L);
-                            for (uint32_t j0 = 0; j0 < n; j0 += 32) {
-                                const uint32_t j = j0 + lane;
-                                const uint32_t t = j < n ? __ldcg(L + 4 + j) : 0u;
-                                const bool keep = j < n && bit_of(s_p32, t);
-                                const unsigned bal = __ballot_sync(CPM_FULL, keep);
-                                const uint32_t at = written + __popc(bal & ((1u << lane) - 1));
-                                if (keep && at < sc) o32[4 + at] = t;
-                                written += __popc(bal);
-                            }
-                        } else {
-                            for (uint64_t v0 = 0; v0 < n2; v0 += 32) {
-                                const uint64_t v = v0 + lane;
-                                ulonglong2 x = make_ulonglong2(0ull, 0ull);
-                                if (v < n2) x = and2(ld_cg(sb + v), s_prefix[v]);
-                                const uint32_t c = (uint32_t)(__popcll(x.x) + __popcll(x.y));
-                                uint32_t incl = c;
-#pragma unroll
-                                for (int o = 1; o < 32; o <<= 1) {
-                                    const uint32_t y = __shfl_up_sync(CPM_FULL, incl, o);
-                                    if (lane >= (unsigned)o) incl += y;
-                                }
-                                uint32_t at = written + incl - c;  // stays below sc unless counts disagree
-                                for (unsigned long long b = x.x; b; b &= b - 1, ++at)
-                                    if (at < sc) o32[4 + at] = (uint32_t)(v * 128 + __ffsll((long long)b) - 1);
-                                for (unsigned long long b = x.y; b; b &= b - 1, ++at)
-                                    if (at < sc) o32[4 + at] = (uint32_t)(v * 128 + 64 + __ffsll((long long)b) - 1);
-                                written += __shfl_sync(CPM_FULL, incl, 31);
+                        uint32_t at = 0;
+                        if (u0 > 0) {
+                            // Ids written by the earlier warps that hold parts of this child.
+                            for (uint32_t w = wid; w-- > 0;) {
+                                at += s_clast[w];
+                                if (wtot * w / nw <= s_off[i]) break;
                             }
                         }
-                        if (lane == 0) {
+                        if (u0 < u1) at = write_list_piece(s_raw[i], u0, u1, s_prefix, s_p32, o32, at, sc, lane);
+                        if (u0 == 0 && lane == 0) {
                             o32[0] = sc;
                             o32[1] = o32[2] = o32[3] = 0u;
-                            if (written != sc) deep_fail(st, DEEP_ERR_INTERNAL);
                         }
-                        // Ids the count promised but the pass did not find (only when the
-                        // counts disagree, an error) become 0, an in-range id.
-                        for (uint32_t j = written + lane; j < sc; j += 32) o32[4 + j] = 0u;
-                        // Zero the padding after the last id.
-                        const uint32_t end = 4 + sc, pad_end = (uint32_t)(list_words(sc) * 2);
-                        if (lane < pad_end - end) o32[end + lane] = 0u;
-                        tagged = reinterpret_cast<unsigned long long>(out) | 1ull;
-                    } else {
-                        ulonglong2 *dst = reinterpret_cast<ulonglong2 *>(out);
-                        for (uint64_t v = lane; v < n2; v += 32) {
-                            ulonglong2 x = ld_cg(sb + v);
-                            if (SMEM_PREFIX) {
-                                x = and2(x, s_prefix[v]);
-                            } else {
-                                x = and2(x, ld_cg(pb + v));
-                                if (mk) x = and2(x, ld_cg(mk + v));
-                            }
-                            dst[v] = x;
+                        if (u1 == units) {
+                            if (lane == 0 && at != sc) deep_fail(st, DEEP_ERR_INTERNAL);
+                            // Ids the count promised but the pass did not find (only when the
+                            // counts disagree, an error) become 0, an in-range id.
+                            for (uint32_t j = at + lane; j < sc; j += 32) o32[4 + j] = 0u;
+                            // Zero the padding after the last id.
+                            const uint32_t end = 4 + sc, pad_end = (uint32_t)(list_words(sc) * 2);
+                            if (lane < pad_end - end) o32[end + lane] = 0u;
                         }
-                        tagged = reinterpret_cast<unsigned long long>(out);
+                    } else if (u0 < u1) {
+                        write_dense_piece<SMEM_PREFIX>(s_raw[i], u0, u1, s_prefix, pb, mk,
+                                                       reinterpret_cast<ulonglong2 *>(out), lane);
                     }
-                    __syncwarp();
-                    if (lane == 0) P.mem_bits[m_out] = reinterpret_cast<const uint64_t *>(tagged);
                 }
-                chunk_base += chunk_total;
+                __syncthreads();  // every piece of this chunk is written
+                if (threadIdx.x < cn) {
+                    const uint64_t *out = P.arena + s_arena_base + s_coff[threadIdx.x];
+                    const bool lst = SMEM_PREFIX && as_list(P, s_cnt[threadIdx.x], stride);
+                    P.mem_bits[s_mem_base + start + threadIdx.x] = reinterpret_cast<const uint64_t *>(
+                        reinterpret_cast<unsigned long long>(out) | (lst ? 1ull : 0ull));
+                }
+                chunk_base += ctot;
                 __syncthreads();
             }
             __threadfence();

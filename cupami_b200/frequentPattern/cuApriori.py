@@ -76,6 +76,9 @@ class cuApriori:
     #: lists for sparse tidsets of databases too big for the L2); 1 bitsets
     #: only; 2 lists wherever possible.
     _TIDSETS = 0
+    #: Deep-level siblings of a unit: 0 automatic, 1 one warp per sibling,
+    #: 2 split over the warps by size.
+    _DEEP_BALANCE = 0
 
     def __init__(self, iFile, minSup, sep=None, use_gds="auto", use_gpu_io="auto"):
         t0 = time.perf_counter()
@@ -121,6 +124,8 @@ class cuApriori:
                 return self._readBinaryFile(Path(source))
             if suffix == ".parquet":
                 return self._readParquetFile(source)
+            if self._tryDeviceText(Path(source)):
+                return None
             with Path(source).open("r", newline="", encoding="utf-8") as stream:
                 return self._readDelimitedFile(stream)
         return self._cleanTransactions(source)
@@ -136,6 +141,27 @@ class cuApriori:
             self._inputBackend["gds_fallback_reason"] = previous
         self._inputBackend["direct_gds_verified"] = False
         return None
+
+    def _tryDeviceText(self, path):
+        """Integer baskets in delimited text, parsed on the GPU (the role of the
+        reference's cuDF reader, _gpu_io.py:34-54); False leaves the file to the
+        CPU reader: use_gpu_io=False, no usable device, or another layout."""
+        if self.use_gpu_io is False:
+            return False
+        try:
+            data = path.read_bytes()
+            head = data.split(b"\n", 1)[0].decode("utf-8", "replace")
+            sep = self.sep if self.sep is not None else ("\t" if "\t" in head else ",")
+            if len(sep) != 1 or not sep.isascii():
+                raise _native.NativeError(_native.CPM_EINVAL, "the GPU text reader takes a one-byte separator")
+            offsets, ids = _native.parse_int_text(self._getCudaModule(), data, sep)
+        except (ImportError, RuntimeError) as error:
+            if self.use_gpu_io is True:
+                raise RuntimeError(f"GPU input unavailable: {error}") from error
+            self._inputBackend = {"backend": "cpu", "reason": str(error)}
+            return False
+        self._useCsr(offsets, ids, "cuda-text", "Integer baskets parsed on the GPU; no Python transactions")
+        return True
 
     def _gdsUnavailable(self):
         reason = "GDS (cuFile/KvikIO) is not part of this engine"
@@ -260,6 +286,7 @@ class cuApriori:
         opts.deep_ctas_per_sm = int(self._DEEP_CTAS_PER_SM)
         opts.autotune = 1
         opts.tidsets = int(self._TIDSETS)
+        opts.deep_balance = int(self._DEEP_BALANCE)
         return opts
 
     def autotune(self):

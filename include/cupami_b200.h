@@ -96,7 +96,9 @@ typedef struct {
                                       memory */
     int32_t  list_div;             /* a tidset is stored as a list when its list takes at most 1/list_div
                                       of its bitset; 0 = the autotuner's choice, else 2 */
-    int32_t  reserved[2];
+    int32_t  deep_balance;         /* deep-level siblings: 0 = automatic (split over warps by size), 1 = a
+                                      warp per sibling, 2 = split over warps by size */
+    int32_t  reserved[1];
 } cpm_opts;
 
 typedef struct {
@@ -271,6 +273,25 @@ int cpm_periodic_counts(cpm_ctx *ctx, const uint32_t *d_bitsets, uint64_t words3
                         const uint32_t *d_candidates, uint64_t n_candidates, uint32_t width,
                         const int64_t *d_timestamps, uint64_t n_transactions, int64_t end,
                         uint64_t *d_supports, int64_t *d_periods);
+
+/* ---- Delimited text of integer baskets, parsed on the device ----------------
+ * Replaces cupami/frequentPattern/_gpu_io.py:34-54 (read_text: cuDF parse of
+ * a CSV/TSV file whose stripped, non-empty lines are unquoted integer baskets,
+ * exploded to rows and items on the GPU), called from cuApriori._tryGpuFile
+ * (cuApriori.py:223-254).  `text` holds the file's bytes; `sep` is the
+ * one-byte separator.  Every line is stripped of ASCII whitespace; blank lines
+ * become empty rows; any other line must be tokens separated by `sep` (with
+ * optional whitespace around it), each token a canonical decimal id (no
+ * leading zero unless "0", at most 4294967295).  A line outside that layout,
+ * a non-ASCII byte or an empty token returns CPM_EINVAL, and the caller reads
+ * the file on the CPU as the reference does for such layouts.  The result is a
+ * host CSR (row k = ids[offsets[k], offsets[k+1])) for cpm_db_from_ids; ids
+ * name the same labels as the tokens' strings. */
+typedef struct cpm_csr cpm_csr;
+int cpm_parse_int_text(cpm_ctx *ctx, const char *text, uint64_t n_bytes, int32_t sep, cpm_csr **out);
+int cpm_csr_size(const cpm_csr *csr, uint64_t *n_rows, uint64_t *nnz);
+int cpm_csr_copy(const cpm_csr *csr, uint64_t *offsets, uint32_t *ids);
+void cpm_csr_free(cpm_csr *csr);
 
 /* ---- Eclat without device allocation ---------------------------------------
  * No counterpart in the reference: cuPAMI allocates through CuPy's pool on

@@ -35,8 +35,9 @@ def main():
         s["transactions"] = int(np.count_nonzero(np.diff(csr.offsets.astype(np.int64)) > 0))
         out.append(s)
     doc = {"workload": "batched_zipf(n_db=512, low=1_000, high=200_000, n_items=200, mean=8, s=1.1, seed=19)",
-           "minSup": 0.01, "databases": out, "patterns": sum(d["patterns"] for d in out),
-           "oracle_seconds": round(time.time() - t, 1), "generator": "tests/golden/make_batched_summary.py"}
+           "minSup": 0.01, "patterns": sum(d["patterns"] for d in out),
+           "oracle_seconds": round(time.time() - t, 1), "generator": "tests/golden/make_batched_summary.py",
+           "databases": out}
     (HERE / "batched_zipf_512_summary.json").write_text(json.dumps(doc, separators=(",", ":")))
     print(doc["patterns"], doc["oracle_seconds"])
 

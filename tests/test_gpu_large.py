@@ -55,3 +55,22 @@ def test_sparse_1m_matches_oracle_summary(workload, expected, scheduler, arena_b
         assert got[key] == expected[key], key
     if arena_bytes:
         assert res.stats["deep_rounds"] > 1
+
+
+def test_all_512_batched_databases_match_oracle_summaries():
+    """The whole 512-database batch (19 M transactions) in one mineBatch call,
+    every database against the oracle's summary of its exact answer."""
+    from make_sparse_summary import summarize
+
+    import cupami_b200
+    from cupami_b200 import datasets
+
+    expected = json.loads((GOLDEN / "batched_zipf_512_summary.json").read_text())
+    csrs = datasets.batched_zipf()
+    miners = cupami_b200.cuEclat.mineBatch(csrs, expected["minSup"])
+    assert len(miners) == len(expected["databases"]) == 512
+    for k, (m, want) in enumerate(zip(miners, expected["databases"])):
+        off, items, sup, labels = m.getPatternArrays()
+        got = summarize(labels, off, items, sup)
+        for key in ("patterns", "per_length", "hash_sum", "hash_xor_sum", "support_sum"):
+            assert got[key] == want[key], (k, key)

@@ -165,11 +165,14 @@ def test_list_and_bitset_tidsets_agree(oracle_lib, name, minsup):
     csr = getattr(datasets, name)()
     out = []
     for tidsets in (2, 1):
-        m = cupami_b200.cuEclat(csr, minsup)
-        m._TIDSETS = tidsets
-        m.mine()
-        out.append((list(m.getPatterns().items()), m.getKernelStats()))
-    assert out[0][0] == out[1][0]
+        for balance in (2, 1):  # siblings split over warps by size, or a warp each
+            m = cupami_b200.cuEclat(csr, minsup)
+            m._TIDSETS = tidsets
+            m._DEEP_BALANCE = balance
+            m.mine()
+            out.append((list(m.getPatterns().items()), m.getKernelStats()))
+    assert all(o[0] == out[0][0] for o in out)
+    out = out[::2]
     labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, minsup)
     assert dict(out[0][0]) == oracle_lib.to_dict(labels, arrays)
     if name == "planted_zipf":  # sparse deep levels: the lists move fewer bytes

@@ -45,6 +45,7 @@ def _pack(offsets, cols, n_items):
 def _pool_usage(device=0):
     """(used high, reserved high, used now, free bytes) of the device's default
     stream-ordered pool, with both watermarks first reset to the current use."""
+    from cuda.bindings import driver as dr
     from cuda.bindings import runtime as rt
 
     err, pool = rt.cudaDeviceGetDefaultMemPool(device)
@@ -58,7 +59,7 @@ def _pool_usage(device=0):
 
     def reset():
         for attr in (A.cudaMemPoolAttrUsedMemHigh, A.cudaMemPoolAttrReservedMemHigh):
-            (e,) = rt.cudaMemPoolSetAttribute(pool, attr, rt.cuuint64_t(0))
+            (e,) = rt.cudaMemPoolSetAttribute(pool, attr, dr.cuuint64_t(0))
             assert e == rt.cudaError_t.cudaSuccess
 
     def read():
