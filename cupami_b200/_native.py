@@ -121,6 +121,8 @@ _SIGNATURES = {
     "cpm_result_from_tree_periodic": (ctypes.c_int, [_P, _P, _P, _P, _U64, ctypes.POINTER(_P)]),
     "cpm_periodic_counts": (ctypes.c_int, [_P, _P, _U64, _P, _U64, ctypes.c_uint32, _P, _U64, ctypes.c_int64,
                                            _P, _P]),
+    "cpm_join_labels": (ctypes.c_int, [_P, _P, _U64, _P, _P, ctypes.c_uint32, ctypes.c_char, ctypes.c_char, _P,
+                                       _U64, ctypes.POINTER(_U64)]),
     "cpm_parse_int_text": (ctypes.c_int, [_P, _P, _U64, ctypes.c_int32, ctypes.POINTER(_P)]),
     "cpm_csr_size": (ctypes.c_int, [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
     "cpm_csr_copy": (ctypes.c_int, [_P, _P, _P]),
@@ -328,6 +330,34 @@ class Database:
             self.close()
         except Exception:
             pass
+
+
+def join_labels(offsets, items, labels, sep="\t"):
+    """Keys of a pattern CSR: every pattern's labels joined by ``sep`` (a list
+    of str), built in one C pass over the arrays."""
+    lib = library()
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+    items = np.ascontiguousarray(items, dtype=np.uint32)
+    n = offsets.size - 1
+    if n <= 0:
+        return []
+    enc = [str(x).encode("utf-8") for x in labels]
+    blob = b"".join(enc)
+    loff = np.zeros(len(enc) + 1, dtype=np.uint64)
+    np.cumsum([len(e) for e in enc], out=loff[1:])
+    src = np.frombuffer(blob, dtype=np.uint8) if blob else np.zeros(1, np.uint8)
+    need = _U64()
+    args = (offsets.ctypes.data, items.ctypes.data if items.size else None, n, src.ctypes.data, loff.ctypes.data,
+            len(enc), sep.encode(), b"\n")
+    if lib.cpm_join_labels(*args, None, 0, ctypes.byref(need)) != CPM_OK:
+        raise NativeError(CPM_EINVAL, "pattern items outside the labels")
+    out = bytearray(need.value)
+    buf = (ctypes.c_char * len(out)).from_buffer(out)
+    if lib.cpm_join_labels(*args, buf, len(out), ctypes.byref(need)) != CPM_OK:
+        raise NativeError(CPM_EINVAL, "pattern items outside the labels")
+    keys = out.decode("utf-8").split("\n")
+    keys.pop()  # after the last end mark
+    return keys
 
 
 def parse_int_text(ctx, data: bytes, sep: str):

@@ -49,6 +49,9 @@ __host__ __device__ __forceinline__ uint64_t list_words(uint64_t n) { return (n 
 constexpr size_t DEEP_SMEM_PREFIX_MAX = 192 * 1024;
 
 constexpr unsigned long long QUEUE_EMPTY = ~0ull;
+// try_wait rounds for a bulk-staged prefix (a copy of at most 192 KB: micro-
+// seconds); running out is an error, not a normal wait.
+constexpr unsigned long long BULK_WAIT_LIMIT = 1ull << 24;
 constexpr uint32_t NO_PATTERN = 0xffffffffu;
 
 struct DFrame {
@@ -116,13 +119,15 @@ struct DeepParams {
     // Diagnostics (null: off): per unit, UNIT_LOG_WORDS words -- claim,
     // prefix-staged, pass-1-done and end times (globaltimer ns), CTA,
     // siblings | survivors << 32, sibling bytes, largest sibling's bytes,
-    // prefix bytes | list prefix << 63 | top-level << 62.
+    // prefix bytes | list prefix << 63 | top-level << 62, then the times the
+    // survivors were compacted, the child block granted and the children
+    // written (0 for units that end after pass 1).
     // unit_log[0] counts the units logged; records start at unit_log + 1.
     unsigned long long *unit_log;
     unsigned long long unit_log_cap;
 };
 
-constexpr int UNIT_LOG_WORDS = 9;
+constexpr int UNIT_LOG_WORDS = 12;
 
 // Child tidset form: a list when it takes at most 1/P.lists of the dense
 // words (P.lists = 0: bitsets only).
@@ -270,6 +275,41 @@ __device__ __forceinline__ uint32_t sibling_count(unsigned long long sraw, uint3
                                             pb, mk, lane);
 }
 
+// Staging of a dense prefix by the copy engine: thread 0 makes the generic
+// stores it acquired visible to the async proxy, arms the CTA's mbarrier with
+// the byte count and issues cp.async.bulk copies of at most 32 KB from global
+// to shared memory (no multicast: the source is this GPU's own arena).
+__device__ __forceinline__ void bulk_stage(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+    for (uint32_t off = 0; off < bytes; off += 32768u) {
+        const uint32_t n = min(32768u, bytes - off);
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(d + off), "l"(reinterpret_cast<const char *>(src) + off), "r"(n), "r"(b)
+                     : "memory");
+    }
+}
+
+// Bounded wait for the mbarrier phase `parity` to complete; false if it ran out.
+__device__ __forceinline__ bool bulk_wait(uint64_t *bar, uint32_t parity, unsigned long long limit) {
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+    for (unsigned long long i = 0; i < limit; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(b), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
 // Child list piece: the ids of the sibling's transactions that the prefix
 // bitmap holds, over work units [lo, hi) of the sibling (list ids or bitset
 // words), written in ascending order to o32[4 + at ...] (never past sc ids).
@@ -370,7 +410,9 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     __shared__ uint32_t s_part[32];      // per-sibling sums when siblings are split over warps
     __shared__ unsigned long long s_maxb;  // largest sibling's bytes (diagnostics only)
     uint32_t *const s_p32 = reinterpret_cast<uint32_t *>(s_prefix);
-    __shared__ unsigned long long lg[4];   // claim, staged, pass 1 done, prefix word (diagnostics only)
+    __shared__ __align__(8) uint64_t s_bulk_bar;  // completes when a bulk-staged prefix has landed
+    __shared__ unsigned long long lg[7];   // claim, staged, pass 1 done, prefix word, compacted, granted,
+                                           // children written (diagnostics only)
 
     const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     DeepState *st = P.st;
@@ -379,6 +421,12 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         // without one the host must not ask for them.
         if (threadIdx.x == 0 && blockIdx.x == 0) deep_fail(st, DEEP_ERR_INTERNAL);
         return;
+    }
+    __shared__ uint32_t s_bulk_phase;  // parity of s_bulk_bar's next phase
+    if (SMEM_PREFIX && threadIdx.x == 0) {
+        s_bulk_phase = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"((uint32_t)__cvta_generic_to_shared(&s_bulk_bar))
+                     : "memory");
     }
     // Per-CTA statistics (thread 0), added to the global counters at exit.
     // Kept in shared memory, not registers: only thread 0 touches them.
@@ -460,6 +508,19 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             __syncthreads();
             if (mk)
                 for (uint64_t v = threadIdx.x; v < n2; v += blockDim.x) s_prefix[v] = and2(s_prefix[v], ld_cg(mk + v));
+        } else if (SMEM_PREFIX && !mk) {
+            // Dense prefix of a deeper frame: one contiguous arena block,
+            // staged by the copy engine while the threads wait.
+            // (thread 0 flips s_bulk_phase after the barrier below, once every
+            // thread has read it)
+            const uint32_t ph = s_bulk_phase;
+            if (threadIdx.x == 0) bulk_stage(s_prefix, pb, (uint32_t)(16 * n2), &s_bulk_bar);
+            if (!bulk_wait(&s_bulk_bar, ph, BULK_WAIT_LIMIT)) {
+                // Never leave with the copy in flight: record the error, then
+                // wait (bounded again) for it to land.
+                if (threadIdx.x == 0) deep_fail(st, DEEP_ERR_SPIN);
+                bulk_wait(&s_bulk_bar, ph, BULK_WAIT_LIMIT);
+            }
         } else if (SMEM_PREFIX) {
             for (uint64_t v = threadIdx.x; v < n2; v += blockDim.x)
                 s_prefix[v] = mk ? and2(ld_cg(pb + v), ld_cg(mk + v)) : ld_cg(pb + v);
@@ -475,6 +536,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             s_ok = ld_acquire_u32(&st->error) == 0;
         }
         __syncthreads();
+        if (SMEM_PREFIX && threadIdx.x == 0 && !mk && !(praw & 1ull)) s_bulk_phase ^= 1u;
         if (threadIdx.x == 0 && P.unit_log) {
             lg[1] = global_ns();
             lg[3] = prefix_bytes | (SMEM_PREFIX && (praw & 1ull) ? 1ull << 63 : 0ull) | (mk ? 1ull << 62 : 0ull);
@@ -592,7 +654,10 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0 && P.unit_log) lg[2] = global_ns();
+        if (threadIdx.x == 0 && P.unit_log) {
+            lg[2] = global_ns();
+            lg[4] = lg[5] = lg[6] = 0;
+        }
         // Diagnostics record of this unit (thread 0, at its end).
         auto log_unit = [&](uint32_t nsurv) {
             const unsigned long long k = atomicAdd(P.unit_log, 1ull);
@@ -601,6 +666,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             r[0] = lg[0]; r[1] = lg[1]; r[2] = lg[2]; r[3] = global_ns(); r[4] = blockIdx.x;
             r[5] = (unsigned long long)cnt | ((unsigned long long)nsurv << 32);
             r[6] = s_bytes - (lg[3] & ((1ull << 62) - 1)); r[7] = s_maxb; r[8] = lg[3];
+            r[9] = lg[4]; r[10] = lg[5]; r[11] = lg[6];
         };
         if (s_nsurv < 2) {
             // No child frame (the common case): nothing to compact, write or
@@ -656,6 +722,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             s_surv = 0;
         }
         __syncthreads();
+        if (threadIdx.x == 0 && P.unit_log) lg[4] = global_ns();
         const uint32_t ns = s_surv;
         const bool expand = ns >= 2;
         // Words of the survivors' child tidsets (each dense or a list, by its support).
@@ -681,6 +748,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             }
         }
         __syncthreads();
+        if (threadIdx.x == 0 && P.unit_log) lg[5] = global_ns();
         // ---- pass 2: child tidsets of the survivors (only when they recurse) ----
         // Per chunk of up to blockDim survivors: their siblings' work (list
         // ids or bitset words) is laid end to end and each warp takes an
@@ -779,7 +847,10 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 __syncthreads();
             }
             __threadfence();
+            // Child blocks may later be staged by cp.async.bulk (async proxy).
+            asm volatile("fence.proxy.async.global;" ::: "memory");
         }
+        if (threadIdx.x == 0 && P.unit_log) lg[6] = global_ns();
         __syncthreads();
         if (threadIdx.x == 0 && s_grant) {
             const unsigned long long nf = atomicAdd(&st->n_frames, 1ull);

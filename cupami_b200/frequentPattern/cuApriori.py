@@ -355,6 +355,11 @@ class cuApriori:
 
     def getPatterns(self):
         """{tab-joined pattern: support} in the reference's insertion order."""
+        res = self._result
+        if self._patterns is None and res is not None and not any("\n" in label for label in self._labels):
+            # Keys joined in C straight from the result arrays: no tuple per pattern.
+            keys = _native.join_labels(res.offsets, res.items, self._labels)
+            return dict(zip(keys, res.supports.tolist()))
         return dict(zip(map("\t".join, self._finalPatterns), self._finalPatterns.values()))
 
     def getPatternsAsDataFrame(self):

@@ -96,8 +96,8 @@ typedef struct {
                                       memory */
     int32_t  list_div;             /* a tidset is stored as a list when its list takes at most 1/list_div
                                       of its bitset; 0 = the autotuner's choice, else 2 */
-    int32_t  deep_balance;         /* deep-level siblings: 0 = automatic (split over warps by size), 1 = a
-                                      warp per sibling, 2 = split over warps by size */
+    int32_t  deep_balance;         /* deep-level siblings: 0 = automatic (a warp per sibling), 1 = a warp
+                                      per sibling, 2 = split over warps by size */
     int32_t  reserved[1];
 } cpm_opts;
 
@@ -273,6 +273,16 @@ int cpm_periodic_counts(cpm_ctx *ctx, const uint32_t *d_bitsets, uint64_t words3
                         const uint32_t *d_candidates, uint64_t n_candidates, uint32_t width,
                         const int64_t *d_timestamps, uint64_t n_transactions, int64_t end,
                         uint64_t *d_supports, int64_t *d_periods);
+
+/* ---- Pattern keys (host only) ------------------------------------------------
+ * The dict keys of getPatterns() (cuApriori.py:537-539: "\t".join of the
+ * pattern's labels) for a result in CSR form, built in C: pattern k's labels
+ * (labels[label_off[c] .. label_off[c+1]) for column c) joined by `sep`, each
+ * key followed by `end`, written back to back into `out`.  *len gets the bytes
+ * needed; with `out` null or `cap` below it nothing is written. */
+int cpm_join_labels(const uint64_t *offsets, const uint32_t *items, uint64_t n_patterns, const char *labels,
+                    const uint64_t *label_off, uint32_t n_labels, char sep, char end, char *out, uint64_t cap,
+                    uint64_t *len);
 
 /* ---- Delimited text of integer baskets, parsed on the device ----------------
  * Replaces cupami/frequentPattern/_gpu_io.py:34-54 (read_text: cuDF parse of
