@@ -616,12 +616,39 @@ extern "C" int cpm_db_from_ids_batch(cpm_ctx *ctx, uint32_t n_db, const uint64_t
         pres_base[d + 1] = pres_base[d] + (uint64_t)max_id[d] / 32 + 1;
     }
     const uint64_t R = row_base[n_db], NNZ = occ_base[n_db], PW = pres_base[n_db];
-    std::vector<uint64_t> h_off(R + 1);
-    std::vector<uint32_t> h_ids(NNZ);
+    // Every database's rebased offsets and ids, back to back in host memory
+    // the context keeps pinned (reused by later loads), filled in parallel and
+    // sent with two copies.  Without pinned memory: ordinary vectors.
+    const size_t off_bytes = (R + 1) * 8, ids_bytes = NNZ * 4;
+    const size_t stage_bytes = ((off_bytes + 255) & ~(size_t)255) + ids_bytes;
+    std::vector<uint64_t> v_off;
+    std::vector<uint32_t> v_ids;
+    uint64_t *h_off = nullptr;
+    uint32_t *h_ids = nullptr;
+    if (ctx->pinned_bytes < stage_bytes) {
+        if (ctx->pinned) cudaFreeHost(ctx->pinned);
+        ctx->pinned = nullptr;
+        ctx->pinned_bytes = 0;
+        if (cudaHostAlloc(&ctx->pinned, std::max<size_t>(stage_bytes, 16ull << 20), cudaHostAllocDefault) ==
+            cudaSuccess)
+            ctx->pinned_bytes = std::max<size_t>(stage_bytes, 16ull << 20);
+        else
+            cudaGetLastError(), ctx->pinned = nullptr;
+    }
+    if (ctx->pinned) {
+        h_off = static_cast<uint64_t *>(ctx->pinned);
+        h_ids = reinterpret_cast<uint32_t *>(static_cast<unsigned char *>(ctx->pinned) +
+                                             ((off_bytes + 255) & ~(size_t)255));
+    } else {
+        v_off.resize(R + 1);
+        v_ids.resize(NNZ);
+        h_off = v_off.data();
+        h_ids = v_ids.data();
+    }
 #pragma omp parallel for schedule(dynamic, 4)
     for (int64_t d = 0; d < (int64_t)n_db; ++d) {
         for (uint64_t r = 0; r + 1 < off[d].size(); ++r) h_off[row_base[d] + r] = occ_base[d] + off[d][r];
-        if (nnz[d]) memcpy(h_ids.data() + occ_base[d], ids[d], nnz[d] * 4);
+        if (nnz[d]) memcpy(h_ids + occ_base[d], ids[d], nnz[d] * 4);
     }
     h_off[R] = NNZ;
     lap("concatenate");
@@ -633,8 +660,8 @@ extern "C" int cpm_db_from_ids_batch(cpm_ctx *ctx, uint32_t n_db, const uint64_t
     CKR(tmp.alloc(&d_occ, n_db));
     CKR(tmp.alloc(&d_pres_base, n_db));
     CKR(tmp.alloc(&d_present, PW));
-    CK(cudaMemcpyAsync(d_off, h_off.data(), (R + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
-    if (NNZ) CK(cudaMemcpyAsync(d_ids, h_ids.data(), NNZ * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_off, h_off, (R + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    if (NNZ) CK(cudaMemcpyAsync(d_ids, h_ids, NNZ * 4, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(d_occ, occ_base.data(), n_db * 8, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(d_pres_base, pres_base.data(), n_db * 8, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(d_present, 0, PW * 4, ctx->stream));

@@ -273,18 +273,20 @@ def batched_zipf(n_db=512, low=1_000, high=200_000, n_items=200, mean=8, s=1.1,
     its own child seed, so any subset can be regenerated on its own.
     ``limit`` keeps only the first ``limit`` databases.
     """
+    return [batched_zipf_database(i, n_db, low, high, n_items, mean, s, seed)
+            for i in range(n_db if limit is None else min(limit, n_db))]
+
+
+def batched_zipf_database(i, n_db=512, low=1_000, high=200_000, n_items=200, mean=8, s=1.1,
+                          seed=19) -> TransactionCSR:
+    """Database ``i`` of ``batched_zipf`` with the same arguments, on its own."""
     root = np.random.SeedSequence(seed)
     rng = np.random.default_rng(root)
     sizes = np.round(np.exp(rng.uniform(math.log(low), math.log(high), n_db))).astype(np.int64)
-    children = root.spawn(n_db)
-    zipf = _zipf_sampler(n_items, s)
-    out = []
-    for i in range(n_db if limit is None else min(limit, n_db)):
-        r = np.random.default_rng(children[i])
-        lengths = np.clip(r.poisson(mean, int(sizes[i])), 1, n_items)
-        offsets, items = _sample_distinct(r, zipf, lengths)
-        out.append(TransactionCSR(offsets, items, n_items))
-    return out
+    r = np.random.default_rng(root.spawn(n_db)[i])
+    lengths = np.clip(r.poisson(mean, int(sizes[i])), 1, n_items)
+    offsets, items = _sample_distinct(r, _zipf_sampler(n_items, s), lengths)
+    return TransactionCSR(offsets, items, n_items)
 
 
 def reference_uniform_baskets(transactions, items, avg_length=None, seed=None):

@@ -22,18 +22,26 @@ sys.path.insert(0, str(HERE.parents[1]))
 sys.path.insert(0, str(HERE))
 
 
-def main():
+def one(i):
+    """Summary of database i (regenerated from its own seed), mined on one thread."""
     import oracle
     from cupami_b200 import datasets
     from make_sparse_summary import summarize
 
+    csr = datasets.batched_zipf_database(i)
+    labels, (po, pi, ps) = oracle.mine_csr(csr.offsets, csr.items, 0.01, threads=1)
+    s = summarize(labels, po, pi, ps)
+    s["transactions"] = int(np.count_nonzero(np.diff(csr.offsets.astype(np.int64)) > 0))
+    return s
+
+
+def main():
+    import multiprocessing as mp
+    import os
+
     t = time.time()
-    out = []
-    for csr in datasets.batched_zipf():
-        labels, (po, pi, ps) = oracle.mine_csr(csr.offsets, csr.items, 0.01)
-        s = summarize(labels, po, pi, ps)
-        s["transactions"] = int(np.count_nonzero(np.diff(csr.offsets.astype(np.int64)) > 0))
-        out.append(s)
+    with mp.get_context("spawn").Pool(os.cpu_count()) as pool:
+        out = pool.map(one, range(512), chunksize=4)
     doc = {"workload": "batched_zipf(n_db=512, low=1_000, high=200_000, n_items=200, mean=8, s=1.1, seed=19)",
            "minSup": 0.01, "patterns": sum(d["patterns"] for d in out),
            "oracle_seconds": round(time.time() - t, 1), "generator": "tests/golden/make_batched_summary.py",

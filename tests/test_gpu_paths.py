@@ -165,7 +165,7 @@ def test_list_and_bitset_tidsets_agree(oracle_lib, name, minsup):
     csr = getattr(datasets, name)()
     out = []
     for tidsets in (2, 1):
-        for balance in (2, 1):  # siblings split over warps by size, or a warp each
+        for balance in (1, 2):  # a warp per sibling, or siblings split over warps by size
             m = cupami_b200.cuEclat(csr, minsup)
             m._TIDSETS = tidsets
             m._DEEP_BALANCE = balance
