@@ -1085,6 +1085,9 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
         CK(cudaMemcpyAsync(b.st, &s0, sizeof s0, cudaMemcpyHostToDevice, ctx->stream));
         P.shallow = shallow_mode;
         P.balance = ctx->deep_balance;
+        // Next ticket taken early when units are queued: measured 1M x 20k
+        // 768 -> 756 ms, dense 65,536 x 128 0.887 -> 0.844 ms, planted equal.
+        P.prefetch = 1;
         // Queue entries beyond the memset stay stale: bound the round's queue.
         P.queue_cap = std::min<uint64_t>(queue_cap, q.size() * 64 + (1u << 20));
         CK(cudaEventRecord(ctx->ev[2], ctx->stream));
@@ -1656,6 +1659,9 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         }
         P.shallow = 0;
         P.balance = ctx->deep_balance;
+        // Next ticket taken early when units are queued: measured 1M x 20k
+        // 768 -> 756 ms, dense 65,536 x 128 0.887 -> 0.844 ms, planted equal.
+        P.prefetch = 1;
         P.lists = use_lists ? list_div : 0u;
         // Root units claimed once the arena is three-quarters full are handed
         // back and finished in memory-bounded rounds after this launch.
@@ -3176,6 +3182,7 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     P.unit_log = nullptr; P.unit_log_cap = 0;
     P.shallow = 0;
     P.balance = 0;
+    P.prefetch = 0;
     P.lists = 0;
     P.root_frames = 0; P.defer_words = 0; P.defer_members = 0; P.defer_frames = 0; P.defer_queue = 0;
     P.root_key = nullptr; P.top_frames = 0; P.keys_in_words = 0; P.admit_words = 0;

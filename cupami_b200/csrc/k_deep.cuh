@@ -105,6 +105,7 @@ struct DeepParams {
     unsigned long long *cta_time;   // optional [2 * grid]: busy ns, exit time (globaltimer)
     uint32_t shallow;               // 1: child frames are recorded, not queued
     uint32_t balance;               // pass 1: 0 a warp per sibling; 1 siblings split over warps by size
+    uint32_t prefetch;              // 1: take the next queue ticket early when units are waiting
     uint32_t lists;                 // list-form threshold divisor (0: bitsets only; needs SMEM_PREFIX)
     // Memory-bounded rounds: a unit of a frame below root_frames (a root
     // unit) claimed while the arena, the member table or the frame table has
@@ -180,14 +181,26 @@ __device__ __forceinline__ void deep_fail(DeepState *st, unsigned bit) { atomicO
 // then a wait on its own queue entry until a producer fills it, or until no
 // unit is queued or running (the ticket will never be filled), or an error.
 // Returns 0 with *item set, or 1 to stop.
-__device__ int deep_claim(const DeepParams &P, unsigned long long *item) {
+//
+// *next is a ticket taken ahead of time (NO_TICKET: none).  When P.prefetch is
+// set and the claimed entry was already filled (units are queued beyond it),
+// the next ticket is taken right away, so that its atomic overlaps the unit
+// that follows; a CTA that had to wait takes its tickets one at a time, and
+// holds none that a free CTA could have used.
+constexpr unsigned long long NO_TICKET = ~0ull;
+__device__ int deep_claim(const DeepParams &P, unsigned long long *item, unsigned long long *next) {
     DeepState *st = P.st;
-    const unsigned long long h = atomicAdd(&st->q_head, 1ull);
+    const unsigned long long h = *next != NO_TICKET ? *next : atomicAdd(&st->q_head, 1ull);
+    *next = NO_TICKET;
     unsigned backoff = 32;  // ns, doubled up to 2 us while waiting
     for (unsigned long long it = 0; it < P.spin_limit; ++it) {
         if (h < P.queue_cap) {
             const unsigned long long v = ld_acquire_u64(P.queue + h);
-            if (v != QUEUE_EMPTY) { *item = v; return 0; }
+            if (v != QUEUE_EMPTY) {
+                *item = v;
+                if (P.prefetch && it == 0) *next = atomicAdd(&st->q_head, 1ull);
+                return 0;
+            }
         }
         if ((it & 7) == 0) {
             if (ld_acquire_u32(&st->error)) return 1;
@@ -408,7 +421,9 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     __shared__ uint64_t s_off[1025];     // child offsets of one chunk of survivors; pass-1 work offsets
     __shared__ unsigned long long s_raw[1024];  // pass 1 (balanced): sibling pointers of one chunk
     __shared__ uint32_t s_cnt[1024];             // pass 1 (balanced): their supports; pass 2: child supports
-    __shared__ uint64_t s_coff[1024];            // pass 2: arena offsets of one chunk's children
+    __shared__ uint32_t s_coff[1024];            // pass 2: arena offsets (words) of one chunk's children
+    __shared__ uint32_t s_pid[1024];             // units of at most blockDim siblings: pattern id of each
+    __shared__ uint16_t s_map[1024];             // ... and, after compaction, each survivor's sibling index
     __shared__ uint32_t s_clast[32];             // pass 2: ids in each warp's last piece of a split child
     __shared__ unsigned long long s_bytes;
     __shared__ uint32_t s_nsurv;         // survivors counted in pass 1
@@ -438,9 +453,10 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     __shared__ unsigned long long c_inter, c_bytes, c_units, c_surv, c_busy, t_unit;
     if (threadIdx.x == 0) c_inter = c_bytes = c_units = c_surv = c_busy = t_unit = 0;
 
+    unsigned long long next_ticket = NO_TICKET;  // thread 0's ticket taken ahead
     for (;;) {
         if (threadIdx.x == 0) {
-            s_stop = deep_claim(P, &s_item);
+            s_stop = deep_claim(P, &s_item, &next_ticket);
             s_skip = 0;
             bool hand_back = false;
             if (!s_stop && P.defer_words && (uint32_t)(s_item >> 32) < P.root_frames) {
@@ -496,6 +512,11 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         const long long minsup = __ldcg(&fp->minsup);
         const uint64_t n2 = stride / 2;
         const uint32_t cnt = m - p - 1;
+        // Units of at most blockDim siblings keep every sibling's pointer,
+        // support and pattern id in shared memory (s_raw, s_cnt, s_pid) and
+        // reserve and write member entries for their survivors only, once
+        // compacted; larger units reserve and write an entry per sibling.
+        const bool fast = cnt <= blockDim.x;
         const unsigned long long praw = ld_raw_ptr(P.mem_bits + mem_off + p);
         const ulonglong2 *pb = reinterpret_cast<const ulonglong2 *>(praw);
         uint64_t prefix_bytes = 8ull * stride;
@@ -535,9 +556,12 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             s_surv = 0;
             s_nsurv = 0;
             s_grant = 0;
-            const unsigned long long mb = atomicAdd(&st->n_members, (unsigned long long)cnt);
-            if (mb + cnt > P.members_cap) deep_fail(st, DEEP_ERR_MEMBERS);
-            s_mem_base = mb;
+            s_mem_base = 0;
+            if (!fast) {
+                const unsigned long long mb = atomicAdd(&st->n_members, (unsigned long long)cnt);
+                if (mb + cnt > P.members_cap) deep_fail(st, DEEP_ERR_MEMBERS);
+                s_mem_base = mb;
+            }
             s_ok = ld_acquire_u32(&st->error) == 0;
         }
         __syncthreads();
@@ -566,7 +590,11 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                     pid32 = (uint32_t)pid;
                 }
             }
-            if (m_out < P.members_cap) {
+            if (fast) {
+                s_raw[q] = sraw;
+                s_cnt[q] = s;
+                s_pid[q] = pid32;
+            } else if (m_out < P.members_cap) {
                 P.mem_pat[m_out] = pid32;
                 P.mem_item[m_out] = sib_item;
                 P.mem_bits[m_out] = reinterpret_cast<const uint64_t *>(sraw);
@@ -692,7 +720,35 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         // Survivors move to the front of the block in member order, so every
         // child frame keeps its members sorted by column (the pattern tree is
         // then a prefix tree: a pattern's parent is itself minus its last item).
-        if (ok && s_mem_base + cnt <= P.members_cap) {
+        if (fast && ok) {
+            const uint32_t q = threadIdx.x;
+            const bool keep = q < cnt && s_pid[q] != NO_PATTERN;
+            const unsigned bal = __ballot_sync(CPM_FULL, keep);
+            if (lane == 0) s_wtot[wid] = __popc(bal);
+            __syncthreads();
+            uint32_t before = 0, total = 0;
+            for (unsigned w = 0; w < nw; ++w) {
+                if (w < wid) before += s_wtot[w];
+                total += s_wtot[w];
+            }
+            if (threadIdx.x == 0) {
+                s_surv = 0;
+                const unsigned long long mb = atomicAdd(&st->n_members, (unsigned long long)total);
+                if (mb + total > P.members_cap) {
+                    deep_fail(st, DEEP_ERR_MEMBERS);
+                } else {
+                    s_mem_base = mb;
+                    s_surv = total;
+                }
+            }
+            __syncthreads();
+            if (keep && s_surv) {
+                const uint32_t pos = before + __popc(bal & ((1u << lane) - 1));
+                s_map[pos] = (uint16_t)q;
+                P.mem_pat[s_mem_base + pos] = s_pid[q];
+                P.mem_item[s_mem_base + pos] = __ldcg(P.mem_item + mem_off + p + 1 + q);
+            }
+        } else if (ok && s_mem_base + cnt <= P.members_cap) {
             uint32_t base = 0;
             for (uint32_t start = 0; start < cnt; start += blockDim.x) {
                 const uint32_t q = start + threadIdx.x;
@@ -732,7 +788,36 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         const bool expand = ns >= 2;
         // Words of the survivors' child tidsets (each dense or a list, by its support).
         uint64_t child_words = (uint64_t)ns * stride;
-        if (expand && P.lists) {
+        uint64_t fast_wtot = 0;
+        if (fast && expand) {
+            // The survivors' siblings and supports, moved to their compacted
+            // places, with their child offsets and work offsets from one scan
+            // (child words in the high half, work units in the low half: each
+            // sum stays below 2^32).
+            const uint32_t i = threadIdx.x;
+            unsigned long long raw = 0;
+            uint32_t sc = 0;
+            uint64_t sz = 0, wk = 0;
+            if (i < ns) {
+                const uint32_t q = s_map[i];
+                raw = s_raw[q];
+                sc = s_cnt[q];
+                sz = (SMEM_PREFIX && as_list(P, sc, stride)) ? list_words(sc) : stride;
+                wk = sibling_units<SMEM_PREFIX>(raw, n2);
+            }
+            uint64_t tot = 0;
+            const uint64_t ex = block_excl_scan_u64((sz << 32) | wk, s_w64, &tot);
+            if (i < ns) {
+                s_raw[i] = raw;
+                s_cnt[i] = sc;
+                s_coff[i] = (uint32_t)(ex >> 32);
+                s_off[i] = ex & 0xffffffffull;
+            }
+            if (i == 0) s_off[ns] = tot & 0xffffffffull;
+            if (threadIdx.x < 32) s_clast[threadIdx.x] = 0;
+            child_words = tot >> 32;
+            fast_wtot = tot & 0xffffffffull;
+        } else if (expand && P.lists) {
             uint64_t part = 0;
             for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) {
                 const uint32_t sc = __ldcg(P.pat_sup + __ldcg(P.mem_pat + s_mem_base + i));
@@ -766,6 +851,8 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             uint64_t chunk_base = 0;
             for (uint32_t start = 0; start < ns; start += blockDim.x) {
                 const uint32_t cn = min((uint32_t)blockDim.x, ns - start);
+                uint64_t ctot = 0, wtot = fast_wtot;
+                if (!fast) {
                 uint64_t sz = 0, wk = 0;
                 if (threadIdx.x < cn) {
                     const uint64_t m_out = s_mem_base + start + threadIdx.x;
@@ -776,15 +863,15 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                     s_raw[threadIdx.x] = raw;
                     s_cnt[threadIdx.x] = sc;
                 }
-                uint64_t ctot = 0, wtot = 0;
                 const uint64_t cex = block_excl_scan_u64(sz, s_w64, &ctot);
                 const uint64_t wex = block_excl_scan_u64(wk, s_w64, &wtot);
                 if (threadIdx.x < cn) {
-                    s_coff[threadIdx.x] = chunk_base + cex;
+                    s_coff[threadIdx.x] = (uint32_t)(chunk_base + cex);
                     s_off[threadIdx.x] = wex;
                 }
                 if (threadIdx.x == 0) s_off[cn] = wtot;
                 if (threadIdx.x < 32) s_clast[threadIdx.x] = 0;
+                }
                 __syncthreads();
                 const uint64_t lo = wtot * wid / nw, hi = wtot * (wid + 1) / nw;
                 uint32_t first = cn;  // first child whose work ends past lo
