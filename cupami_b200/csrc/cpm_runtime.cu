@@ -2561,14 +2561,18 @@ static int result_copy(const cpm_result *res, int order, uint64_t *offsets, uint
         std::vector<uint64_t> roots;
         for (uint64_t k = 0; k < n; ++k)
             if (par[k] == 0xffffffffu) roots.push_back(k);
-            else coff[par[k] + 1]++;
+#pragma omp parallel for schedule(static, 65536)
+        for (int64_t k = 0; k < (int64_t)n; ++k)
+            if (par[k] != 0xffffffffu) __atomic_fetch_add(&coff[par[k] + 1], 1ull, __ATOMIC_RELAXED);
         for (uint64_t k = 0; k < n; ++k) coff[k + 1] += coff[k];
         if (kids_s.size() < coff[n] + 1) kids_s.resize(coff[n] + 1);
         if (fill_s.size() < n + 1) fill_s.resize(n + 1);
         uint64_t *kids = kids_s.data(), *fill = fill_s.data();
         std::copy(coff, coff + n, fill);
-        for (uint64_t k = 0; k < n; ++k)
-            if (par[k] != 0xffffffffu) kids[fill[par[k]]++] = k;
+        // Children in any order here: every list is sorted by item below.
+#pragma omp parallel for schedule(static, 65536)
+        for (int64_t k = 0; k < (int64_t)n; ++k)
+            if (par[k] != 0xffffffffu) kids[__atomic_fetch_add(&fill[par[k]], 1ull, __ATOMIC_RELAXED)] = (uint64_t)k;
         lap("children");
         auto by_item = [&](uint64_t a, uint64_t b) { return itm[a] < itm[b]; };
         std::sort(roots.begin(), roots.end(), by_item);
@@ -2602,9 +2606,36 @@ static int result_copy(const cpm_result *res, int order, uint64_t *offsets, uint
                     for (uint64_t c = coff[r]; c < coff[r + 1]; ++c) pairs.push_back(kids[c]);
                 for (uint64_t q : pairs) idx[w++] = q;
             }
-            std::vector<std::pair<uint64_t, uint64_t>> stack;  // (node, next child to descend)
-            for (uint64_t q : pairs) {
-                for (uint64_t c = coff[q]; c < coff[q + 1]; ++c) idx[w++] = kids[c];
+            // Every pair's descendants take a contiguous range of the order:
+            // descendant counts bottom up (deepest level first; parents
+            // precede children, so the levels are the depths), then each
+            // pair's range is walked on its own thread.
+            std::vector<uint64_t> desc(n, 0);
+            uint32_t max_depth = 0;
+            for (uint64_t k = 0; k < n; ++k) max_depth = std::max(max_depth, depth[k]);
+            std::vector<uint64_t> doff(max_depth + 2, 0), dnode(n);
+            for (uint64_t k = 0; k < n; ++k) ++doff[depth[k] + 1];
+            for (uint32_t d = 0; d <= max_depth; ++d) doff[d + 1] += doff[d];
+            {
+                std::vector<uint64_t> dfill(doff.begin(), doff.end() - 1);
+                for (uint64_t k = 0; k < n; ++k) dnode[dfill[depth[k]]++] = k;
+            }
+            for (uint32_t d = max_depth; d >= 2; --d) {
+#pragma omp parallel for schedule(static, 16384)
+                for (int64_t i = (int64_t)doff[d]; i < (int64_t)doff[d + 1]; ++i) {
+                    const uint64_t k = dnode[i];
+                    __atomic_fetch_add(&desc[par[k]], desc[k] + 1, __ATOMIC_RELAXED);
+                }
+            }
+            std::vector<uint64_t> pstart(pairs.size() + 1, w);
+            for (size_t i = 0; i < pairs.size(); ++i) pstart[i + 1] = pstart[i] + desc[pairs[i]];
+            if (pstart[pairs.size()] != n) return CPM_EINTERNAL;
+#pragma omp parallel for schedule(dynamic, 1)
+            for (int64_t i = 0; i < (int64_t)pairs.size(); ++i) {
+                std::vector<std::pair<uint64_t, uint64_t>> stack;  // (node, next child to descend)
+                uint64_t at = pstart[i];
+                const uint64_t q = pairs[i];
+                for (uint64_t c = coff[q]; c < coff[q + 1]; ++c) idx[at++] = kids[c];
                 stack.push_back({q, coff[q]});
                 while (!stack.empty()) {
                     auto &top = stack.back();
@@ -2613,10 +2644,11 @@ static int result_copy(const cpm_result *res, int order, uint64_t *offsets, uint
                         continue;
                     }
                     const uint64_t child = kids[top.second++];
-                    for (uint64_t c = coff[child]; c < coff[child + 1]; ++c) idx[w++] = kids[c];
+                    for (uint64_t c = coff[child]; c < coff[child + 1]; ++c) idx[at++] = kids[c];
                     stack.push_back({child, coff[child]});
                 }
             }
+            w = n;
         }
         if (w != n) return CPM_EINTERNAL;
     } else if (order != CPM_ORDER_NONE || !prefix_tree) {
@@ -2659,8 +2691,27 @@ static int result_copy(const cpm_result *res, int order, uint64_t *offsets, uint
         }
     }
     lap("order");
+    // offsets: exclusive sum of the depths in order (two parallel passes)
     offsets[0] = 0;
-    for (uint64_t r = 0; r < n; ++r) offsets[r + 1] = offsets[r] + depth[idx[r]];
+    {
+        const int64_t chunk = 1 << 18, nc = (int64_t)((n + chunk - 1) / chunk);
+        std::vector<uint64_t> part(nc + 1, 0);
+#pragma omp parallel for schedule(static)
+        for (int64_t c = 0; c < nc; ++c) {
+            uint64_t sum = 0;
+            for (int64_t r = c * chunk; r < std::min<int64_t>((int64_t)n, (c + 1) * chunk); ++r) sum += depth[idx[r]];
+            part[c + 1] = sum;
+        }
+        for (int64_t c = 0; c < nc; ++c) part[c + 1] += part[c];
+#pragma omp parallel for schedule(static)
+        for (int64_t c = 0; c < nc; ++c) {
+            uint64_t sum = part[c];
+            for (int64_t r = c * chunk; r < std::min<int64_t>((int64_t)n, (c + 1) * chunk); ++r) {
+                sum += depth[idx[r]];
+                offsets[r + 1] = sum;
+            }
+        }
+    }
     lap("offsets");
 #pragma omp parallel for schedule(static, 65536)
     for (int64_t r = 0; r < (int64_t)n; ++r) {

@@ -517,6 +517,15 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         // reserve and write member entries for their survivors only, once
         // compacted; larger units reserve and write an entry per sibling.
         const bool fast = cnt <= blockDim.x;
+        // Fewer siblings than warps: split every sibling into equal slices
+        // (at least 4 KB of bitset each) so that every warp has work.
+        const uint32_t parts = (cnt && cnt < nw) ? max(1u, min(nw / cnt, (uint32_t)(n2 >> 8))) : 1u;
+        // Each warp's first sibling pointer is loaded now and its list
+        // header after the staging, so that their latency overlaps it.
+        const uint32_t first_q = parts == 1 ? wid : wid / parts;
+        unsigned long long first_raw = 0;
+        uint64_t first_units = 0;
+        if (!P.balance && first_q < cnt) first_raw = ld_raw_ptr(P.mem_bits + mem_off + p + 1 + first_q);
         const unsigned long long praw = ld_raw_ptr(P.mem_bits + mem_off + p);
         const ulonglong2 *pb = reinterpret_cast<const ulonglong2 *>(praw);
         uint64_t prefix_bytes = 8ull * stride;
@@ -551,6 +560,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             for (uint64_t v = threadIdx.x; v < n2; v += blockDim.x)
                 s_prefix[v] = mk ? and2(ld_cg(pb + v), ld_cg(mk + v)) : ld_cg(pb + v);
         }
+        if (!P.balance && first_q < cnt) first_units = sibling_units<SMEM_PREFIX>(first_raw, n2);
         if (threadIdx.x == 0) {
             s_bytes = prefix_bytes;
             s_surv = 0;
@@ -601,9 +611,6 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             }
             if (pid32 != NO_PATTERN) atomicAdd(&s_nsurv, 1u);
         };
-        // Fewer siblings than warps: split every sibling into equal slices
-        // (at least 4 KB of bitset each) so that every warp has work.
-        const uint32_t parts = (cnt && cnt < nw) ? max(1u, min(nw / cnt, (uint32_t)(n2 >> 8))) : 1u;
         if (P.balance) {
             // Siblings split over warps by size.  Per chunk of up to blockDim
             // siblings: every sibling's work (bitset words or list ids) is
@@ -654,10 +661,12 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         } else if (parts == 1) {
             for (uint32_t q = wid; ok && q < cnt; q += nw) {
                 const uint64_t mi = mem_off + p + 1 + q;
-                const unsigned long long sraw = ld_raw_ptr(P.mem_bits + mi);
+                const bool first = q == wid;
+                const unsigned long long sraw = first ? first_raw : ld_raw_ptr(P.mem_bits + mi);
                 const uint32_t sib_item = __ldcg(P.mem_item + mi);
-                uint64_t b = 0;
-                uint32_t s = sibling_count<SMEM_PREFIX>(sraw, 0, 1, n2, s_prefix, s_p32, pb, mk, lane, &b);
+                const uint64_t units = first ? first_units : sibling_units<SMEM_PREFIX>(sraw, n2);
+                const uint64_t b = sibling_bytes<SMEM_PREFIX>(sraw, units);
+                uint32_t s = sibling_count_range<SMEM_PREFIX>(sraw, 0, units, s_prefix, s_p32, pb, mk, lane);
                 s = warp_sum_u32(s);
                 if (lane == 0) {
                     atomicAdd(&s_bytes, (unsigned long long)b);
@@ -669,10 +678,12 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             if (threadIdx.x < 32) s_part[threadIdx.x] = 0;
             __syncthreads();
             for (uint32_t it = wid; ok && it < cnt * parts; it += nw) {
-                const uint32_t q = it / parts, j = it - q * parts;
-                const unsigned long long sraw = ld_raw_ptr(P.mem_bits + mem_off + p + 1 + q);
-                uint64_t b = 0;
-                uint32_t s = sibling_count<SMEM_PREFIX>(sraw, j, parts, n2, s_prefix, s_p32, pb, mk, lane, &b);
+                const uint32_t q = it / parts, j = it - q * parts;  // q == first_q: one part per warp
+                const unsigned long long sraw = first_raw;
+                const uint64_t units = first_units;
+                const uint64_t b = sibling_bytes<SMEM_PREFIX>(sraw, units);
+                uint32_t s = sibling_count_range<SMEM_PREFIX>(sraw, units * j / parts, units * (j + 1) / parts,
+                                                              s_prefix, s_p32, pb, mk, lane);
                 s = warp_sum_u32(s);
                 if (lane == 0) {
                     atomicAdd(&s_part[q], s);
