@@ -162,16 +162,18 @@ __global__ void __launch_bounds__(tc::THREADS, 1)
             g < F ? reinterpret_cast<const ulonglong2 *>(bits + (uint64_t)freq[g] * stride + kw_begin) : nullptr;
         const uint32_t atom = row >> 3, rr = row & 7;
         const uint32_t row_off = (is_a ? 0u : (uint32_t)A_BYTES) + atom * 1024u + rr * 128u;
-        // Loads run two stages ahead of the expansion, so that their latency
-        // overlaps the wait for a free stage and the expansion before it.
+        // Loads run three stages ahead of the expansion, so that their latency
+        // overlaps the wait for a free stage and the expansions before it.
         const ulonglong2 zero = make_ulonglong2(0, 0);
-        ulonglong2 w_next = (src && n_k > 0) ? src[0] : zero;
-        ulonglong2 w_after = (src && n_k > 1) ? src[1] : zero;
+        ulonglong2 w1 = (src && n_k > 0) ? src[0] : zero;
+        ulonglong2 w2 = (src && n_k > 1) ? src[1] : zero;
+        ulonglong2 w3 = (src && n_k > 2) ? src[2] : zero;
         for (uint32_t kt = 0; kt < n_k; ++kt) {
             const uint32_t s = kt % STAGES, ph = (kt / STAGES) & 1u;
-            const ulonglong2 w = w_next;
-            w_next = w_after;
-            w_after = (src && kt + 2 < n_k) ? src[kt + 2] : zero;
+            const ulonglong2 w = w1;
+            w1 = w2;
+            w2 = w3;
+            w3 = (src && kt + 3 < n_k) ? src[kt + 3] : zero;
             if (!tc::mbar_wait(tc::smem_u32(&empty_bar[s]), ph ^ 1u, abort)) break;
             unsigned char *dst = smem + (uint32_t)s * STAGE_BYTES + row_off;
 #pragma unroll
