@@ -910,7 +910,7 @@ def run_ours(args, world, rank, local):
                 "peak_source": src, "frac_of": "HBM copy bandwidth (" + src + "); algorithmic bytes / kernel time",
                 "frac_of_8tbs_spec": achieved / 8000.0,
                 "dram_share_of_alg_bytes": traffic / deep_bytes if traffic and deep_bytes else None,
-                "l2_throughput_pct": tr.get("l2_throughput_pct") if tr else None,
+                "l2_bytes_per_launch": tr.get("l2_bytes_per_launch") if tr else None,
                 "traffic_source": ("profiles/k_deep_traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum "
                                    "of one launch): " + tr["profile"]) if tr else None,
                 "ms_per_launch": deep_ms, "alg_bytes_per_launch": deep_bytes,

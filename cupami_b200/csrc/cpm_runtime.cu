@@ -1954,11 +1954,29 @@ struct LevelScratch {
 // k-subsets are in the level (slot 7).  One host round trip: n_pairs is the
 // candidate count (0: the search is over) and n_pat the pattern count so far
 // (d_cnt2[1]).  Scratch slots 0-7 are used.
+// Levels of at most this many rows (and candidate sets of at most this many)
+// go through the one-CTA kernels k_level_prep / k_level_keep.
+constexpr uint64_t APRIORI_SMALL_LEVEL = 65536;
+
 static int level_join(cpm_ctx *ctx, LevelScratch &scratch, DevScope &lvl, const uint32_t *L, uint64_t n_ub,
                       const uint64_t *d_cnt2, uint32_t k, uint64_t *d_tot, uint64_t &n_pairs, uint64_t &n_pat,
                       uint32_t *&cand, uint32_t *&left, uint32_t *&okf, uint64_t &launches) {
     uint32_t *gflag = nullptr, *partners = nullptr;
     uint64_t *gid = nullptr, *gfirst = nullptr, *poff = nullptr;
+    if (n_ub <= APRIORI_SMALL_LEVEL) {
+        // One CTA does the prefix groups, the partners and their sum.
+        CKR(scratch.get(2, &partners, n_ub));
+        CKR(scratch.get(3, &poff, n_ub));
+        k_level_prep<<<1, 1024, 0, ctx->stream>>>(L, n_ub, d_cnt2, k, partners, poff, d_tot);
+        CK(cudaGetLastError());
+        uint64_t counts[3] = {0, 0, 0};
+        CK(cudaMemcpyAsync(counts, d_cnt2, 16, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(counts + 2, d_tot, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        n_pat = counts[1];
+        n_pairs = counts[2];
+        launches += 1;
+    } else {
     CKR(scratch.get(0, &gflag, n_ub));
     CKR(scratch.get(1, &gid, n_ub));
     CKR(scratch.get(2, &partners, n_ub));
@@ -1977,6 +1995,7 @@ static int level_join(cpm_ctx *ctx, LevelScratch &scratch, DevScope &lvl, const 
     CKR(scan_u32(ctx, lvl, partners, poff, n_ub, &n_pairs, d_tot));  // synchronises: counts are in
     n_pat = counts[1];
     launches += 7;
+    }
     cand = left = okf = nullptr;
     if (!n_pairs) return CPM_OK;
     CKR(scratch.get(5, &cand, n_pairs * (k + 1)));
@@ -2101,20 +2120,27 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
                 st.bytes_alg += n_pairs * w * db->stride * 8;
             }
             CK(cudaGetLastError());
-            CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, nullptr, d_tot));
-            st.kernel_launches += 3;
+            if (n_pairs > APRIORI_SMALL_LEVEL) CKR(scan_u32(ctx, lvl, pass, pos, n_pairs, nullptr, d_tot));
+            st.kernel_launches += n_pairs > APRIORI_SMALL_LEVEL ? 3 : 1;
             st.intersections += n_pairs * (w - 1);
             // Survivors: at most n_pairs rows and patterns.
             uint32_t *L2 = nullptr, *pid2 = nullptr;
             CKR(patterns_reserve(ctx, pa, n_pat, pat_ub + n_pairs));
             CKR(dalloc(ctx, &L2, n_pairs * w));
             CKR(dalloc(ctx, &pid2, n_pairs));
-            k_apriori_keep<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(
-                cand, left, sup, pass, pos, n_pairs, w, pid, d_cnt2 + 1, L2, pid2, pa.parent, pa.item, pa.sup);
-            CK(cudaGetLastError());
-            k_level_close<<<1, 1, 0, ctx->stream>>>(pos, pass, n_pairs, d_cnt2, d_cnt2 + 1);
-            CK(cudaGetLastError());
-            st.kernel_launches += 2;
+            if (n_pairs <= APRIORI_SMALL_LEVEL) {
+                k_level_keep<<<1, 1024, 0, ctx->stream>>>(cand, left, sup, pass, n_pairs, w, pid, d_cnt2, L2, pid2,
+                                                          pa.parent, pa.item, pa.sup);
+                CK(cudaGetLastError());
+                st.kernel_launches += 1;
+            } else {
+                k_apriori_keep<<<(unsigned)((n_pairs + 255) / 256), 256, 0, ctx->stream>>>(
+                    cand, left, sup, pass, pos, n_pairs, w, pid, d_cnt2 + 1, L2, pid2, pa.parent, pa.item, pa.sup);
+                CK(cudaGetLastError());
+                k_level_close<<<1, 1, 0, ctx->stream>>>(pos, pass, n_pairs, d_cnt2, d_cnt2 + 1);
+                CK(cudaGetLastError());
+                st.kernel_launches += 2;
+            }
             dfree(ctx, L);
             dfree(ctx, pid);
             L = L2;
@@ -2752,15 +2778,24 @@ extern "C" int cpm_results_copy(cpm_result *const *res, uint32_t n, int order, u
     for (uint32_t k = 0; k < n; ++k)
         if (!res[k] || cpm_result_size(res[k], &sizes[2 * k], &sizes[2 * k + 1]) != CPM_OK) return CPM_EINVAL;
     if (!offsets || !supports) return CPM_OK;
-    uint64_t o = 0, it = 0, sp = 0;
+    // Every result's place in the outputs first, then the results ordered in
+    // parallel (each ordering keeps its scratch per thread).
+    std::vector<uint64_t> o(n + 1, 0), it(n + 1, 0), sp(n + 1, 0);
     for (uint32_t k = 0; k < n; ++k) {
-        const int r = cpm_result_copy(res[k], order, offsets + o, items ? items + it : nullptr, supports + sp);
-        if (r != CPM_OK) return r;
-        o += sizes[2 * k] + 1;
-        it += sizes[2 * k + 1];
-        sp += sizes[2 * k];
+        o[k + 1] = o[k] + sizes[2 * k] + 1;
+        it[k + 1] = it[k] + sizes[2 * k + 1];
+        sp[k + 1] = sp[k] + sizes[2 * k];
     }
-    return CPM_OK;
+    int status = CPM_OK;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t k = 0; k < (int64_t)n; ++k) {
+        const int r = cpm_result_copy(res[k], order, offsets + o[k], items ? items + it[k] : nullptr, supports + sp[k]);
+        if (r != CPM_OK) {
+#pragma omp critical
+            status = r;
+        }
+    }
+    return status;
 }
 
 extern "C" int cpm_result_from_tree(const int64_t *parent, const uint32_t *item, const uint64_t *support,

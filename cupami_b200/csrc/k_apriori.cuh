@@ -195,6 +195,120 @@ __global__ void __launch_bounds__(256) k_count_grouped(const uint64_t *__restric
     if (!lane && rows_read) atomicAdd(bytes_alg, rows_read * 8ull * stride);
 }
 
+// ---- one-CTA forms for small levels (fewer launches per level) ----
+
+// Exclusive sum over a CTA of up to 1024 threads (every thread calls it);
+// *total gets the CTA's sum.  s_w holds 32 partial sums.
+__device__ __forceinline__ uint64_t cta_excl_sum(uint64_t v, uint64_t *s_w, uint64_t *total) {
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint64_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(CPM_FULL, incl, o);
+        if (lane >= (unsigned)o) incl += y;
+    }
+    if (lane == 31) s_w[wid] = incl;
+    __syncthreads();
+    uint64_t before = 0, tot = 0;
+    for (unsigned w = 0; w < nw; ++w) {
+        if (w < wid) before += s_w[w];
+        tot += s_w[w];
+    }
+    __syncthreads();
+    *total = tot;
+    return before + incl - v;
+}
+
+// The join partners of every row of a level and their exclusive sum, in one
+// CTA (what k_group_start, the group scan, k_group_first, k_partners and the
+// partner scan do in five launches).  A row's partners are the later rows of
+// its prefix group: from the row up to the next row that starts a group
+// (whose first k-1 items differ from its predecessor's), found last chunk
+// first with a suffix minimum.  *n_pairs gets the candidate count; rows at or
+// past *d_n (up to n_ub) have no partners.
+__global__ void __launch_bounds__(1024) k_level_prep(const uint32_t *__restrict__ L, uint64_t n_ub,
+                                                     const uint64_t *__restrict__ d_n, uint32_t k,
+                                                     uint32_t *__restrict__ partners, uint64_t *__restrict__ poff,
+                                                     uint64_t *__restrict__ n_pairs) {
+    __shared__ uint64_t s_w[32];
+    __shared__ uint64_t s_carry;
+    const unsigned lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint64_t n = *d_n;
+    if (threadIdx.x == 0) s_carry = n;
+    __syncthreads();
+    const int64_t chunks = (int64_t)((n + blockDim.x - 1) / blockDim.x);
+    for (int64_t c = chunks - 1; c >= 0; --c) {
+        const uint64_t a = (uint64_t)c * blockDim.x + threadIdx.x;
+        // the smallest group start after row a, within this chunk's rows
+        uint64_t m = (a + 1 < n && cmp_rows(L + a * k, L + (a + 1) * k, k - 1)) ? a + 1 : ~0ull;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_down_sync(CPM_FULL, m, o);
+            if (lane + o < 32) m = min(m, y);
+        }
+        if (lane == 0) s_w[wid] = m;
+        __syncthreads();
+        uint64_t end = min(m, s_carry);
+        for (unsigned w = wid + 1; w < nw; ++w) end = min(end, s_w[w]);
+        if (a < n) partners[a] = (uint32_t)(end - a - 1);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint64_t cm = s_carry;
+            for (unsigned w = 0; w < nw; ++w) cm = min(cm, s_w[w]);
+            s_carry = cm;
+        }
+        __syncthreads();
+    }
+    for (uint64_t a = n + threadIdx.x; a < n_ub; a += blockDim.x) partners[a] = 0;
+    __syncthreads();
+    uint64_t run = 0;
+    for (uint64_t base = 0; base < n; base += blockDim.x) {
+        const uint64_t a = base + threadIdx.x;
+        const uint64_t v = a < n ? partners[a] : 0;
+        uint64_t tot = 0;
+        const uint64_t ex = cta_excl_sum(v, s_w, &tot);
+        if (a < n) poff[a] = run + ex;
+        run += tot;
+    }
+    if (threadIdx.x == 0) *n_pairs = run;
+}
+
+// k_apriori_keep and k_level_close with the scan of the pass flags, in one
+// CTA: survivors become the next level's rows and pattern records, in
+// candidate order, and the level's row and pattern counts move on.
+__global__ void __launch_bounds__(1024) k_level_keep(const uint32_t *__restrict__ cand,
+                                                     const uint32_t *__restrict__ cand_left,
+                                                     const uint32_t *__restrict__ sup,
+                                                     const uint32_t *__restrict__ pass, uint64_t n, uint32_t w,
+                                                     const uint32_t *__restrict__ pid_prev, uint64_t *__restrict__ d_cnt2,
+                                                     uint32_t *__restrict__ L_next, uint32_t *__restrict__ pid_next,
+                                                     uint32_t *__restrict__ pat_parent, uint32_t *__restrict__ pat_item,
+                                                     uint32_t *__restrict__ pat_sup) {
+    __shared__ uint64_t s_w[32];
+    const uint64_t pid_base = d_cnt2[1];
+    uint64_t run = 0;
+    for (uint64_t base = 0; base < n; base += blockDim.x) {
+        const uint64_t i = base + threadIdx.x;
+        const uint32_t f = i < n ? pass[i] : 0u;
+        uint64_t tot = 0;
+        const uint64_t p = run + cta_excl_sum(f, s_w, &tot);
+        if (f) {
+            for (uint32_t j = 0; j < w; ++j) L_next[p * w + j] = cand[i * w + j];
+            const uint64_t pid = pid_base + p;
+            pid_next[p] = (uint32_t)pid;
+            pat_parent[pid] = pid_prev[cand_left[i]];
+            pat_item[pid] = cand[i * w + w - 1];
+            pat_sup[pid] = sup[i];
+        }
+        run += tot;
+    }
+    __syncthreads();  // every thread has read d_cnt2[1]
+    if (threadIdx.x == 0) {
+        d_cnt2[0] = run;
+        d_cnt2[1] = pid_base + run;
+    }
+}
+
 // Survivors, in candidate order, become the next level and pattern records.
 __global__ void k_apriori_keep(const uint32_t *__restrict__ cand, const uint32_t *__restrict__ cand_left,
                                const uint32_t *__restrict__ sup, const uint32_t *__restrict__ flag,
