@@ -1332,8 +1332,10 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
                     (o.tidsets == 2 || biggest > (uint64_t)ctx->l2_bytes / 2);
     }
     // A tidset becomes a list when its list takes at most 1/list_div of its
-    // bitset (set by the options or the autotuner; 2 by default).
-    uint32_t list_div = o.list_div > 0 ? (uint32_t)o.list_div : 2u;
+    // bitset (set by the options or the autotuner; 1 by default: measured on
+    // the 1M x 20k workload, deep phase 740 / 752 / 851 ms for divisors
+    // 1 / 2 / 4).
+    uint32_t list_div = o.list_div > 0 ? (uint32_t)o.list_div : 1u;
     if (o.tidsets == 0 && !o.list_div && o.autotune) {
         const auto it = ctx->tune_lists.find(63 - __builtin_clzll(std::max<uint64_t>(1, max_stride)));
         if (it != ctx->tune_lists.end()) {
@@ -2192,11 +2194,20 @@ static int mine_apriori(cpm_ctx *ctx, cpm_db *db, long long ms, const cpm_opts &
 // (CPM_ORDER_DEPTH_FIRST for cuPFEclat, CPM_ORDER_APRIORI for cuPFApriori).
 // Warps per candidate for k_periodic: enough for about 32 resident warps per
 // SM when a level has few candidates, at most one per step of a row.
+// Candidates are split into parts (segments of their rows, joined by
+// k_periodic_join): levels of few candidates into enough parts to fill the
+// GPU, and every other level into PERIODIC_OVERSPLIT parts, so that the
+// densest candidates (pairs of the most frequent items hold tens of thousands
+// of rows, against a few hundred on average) do not leave a tail of single
+// warps walking their rows.
+constexpr uint64_t PERIODIC_OVERSPLIT = 4;
+
 static uint32_t periodic_parts(const cpm_ctx *ctx, uint64_t n, uint64_t words) {
     const uint64_t tiles = (words + PERIODIC_TILE - 1) / PERIODIC_TILE;
     const uint64_t target = (uint64_t)ctx->sms * 32;
-    if (!n || n >= target || tiles <= 1) return 1;
-    return (uint32_t)std::min<uint64_t>(std::min<uint64_t>((target + n - 1) / n, tiles), 1024);
+    if (!n || tiles <= 1) return 1;
+    const uint64_t want = n >= target ? PERIODIC_OVERSPLIT : (target + n - 1) / n;
+    return (uint32_t)std::min<uint64_t>(std::min<uint64_t>(want, tiles), 1024);
 }
 
 // k_periodic over n candidates, split `parts` ways (seg: n * parts summaries),

@@ -22,7 +22,7 @@
 // the count n, then the n transaction ids in ascending order, padded to a
 // 16-byte multiple.  At one bit per transaction a bitset is the smaller form
 // until fewer than one transaction in 32 holds the pattern; below that (list
-// at most half the dense size) children are written as lists, and frequent
+// at most the dense size, by default) children are written as lists, and frequent
 // items that sparse serve as list members of the top-level classes.  The
 // prefix of a unit is always staged as a dense bitmap in shared memory; a
 // list sibling is intersected by testing its ids against that bitmap.  Lists
@@ -483,8 +483,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 const unsigned long long di = atomicAdd(&st->n_deferred, 1ull);
                 if (di < P.deferred_cap) P.deferred[di] = s_item;
                 else deep_fail(st, DEEP_ERR_QUEUE);
-                __threadfence();
-                atomicAdd(&st->pending, ~0ull);  // pending -= 1
+                atomicAdd(&st->pending, ~0ull);  // pending -= 1 (deferred[] is read after the kernel)
                 s_skip = 1;
             }
         }
@@ -495,6 +494,10 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             continue;
         }
         if (threadIdx.x == 0 && P.cta_time) t_unit = global_ns();
+        // The error word, read now and looked at after the staging, so that
+        // its latency overlaps the staging (thread 0 only; a hint that lets a
+        // failed launch stop early, nothing is ordered by it).
+        const unsigned err_seen = threadIdx.x == 0 ? ld_relaxed_u32(&st->error) : 0u;
         if (threadIdx.x == 0 && P.unit_log) {
             lg[0] = global_ns();
             s_maxb = 0;
@@ -572,7 +575,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 if (mb + cnt > P.members_cap) deep_fail(st, DEEP_ERR_MEMBERS);
                 s_mem_base = mb;
             }
-            s_ok = ld_acquire_u32(&st->error) == 0;
+            s_ok = err_seen == 0;
         }
         __syncthreads();
         if (SMEM_PREFIX && threadIdx.x == 0 && !mk && !(praw & 1ull) && n2 >= BULK_MIN_WORDS2) s_bulk_phase ^= 1u;
@@ -723,7 +726,8 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 c_surv += s_nsurv;
                 if (P.root_cost) atomicAdd(P.root_cost + root, (unsigned long long)cnt);
                 if (P.cta_time) c_busy += global_ns() - t_unit;
-                __threadfence();
+                // No fence: nothing this unit wrote is read before the kernel
+                // ends, and pending only falls to zero when every unit is done.
                 atomicAdd(&st->pending, ~0ull);  // pending -= 1
             }
             continue;
@@ -841,7 +845,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         if (threadIdx.x == 0) {
             s_grant = 0;
             s_fid = ~0ull;
-            if (expand && ld_acquire_u32(&st->error) == 0) {
+            if (expand && ld_relaxed_u32(&st->error) == 0) {
                 const unsigned long long ab = atomicAdd(&st->arena_next, (unsigned long long)child_words);
                 if (ab + (unsigned long long)child_words > P.arena_words) deep_fail(st, DEEP_ERR_ARENA);
                 else s_grant = 1;
@@ -997,7 +1001,8 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             c_surv += ns;
             if (P.root_cost) atomicAdd(P.root_cost + root, (unsigned long long)cnt);
             if (P.cta_time) c_busy += global_ns() - t_unit;
-            __threadfence();
+            // The child frame was published (fenced) above; its units were
+            // added to pending before this unit leaves it.
             atomicAdd(&st->pending, ~0ull);  // pending -= 1
         }
     }

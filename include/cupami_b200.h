@@ -90,12 +90,12 @@ typedef struct {
     int32_t  deep_ctas_per_sm;     /* resident deep-level CTAs per SM, 1-4 (capped by occupancy); 0 = automatic */
     int32_t  autotune;             /* 1: use the launch shape cpm_autotune found for this tidset length */
     int32_t  tidsets;              /* deep-level tidset forms.  0: bitsets, plus transaction-id lists for
-                                      tidsets held by under 1/64 of the transactions when a database's
+                                      tidsets held by under 1/32 of the transactions when a database's
                                       frequent bitsets exceed half the L2 and one bitset fits in shared
                                       memory; 1: bitsets only; 2: lists wherever a bitset fits in shared
                                       memory */
     int32_t  list_div;             /* a tidset is stored as a list when its list takes at most 1/list_div
-                                      of its bitset; 0 = the autotuner's choice, else 2 */
+                                      of its bitset; 0 = the autotuner's choice, else 1 */
     int32_t  deep_balance;         /* deep-level siblings: 0 = automatic (a warp per sibling), 1 = a warp
                                       per sibling, 2 = split over warps by size */
     int32_t  reserved[1];
