@@ -58,7 +58,7 @@ class Opts(ctypes.Structure):
         ("arena_bytes", ctypes.c_uint64), ("spin_limit", ctypes.c_uint64),
         ("collect_trace", ctypes.c_int32), ("deep_block", ctypes.c_int32),
         ("deep_ctas_per_sm", ctypes.c_int32), ("autotune", ctypes.c_int32), ("tidsets", ctypes.c_int32),
-        ("list_div", ctypes.c_int32), ("deep_balance", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("list_div", ctypes.c_int32), ("deep_balance", ctypes.c_int32), ("deep_project", ctypes.c_int32),
     ]
 
 
@@ -67,7 +67,8 @@ class Stats(ctypes.Structure):
         "n_patterns", "n_frequent_items", "n_frequent_pairs", "frames", "work_items",
         "intersections", "bytes_alg", "pair_ops", "kernel_launches", "retries", "deep_rounds")] + [
         (n, ctypes.c_double) for n in (
-            "ms_pack", "ms_pairs", "ms_deep", "ms_total", "deep_gbs", "pair_tops")]
+            "ms_pack", "ms_pairs", "ms_deep", "ms_total", "deep_gbs", "pair_tops")] + [
+        ("projected_units", ctypes.c_uint64), ("ms_local", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

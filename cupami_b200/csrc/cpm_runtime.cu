@@ -11,6 +11,7 @@
 #include "k_batch.cuh"
 #include "k_gram_tc.cuh"
 #include "k_deep.cuh"
+#include "k_local.cuh"
 #include "k_apriori.cuh"
 #include "k_periodic.cuh"
 #include "k_costmodel.cuh"
@@ -55,6 +56,7 @@ struct cpm_ctx {
     int deep_occ_smem = -1;   // k_deep<true> CTAs per SM, for deep_occ_bytes of prefix
     size_t deep_occ_bytes = 0;
     int deep_occ_global = -1; // k_deep<false> CTAs per SM
+    int local_occ = -1;       // k_local CTAs per SM
     unsigned deep_occ_block = 0;  // block size the occupancies above were taken for
     std::vector<float> model;  // cost-model parameters (empty: none loaded)
     float last_deep_ms = 0.f;  // deep-phase kernel time of the last bounded-round run
@@ -901,6 +903,7 @@ struct DeepBuffers {
     uint32_t *mem_pat = nullptr, *mem_item = nullptr;
     const uint64_t **mem_bits = nullptr;
     unsigned long long *queue = nullptr;
+    unsigned long long *lq = nullptr;  // projected units (k_local), queue_cap entries
     uint64_t *arena = nullptr;
     uint32_t *pat_parent = nullptr, *pat_item = nullptr, *pat_sup = nullptr, *pat_db = nullptr;
     unsigned long long *root_cost = nullptr;
@@ -912,7 +915,7 @@ struct DeepBuffers {
     }
     void release(cpm_ctx *ctx) {
         dfree(ctx, frames); dfree(ctx, mem_pat); dfree(ctx, mem_item); dfree(ctx, mem_bits);
-        dfree(ctx, queue); dfree(ctx, arena); dfree(ctx, pat_parent); dfree(ctx, pat_item);
+        dfree(ctx, queue); dfree(ctx, lq); dfree(ctx, arena); dfree(ctx, pat_parent); dfree(ctx, pat_item);
         dfree(ctx, pat_sup); dfree(ctx, pat_db); dfree(ctx, root_cost); dfree(ctx, st);
     }
 };
@@ -927,6 +930,7 @@ static int grow(cpm_ctx *ctx, DeepBuffers &b, uint64_t frames_cap, uint64_t memb
     CKR(dalloc(ctx, &b.mem_item, members_cap));
     CKR(dalloc(ctx, &b.mem_bits, members_cap));
     CKR(dalloc(ctx, &b.queue, queue_cap));
+    CKR(dalloc(ctx, &b.lq, queue_cap));
     CKR(dalloc(ctx, &b.arena, arena_words));
     CKR(dalloc(ctx, &b.pat_parent, pat_cap));
     CKR(dalloc(ctx, &b.pat_item, pat_cap));
@@ -937,6 +941,42 @@ static int grow(cpm_ctx *ctx, DeepBuffers &b, uint64_t frames_cap, uint64_t memb
     return CPM_OK;
 }
 
+
+// Projection of small prefixes by k_deep and the projected levels (k_local):
+// on unless the options turn it off, and only where the prefix bitmap and its
+// rank directory (2 bytes per 16-byte word) fit in shared memory.
+static uint32_t deep_local_max(const cpm_opts &o, bool smem_prefix, uint64_t max_stride) {
+    if (o.deep_project == 1 || !smem_prefix) return 0;
+    if (max_stride * 8 + max_stride > DEEP_SMEM_PREFIX_MAX) return 0;
+    return LOCAL_MAX_BITS;
+}
+
+// k_deep<true>'s dynamic shared memory: the prefix bitmap, then the rank directory.
+static size_t deep_smem_bytes(uint64_t max_stride, uint32_t local_max) {
+    return max_stride * 8 + (local_max ? max_stride : 0);
+}
+
+// Projection fields of a launch (local_max 0: off).
+static void deep_set_local(DeepParams &P, const DeepBuffers &b, uint64_t max_stride, uint32_t local_max) {
+    P.local_max = local_max;
+    P.lq = local_max ? b.lq : nullptr;
+    P.lq_cap = local_max ? b.queue_cap : 0;
+    P.dir_off = (uint32_t)(max_stride * 8);
+}
+
+// The projected units k_deep queued, after it (same stream).
+static int launch_local(cpm_ctx *ctx, const DeepParams &P, cpm_stats &st) {
+    if (!P.local_max) return CPM_OK;
+    if (ctx->local_occ < 0) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->local_occ, k_local, (int)LOCAL_BLOCK, 0));
+        ctx->local_occ = std::max(1, ctx->local_occ);
+    }
+    CK(cudaEventRecord(ctx->ev[7], ctx->stream));  // k_local's start (it ends at the caller's ev[3])
+    k_local<<<(unsigned)(ctx->sms * ctx->local_occ), LOCAL_BLOCK, 0, ctx->stream>>>(P);
+    CK(cudaGetLastError());
+    st.kernel_launches++;
+    return CPM_OK;
+}
 
 // Part of the arena kept free for frames that shallow expansion keeps.
 
@@ -952,7 +992,7 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
                            const uint32_t *d_uid, const float *d_key, const float *d_unit_key, uint64_t n_units,
                            uint64_t P2_total,
                            uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix, uint64_t spin,
-                           bool keys_in_words, uint32_t lists, const std::vector<unsigned long long> *cont,
+                           bool keys_in_words, uint32_t lists, uint32_t local_max, const std::vector<unsigned long long> *cont,
                            uint64_t arena_words, uint64_t pat_cap, DeepState &hs, cpm_stats &st);
 
 static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::vector<DFrame> &top_frames,
@@ -961,11 +1001,11 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
                        uint64_t P2_total, uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix,
                        uint64_t spin,
                        uint64_t pat_need, bool with_db, uint64_t arena_limit_words, bool keys_in_words,
-                       uint32_t lists, const std::vector<unsigned long long> *cont, DeepState &hs, cpm_stats &st) {
+                       uint32_t lists, uint32_t local_max, const std::vector<unsigned long long> *cont, DeepState &hs, cpm_stats &st) {
     const bool dbg = getenv("CPM_DEBUG") != nullptr;
     if (cont) return deep_rounds_run(ctx, ds, b, top_frames, nullptr, nullptr, d_unit_key, 0, P2_total, max_stride,
                                      grid, block,
-                                     smem_prefix, spin, keys_in_words, lists, cont, b.arena_words, b.pat_cap, hs, st);
+                                     smem_prefix, spin, keys_in_words, lists, local_max, cont, b.arena_words, b.pat_cap, hs, st);
     // Fixed tables large enough for any round; the arena takes the rest.
     const uint64_t frames_cap = 32ull << 20, members_cap = 256ull << 20, queue_cap = 64ull << 20;
     const uint64_t pat_cap = std::max<uint64_t>(pat_need, 96ull << 20);
@@ -1002,7 +1042,7 @@ static int deep_rounds(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std::ve
     hs.n_patterns = base_patterns;
     return deep_rounds_run(ctx, ds, b, top_frames, d_uid, d_key, d_unit_key, n_units, P2_total, max_stride, grid,
                            block,
-                           smem_prefix, spin, keys_in_words, lists, nullptr, arena_words, pat_cap, hs, st);
+                           smem_prefix, spin, keys_in_words, lists, local_max, nullptr, arena_words, pat_cap, hs, st);
 }
 
 // The rounds themselves.  Fresh start (cont null): every root unit d_uid /
@@ -1013,7 +1053,7 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
                            const uint32_t *d_uid, const float *d_key, const float *d_unit_key, uint64_t n_units,
                            uint64_t P2_total,
                            uint64_t max_stride, unsigned grid, unsigned block, bool smem_prefix, uint64_t spin,
-                           bool keys_in_words, uint32_t lists, const std::vector<unsigned long long> *cont,
+                           bool keys_in_words, uint32_t lists, uint32_t local_max, const std::vector<unsigned long long> *cont,
                            uint64_t arena_words, uint64_t pat_cap, DeepState &hs, cpm_stats &st) {
     const bool dbg = getenv("CPM_DEBUG") != nullptr;
     const uint64_t queue_cap = b.queue_cap;
@@ -1064,10 +1104,12 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
     P.root_cost = nullptr; P.st = b.st; P.max_stride = max_stride; P.spin_limit = spin; P.cta_time = nullptr;
     P.unit_log = nullptr; P.unit_log_cap = 0;
     P.lists = lists;
+    deep_set_local(P, b, max_stride, local_max);
+    if (local_max) CK(cudaMemsetAsync(b.lq, 0xff, b.queue_cap * 8, ctx->stream));
     P.root_frames = 0; P.defer_words = 0; P.defer_members = 0; P.defer_frames = 0; P.defer_queue = 0;
     P.root_key = nullptr; P.top_frames = 0; P.keys_in_words = 0; P.admit_words = 0;
     P.deferred = nullptr; P.deferred_cap = 0;
-    const size_t prefix_bytes = max_stride * 8;
+    const size_t smem_bytes = deep_smem_bytes(max_stride, local_max);
     uint64_t rounds = 0, failed = 0, shallow = 0;
     float deep_ms = 0.f;
     auto launch = [&](size_t n_take, uint32_t shallow_mode) -> int {
@@ -1091,14 +1133,19 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
         // Queue entries beyond the memset stay stale: bound the round's queue.
         P.queue_cap = std::min<uint64_t>(queue_cap, q.size() * 64 + (1u << 20));
         CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-        if (smem_prefix) k_deep<true><<<grid, block, prefix_bytes, ctx->stream>>>(P);
+        if (smem_prefix) k_deep<true><<<grid, block, smem_bytes, ctx->stream>>>(P);
         else k_deep<false><<<grid, block, 0, ctx->stream>>>(P);
         CK(cudaGetLastError());
+        CKR(launch_local(ctx, P, st));
         CK(cudaEventRecord(ctx->ev[3], ctx->stream));
         CK(cudaMemcpyAsync(&hs, b.st, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        // The projected queue is empty again for the next round.
+        if (local_max && hs.lq_tail)
+            CK(cudaMemsetAsync(b.lq, 0xff, std::min<uint64_t>(hs.lq_tail, b.queue_cap) * 8, ctx->stream));
         const float round_ms = (float)elapsed_ms(ctx, 2, 3);
         deep_ms += round_ms;
+        if (P.local_max) st.ms_local += elapsed_ms(ctx, 7, 3);
         if (dbg)
             fprintf(stderr, "cpm: round %llu: %zu units, %.3f ms, %.3g bytes, %.0f GB/s, deferred %llu, error 0x%x, "
                     "admitted %llu of %llu, arena %llu (hand back at %llu), members %llu (%llu), frames %llu (%llu), "
@@ -1115,6 +1162,7 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
             st.intersections += hs.intersections;
             st.bytes_alg += hs.bytes_alg;
             st.work_items += hs.work_items;
+            st.projected_units += hs.local_units;
         }
         ++rounds;
         return CPM_OK;
@@ -1259,6 +1307,7 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
     // these counters.
     hs.n_patterns = committed;
     hs.work_items = st.work_items;
+    hs.local_units = st.projected_units;
     hs.intersections = st.intersections;
     hs.bytes_alg = st.bytes_alg;
     hs.n_frames = persist_frames;
@@ -1523,6 +1572,8 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     const uint64_t spin = o.spin_limit ? o.spin_limit : (1ull << 26);
     const size_t prefix_bytes = max_stride * 8;
     const bool smem_prefix = prefix_bytes <= DEEP_SMEM_PREFIX_MAX;
+    const uint32_t local_max = deep_local_max(o, smem_prefix, max_stride);
+    const size_t smem_bytes = deep_smem_bytes(max_stride, local_max);
     // Long tidsets leave room for fewer CTAs per SM: give each 16 or 32 warps
     // so that enough loads stay in flight; short ones run up to four 8-warp
     // CTAs.  Measured (deep phase): 1,564-word tidsets (planted-100k) 0.25 ms
@@ -1547,9 +1598,9 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
             return set_err(ctx, CPM_EINVAL, "deep_ctas_per_sm must be 1-4 (got %d)", o.deep_ctas_per_sm);
         want_ctas = o.deep_ctas_per_sm;
     }
-    if (smem_prefix && (ctx->deep_occ_smem < 0 || ctx->deep_occ_bytes != prefix_bytes || ctx->deep_occ_block != block)) {
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_smem, k_deep<true>, block, prefix_bytes));
-        ctx->deep_occ_bytes = prefix_bytes;
+    if (smem_prefix && (ctx->deep_occ_smem < 0 || ctx->deep_occ_bytes != smem_bytes || ctx->deep_occ_block != block)) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_smem, k_deep<true>, block, smem_bytes));
+        ctx->deep_occ_bytes = smem_bytes;
         ctx->deep_occ_block = block;
     } else if (!smem_prefix && (ctx->deep_occ_global < 0 || ctx->deep_occ_block != block)) {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->deep_occ_global, k_deep<false>, block, 0));
@@ -1605,6 +1656,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         CK(cudaMemcpyAsync(b.frames, frames.data(), frames.size() * sizeof(DFrame), cudaMemcpyHostToDevice,
                            ctx->stream));
         CK(cudaMemsetAsync(b.queue, 0xff, b.queue_cap * 8, ctx->stream));
+        if (local_max) CK(cudaMemsetAsync(b.lq, 0xff, b.queue_cap * 8, ctx->stream));
         // Key every root unit (size, or predicted cost), sort largest first
         // (stable), write the queue -- all on the device.
         k_unit_keys<<<(unsigned)((n_units + 127) / 128), 128, 0, ctx->stream>>>(
@@ -1675,14 +1727,17 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         P.deferred = d_deferred;
         P.deferred_cap = n_units;
         P.root_key = nullptr; P.top_frames = 0; P.keys_in_words = 0; P.admit_words = 0;
+        deep_set_local(P, b, max_stride, local_max);
         CK(cudaEventRecord(ctx->ev[2], ctx->stream));
-        if (smem_prefix) k_deep<true><<<grid, block, prefix_bytes, ctx->stream>>>(P);
+        if (smem_prefix) k_deep<true><<<grid, block, smem_bytes, ctx->stream>>>(P);
         else k_deep<false><<<grid, block, 0, ctx->stream>>>(P);
         CK(cudaGetLastError());
+        CKR(launch_local(ctx, P, st));
         CK(cudaEventRecord(ctx->ev[3], ctx->stream));
         st.kernel_launches++;
         CK(cudaMemcpyAsync(&hs, b.st, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        st.ms_local = local_max ? elapsed_ms(ctx, 7, 3) : 0.0;
         if (P.unit_log) {
             unsigned long long n_log = 0;
             CK(cudaMemcpy(&n_log, P.unit_log, 8, cudaMemcpyDeviceToHost));
@@ -1736,7 +1791,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         // every buffer past them (one overflow usually means several).
         frames_cap = std::max<uint64_t>(frames_cap * 8, hs.n_frames * 8);
         members_cap = std::max<uint64_t>(members_cap * 8, hs.n_members * 8);
-        queue_cap = std::max<uint64_t>(queue_cap * 8, hs.q_tail * 8);
+        queue_cap = std::max<uint64_t>(queue_cap * 8, std::max(hs.q_tail, hs.lq_tail) * 8);
         pat_cap = std::max<uint64_t>(pat_cap * 8, hs.n_patterns * 8);
         if ((hs.error & DEEP_ERR_ARENA) && arena_words >= arena_budget) {
             rounds = true;  // the child tidsets do not fit at once: bounded rounds below
@@ -1757,22 +1812,25 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         st.intersections = hs.intersections;
         st.bytes_alg = hs.bytes_alg;
         st.work_items = hs.work_items;
+        st.projected_units = hs.local_units;
         CKR(deep_rounds(ctx, ds, b, frames, nullptr, nullptr, d_key, 0, base_patterns, P2_total, max_stride, grid, block,
-                        smem_prefix, spin, 0, with_db, 0, learned, use_lists ? list_div : 0u, &cont, hs, st));
+                        smem_prefix, spin, 0, with_db, 0, learned, use_lists ? list_div : 0u, local_max, &cont, hs, st));
         rounds = continued = true;
         ++st.deep_rounds;  // the first launch
     } else if (rounds) {
+        st.ms_local = 0.0;  // the first launch's time is not part of ms_deep either
         CKR(deep_rounds(ctx, ds, b, frames, d_uid2, d_key2, d_key, n_units, base_patterns, P2_total, max_stride, grid,
                         block,
                         smem_prefix, spin, pat_cap + base_patterns, with_db, o.arena_bytes ? o.arena_bytes / 8 : 0,
-                        learned, use_lists ? list_div : 0u, nullptr, hs, st));
+                        learned, use_lists ? list_div : 0u, local_max, nullptr, hs, st));
     }
     lap("deep phase");
     if (n_db == 1) {
         // Remember what this database needed so that the next mine() starts there.
         db0->hint_frames = std::max<uint64_t>(db0->hint_frames, hs.n_frames + hs.n_frames / 4 + 64);
         db0->hint_members = std::max<uint64_t>(db0->hint_members, hs.n_members + hs.n_members / 4 + 64);
-        db0->hint_queue = std::max<uint64_t>(db0->hint_queue, hs.q_tail + hs.q_tail / 4 + 64);
+        const uint64_t q_used = std::max(hs.q_tail, hs.lq_tail);
+        db0->hint_queue = std::max<uint64_t>(db0->hint_queue, q_used + q_used / 4 + 64);
         db0->hint_patterns = std::max<uint64_t>(db0->hint_patterns, hs.n_patterns + hs.n_patterns / 4 + 64);
         // After rounds the arena counter covers one round only; what is known
         // then is whether one launch overflowed the whole budget.
@@ -1803,6 +1861,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     CK(cudaStreamSynchronize(ctx->stream));
     st.frames = hs.n_frames;
     st.work_items = hs.work_items;
+    st.projected_units = hs.local_units;
     st.intersections = hs.intersections;
     st.bytes_alg = hs.bytes_alg;
     st.ms_pairs = rows ? elapsed_ms(ctx, 5, 6) : 0.0;
@@ -3281,6 +3340,7 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     P.balance = 0;
     P.prefetch = 0;
     P.lists = 0;
+    P.local_max = 0; P.lq = nullptr; P.lq_cap = 0; P.dir_off = 0;  // no projection: one launch, fixed scratch
     P.root_frames = 0; P.defer_words = 0; P.defer_members = 0; P.defer_frames = 0; P.defer_queue = 0;
     P.root_key = nullptr; P.top_frames = 0; P.keys_in_words = 0; P.admit_words = 0;
     P.deferred = nullptr; P.deferred_cap = 0;

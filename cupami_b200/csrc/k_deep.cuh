@@ -68,6 +68,10 @@ struct DFrame {
     uint32_t stride;       // words per tidset in this frame's database (even)
     uint32_t db;           // database index within the batch
     long long minsup;      // that database's threshold
+    // Projected frames only (null otherwise): the members' tidsets, each
+    // `stride` words, member q at bits + q * stride.  Their transactions are
+    // numbered by rank within the tidset of the unit that made the frame.
+    const uint64_t *bits = nullptr;
 };
 
 // Every counter that CTAs update or poll sits on its own 128-byte line, so
@@ -87,6 +91,10 @@ struct DeepState {
     CPM_LINE(survivors);
     CPM_LINE(n_deferred);   // root units handed back to the host (memory-bounded rounds)
     CPM_LINE(admitted);     // predicted cost of the root units started (memory-bounded rounds)
+    CPM_LINE(lq_head);      // projected units: next ticket (k_local)
+    CPM_LINE(lq_tail);      // projected units: entries reserved
+    CPM_LINE(lq_pending);   // projected units queued or running
+    CPM_LINE(local_units);  // projected units run
     unsigned int error;
     unsigned int pad[31];
 };
@@ -131,6 +139,15 @@ struct DeepParams {
     // unit_log[0] counts the units logged; records start at unit_log + 1.
     unsigned long long *unit_log;
     unsigned long long unit_log_cap;
+    // Projection (0: off; needs SMEM_PREFIX and !shallow): a unit whose
+    // prefix holds 1..local_max transactions writes its children as bitsets
+    // of that many bits, numbered by rank within the prefix, and queues the
+    // child frame's units in lq for k_local.  The rank directory sits at byte
+    // dir_off of the dynamic shared memory.
+    unsigned long long *lq;
+    uint64_t lq_cap;
+    uint32_t local_max;
+    uint32_t dir_off;
 };
 
 constexpr int UNIT_LOG_WORDS = 12;
@@ -407,6 +424,150 @@ __device__ __forceinline__ void write_dense_piece(unsigned long long sraw, uint6
         for (int u = 0; u < 4; ++u) dst[v + 32 * u] = with_prefix(x[u], v + 32 * u);
     }
     for (; v < hi; v += 32) dst[v] = with_prefix(ld_cg(sb + v), v);
+}
+
+// ---- Projection: children numbered by rank within the prefix ----
+// A child of unit (F, p) is t(prefix) & t(sibling), a subset of the prefix's
+// n_p transactions.  Numbering them by their rank in the prefix (the j-th
+// transaction of the prefix becomes j) turns every descendant tidset into a
+// bitset of n_p bits: for a prefix of a few thousand transactions among a
+// million that is a few hundred bytes, instead of a list of 4-byte ids, and
+// its units need no million-bit bitmap.
+
+// dir[v] = set bits of the staged prefix before its 16-byte word v (below
+// 2^16: projection needs n_p <= local_max <= 65535).  Every thread calls it.
+__device__ __forceinline__ void build_rank_dir(const ulonglong2 *s_prefix, uint64_t n2, uint16_t *dir,
+                                               uint64_t *s_w64) {
+    const uint64_t per = (n2 + blockDim.x - 1) / blockDim.x;
+    const uint64_t a = min(n2, (uint64_t)threadIdx.x * per), b = min(n2, a + per);
+    uint64_t c = 0;
+    for (uint64_t v = a; v < b; ++v) c += popc2(s_prefix[v]);
+    uint64_t tot = 0;
+    uint64_t run = block_excl_scan_u64(c, s_w64, &tot);
+    for (uint64_t v = a; v < b; ++v) {
+        dir[v] = (uint16_t)run;
+        run += popc2(s_prefix[v]);
+    }
+}
+
+// The bits of x at the set positions of m, packed to the low end in order
+// (the "compress" or generalized extract of H. S. Warren, Hacker's Delight,
+// 2nd ed., section 7-4, parallel-suffix method, here for 64 bits): at round
+// i every bit still to move by an odd multiple of 2^i moves right by 2^i.
+__device__ __forceinline__ unsigned long long compress64(unsigned long long x, unsigned long long m) {
+    x &= m;
+    unsigned long long mk = ~m << 1;  // zeros of m to the right of each bit, counted below
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        unsigned long long mp = mk ^ (mk << 1);  // parallel suffix (XOR) of mk
+        mp ^= mp << 2;
+        mp ^= mp << 4;
+        mp ^= mp << 8;
+        mp ^= mp << 16;
+        mp ^= mp << 32;
+        const unsigned long long mv = mp & m;  // bits of m that move this round
+        m = (m ^ mv) | (mv >> (1 << i));
+        const unsigned long long t = x & mv;
+        x = (x ^ t) | (t >> (1 << i));
+        mk &= ~mp;
+    }
+    return x;
+}
+
+// Transactions of the prefix below transaction t.
+__device__ __forceinline__ uint32_t rank_of(const ulonglong2 *s_prefix, const uint16_t *dir, uint32_t t) {
+    const ulonglong2 w = s_prefix[t >> 7];
+    const uint32_t b = t & 127u;
+    uint32_t r = dir[t >> 7];
+    if (b < 64) r += __popcll(w.x & ((1ull << b) - 1ull));
+    else r += __popcll(w.x) + __popcll(w.y & ((1ull << (b - 64)) - 1ull));
+    return r;
+}
+
+// Sets bit r of out32 for the lanes that keep theirs, one atomicOr per
+// 32-bit word touched: r must not decrease from lane to lane (lanes that
+// keep nothing carry the rank they would have), so lanes with the same word
+// are neighbours and a segmented OR gathers their bits in the word's first lane.
+__device__ __forceinline__ void or_ranks(uint32_t *out32, uint32_t nw32, uint32_t r, bool keep, unsigned lane) {
+    const uint32_t w = r >> 5;
+    uint32_t v = keep ? 1u << (r & 31u) : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t vo = __shfl_down_sync(CPM_FULL, v, o);
+        const uint32_t wo = __shfl_down_sync(CPM_FULL, w, o);
+        if (lane + o < 32 && wo == w) v |= vo;
+    }
+    const uint32_t wp = __shfl_up_sync(CPM_FULL, w, 1);
+    if ((lane == 0 || wp != w) && v && w < nw32) atomicOr(out32 + w, v);
+}
+
+// Projected child piece: over work units [lo, hi) of the sibling (list ids
+// or bitset words), every transaction t the prefix holds sets bit rank(t)
+// of the child bitset out32 (nw32 words), which is zeroed before the pass.
+// Ranks stay below the prefix's count, which the caller checks against the
+// bitset's size; the writes are bounded by nw32 all the same.
+__device__ __forceinline__ void write_proj_piece(unsigned long long sraw, uint64_t lo, uint64_t hi,
+                                                 const ulonglong2 *s_prefix, const uint32_t *s_p32,
+                                                 const uint16_t *dir, uint32_t *out32, uint32_t nw32, unsigned lane) {
+    if (sraw & 1ull) {
+        const uint32_t *I = reinterpret_cast<const uint32_t *>(sraw & ~1ull) + 4;
+        for (uint64_t w0 = lo; w0 < hi; w0 += 256) {
+            uint32_t t[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const uint64_t j = w0 + 32 * u + lane;
+                t[u] = j < hi ? __ldcg(I + j) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const bool in = w0 + 32 * u + lane < hi;
+                // Ids ascend from lane to lane and past the end come last: ranks never fall.
+                const uint32_t r = in ? rank_of(s_prefix, dir, t[u]) : 0xffffffffu;
+                or_ranks(out32, nw32, r, in && bit_of(s_p32, t[u]), lane);
+            }
+        }
+        return;
+    }
+    // Bitset sibling: the kept bits of a 64-bit half-word x under prefix
+    // half-word m land on ranks r .. r + popc(m) - 1 in order, i.e. they are
+    // compress(x, m) shifted to bit r.  A half-word of a few prefix bits is
+    // walked bit by bit (gathered per 32-bit output word in a register);
+    // a fuller one is compressed and OR-ed in with one or two 64-bit atomics.
+    const ulonglong2 *sb = reinterpret_cast<const ulonglong2 *>(sraw);
+    unsigned long long *out64 = reinterpret_cast<unsigned long long *>(out32);
+    const uint32_t nw64 = nw32 / 2;
+    uint32_t cw = 0xffffffffu, cv = 0;
+    for (uint64_t v = lo + lane; v < hi; v += 32) {
+        const ulonglong2 pw = s_prefix[v];
+        if (!(pw.x | pw.y)) continue;  // no transaction of the prefix here: nothing to read
+        const ulonglong2 x = and2(ld_cg(sb + v), pw);
+        uint32_t r0 = dir[v];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const unsigned long long m = h ? pw.y : pw.x;
+            const unsigned long long xh = h ? x.y : x.x;
+            const uint32_t pm = __popcll(m);
+            if (xh && pm > 4) {
+                const unsigned long long c = compress64(xh, m);
+                const uint32_t w = r0 >> 6, sh = r0 & 63u;
+                if (w < nw64) atomicOr(out64 + w, c << sh);
+                if (sh && (c >> (64 - sh)) && w + 1 < nw64) atomicOr(out64 + w + 1, c >> (64 - sh));
+            } else {
+                for (unsigned long long b = xh; b; b &= b - 1) {
+                    const int bit = __ffsll((long long)b) - 1;
+                    const uint32_t r = r0 + __popcll(m & ((1ull << bit) - 1ull));
+                    if ((r >> 5) != cw) {
+                        if (cv && cw < nw32) atomicOr(out32 + cw, cv);
+                        cw = r >> 5;
+                        cv = 0;
+                    }
+                    cv |= 1u << (r & 31u);
+                }
+            }
+            r0 += pm;
+        }
+    }
+    if (cv && cw < nw32) atomicOr(out32 + cw, cv);
 }
 
 template <bool SMEM_PREFIX>
@@ -801,6 +962,14 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         if (threadIdx.x == 0 && P.unit_log) lg[4] = global_ns();
         const uint32_t ns = s_surv;
         const bool expand = ns >= 2;
+        // Projected children (bitsets of lstride words, numbered by rank in
+        // the prefix) when the prefix holds at most local_max transactions.
+        uint32_t lstride = 0, n_pre = 0;
+        if (SMEM_PREFIX && P.local_max && !P.shallow && expand) {
+            n_pre = __ldcg(P.pat_sup + parent_pat);
+            if (n_pre >= 1 && n_pre <= P.local_max) lstride = 2u * ((n_pre + 127u) / 128u);
+        }
+        const bool proj = lstride != 0;
         // Words of the survivors' child tidsets (each dense or a list, by its support).
         uint64_t child_words = (uint64_t)ns * stride;
         uint64_t fast_wtot = 0;
@@ -817,7 +986,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 const uint32_t q = s_map[i];
                 raw = s_raw[q];
                 sc = s_cnt[q];
-                sz = (SMEM_PREFIX && as_list(P, sc, stride)) ? list_words(sc) : stride;
+                sz = proj ? lstride : (SMEM_PREFIX && as_list(P, sc, stride)) ? list_words(sc) : stride;
                 wk = sibling_units<SMEM_PREFIX>(raw, n2);
             }
             uint64_t tot = 0;
@@ -832,6 +1001,8 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             if (threadIdx.x < 32) s_clast[threadIdx.x] = 0;
             child_words = tot >> 32;
             fast_wtot = tot & 0xffffffffull;
+        } else if (expand && proj) {
+            child_words = (uint64_t)ns * lstride;
         } else if (expand && P.lists) {
             uint64_t part = 0;
             for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x) {
@@ -853,6 +1024,22 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             }
         }
         __syncthreads();
+        uint16_t *const s_dir = reinterpret_cast<uint16_t *>(reinterpret_cast<char *>(s_prefix) + P.dir_off);
+        if (SMEM_PREFIX && proj && s_grant) {
+            // Rank directory of the prefix, and the child block zeroed for
+            // the bits the projected writers OR in.
+            build_rank_dir(s_prefix, n2, s_dir, s_w64);
+            uint64_t *blk = P.arena + s_arena_base;
+            for (uint64_t i = threadIdx.x; i < child_words; i += blockDim.x) blk[i] = 0ull;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                // The directory's total is the prefix's count: it must be the
+                // support the projection was sized by (the writers stay inside
+                // the child bitsets either way).
+                const uint32_t last = (uint32_t)n2 - 1u;
+                if ((uint32_t)s_dir[last] + popc2(s_prefix[last]) != n_pre) deep_fail(st, DEEP_ERR_INTERNAL);
+            }
+        }
         if (threadIdx.x == 0 && P.unit_log) lg[5] = global_ns();
         // ---- pass 2: child tidsets of the survivors (only when they recurse) ----
         // Per chunk of up to blockDim survivors: their siblings' work (list
@@ -873,7 +1060,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                     const uint64_t m_out = s_mem_base + start + threadIdx.x;
                     const unsigned long long raw = ld_raw_ptr(P.mem_bits + m_out);
                     const uint32_t sc = P.lists ? __ldcg(P.pat_sup + __ldcg(P.mem_pat + m_out)) : 0u;
-                    sz = (SMEM_PREFIX && as_list(P, sc, stride)) ? list_words(sc) : stride;
+                    sz = proj ? lstride : (SMEM_PREFIX && as_list(P, sc, stride)) ? list_words(sc) : stride;
                     wk = sibling_units<SMEM_PREFIX>(raw, n2);
                     s_raw[threadIdx.x] = raw;
                     s_cnt[threadIdx.x] = sc;
@@ -900,7 +1087,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                     // The child this slice ends in, when it goes on past the slice.
                     uint32_t z = first;
                     while (z + 1 < cn && s_off[z + 1] < hi) ++z;
-                    const bool list_child = SMEM_PREFIX && as_list(P, s_cnt[z], stride);
+                    const bool list_child = SMEM_PREFIX && !proj && as_list(P, s_cnt[z], stride);
                     if (list_child && s_off[z + 1] > hi) {
                         uint32_t c = sibling_count_range<SMEM_PREFIX>(s_raw[z], max(lo, s_off[z]) - s_off[z],
                                                                       hi - s_off[z], s_prefix, s_p32, pb, mk, lane);
@@ -914,7 +1101,11 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                     const uint64_t units = s_off[i + 1] - s_off[i];
                     uint64_t *out = P.arena + s_arena_base + s_coff[i];
                     const uint32_t sc = s_cnt[i];
-                    if (SMEM_PREFIX && as_list(P, sc, stride)) {
+                    if (SMEM_PREFIX && proj) {
+                        if (u0 < u1)
+                            write_proj_piece(s_raw[i], u0, u1, s_prefix, s_p32, s_dir, reinterpret_cast<uint32_t *>(out),
+                                             2u * lstride, lane);
+                    } else if (SMEM_PREFIX && as_list(P, sc, stride)) {
                         uint32_t *o32 = reinterpret_cast<uint32_t *>(out);
                         uint32_t at = 0;
                         if (u0 > 0) {
@@ -946,7 +1137,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 __syncthreads();  // every piece of this chunk is written
                 if (threadIdx.x < cn) {
                     const uint64_t *out = P.arena + s_arena_base + s_coff[threadIdx.x];
-                    const bool lst = SMEM_PREFIX && as_list(P, s_cnt[threadIdx.x], stride);
+                    const bool lst = SMEM_PREFIX && !proj && as_list(P, s_cnt[threadIdx.x], stride);
                     P.mem_bits[s_mem_base + start + threadIdx.x] = reinterpret_cast<const uint64_t *>(
                         reinterpret_cast<unsigned long long>(out) | (lst ? 1ull : 0ull));
                 }
@@ -963,22 +1154,24 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             const unsigned long long nf = atomicAdd(&st->n_frames, 1ull);
             // Shallow launches keep the child frame for the host (its
             // positions become root units of later rounds) instead of
-            // queueing them.
-            const unsigned long long qb = P.shallow ? 0ull : atomicAdd(&st->q_tail, (unsigned long long)(ns - 1));
+            // queueing them.  A projected frame's units go to k_local's queue.
+            const unsigned long long qb =
+                P.shallow ? 0ull : atomicAdd(proj ? &st->lq_tail : &st->q_tail, (unsigned long long)(ns - 1));
             if (nf >= P.frames_cap) deep_fail(st, DEEP_ERR_FRAMES);
-            else if (!P.shallow && qb + ns - 1 > P.queue_cap) deep_fail(st, DEEP_ERR_QUEUE);
+            else if (!P.shallow && qb + ns - 1 > (proj ? P.lq_cap : P.queue_cap)) deep_fail(st, DEEP_ERR_QUEUE);
             else {
                 DFrame c;
                 c.mask = nullptr;
                 c.mem_off = s_mem_base;
                 c.m = ns;
                 c.root = root;
-                c.stride = stride;
+                c.stride = proj ? lstride : stride;
                 c.db = db;
                 c.minsup = minsup;
+                c.bits = proj ? P.arena + s_arena_base : nullptr;
                 P.frames[nf] = c;
                 if (!P.shallow) {
-                    atomicAdd(&st->pending, (unsigned long long)(ns - 1));
+                    atomicAdd(proj ? &st->lq_pending : &st->pending, (unsigned long long)(ns - 1));
                     __threadfence();
                     s_fid = nf;
                     s_qbase = qb;
@@ -990,7 +1183,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         __syncthreads();
         if (s_fid != ~0ull) {
             for (uint32_t i = threadIdx.x; i + 1 < ns; i += blockDim.x)
-                st_release_u64(P.queue + s_qbase + i, (s_fid << 32) | i);
+                st_release_u64((proj ? P.lq : P.queue) + s_qbase + i, (s_fid << 32) | i);
         }
         __syncthreads();
         if (threadIdx.x == 0) {

@@ -79,6 +79,10 @@ class cuApriori:
     #: Deep-level siblings of a unit: 0 automatic, 1 one warp per sibling,
     #: 2 split over the warps by size.
     _DEEP_BALANCE = 0
+    #: Deep levels below small prefixes: 0 automatic (children of a prefix of
+    #: at most 65,408 transactions become bitsets numbered by rank within it,
+    #: mined one unit per warp); 1 off.
+    _DEEP_PROJECT = 0
 
     def __init__(self, iFile, minSup, sep=None, use_gds="auto", use_gpu_io="auto"):
         t0 = time.perf_counter()
@@ -287,6 +291,7 @@ class cuApriori:
         opts.autotune = 1
         opts.tidsets = int(self._TIDSETS)
         opts.deep_balance = int(self._DEEP_BALANCE)
+        opts.deep_project = int(self._DEEP_PROJECT)
         return opts
 
     def autotune(self):

@@ -98,7 +98,9 @@ typedef struct {
                                       of its bitset; 0 = the autotuner's choice, else 1 */
     int32_t  deep_balance;         /* deep-level siblings: 0 = automatic (a warp per sibling), 1 = a warp
                                       per sibling, 2 = split over warps by size */
-    int32_t  reserved[1];
+    int32_t  deep_project;         /* deep levels: 0 = automatic (a unit whose prefix holds at most 65,408
+                                      transactions writes its children as bitsets numbered by rank within
+                                      the prefix, mined one unit per warp), 1 = off */
 } cpm_opts;
 
 typedef struct {
@@ -119,6 +121,8 @@ typedef struct {
     double   ms_total;
     double   deep_gbs;             /* bytes_alg / ms_deep */
     double   pair_tops;            /* pair_ops / ms_pairs */
+    uint64_t projected_units;      /* of work_items: units below a projected prefix (one warp each) */
+    double   ms_local;             /* of ms_deep: the launches that mine those units */
 } cpm_stats;
 
 /* ---- context ------------------------------------------------------------ */

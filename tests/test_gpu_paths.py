@@ -107,9 +107,10 @@ def test_cli_writes_reference_format(tmp_path):
     assert out.read_text() == "1 : 2\n2 : 2\n"
 
 
-@pytest.mark.parametrize("arena_kb", [64, 512])
-def test_memory_bounded_rounds_are_exact(oracle_lib, arena_kb):
-    """A small child-tidset arena forces bounded rounds, halving and shallow splits."""
+@pytest.mark.parametrize("arena_kb,project", [(64, 0), (64, 1), (512, 1)])
+def test_memory_bounded_rounds_are_exact(oracle_lib, arena_kb, project):
+    """A small child-tidset arena forces bounded rounds, halving and shallow
+    splits (with projected levels, whose children are smaller, and without)."""
     import cupami_b200
     from cupami_b200 import TransactionCSR
 
@@ -119,6 +120,7 @@ def test_memory_bounded_rounds_are_exact(oracle_lib, arena_kb):
     csr = TransactionCSR.from_rows(rows, universe=20)
     m = cupami_b200.cuEclat(csr, 0.2)
     m._ARENA_BYTES = arena_kb * 1024
+    m._DEEP_PROJECT = project
     m.mine()
     stats = m.getKernelStats()
     assert stats["deep_rounds"] > 1
@@ -196,6 +198,7 @@ def test_lists_in_memory_bounded_rounds_and_batches(oracle_lib):
         m = cuEclat(csr, 0.005)
         m._ARENA_BYTES = arena
         m._TIDSETS = 2
+        m._DEEP_PROJECT = 1  # child lists, not projected bitsets
         m.mine()
         assert m.getPatterns() == want
         if arena:
@@ -229,3 +232,60 @@ def test_interpreter_exit_with_live_databases():
     r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=240)
     assert r.returncode == 1, (r.returncode, r.stderr[-2000:])
     assert "left with a live database" in r.stderr
+
+
+@pytest.mark.parametrize("name,minsup", [("planted_zipf", 0.005), ("uniform_poisson", 0.01),
+                                         ("dense_bernoulli", 0.6), ("sparse_zipf_small", 0.003)])
+def test_projected_levels_agree(oracle_lib, name, minsup):
+    """Children of small prefixes numbered by rank within them (mined by the
+    warp-per-unit kernel) give the same patterns, in order, as the deep kernel
+    alone and as the oracle, with bitsets only and with lists."""
+    import cupami_b200
+    from cupami_b200 import datasets
+
+    if name == "sparse_zipf_small":
+        csr = datasets.sparse_zipf(n=50_000, n_items=2_000, mean=20, seed=5)
+    else:
+        csr = getattr(datasets, name)()
+    out = {}
+    for project in (0, 1):
+        for tidsets in (0, 1, 2):
+            m = cupami_b200.cuEclat(csr, minsup)
+            m._DEEP_PROJECT, m._TIDSETS = project, tidsets
+            m.mine()
+            out[project, tidsets] = (list(m.getPatterns().items()), m.getKernelStats())
+    want = out[1, 0][0]
+    assert all(v[0] == want for v in out.values())
+    labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, minsup)
+    assert dict(want) == oracle_lib.to_dict(labels, arrays)
+    # Projection moved units to the warp-per-unit kernel; without it none.
+    # (uniform_poisson has no frequent 3-itemset, and every dense_bernoulli
+    # prefix holds over 39,000 transactions: nothing is projected there.)
+    if name in ("planted_zipf", "sparse_zipf_small"):
+        assert out[0, 0][1]["projected_units"] > 0
+    assert out[1, 0][1]["projected_units"] == 0
+
+
+def test_projected_levels_in_rounds_and_batches(oracle_lib):
+    """Projection inside memory-bounded rounds and batched launches stays exact."""
+    from cupami_b200 import TransactionCSR, cuEclat, datasets
+
+    rng = np.random.default_rng(23)
+    p = rng.uniform(0.02, 0.4, 40)
+    rows = [[int(i) for i in np.nonzero(rng.random(40) < p)[0]] for _ in range(6000)]
+    csr = TransactionCSR.from_rows(rows, universe=40)
+    labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, 0.004)
+    want = oracle_lib.to_dict(labels, arrays)
+    for arena in (64 << 10, 512 << 10, 0):
+        m = cuEclat(csr, 0.004)
+        m._ARENA_BYTES = arena
+        m.mine()
+        assert m.getPatterns() == want, arena
+        if arena:
+            assert m.getKernelStats()["deep_rounds"] > 1
+    csrs = datasets.batched_zipf(limit=16)
+    for project in (0, 1):
+        cls = type("E", (cuEclat,), {"_DEEP_PROJECT": project})
+        for c, m in zip(csrs, cls.mineBatch(csrs, 0.01)):
+            labels, arrays = oracle_lib.mine_csr(c.offsets, c.items, 0.01)
+            assert m.getPatterns() == oracle_lib.to_dict(labels, arrays)
