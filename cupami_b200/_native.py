@@ -59,6 +59,7 @@ class Opts(ctypes.Structure):
         ("collect_trace", ctypes.c_int32), ("deep_block", ctypes.c_int32),
         ("deep_ctas_per_sm", ctypes.c_int32), ("autotune", ctypes.c_int32), ("tidsets", ctypes.c_int32),
         ("list_div", ctypes.c_int32), ("deep_balance", ctypes.c_int32), ("deep_project", ctypes.c_int32),
+        ("deep_rows", ctypes.c_int32),
     ]
 
 
@@ -68,7 +69,7 @@ class Stats(ctypes.Structure):
         "intersections", "bytes_alg", "pair_ops", "kernel_launches", "retries", "deep_rounds")] + [
         (n, ctypes.c_double) for n in (
             "ms_pack", "ms_pairs", "ms_deep", "ms_total", "deep_gbs", "pair_tops")] + [
-        ("projected_units", ctypes.c_uint64), ("ms_local", ctypes.c_double)]
+        ("projected_units", ctypes.c_uint64), ("ms_local", ctypes.c_double), ("row_units", ctypes.c_uint64)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -12,6 +12,7 @@
 #include "k_gram_tc.cuh"
 #include "k_deep.cuh"
 #include "k_local.cuh"
+#include "k_rows.cuh"
 #include "k_apriori.cuh"
 #include "k_periodic.cuh"
 #include "k_costmodel.cuh"
@@ -943,12 +944,21 @@ static int grow(cpm_ctx *ctx, DeepBuffers &b, uint64_t frames_cap, uint64_t memb
 
 
 // Projection of small prefixes by k_deep and the projected levels (k_local):
-// on unless the options turn it off, and only where the prefix bitmap and its
-// rank directory (2 bytes per 16-byte word) fit in shared memory.
-static uint32_t deep_local_max(const cpm_opts &o, bool smem_prefix, uint64_t max_stride) {
+// only where the prefix bitmap and its rank directory (2 bytes per 16-byte
+// word) fit in shared memory.  deep_project >= 128 sets the largest
+// projected prefix; 0 projects prefixes of up to LOCAL_MAX_BITS transactions
+// when there are at least PROJECT_MIN_ROOTS_PER_SM root units per SM.  A
+// search of fewer is short and bound by its chain of dependent units, which
+// a warp per unit only lengthens (planted 100,000 x 1,000, ~1,000 root units:
+// deep phase 0.22 ms without projection, 1.11 ms with it; 1M x 20k, 65,000
+// root units: 718 -> 384 ms).
+constexpr uint64_t PROJECT_MIN_ROOTS_PER_SM = 16;
+static uint32_t deep_local_max(const cpm_ctx *ctx, const cpm_opts &o, bool smem_prefix, uint64_t max_stride,
+                               uint64_t n_roots) {
     if (o.deep_project == 1 || !smem_prefix) return 0;
     if (max_stride * 8 + max_stride > DEEP_SMEM_PREFIX_MAX) return 0;
-    return LOCAL_MAX_BITS;
+    if (o.deep_project >= 128) return std::min<uint32_t>((uint32_t)o.deep_project, LOCAL_MAX_BITS);
+    return n_roots >= PROJECT_MIN_ROOTS_PER_SM * (uint64_t)ctx->sms ? LOCAL_MAX_BITS : 0;
 }
 
 // k_deep<true>'s dynamic shared memory: the prefix bitmap, then the rank directory.
@@ -962,6 +972,9 @@ static void deep_set_local(DeepParams &P, const DeepBuffers &b, uint64_t max_str
     P.lq = local_max ? b.lq : nullptr;
     P.lq_cap = local_max ? b.queue_cap : 0;
     P.dir_off = (uint32_t)(max_stride * 8);
+    // Row-wise units off unless the caller sets them (one database only).
+    P.h_off = nullptr; P.h_rows = nullptr; P.h_fidx = nullptr; P.h_F = 0; P.h_cost = 0.f;
+    P.h_scratch = nullptr; P.h_scratch_words = 0; P.h_table_off = 0;
 }
 
 // The projected units k_deep queued, after it (same stream).
@@ -1317,6 +1330,9 @@ static int deep_rounds_run(cpm_ctx *ctx, DevScope &ds, DeepBuffers &b, const std
 
 // Eclat over a batch of databases (a single database is a batch of one).
 // Host syncs: frequent counts; pair counts; end of the deep phase.
+static int scan_u32(cpm_ctx *ctx, DevScope &ds, const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *total,
+                    uint64_t *d_tot = nullptr);
+
 static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const long long *ms, const cpm_opts &o,
                             cpm_result **res) {
     cpm_stats st{};
@@ -1572,8 +1588,14 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     const uint64_t spin = o.spin_limit ? o.spin_limit : (1ull << 26);
     const size_t prefix_bytes = max_stride * 8;
     const bool smem_prefix = prefix_bytes <= DEEP_SMEM_PREFIX_MAX;
-    const uint32_t local_max = deep_local_max(o, smem_prefix, max_stride);
-    const size_t smem_bytes = deep_smem_bytes(max_stride, local_max);
+    const uint32_t local_max = deep_local_max(ctx, o, smem_prefix, max_stride, n_units);
+    // Row-wise units (k_rows.cuh): one database, projection on, frequent
+    // indices below 2^16, and their F-entry table after the rank directory.
+    const uint32_t F0 = n_db == 1 ? F[0] : 0u;
+    const size_t h_table_bytes = ((size_t)F0 * 2 + 15) / 16 * 16;
+    const bool h_on = n_db == 1 && local_max && o.deep_rows != 1 && F0 >= 2 && F0 < H_NONE &&
+                      deep_smem_bytes(max_stride, local_max) + h_table_bytes <= DEEP_SMEM_PREFIX_MAX;
+    const size_t smem_bytes = deep_smem_bytes(max_stride, local_max) + (h_on ? h_table_bytes : 0);
     // Long tidsets leave room for fewer CTAs per SM: give each 16 or 32 warps
     // so that enough loads stay in flight; short ones run up to four 8-warp
     // CTAs.  Measured (deep phase): 1,564-word tidsets (planted-100k) 0.25 ms
@@ -1593,6 +1615,10 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
             return set_err(ctx, CPM_EINVAL, "deep_block must be 128, 256, 512 or 1024 (got %d)", o.deep_block);
         block = (unsigned)o.deep_block;
     }
+    if (o.deep_rows < 0 || o.deep_rows > 1)
+        return set_err(ctx, CPM_EINVAL, "deep_rows must be 0 or 1 (got %d)", o.deep_rows);
+    if (o.deep_project < 0 || (o.deep_project > 1 && o.deep_project < 128))
+        return set_err(ctx, CPM_EINVAL, "deep_project must be 0, 1 or 128-65408 (got %d)", o.deep_project);
     if (o.deep_ctas_per_sm) {
         if (o.deep_ctas_per_sm < 1 || o.deep_ctas_per_sm > 4)
             return set_err(ctx, CPM_EINVAL, "deep_ctas_per_sm must be 1-4 (got %d)", o.deep_ctas_per_sm);
@@ -1610,6 +1636,40 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     const unsigned grid = (unsigned)(ctx->sms * cta_per_sm);
     ctx->last_deep_block = (int)block;
     ctx->last_deep_ctas = cta_per_sm;
+    // Rows of the frequent indices and the row-wise units' other inputs.
+    uint64_t *d_hoff = nullptr;
+    uint16_t *d_hrows = nullptr, *d_hfidx = nullptr;
+    uint32_t *d_hscr = nullptr;
+    float h_cost = 0.f;
+    if (h_on) {
+        const cpm_db *d0 = dbs[0];
+        uint32_t *d_hlen = nullptr;
+        CKR(ds.alloc(&d_hlen, d0->n_tx + 1));
+        CKR(ds.alloc(&d_hoff, d0->n_tx + 1));
+        CK(cudaMemsetAsync(d_hlen + d0->n_tx, 0, 4, ctx->stream));
+        const unsigned nb = (unsigned)((d0->n_tx + 255) / 256);
+        if (d0->n_tx) {
+            k_hrows<false><<<nb, 256, 0, ctx->stream>>>(d0->d_bits, d0->stride, freq_all, F0, d0->n_tx, d_hlen,
+                                                        nullptr, nullptr);
+            CK(cudaGetLastError());
+        }
+        uint64_t nnz_f = 0;
+        CKR(scan_u32(ctx, ds, d_hlen, d_hoff, d0->n_tx + 1, &nnz_f));
+        CKR(ds.alloc(&d_hrows, std::max<uint64_t>(1, nnz_f)));
+        if (d0->n_tx) {
+            k_hrows<true><<<nb, 256, 0, ctx->stream>>>(d0->d_bits, d0->stride, freq_all, F0, d0->n_tx, nullptr,
+                                                       d_hoff, d_hrows);
+            CK(cudaGetLastError());
+        }
+        CKR(ds.alloc(&d_hfidx, std::max<uint32_t>(1, d0->n_items)));
+        CK(cudaMemsetAsync(d_hfidx, 0xff, (size_t)std::max<uint32_t>(1, d0->n_items) * 2, ctx->stream));
+        k_hrow_fidx<<<(F0 + 255) / 256, 256, 0, ctx->stream>>>(freq_all, F0, d_hfidx);
+        CK(cudaGetLastError());
+        CKR(ds.alloc(&d_hscr, (uint64_t)grid * local_max));
+        // A row visit: its frequent indices plus about three for the id and offsets.
+        h_cost = d0->n_tx ? (float)((double)nnz_f / (double)d0->n_tx) + 3.f : 0.f;
+        st.kernel_launches += 4;
+    }
     DeepState hs{};
     bool rounds = false, arena_exceeded = false;
     std::vector<float> features;  // per root unit, when traced (cost-model inputs)
@@ -1728,6 +1788,9 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         P.deferred_cap = n_units;
         P.root_key = nullptr; P.top_frames = 0; P.keys_in_words = 0; P.admit_words = 0;
         deep_set_local(P, b, max_stride, local_max);
+        P.h_off = d_hoff; P.h_rows = d_hrows; P.h_fidx = d_hfidx; P.h_F = F0; P.h_cost = h_cost;
+        P.h_scratch = d_hscr; P.h_scratch_words = local_max;
+        P.h_table_off = (uint32_t)deep_smem_bytes(max_stride, local_max);
         CK(cudaEventRecord(ctx->ev[2], ctx->stream));
         if (smem_prefix) k_deep<true><<<grid, block, smem_bytes, ctx->stream>>>(P);
         else k_deep<false><<<grid, block, 0, ctx->stream>>>(P);
@@ -1813,6 +1876,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
         st.bytes_alg = hs.bytes_alg;
         st.work_items = hs.work_items;
         st.projected_units = hs.local_units;
+        st.row_units = hs.h_units;
         CKR(deep_rounds(ctx, ds, b, frames, nullptr, nullptr, d_key, 0, base_patterns, P2_total, max_stride, grid, block,
                         smem_prefix, spin, 0, with_db, 0, learned, use_lists ? list_div : 0u, local_max, &cont, hs, st));
         rounds = continued = true;
@@ -1862,6 +1926,7 @@ static int mine_eclat_batch(cpm_ctx *ctx, cpm_db **dbs, uint32_t n_db, const lon
     st.frames = hs.n_frames;
     st.work_items = hs.work_items;
     st.projected_units = hs.local_units;
+    if (!rounds) st.row_units = hs.h_units;  // (rounds run no row-wise units)
     st.intersections = hs.intersections;
     st.bytes_alg = hs.bytes_alg;
     st.ms_pairs = rows ? elapsed_ms(ctx, 5, 6) : 0.0;
@@ -1922,7 +1987,7 @@ struct U32ToU64 {
 // Exclusive sum of n counts into out; with total, also its sum (one
 // device-to-host copy and a sync), without it nothing leaves the device.
 static int scan_u32(cpm_ctx *ctx, DevScope &ds, const uint32_t *in, uint64_t *out, uint64_t n, uint64_t *total,
-                    uint64_t *d_tot = nullptr) {
+                    uint64_t *d_tot) {
     if (total) *total = 0;
     if (!n) return CPM_OK;
     if (n <= 4096) {
@@ -3341,6 +3406,8 @@ extern "C" int cpm_mine_eclat_noalloc(cpm_ctx *ctx, const uint64_t *d_bits, uint
     P.prefetch = 0;
     P.lists = 0;
     P.local_max = 0; P.lq = nullptr; P.lq_cap = 0; P.dir_off = 0;  // no projection: one launch, fixed scratch
+    P.h_off = nullptr; P.h_rows = nullptr; P.h_fidx = nullptr; P.h_F = 0; P.h_cost = 0.f;
+    P.h_scratch = nullptr; P.h_scratch_words = 0; P.h_table_off = 0;
     P.root_frames = 0; P.defer_words = 0; P.defer_members = 0; P.defer_frames = 0; P.defer_queue = 0;
     P.root_key = nullptr; P.top_frames = 0; P.keys_in_words = 0; P.admit_words = 0;
     P.deferred = nullptr; P.deferred_cap = 0;

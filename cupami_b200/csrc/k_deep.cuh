@@ -95,6 +95,7 @@ struct DeepState {
     CPM_LINE(lq_tail);      // projected units: entries reserved
     CPM_LINE(lq_pending);   // projected units queued or running
     CPM_LINE(local_units);  // projected units run
+    CPM_LINE(h_units);      // row-wise units run
     unsigned int error;
     unsigned int pad[31];
 };
@@ -148,7 +149,25 @@ struct DeepParams {
     uint64_t lq_cap;
     uint32_t local_max;
     uint32_t dir_off;
+    // Row-wise units (h_rows null: off; one database, projection on): the
+    // rows of its frequent indices (k_rows.cuh: row t at h_rows[h_off[t]
+    // .. h_off[t + 1])), the column -> frequent index map, the work of one
+    // row visit against one sibling id or 16-byte word, a per-CTA scratch of
+    // h_scratch_words transaction ids, and the byte offset in the dynamic
+    // shared memory of the h_F-entry frequent index -> sibling table.
+    const uint64_t *h_off;
+    const uint16_t *h_rows;
+    const uint16_t *h_fidx;
+    uint32_t h_F;
+    float h_cost;
+    uint32_t *h_scratch;
+    uint32_t h_scratch_words;
+    uint32_t h_table_off;
 };
+
+// Row-wise units need at least this many siblings.
+constexpr uint32_t H_MIN_SIBLINGS = 8;
+constexpr uint16_t H_NONE = 0xffffu;
 
 constexpr int UNIT_LOG_WORDS = 12;
 
@@ -586,6 +605,9 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     __shared__ uint32_t s_pid[1024];             // units of at most blockDim siblings: pattern id of each
     __shared__ uint16_t s_map[1024];             // ... and, after compaction, each survivor's sibling index
     __shared__ uint32_t s_clast[32];             // pass 2: ids in each warp's last piece of a split child
+    __shared__ uint16_t s_f[1024];               // row-wise units: frequent index of each sibling
+    __shared__ const uint32_t *s_hids;           // ... the prefix's transaction ids, and their count
+    __shared__ uint32_t s_hn;
     __shared__ unsigned long long s_bytes;
     __shared__ uint32_t s_nsurv;         // survivors counted in pass 1
     __shared__ uint32_t s_part[32];      // per-sibling sums when siblings are split over warps
@@ -613,6 +635,11 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     // Kept in shared memory, not registers: only thread 0 touches them.
     __shared__ unsigned long long c_inter, c_bytes, c_units, c_surv, c_busy, t_unit;
     if (threadIdx.x == 0) c_inter = c_bytes = c_units = c_surv = c_busy = t_unit = 0;
+
+    // Row-wise units' frequent index -> sibling table: empty between units.
+    uint16_t *const s_tab = reinterpret_cast<uint16_t *>(reinterpret_cast<char *>(s_prefix) + P.h_table_off);
+    if (SMEM_PREFIX && P.h_rows)
+        for (uint32_t i = threadIdx.x; i < P.h_F; i += blockDim.x) s_tab[i] = H_NONE;
 
     unsigned long long next_ticket = NO_TICKET;  // thread 0's ticket taken ahead
     for (;;) {
@@ -693,7 +720,29 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         const unsigned long long praw = ld_raw_ptr(P.mem_bits + mem_off + p);
         const ulonglong2 *pb = reinterpret_cast<const ulonglong2 *>(praw);
         uint64_t prefix_bytes = 8ull * stride;
-        if (SMEM_PREFIX && (praw & 1ull)) {
+        // Row-wise unit: a list prefix of at most local_max transactions whose
+        // rows (each ~h_cost work) take less work than the siblings' ids and
+        // words.  Every input is the same on every thread, so is the choice.
+        bool hmode = false;
+        uint32_t h_np = 0;
+        if (SMEM_PREFIX && P.h_rows && fast && cnt >= H_MIN_SIBLINGS && (praw & 1ull) && !P.shallow) {
+            h_np = __ldcg(P.pat_sup + __ldcg(P.mem_pat + mem_off + p));
+            if (h_np >= 1 && h_np <= P.local_max) {
+                uint64_t work = 0;
+                if (threadIdx.x < cnt) {
+                    const unsigned long long raw = ld_raw_ptr(P.mem_bits + mem_off + p + 1 + threadIdx.x);
+                    s_raw[threadIdx.x] = raw;
+                    work = sibling_units<SMEM_PREFIX>(raw, n2);
+                }
+                uint64_t tot = 0;
+                block_excl_scan_u64(work, s_w64, &tot);
+                hmode = (double)h_np * (double)P.h_cost < (double)tot;
+            }
+        }
+        if (SMEM_PREFIX && hmode) {
+            // No bitmap: the prefix is read as its list of transactions.
+            prefix_bytes = 8ull * list_words(h_np);
+        } else if (SMEM_PREFIX && (praw & 1ull)) {
             // List prefix: clear the bitmap, set its transactions, then apply the mask.
             const uint32_t *L = reinterpret_cast<const uint32_t *>(praw & ~1ull);
             const uint32_t n = __ldcg(L);
@@ -739,7 +788,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             s_ok = err_seen == 0;
         }
         __syncthreads();
-        if (SMEM_PREFIX && threadIdx.x == 0 && !mk && !(praw & 1ull) && n2 >= BULK_MIN_WORDS2) s_bulk_phase ^= 1u;
+        if (SMEM_PREFIX && threadIdx.x == 0 && !hmode && !mk && !(praw & 1ull) && n2 >= BULK_MIN_WORDS2) s_bulk_phase ^= 1u;
         if (threadIdx.x == 0 && P.unit_log) {
             lg[1] = global_ns();
             lg[3] = prefix_bytes | (SMEM_PREFIX && (praw & 1ull) ? 1ull << 63 : 0ull) | (mk ? 1ull << 62 : 0ull);
@@ -775,7 +824,80 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             }
             if (pid32 != NO_PATTERN) atomicAdd(&s_nsurv, 1u);
         };
-        if (P.balance) {
+        // Row-wise units: the prefix's transactions, as ids (kept for pass 2).
+        const uint32_t *h_ids = nullptr;
+        uint32_t h_n = 0;
+        if (SMEM_PREFIX && hmode) {
+            // The member's list, or for a top-level class the ids of it that
+            // the class item's tidset holds, compacted in order into this
+            // CTA's scratch.
+            const uint32_t *L = reinterpret_cast<const uint32_t *>(praw & ~1ull);
+            const uint32_t n_m = __ldcg(L);
+            if (!mk) {
+                h_ids = L + 4;
+                h_n = n_m;
+            } else {
+                uint32_t *scr = P.h_scratch + (uint64_t)blockIdx.x * P.h_scratch_words;
+                const unsigned long long *m64 = reinterpret_cast<const unsigned long long *>(mk);
+                const uint32_t per = (n_m + blockDim.x - 1) / blockDim.x;
+                const uint32_t a = min(n_m, threadIdx.x * per), b = min(n_m, a + per);
+                uint32_t c = 0;
+                for (uint32_t j = a; j < b; ++j) {
+                    const uint32_t t = __ldcg(L + 4 + j);
+                    c += (uint32_t)(__ldcg(m64 + (t >> 6)) >> (t & 63)) & 1u;
+                }
+                uint64_t tot = 0;
+                uint64_t at = block_excl_scan_u64(c, s_w64, &tot);
+                for (uint32_t j = a; j < b; ++j) {
+                    const uint32_t t = __ldcg(L + 4 + j);
+                    if ((__ldcg(m64 + (t >> 6)) >> (t & 63)) & 1ull) {
+                        if (at < P.h_scratch_words) scr[at] = t;
+                        ++at;
+                    }
+                }
+                h_ids = scr;
+                h_n = (uint32_t)(tot < P.h_scratch_words ? tot : (uint64_t)P.h_scratch_words);
+            }
+            // The prefix's count sized the projection: anything else is an error,
+            // and no more than that many transactions are read.
+            if (h_n != h_np && threadIdx.x == 0) deep_fail(st, DEEP_ERR_INTERNAL);
+            h_n = min(h_n, h_np);
+            if (threadIdx.x == 0) {
+                s_hids = h_ids;
+                s_hn = h_n;
+                atomicAdd(&st->h_units, 1ull);
+            }
+            uint32_t my_f = H_NONE;
+            if (threadIdx.x < cnt) {
+                my_f = __ldg(P.h_fidx + __ldcg(P.mem_item + mem_off + p + 1 + threadIdx.x));
+                s_f[threadIdx.x] = (uint16_t)my_f;
+                s_cnt[threadIdx.x] = 0;
+                if (my_f < P.h_F) s_tab[my_f] = (uint16_t)threadIdx.x;
+                else deep_fail(st, DEEP_ERR_INTERNAL);
+            }
+            __syncthreads();  // the table and the scratch ids are in place
+            // Every row of the prefix: each frequent index that is a later
+            // member adds one to that member's support.
+            unsigned long long visited = 0, nrows = 0;
+            for (uint32_t j = threadIdx.x; j < h_n; j += blockDim.x) {
+                const uint32_t t = __ldcg(h_ids + j);
+                const uint32_t ra = __ldg(P.h_off + t), rb = __ldg(P.h_off + t + 1);
+                visited += rb - ra;
+                ++nrows;
+                for (uint32_t k = ra; k < rb; ++k) {
+                    const uint32_t sib = s_tab[__ldg(P.h_rows + k)];
+                    if (sib != H_NONE) atomicAdd(&s_cnt[sib], 1u);
+                }
+            }
+            // Bytes read: an id and two offsets per row, two per frequent index.
+            if (nrows) atomicAdd(&s_bytes, 2ull * visited + 12ull * nrows);
+            __syncthreads();  // every count is in
+            if (ok && threadIdx.x < cnt) {
+                const uint32_t q = threadIdx.x;
+                emit(q, s_cnt[q], __ldcg(P.mem_item + mem_off + p + 1 + q), s_raw[q]);
+            }
+            if (threadIdx.x < cnt && my_f < P.h_F) s_tab[my_f] = H_NONE;  // nobody reads it before the next barrier
+        } else if (P.balance) {
             // Siblings split over warps by size.  Per chunk of up to blockDim
             // siblings: every sibling's work (bitset words or list ids) is
             // laid end to end, each warp takes an equal slice of the total
@@ -1025,7 +1147,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         }
         __syncthreads();
         uint16_t *const s_dir = reinterpret_cast<uint16_t *>(reinterpret_cast<char *>(s_prefix) + P.dir_off);
-        if (SMEM_PREFIX && proj && s_grant) {
+        if (SMEM_PREFIX && proj && s_grant && !hmode) {
             // Rank directory of the prefix, and the child block zeroed for
             // the bits the projected writers OR in.
             build_rank_dir(s_prefix, n2, s_dir, s_w64);
@@ -1049,7 +1171,55 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         // each piece's first output position: a warp whose slice ends inside
         // a list child first counts that last piece (s_clast), and a warp that
         // starts inside one adds up the counts of the warps before it.
-        if (s_grant) {
+        if (SMEM_PREFIX && hmode && s_grant) {
+            // Row-wise children (projected): survivor k's child has bit j set
+            // when the j-th transaction of the prefix holds survivor k's item.
+            // A warp takes 32 consecutive transactions, each lane marks the
+            // survivors in its row (64 at a time), and one ballot per survivor
+            // is a whole 32-bit word of its child: plain stores, every word
+            // written once, the padding after the last transaction zeroed.
+            uint32_t *blk32 = reinterpret_cast<uint32_t *>(P.arena + s_arena_base);
+            const uint32_t *const h_ids2 = s_hids;
+            const uint32_t h_n2 = s_hn;
+            const uint32_t nw32 = 2u * lstride, used32 = (h_n2 + 31u) / 32u;
+            for (uint32_t g0 = 0; g0 < ns; g0 += 64) {
+                const uint32_t gn = min(64u, ns - g0);
+                if (threadIdx.x < gn) {
+                    const uint32_t f = s_f[s_map[g0 + threadIdx.x]];
+                    if (f < P.h_F) s_tab[f] = (uint16_t)threadIdx.x;  // (pass 1 flagged any other)
+                }
+                __syncthreads();
+                for (uint32_t w = wid; w < used32; w += nw) {
+                    const uint32_t j = w * 32u + lane;
+                    unsigned long long mark = 0;
+                    if (j < h_n2) {
+                        const uint32_t t = __ldcg(h_ids2 + j);
+                        const uint32_t ra = __ldg(P.h_off + t), rb = __ldg(P.h_off + t + 1);
+                        for (uint32_t k = ra; k < rb; ++k) {
+                            const uint32_t g = s_tab[__ldg(P.h_rows + k)];
+                            if (g < 64u) mark |= 1ull << g;
+                        }
+                    }
+                    for (uint32_t k = 0; k < gn; ++k) {
+                        const unsigned word = __ballot_sync(CPM_FULL, (unsigned)(mark >> k) & 1u);
+                        if (lane == (k & 31u)) blk32[(uint64_t)(g0 + k) * nw32 + w] = word;
+                    }
+                }
+                __syncthreads();  // the group's rows are read
+                if (threadIdx.x < gn) {
+                    const uint32_t f = s_f[s_map[g0 + threadIdx.x]];
+                    if (f < P.h_F) s_tab[f] = H_NONE;
+                }
+                __syncthreads();  // the table is empty again
+            }
+            const uint32_t pad = nw32 - used32;
+            for (uint64_t i = threadIdx.x; i < (uint64_t)ns * pad; i += blockDim.x)
+                blk32[(i / pad) * nw32 + used32 + i % pad] = 0u;
+            if (threadIdx.x < ns)
+                P.mem_bits[s_mem_base + threadIdx.x] =
+                    reinterpret_cast<const uint64_t *>(P.arena + s_arena_base + (uint64_t)threadIdx.x * lstride);
+            __threadfence();
+        } else if (s_grant) {
             uint64_t chunk_base = 0;
             for (uint32_t start = 0; start < ns; start += blockDim.x) {
                 const uint32_t cn = min((uint32_t)blockDim.x, ns - start);

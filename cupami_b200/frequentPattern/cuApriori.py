@@ -81,8 +81,13 @@ class cuApriori:
     _DEEP_BALANCE = 0
     #: Deep levels below small prefixes: 0 automatic (children of a prefix of
     #: at most 65,408 transactions become bitsets numbered by rank within it,
-    #: mined one unit per warp); 1 off.
+    #: mined one unit per warp, when the search is large enough); 1 off;
+    #: 128-65408 the largest projected prefix, always.
     _DEEP_PROJECT = 0
+    #: Deep levels of one database with projection: 0 automatic (units whose
+    #: prefix rows are cheaper than their siblings' tidsets count row by
+    #: row); 1 off.
+    _DEEP_ROWS = 0
 
     def __init__(self, iFile, minSup, sep=None, use_gds="auto", use_gpu_io="auto"):
         t0 = time.perf_counter()
@@ -292,6 +297,7 @@ class cuApriori:
         opts.tidsets = int(self._TIDSETS)
         opts.deep_balance = int(self._DEEP_BALANCE)
         opts.deep_project = int(self._DEEP_PROJECT)
+        opts.deep_rows = int(self._DEEP_ROWS)
         return opts
 
     def autotune(self):

@@ -98,9 +98,13 @@ typedef struct {
                                       of its bitset; 0 = the autotuner's choice, else 1 */
     int32_t  deep_balance;         /* deep-level siblings: 0 = automatic (a warp per sibling), 1 = a warp
                                       per sibling, 2 = split over warps by size */
-    int32_t  deep_project;         /* deep levels: 0 = automatic (a unit whose prefix holds at most 65,408
-                                      transactions writes its children as bitsets numbered by rank within
-                                      the prefix, mined one unit per warp), 1 = off */
+    int32_t  deep_project;         /* deep levels: a unit whose prefix holds at most L transactions writes
+                                      its children as bitsets numbered by rank within the prefix, mined one
+                                      unit per warp.  0 = automatic (L = 65,408 when the search has at least
+                                      16 root units per SM, else off), 1 = off, 128..65408 = L */
+    int32_t  deep_rows;            /* deep levels of one database, with projection: 0 = automatic (a unit
+                                      whose prefix rows take less work than its siblings' tidsets counts
+                                      and writes its children row by row), 1 = off */
 } cpm_opts;
 
 typedef struct {
@@ -123,6 +127,7 @@ typedef struct {
     double   pair_tops;            /* pair_ops / ms_pairs */
     uint64_t projected_units;      /* of work_items: units below a projected prefix (one warp each) */
     double   ms_local;             /* of ms_deep: the launches that mine those units */
+    uint64_t row_units;            /* of work_items: units counted row by row (deep_rows) */
 } cpm_stats;
 
 /* ---- context ------------------------------------------------------------ */

@@ -107,7 +107,7 @@ def test_cli_writes_reference_format(tmp_path):
     assert out.read_text() == "1 : 2\n2 : 2\n"
 
 
-@pytest.mark.parametrize("arena_kb,project", [(64, 0), (64, 1), (512, 1)])
+@pytest.mark.parametrize("arena_kb,project", [(64, 65408), (64, 1), (512, 1)])
 def test_memory_bounded_rounds_are_exact(oracle_lib, arena_kb, project):
     """A small child-tidset arena forces bounded rounds, halving and shallow
     splits (with projected levels, whose children are smaller, and without)."""
@@ -248,21 +248,33 @@ def test_projected_levels_agree(oracle_lib, name, minsup):
     else:
         csr = getattr(datasets, name)()
     out = {}
-    for project in (0, 1):
+    # automatic, off, and prefixes of at most 1,000 / 16,384 / 65,408 transactions
+    for project in (0, 1, 1000, 16384, 65408):
         for tidsets in (0, 1, 2):
             m = cupami_b200.cuEclat(csr, minsup)
             m._DEEP_PROJECT, m._TIDSETS = project, tidsets
             m.mine()
             out[project, tidsets] = (list(m.getPatterns().items()), m.getKernelStats())
+    # Row-wise counting of small prefixes (one database, projection on), off and on.
+    for rows in (0, 1):
+        for tidsets in (0, 2):
+            m = cupami_b200.cuEclat(csr, minsup)
+            m._DEEP_PROJECT, m._TIDSETS, m._DEEP_ROWS = 65408, tidsets, rows
+            m.mine()
+            out["rows", rows, tidsets] = (list(m.getPatterns().items()), m.getKernelStats())
     want = out[1, 0][0]
     assert all(v[0] == want for v in out.values())
+    assert out["rows", 1, 0][1]["row_units"] == 0
+    if name == "sparse_zipf_small":  # list prefixes with many long list siblings
+        assert out["rows", 0, 2][1]["row_units"] > 0
     labels, arrays = oracle_lib.mine_csr(csr.offsets, csr.items, minsup)
     assert dict(want) == oracle_lib.to_dict(labels, arrays)
     # Projection moved units to the warp-per-unit kernel; without it none.
     # (uniform_poisson has no frequent 3-itemset, and every dense_bernoulli
     # prefix holds over 39,000 transactions: nothing is projected there.)
     if name in ("planted_zipf", "sparse_zipf_small"):
-        assert out[0, 0][1]["projected_units"] > 0
+        assert out[16384, 0][1]["projected_units"] > 0
+        assert out[65408, 0][1]["projected_units"] >= out[16384, 0][1]["projected_units"]
     assert out[1, 0][1]["projected_units"] == 0
 
 
@@ -279,12 +291,14 @@ def test_projected_levels_in_rounds_and_batches(oracle_lib):
     for arena in (64 << 10, 512 << 10, 0):
         m = cuEclat(csr, 0.004)
         m._ARENA_BYTES = arena
+        m._DEEP_PROJECT = 65408  # a small search: projected only when asked
         m.mine()
+        assert m.getKernelStats()["projected_units"] > 0
         assert m.getPatterns() == want, arena
         if arena:
             assert m.getKernelStats()["deep_rounds"] > 1
     csrs = datasets.batched_zipf(limit=16)
-    for project in (0, 1):
+    for project in (0, 1, 65408):
         cls = type("E", (cuEclat,), {"_DEEP_PROJECT": project})
         for c, m in zip(csrs, cls.mineBatch(csrs, 0.01)):
             labels, arrays = oracle_lib.mine_csr(c.offsets, c.items, 0.01)
