@@ -894,28 +894,37 @@ def run_ours(args, world, rank, local):
         # The last collective: rank 0's baselines below run on its own, so no
         # rank waits on a barrier while they do.
         pg.destroy_process_group()
-    # Roofline of the deep-level intersection kernel (k_deep), the step's
-    # dominant kernel on Eclat workloads, from its own CUDA events.
+    # Roofline of the deep phase (k_deep, then k_local for the units below
+    # projected prefixes), the step's dominant part on Eclat workloads, from
+    # its own CUDA events.
     hbm, bf16, src = peaks()
     eclat_stats = [[st for a, st, _ in out if a != "apriori"] for out in per_kernel]
     roof = None
     if eclat_stats and eclat_stats[0]:
         deep_ms = statistics.mean(sum(s["ms_deep"] for s in st) for st in eclat_stats)
         deep_bytes = statistics.mean(sum(s["bytes_alg"] for s in st) for st in eclat_stats)
+        local_ms = statistics.mean(sum(s.get("ms_local", 0.0) for s in st) for st in eclat_stats)
+        proj_units = statistics.mean(sum(s.get("projected_units", 0) for s in st) for st in eclat_stats)
+        row_units = statistics.mean(sum(s.get("row_units", 0) for s in st) for st in eclat_stats)
+        units = statistics.mean(sum(s.get("work_items", 0) for s in st) for st in eclat_stats)
         achieved = deep_bytes / (deep_ms * 1e-3) / 1e9 if deep_ms else 0.0
         tr = deep_traffic(args.workload, args.tidsets, args.arena_mb)
         traffic = tr["dram_bytes_per_launch"] if tr else None
-        roof = {"kernel": "k_deep (deep-level AND+popcount, persistent)", "bound": deep_bound(traffic, deep_bytes),
+        roof = {"kernel": "deep phase: k_deep (persistent, a CTA per unit) then k_local (a warp per projected unit)",
+                "bound": deep_bound(traffic, deep_bytes),
                 "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                 "peak_source": src, "frac_of": "HBM copy bandwidth (" + src + "); algorithmic bytes / kernel time",
                 "frac_of_8tbs_spec": achieved / 8000.0,
                 "dram_share_of_alg_bytes": traffic / deep_bytes if traffic and deep_bytes else None,
                 "l2_bytes_per_launch": tr.get("l2_bytes_per_launch") if tr else None,
                 "traffic_source": ("profiles/k_deep_traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                   "of one launch): " + tr["profile"]) if tr else None,
-                "ms_per_launch": deep_ms, "alg_bytes_per_launch": deep_bytes,
+                                   "of one launch of each kernel): " + tr["profile"]) if tr else None,
+                "ms_per_launch": deep_ms, "ms_k_local": local_ms, "alg_bytes_per_launch": deep_bytes,
+                "units": units, "projected_units": proj_units, "row_units": row_units,
                 "alg_bytes": "sum over units of the prefix, every sibling and every child written, each at its "
-                             "own form's size (bitset 8*W, list 16 + 4*ids)"}
+                             "own form's size (bitset 8*W, list 16 + 4*ids, projected bitset 16*ceil(n/128)); "
+                             "row-wise units count their prefix's rows instead of the siblings (12 B per row "
+                             "+ 2 B per frequent index)"}
     pair_ms = statistics.mean(sum(st["ms_pairs"] for _, st, _ in out) for out in per_kernel)
     pair_ops = statistics.mean(sum(st["pair_ops"] for _, st, _ in out) for out in per_kernel)
     int8_peak = int8_peak_tops()

@@ -287,18 +287,30 @@ __global__ void __launch_bounds__(1024) k_level_keep(const uint32_t *__restrict_
     __shared__ uint64_t s_w[32];
     const uint64_t pid_base = d_cnt2[1];
     uint64_t run = 0;
-    for (uint64_t base = 0; base < n; base += blockDim.x) {
-        const uint64_t i = base + threadIdx.x;
-        const uint32_t f = i < n ? pass[i] : 0u;
+    // Each thread takes eight consecutive candidates per round, so that a
+    // level of n candidates costs n / (8 * blockDim) block scans.
+    constexpr uint32_t PER = 8;
+    for (uint64_t base = 0; base < n; base += (uint64_t)blockDim.x * PER) {
+        const uint64_t i0 = base + (uint64_t)threadIdx.x * PER;
+        uint32_t f[PER], c = 0;
+#pragma unroll
+        for (uint32_t u = 0; u < PER; ++u) {
+            f[u] = i0 + u < n ? pass[i0 + u] : 0u;
+            c += f[u] ? 1u : 0u;
+        }
         uint64_t tot = 0;
-        const uint64_t p = run + cta_excl_sum(f, s_w, &tot);
-        if (f) {
+        uint64_t p = run + cta_excl_sum(c, s_w, &tot);
+#pragma unroll
+        for (uint32_t u = 0; u < PER; ++u) {
+            if (!f[u]) continue;
+            const uint64_t i = i0 + u;
             for (uint32_t j = 0; j < w; ++j) L_next[p * w + j] = cand[i * w + j];
             const uint64_t pid = pid_base + p;
             pid_next[p] = (uint32_t)pid;
             pat_parent[pid] = pid_prev[cand_left[i]];
             pat_item[pid] = cand[i * w + w - 1];
             pat_sup[pid] = sup[i];
+            ++p;
         }
         run += tot;
     }

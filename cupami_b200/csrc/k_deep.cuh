@@ -134,7 +134,7 @@ struct DeepParams {
     // Diagnostics (null: off): per unit, UNIT_LOG_WORDS words -- claim,
     // prefix-staged, pass-1-done and end times (globaltimer ns), CTA,
     // siblings | survivors << 32, sibling bytes, largest sibling's bytes,
-    // prefix bytes | list prefix << 63 | top-level << 62, then the times the
+    // prefix bytes | list prefix << 63 | top-level << 62 | row-wise << 61, then the times the
     // survivors were compacted, the child block granted and the children
     // written (0 for units that end after pass 1).
     // unit_log[0] counts the units logged; records start at unit_log + 1.
@@ -167,6 +167,10 @@ struct DeepParams {
 
 // Row-wise units need at least this many siblings.
 constexpr uint32_t H_MIN_SIBLINGS = 8;
+// The projected writers' instructions per sibling id or 16-byte word (a rank
+// lookup and a segmented OR, or a compress and atomics) over a row visit's
+// per frequent index (a load and a table lookup): about four.
+constexpr double H_P2_WEIGHT = 4.0;
 constexpr uint16_t H_NONE = 0xffffu;
 
 constexpr int UNIT_LOG_WORDS = 12;
@@ -605,8 +609,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
     __shared__ uint32_t s_pid[1024];             // units of at most blockDim siblings: pattern id of each
     __shared__ uint16_t s_map[1024];             // ... and, after compaction, each survivor's sibling index
     __shared__ uint32_t s_clast[32];             // pass 2: ids in each warp's last piece of a split child
-    __shared__ uint16_t s_f[1024];               // row-wise units: frequent index of each sibling
-    __shared__ const uint32_t *s_hids;           // ... the prefix's transaction ids, and their count
+    __shared__ const uint32_t *s_hids;           // row-wise pass 2: the prefix's transaction ids, and their count
     __shared__ uint32_t s_hn;
     __shared__ unsigned long long s_bytes;
     __shared__ uint32_t s_nsurv;         // survivors counted in pass 1
@@ -791,7 +794,8 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         if (SMEM_PREFIX && threadIdx.x == 0 && !hmode && !mk && !(praw & 1ull) && n2 >= BULK_MIN_WORDS2) s_bulk_phase ^= 1u;
         if (threadIdx.x == 0 && P.unit_log) {
             lg[1] = global_ns();
-            lg[3] = prefix_bytes | (SMEM_PREFIX && (praw & 1ull) ? 1ull << 63 : 0ull) | (mk ? 1ull << 62 : 0ull);
+            lg[3] = prefix_bytes | (SMEM_PREFIX && (praw & 1ull) ? 1ull << 63 : 0ull) | (mk ? 1ull << 62 : 0ull) |
+                    (hmode ? 1ull << 61 : 0ull);
         }
         const bool ok = s_ok != 0;
         const uint32_t parent_pat = __ldcg(P.mem_pat + mem_off + p);
@@ -842,18 +846,32 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 const uint32_t per = (n_m + blockDim.x - 1) / blockDim.x;
                 const uint32_t a = min(n_m, threadIdx.x * per), b = min(n_m, a + per);
                 uint32_t c = 0;
-                for (uint32_t j = a; j < b; ++j) {
-                    const uint32_t t = __ldcg(L + 4 + j);
-                    c += (uint32_t)(__ldcg(m64 + (t >> 6)) >> (t & 63)) & 1u;
+                // Eight ids, then their eight mask words, in flight at a time.
+                for (uint32_t j0 = a; j0 < b; j0 += 8) {
+                    uint32_t t[8];
+                    unsigned long long mw[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) t[u] = j0 + u < b ? __ldcg(L + 4 + j0 + u) : 0u;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) mw[u] = j0 + u < b ? __ldcg(m64 + (t[u] >> 6)) : 0ull;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) c += (uint32_t)(mw[u] >> (t[u] & 63)) & 1u;
                 }
                 uint64_t tot = 0;
                 uint64_t at = block_excl_scan_u64(c, s_w64, &tot);
-                for (uint32_t j = a; j < b; ++j) {
-                    const uint32_t t = __ldcg(L + 4 + j);
-                    if ((__ldcg(m64 + (t >> 6)) >> (t & 63)) & 1ull) {
-                        if (at < P.h_scratch_words) scr[at] = t;
-                        ++at;
-                    }
+                for (uint32_t j0 = a; j0 < b; j0 += 8) {
+                    uint32_t t[8];
+                    unsigned long long mw[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) t[u] = j0 + u < b ? __ldcg(L + 4 + j0 + u) : 0u;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) mw[u] = j0 + u < b ? __ldcg(m64 + (t[u] >> 6)) : 0ull;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if ((mw[u] >> (t[u] & 63)) & 1ull) {
+                            if (at < P.h_scratch_words) scr[at] = t[u];
+                            ++at;
+                        }
                 }
                 h_ids = scr;
                 h_n = (uint32_t)(tot < P.h_scratch_words ? tot : (uint64_t)P.h_scratch_words);
@@ -870,12 +888,23 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             uint32_t my_f = H_NONE;
             if (threadIdx.x < cnt) {
                 my_f = __ldg(P.h_fidx + __ldcg(P.mem_item + mem_off + p + 1 + threadIdx.x));
-                s_f[threadIdx.x] = (uint16_t)my_f;
                 s_cnt[threadIdx.x] = 0;
                 if (my_f < P.h_F) s_tab[my_f] = (uint16_t)threadIdx.x;
                 else deep_fail(st, DEEP_ERR_INTERNAL);
             }
-            __syncthreads();  // the table and the scratch ids are in place
+            // Counters: copies in the (unused) prefix-bitmap region, one per
+            // group of warps, so that the many rows holding a popular item do
+            // not all add to one shared word; else s_cnt alone.
+            uint32_t copies = 1;
+            {
+                const uint64_t fit = (P.max_stride * 8) / (4ull * cnt);
+                while (copies * 2 <= nw && copies * 2 <= fit) copies *= 2;
+            }
+            uint32_t *const s_wc = copies > 1 ? reinterpret_cast<uint32_t *>(s_prefix) : s_cnt;
+            if (copies > 1)
+                for (uint32_t i = threadIdx.x; i < copies * cnt; i += blockDim.x) s_wc[i] = 0u;
+            uint32_t *const my_wc = s_wc + (wid & (copies - 1)) * cnt;
+            __syncthreads();  // the table, the counters and the scratch ids are in place
             // Every row of the prefix: each frequent index that is a later
             // member adds one to that member's support.
             unsigned long long visited = 0, nrows = 0;
@@ -884,9 +913,17 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                 const uint32_t ra = __ldg(P.h_off + t), rb = __ldg(P.h_off + t + 1);
                 visited += rb - ra;
                 ++nrows;
-                for (uint32_t k = ra; k < rb; ++k) {
-                    const uint32_t sib = s_tab[__ldg(P.h_rows + k)];
-                    if (sib != H_NONE) atomicAdd(&s_cnt[sib], 1u);
+                // Eight frequent indices of the row in flight at a time.
+                for (uint32_t k0 = ra; k0 < rb; k0 += 8) {
+                    uint32_t f[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) f[u] = k0 + u < rb ? (uint32_t)__ldg(P.h_rows + k0 + u) : H_NONE;
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (f[u] != H_NONE) {
+                            const uint32_t sib = s_tab[f[u]];
+                            if (sib != H_NONE) atomicAdd(my_wc + sib, 1u);
+                        }
                 }
             }
             // Bytes read: an id and two offsets per row, two per frequent index.
@@ -894,7 +931,9 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             __syncthreads();  // every count is in
             if (ok && threadIdx.x < cnt) {
                 const uint32_t q = threadIdx.x;
-                emit(q, s_cnt[q], __ldcg(P.mem_item + mem_off + p + 1 + q), s_raw[q]);
+                uint32_t sup = 0;
+                for (uint32_t c = 0; c < copies; ++c) sup += s_wc[c * cnt + q];
+                emit(q, sup, __ldcg(P.mem_item + mem_off + p + 1 + q), s_raw[q]);
             }
             if (threadIdx.x < cnt && my_f < P.h_F) s_tab[my_f] = H_NONE;  // nobody reads it before the next barrier
         } else if (P.balance) {
@@ -995,7 +1034,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             unsigned long long *r = P.unit_log + 1 + k * UNIT_LOG_WORDS;
             r[0] = lg[0]; r[1] = lg[1]; r[2] = lg[2]; r[3] = global_ns(); r[4] = blockIdx.x;
             r[5] = (unsigned long long)cnt | ((unsigned long long)nsurv << 32);
-            r[6] = s_bytes - (lg[3] & ((1ull << 62) - 1)); r[7] = s_maxb; r[8] = lg[3];
+            r[6] = s_bytes - (lg[3] & ((1ull << 61) - 1)); r[7] = s_maxb; r[8] = lg[3];
             r[9] = lg[4]; r[10] = lg[5]; r[11] = lg[6];
         };
         if (s_nsurv < 2) {
@@ -1135,6 +1174,16 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             block_excl_scan_u64(part, s_w64, &tot);
             child_words = tot;
         }
+        // Children written row by row (the row-wise pass 2 below): always for
+        // row-wise units, and for the other projected units of one database
+        // when the prefix's rows (plus a ballot per 32 transactions and
+        // survivor) are less work than the projected writers' pass over the
+        // survivors' siblings, weighted by H_P2_WEIGHT (units of more than
+        // blockDim siblings: always).
+        const bool rows_p2 =
+            SMEM_PREFIX && proj && P.h_rows &&
+            (hmode || !fast ||
+             (double)n_pre * ((double)P.h_cost + ns / 32.0) < H_P2_WEIGHT * (double)fast_wtot);
         if (threadIdx.x == 0) {
             s_grant = 0;
             s_fid = ~0ull;
@@ -1147,7 +1196,30 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         }
         __syncthreads();
         uint16_t *const s_dir = reinterpret_cast<uint16_t *>(reinterpret_cast<char *>(s_prefix) + P.dir_off);
-        if (SMEM_PREFIX && proj && s_grant && !hmode) {
+        if (SMEM_PREFIX && rows_p2 && s_grant && !hmode) {
+            // The prefix's transaction ids, in order, from its bitmap and rank
+            // directory into this CTA's scratch, for the row-wise pass 2.
+            build_rank_dir(s_prefix, n2, s_dir, s_w64);
+            __syncthreads();
+            uint32_t *scr = P.h_scratch + (uint64_t)blockIdx.x * P.h_scratch_words;
+            for (uint64_t v = threadIdx.x; v < n2; v += blockDim.x) {
+                const ulonglong2 w = s_prefix[v];
+                uint32_t r = s_dir[v];
+                for (unsigned long long b = w.x; b; b &= b - 1, ++r)
+                    if (r < P.h_scratch_words) scr[r] = (uint32_t)(v * 128 + __ffsll((long long)b) - 1);
+                for (unsigned long long b = w.y; b; b &= b - 1, ++r)
+                    if (r < P.h_scratch_words) scr[r] = (uint32_t)(v * 128 + 64 + __ffsll((long long)b) - 1);
+            }
+            if (threadIdx.x == 0) {
+                const uint32_t last = (uint32_t)n2 - 1u;
+                const uint32_t tot = (uint32_t)s_dir[last] + popc2(s_prefix[last]);
+                if (tot != n_pre) deep_fail(st, DEEP_ERR_INTERNAL);
+                s_hids = scr;
+                s_hn = min(min(tot, n_pre), P.h_scratch_words);
+            }
+            __syncthreads();  // the ids are in place
+        }
+        if (SMEM_PREFIX && proj && s_grant && !rows_p2) {
             // Rank directory of the prefix, and the child block zeroed for
             // the bits the projected writers OR in.
             build_rank_dir(s_prefix, n2, s_dir, s_w64);
@@ -1171,7 +1243,7 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
         // each piece's first output position: a warp whose slice ends inside
         // a list child first counts that last piece (s_clast), and a warp that
         // starts inside one adds up the counts of the warps before it.
-        if (SMEM_PREFIX && hmode && s_grant) {
+        if (SMEM_PREFIX && rows_p2 && s_grant) {
             // Row-wise children (projected): survivor k's child has bit j set
             // when the j-th transaction of the prefix holds survivor k's item.
             // A warp takes 32 consecutive transactions, each lane marks the
@@ -1184,9 +1256,12 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
             const uint32_t nw32 = 2u * lstride, used32 = (h_n2 + 31u) / 32u;
             for (uint32_t g0 = 0; g0 < ns; g0 += 64) {
                 const uint32_t gn = min(64u, ns - g0);
+                // Survivor k's frequent index, from its member entry (in survivor order).
+                uint32_t gf = H_NONE;
                 if (threadIdx.x < gn) {
-                    const uint32_t f = s_f[s_map[g0 + threadIdx.x]];
-                    if (f < P.h_F) s_tab[f] = (uint16_t)threadIdx.x;  // (pass 1 flagged any other)
+                    gf = __ldg(P.h_fidx + __ldcg(P.mem_item + s_mem_base + g0 + threadIdx.x));
+                    if (gf < P.h_F) s_tab[gf] = (uint16_t)threadIdx.x;
+                    else deep_fail(st, DEEP_ERR_INTERNAL);
                 }
                 __syncthreads();
                 for (uint32_t w = wid; w < used32; w += nw) {
@@ -1195,9 +1270,17 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                     if (j < h_n2) {
                         const uint32_t t = __ldcg(h_ids2 + j);
                         const uint32_t ra = __ldg(P.h_off + t), rb = __ldg(P.h_off + t + 1);
-                        for (uint32_t k = ra; k < rb; ++k) {
-                            const uint32_t g = s_tab[__ldg(P.h_rows + k)];
-                            if (g < 64u) mark |= 1ull << g;
+                        for (uint32_t k0 = ra; k0 < rb; k0 += 8) {
+                            uint32_t f[8];
+#pragma unroll
+                            for (int u = 0; u < 8; ++u)
+                                f[u] = k0 + u < rb ? (uint32_t)__ldg(P.h_rows + k0 + u) : H_NONE;
+#pragma unroll
+                            for (int u = 0; u < 8; ++u)
+                                if (f[u] != H_NONE) {
+                                    const uint32_t g = s_tab[f[u]];
+                                    if (g < 64u) mark |= 1ull << g;
+                                }
                         }
                     }
                     for (uint32_t k = 0; k < gn; ++k) {
@@ -1206,18 +1289,14 @@ __global__ void __launch_bounds__(1024) k_deep(DeepParams P) {
                     }
                 }
                 __syncthreads();  // the group's rows are read
-                if (threadIdx.x < gn) {
-                    const uint32_t f = s_f[s_map[g0 + threadIdx.x]];
-                    if (f < P.h_F) s_tab[f] = H_NONE;
-                }
+                if (threadIdx.x < gn && gf < P.h_F) s_tab[gf] = H_NONE;
                 __syncthreads();  // the table is empty again
             }
             const uint32_t pad = nw32 - used32;
             for (uint64_t i = threadIdx.x; i < (uint64_t)ns * pad; i += blockDim.x)
                 blk32[(i / pad) * nw32 + used32 + i % pad] = 0u;
-            if (threadIdx.x < ns)
-                P.mem_bits[s_mem_base + threadIdx.x] =
-                    reinterpret_cast<const uint64_t *>(P.arena + s_arena_base + (uint64_t)threadIdx.x * lstride);
+            for (uint32_t k = threadIdx.x; k < ns; k += blockDim.x)
+                P.mem_bits[s_mem_base + k] = reinterpret_cast<const uint64_t *>(P.arena + s_arena_base + (uint64_t)k * lstride);
             __threadfence();
         } else if (s_grant) {
             uint64_t chunk_base = 0;
