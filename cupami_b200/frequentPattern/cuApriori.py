@@ -30,6 +30,7 @@ import math
 import struct
 import sys
 import time
+from collections.abc import Sequence
 from itertools import chain
 from pathlib import Path
 from urllib.parse import urlparse
@@ -41,6 +42,30 @@ from .. import _native
 from ..datasets import TransactionCSR
 
 _BIN_MAGIC = b"CUPAMI01"
+
+
+class IdLabels(Sequence):
+    """Column labels of a database loaded from integer ids: the decimal string
+    of each column's id, made on first use (a batch of databases need not
+    build them while it mines)."""
+
+    def __init__(self, ids):
+        self._ids = ids
+        self._str = None
+
+    def _strings(self):
+        if self._str is None:
+            self._str = [str(v) for v in self._ids.tolist()]
+        return self._str
+
+    def __len__(self):
+        return len(self._ids)
+
+    def __getitem__(self, i):
+        return self._strings()[i]
+
+    def __iter__(self):
+        return iter(self._strings())
 
 
 class _PatternDict(dict):
@@ -271,8 +296,7 @@ class cuApriori:
         if self._csr is not None:
             offsets, ids = self._csr
             db = _native.Database.from_ids(ctx, offsets, ids)
-            labels = [str(v) for v in db.labels.tolist()]
-            return db, labels
+            return db, IdLabels(db.labels)
         flat = list(chain.from_iterable(self._Database))
         labels = sorted(set(flat))
         index = dict(zip(labels, range(len(labels))))
@@ -358,7 +382,7 @@ class cuApriori:
         res = self._result
         if res is None:
             return (np.zeros(1, np.uint64), np.zeros(0, np.uint32), np.zeros(0, np.uint64), [])
-        return res.offsets, res.items, res.supports, list(self._labels)
+        return res.offsets, res.items, res.supports, self._labels
 
     def getKernelStats(self):
         """Device-side counters of the latest mine() (launches, bytes, times)."""
@@ -367,7 +391,8 @@ class cuApriori:
     def getPatterns(self):
         """{tab-joined pattern: support} in the reference's insertion order."""
         res = self._result
-        if self._patterns is None and res is not None and not any("\n" in label for label in self._labels):
+        if self._patterns is None and res is not None and (
+                isinstance(self._labels, IdLabels) or not any("\n" in label for label in self._labels)):
             # Keys joined in C straight from the result arrays: no tuple per pattern.
             keys = _native.join_labels(res.offsets, res.items, self._labels)
             return dict(zip(keys, res.supports.tolist()))

@@ -22,7 +22,7 @@ from itertools import combinations, islice
 
 from .. import _native
 from . import _bitsets
-from .cuApriori import _cli, cuApriori
+from .cuApriori import IdLabels, _cli, cuApriori
 
 
 class cuEclat(cuApriori):
@@ -70,7 +70,7 @@ class cuEclat(cuApriori):
         if all(m._csr is not None for m in miners):
             # Integer-id sources: one upload and one packing pass for the whole batch.
             dbs = _native.Database.from_ids_batch(ctx, [m._csr for m in miners])
-            labels = [[str(v) for v in db.labels.tolist()] for db in dbs]
+            labels = [IdLabels(db.labels) for db in dbs]  # strings on first use
         else:
             dbs, labels = zip(*(m._deviceDatabase(ctx) for m in miners))
         try:

@@ -249,3 +249,16 @@ def test_timing_labels_exclude_idle_time(cls_name):
     miner._startTime, miner._endTime = 100, 104
     assert miner.getMiningTime() == 4 and miner.getRuntime() == 4
     assert miner.getTotalRuntime() == 6.5
+
+
+def test_id_labels_are_decimal_strings_on_first_use():
+    """Labels of integer-id databases: a sequence of the ids' decimal strings,
+    built only when read (a batch of miners does not build them while mining)."""
+    import numpy as np
+
+    from cupami_b200.frequentPattern.cuApriori import IdLabels
+
+    lab = IdLabels(np.array([7, 10, 300], dtype=np.uint32))
+    assert lab._str is None and len(lab) == 3
+    assert lab[1] == "10" and list(lab) == ["7", "10", "300"] and lab[-1] == "300"
+    assert list(lab[0:2]) == ["7", "10"]
