@@ -917,6 +917,8 @@ def run_ours(args, world, rank, local):
                 "frac_of_8tbs_spec": achieved / 8000.0,
                 "dram_share_of_alg_bytes": traffic / deep_bytes if traffic and deep_bytes else None,
                 "l2_bytes_per_launch": tr.get("l2_bytes_per_launch") if tr else None,
+                # per kernel: DRAM and L2 bytes, L2 bytes/s and the L2 throughput % of peak (ncu)
+                "by_kernel": tr.get("kernels") if tr else None,
                 "traffic_source": ("profiles/k_deep_traffic.json (ncu dram__bytes_read.sum + dram__bytes_write.sum "
                                    "of one launch of each kernel): " + tr["profile"]) if tr else None,
                 "ms_per_launch": deep_ms, "ms_k_local": local_ms, "alg_bytes_per_launch": deep_bytes,
