@@ -10,7 +10,8 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 SOURCES = [PKG / "csrc" / "cpm_runtime.cu"]
-HEADERS = sorted((PKG / "csrc").glob("*.cuh")) + [ROOT / "include" / "cupami_b200.h"]
+HEADERS = (sorted((PKG / "csrc").glob("*.cuh")) + sorted((PKG / "csrc").glob("*.inc"))
+           + [ROOT / "include" / "cupami_b200.h"])
 OUTPUT = PKG / "libcupami_b200.so"
 
 NVCC_FLAGS = [
